@@ -1,0 +1,362 @@
+"""Benchmark of the per-step hot path (System::step_the_clock) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl bsnn|reference] [--workload NAME]
+
+A bench "step" is one recording interval of simulation (--sim-steps clock steps, default 10,000
+= 1 simulated second at dt = 0.1 ms) of the workload, run through libbsnn's C-ABI.  The default
+workload is the reference example network (2,500 E + 625 I, ~9.8 M dense FP32 synapses, triplet
+STDP on E->E and iSTDP on I->E, Poisson background, 4 stimulus pulses, all spikes and 50
+voltages recorded), built from seeded synthetic inputs (no dataset is involved).
+
+Metric: simulated seconds per wall second (whole job, all ranks); the line also carries dense
+synaptic updates/s and spike-driven synaptic events/s.  With N > 1 every rank runs an
+independent replica (the single-network path is not sharded): weak scaling, no collective on
+the data path.
+
+--impl reference times the reference's own implementation of the path: its CUDA build
+(oracle/_ref/ref_harness, the unmodified cpp_src components) driving the same network on this
+GPU, or, when that binary is absent, the CPU oracle on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "example-cuda-spiking-nn_b200"))
+
+DT = 1e-4
+STEPS_PER_LAUNCH = 1000
+PROFILE_TRAFFIC = ROOT / "profiles" / "traffic.json"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="bsnn", choices=["bsnn", "reference"])
+    ap.add_argument("--workload", default="example_plastic_3125")
+    ap.add_argument("--sim-steps", type=int, default=10000)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bounded CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.lines:
+            return None
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def algorithmic_bytes_per_step(spec) -> float:
+    """Weight read of every connection once (FP32), read+write of the plastic matrices (the
+    update and the row normalisation, counted once at 4 B), and ~100 B/neuron of state."""
+    b = sum(c.weights.size * 4 for c in spec.conns)
+    plastic = {p.conn for p in spec.plasts}
+    b += sum(2 * spec.conns[c].weights.size * 4 for c in plastic)
+    return float(b + 100 * spec.num_neurons)
+
+
+def nnz_out(spec):
+    """Nonzero outgoing synapses per neuron (for spike-driven event counts)."""
+    out = np.zeros(spec.num_neurons, np.int64)
+    for c in spec.conns:
+        off = spec.groups[c.pre]["offset"]
+        out[off:off + c.weights.shape[0]] += (c.weights != 0).sum(axis=1)
+    return out
+
+
+def spike_events_from_bits(bits, group_offset, n, nnz):
+    unpacked = ((bits[:, :, None] >> np.arange(32, dtype=np.uint32)) & 1).reshape(bits.shape[0], -1)[:, :n]
+    per_neuron = unpacked.sum(axis=0)
+    return int(per_neuron.sum()), int((per_neuron * nnz[group_offset:group_offset + n]).sum())
+
+
+def cpu_baseline(spec, seconds: float):
+    """The CPU oracle (FP32 restatement of the reference step, all host threads) on a bounded
+    sample of the same workload."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    o = oracle.OracleSimulation(spec.num_excitatory, spec.num_inhibitory, **spec.sim_kwargs())
+    spec.build(o)
+    o.run(0, 2)
+    t0 = time.perf_counter()
+    n = 0
+    while time.perf_counter() - t0 < seconds and n < 20000:
+        o.run(2 + n, 10)
+        n += 10
+    el = time.perf_counter() - t0
+    threads = int(os.environ.get("ORACLE_THREADS", os.cpu_count() or 1))
+    return {"value": n * DT / el, "unit": "simulated-s/wall-s", "cores": threads, "kind": "port",
+            "sample": f"{n} clock steps of {spec.name} (FP32 oracle, {threads} threads), {el:.1f} s"}
+
+
+def run_bsnn(args, rank, world):
+    import torch
+
+    import bsnn
+    torch.cuda.set_device(rank % max(1, torch.cuda.device_count()))
+    dev = torch.cuda.current_device()
+    S, K, W = args.sim_steps, args.steps, args.warmup
+    total = (W + K) * S + 1
+    spec = bsnn.synthetic_network(args.workload, steps=total, weight_values="uniform", recording_interval_steps=S,
+                                  seed=bsnn.network.WORKLOADS[args.workload]["seed"] + rank)
+    sim = bsnn.Simulation(spec.num_excitatory, spec.num_inhibitory, device=dev, **spec.sim_kwargs())
+    spec.build(sim)
+    sim.set_steps_per_launch(STEPS_PER_LAUNCH)
+    stream = torch.cuda.ExternalStream(sim.stream())
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
+    nnz = nnz_out(spec)
+    clock = 0
+    for _ in range(W):
+        sim.run(clock, S)
+        clock += S
+    sim.synchronize()
+    for m in (0, 1):
+        sim.read_spike_bits(m, flush=True)
+    sim.read_voltage_history(2, flush=True)
+    info0 = sim.info()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    times_ms = []
+    spikes = events = 0
+    with ClockSampler(dev) as clocks:
+        for _ in range(K):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            sim.run(clock, S)
+            e1.record(stream)
+            e1.synchronize()
+            clock += S
+            times_ms.append(e0.elapsed_time(e1))
+            for m, g in ((0, 0), (1, 1)):
+                bits = sim.read_spike_bits(m, flush=True)
+                s_, e_ = spike_events_from_bits(bits, spec.groups[g]["offset"], spec.groups[g]["num_neurons"], nnz)
+                spikes += s_
+                events += e_
+        sim.synchronize()
+    info1 = sim.info()
+    t_ms = float(sum(times_ms))
+    if world > 1:
+        t = torch.tensor([t_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        t_ms = float(t.item())
+        ev = torch.tensor([float(events), float(spikes)], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(ev)
+        events, spikes = int(ev[0].item()), int(ev[1].item())
+    launches = int(info1.kernel_launches - info0.kernel_launches)
+    sim_seconds = K * S * DT * world
+    value = sim_seconds / (t_ms / 1e3)
+    steps_per_s = K * S * world / (t_ms / 1e3)
+    per_launch_ms = t_ms / max(1, launches)
+    bytes_step = algorithmic_bytes_per_step(spec)
+    achieved = bytes_step * STEPS_PER_LAUNCH / (per_launch_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = None
+    if PROFILE_TRAFFIC.exists():
+        tr = json.loads(PROFILE_TRAFFIC.read_text()).get(args.workload)
+        if tr:
+            traffic = tr["dram_bytes_per_launch"]
+    line = {
+        "metric": "simulated-s per wall-s (and synaptic events/s) at 1 B200",
+        "value": value,
+        "unit": "simulated-s/wall-s",
+        "n_gpus": world,
+        "steps": K,
+        "warmup": W,
+        "ms_per_step": t_ms / K,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded; reference example shapes, uniform[0, max_weight] weights)",
+        "config": {"workload": args.workload, "neurons": spec.num_neurons, "synapse_entries": spec.synapse_entries(),
+                   "clock_steps_per_bench_step": S, "dt_s": DT, "plasticity": "triplet(E->E)+iSTDP(I->E)",
+                   "form": "plain FP32 (reference arithmetic)", "parallelism": f"replicas x{world}",
+                   "l2": "flushed (256 MB write) between timed steps"},
+        "dense_synaptic_updates_per_s": spec.synapse_entries() * steps_per_s,
+        "spike_driven_events_per_s": events / (t_ms / 1e3),
+        "spikes_per_s_simulated": spikes / max(sim_seconds, 1e-12),
+        "clock_steps_per_s": steps_per_s,
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_source": peak_kind,
+                     "bytes_per_clock_step": bytes_step, "clock_steps_per_launch": STEPS_PER_LAUNCH,
+                     "launch_ms": per_launch_ms,
+                     "note": "working set (~40 MB) is L2-resident, so frac of HBM peak can exceed 1"},
+        "clocks": clocks.summary(),
+    }
+    sim.close()
+    return line, spec
+
+
+def run_e2e(args, dev):
+    """Same metric through the public API with host buffers: build from host arrays (H2D of
+    weights, parameters, stimulus), run, drain the spike and voltage rings to host memory every
+    bench step, read the plastic weights back at the end.  Wall clock around all of it."""
+    import torch
+
+    import bsnn
+    S, K = args.sim_steps, args.steps
+    spec = bsnn.synthetic_network(args.workload, steps=K * S + 1, weight_values="uniform", recording_interval_steps=S)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sim = bsnn.Simulation(spec.num_excitatory, spec.num_inhibitory, device=dev, **spec.sim_kwargs())
+    spec.build(sim)
+    sim.set_steps_per_launch(STEPS_PER_LAUNCH)
+    d2h = 0
+    for k in range(K):
+        sim.run(k * S, S)
+        for m in (0, 1):
+            d2h += sim.read_spike_bits(m, flush=True).nbytes
+        d2h += sim.read_voltage_history(2, flush=True).nbytes
+    w = sim.read_weights(0)
+    d2h += w.nbytes
+    sim.synchronize()
+    el = time.perf_counter() - t0
+    h2d = sum(c.weights.nbytes for c in spec.conns) + sum(np.asarray(a).nbytes for a in spec.stimulus)
+    sim.close()
+    return {"value": K * S * DT / el, "unit": "simulated-s/wall-s", "h2d_bytes_per_step": h2d // K,
+            "d2h_bytes_per_step": d2h // K, "includes": "create+upload, run, per-step ring drains, final weight read"}
+
+
+def run_reference(args, rank, world):
+    """The reference's own implementation: its CUDA build (oracle/_ref/ref_harness) on this GPU,
+    timed over a bounded sample; falls back to the CPU oracle when the build is absent."""
+    import bsnn
+    sys.path.insert(0, str(ROOT / "oracle"))
+    spec_steps = 3000
+    spec = bsnn.synthetic_network(args.workload, steps=spec_steps + 1, weight_values="uniform",
+                                  recording_interval_steps=args.sim_steps)
+    harness = ROOT / "oracle" / "_ref" / "ref_harness"
+    base = {"metric": "simulated-s per wall-s (and synaptic events/s) at 1 B200", "unit": "simulated-s/wall-s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "impl": "reference", "data": "synthetic (seeded)",
+            "config": {"workload": args.workload, "neurons": spec.num_neurons,
+                       "synapse_entries": spec.synapse_entries(), "dt_s": DT}}
+    gpu_ok = False
+    try:
+        import torch
+        gpu_ok = torch.cuda.is_available()
+    except Exception:
+        pass
+    if harness.exists() and gpu_ok:
+        import refnet
+        with tempfile.TemporaryDirectory() as td:
+            r = refnet.run_time(spec, 100, 2000, td)
+        value = r["steps"] * DT / r["seconds"]
+        sample = (f"{r['steps']} clock steps of System::step_the_clock after 100 warm-up steps, reference CUDA build "
+                  f"(cpp_src, sm_100a, cuBLAS) on this GPU, driven by 1 host thread")
+        kind, cores = "reference", 1
+    else:
+        cb = cpu_baseline(spec, args.cpu_seconds)
+        value, sample, kind, cores = cb["value"], cb["sample"], "port", cb["cores"]
+    line = dict(base, value=value, ms_per_step=args.sim_steps * DT / value * 1e3,
+                cpu_baseline={"value": value, "unit": "simulated-s/wall-s", "cores": cores, "kind": kind,
+                              "sample": sample},
+                e2e={"value": value, "unit": "simulated-s/wall-s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                dense_synaptic_updates_per_s=spec.synapse_entries() * value / DT)
+    return line
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args, rank, world)), flush=True)
+        return
+    import torch
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    line, spec = run_bsnn(args, int(os.environ.get("LOCAL_RANK", "0")), world)
+    if rank == 0:
+        if not args.no_e2e:
+            line["e2e"] = run_e2e(args, torch.cuda.current_device())
+        if not args.no_cpu_baseline and world == 1:
+            line["cpu_baseline"] = cpu_baseline(spec, args.cpu_seconds)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1171 @@
+// bsnn_api.cu -- host side of libbsnn: the C-ABI of include/bsnn.h.
+//
+// Component calls only record host-side descriptions.  The first call that needs the device
+// (a step, a read) "finalizes" the sim: it plans the per-CTA work of the fused step kernel,
+// allocates ONE device arena for all state, and uploads everything, i.e. what the reference
+// spreads over GpuSimulationState::initialize_device_buffers and the upload_*_view helpers
+// (cpp_src/gpu_core/gpu_simulation_state.cu:35-86, 107-208).  After that, components can no
+// longer be added.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/bsnn.h"
+#include "bsnn_device.cuh"
+#include "step_kernel.cuh"
+
+using namespace bsnn;
+
+namespace {
+
+struct ApiError : std::runtime_error {
+    bsnn_status code;
+    ApiError(bsnn_status c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void cuda_check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw ApiError(BSNN_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+thread_local std::string g_thread_error;
+
+uint32_t round_up(uint32_t x, uint32_t m) { return (x + m - 1) / m * m; }
+
+struct HostGroup {
+    bsnn_neuron_group_params p;
+};
+struct HostConn {
+    uint32_t pre, post;
+    bsnn_connection_params p;
+    std::vector<float> w;  // row-major [n_pre][n_post]
+    float r_decay, d_decay, norm;
+};
+struct HostPlast {
+    int32_t kind;
+    uint32_t conn;
+    bsnn_plasticity_params p;
+};
+struct HostMon {
+    int32_t kind;
+    uint32_t group, interval;
+    std::vector<uint32_t> sel;
+};
+struct HostStim {
+    std::vector<uint32_t> counts, ids, offs;
+    std::vector<float> deltas;
+};
+
+// Simple bump allocator over the device arena.
+struct Arena {
+    size_t size = 0;
+    size_t take(size_t bytes) {
+        const size_t off = (size + 255) & ~size_t(255);
+        size = off + bytes;
+        return off;
+    }
+};
+
+}  // namespace
+
+struct bsnn_sim {
+    bsnn_state_desc desc{};
+    uint32_t N = 0;
+    std::string err;
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+
+    std::vector<HostGroup> groups;
+    std::vector<HostConn> conns;
+    std::vector<HostPlast> plasts;
+    std::vector<HostMon> mons;
+    std::vector<HostStim> stims;
+    int32_t noise_mode = BSNN_NOISE_PHILOX;
+    std::vector<uint8_t> replay;
+    uint32_t replay_steps = 0;
+
+    bool finalized = false;
+    bool failed = false;
+    unsigned char* arena = nullptr;
+    size_t arena_bytes = 0;
+    size_t weight_bytes = 0;
+    DSim h{};
+    DSim* d_sim = nullptr;
+    uint32_t grid = 0, block = 0;
+    size_t smem_bytes = 0;
+    uint64_t steps_done = 0;
+    uint32_t next_clock = 0;
+    uint32_t steps_per_launch = 1000;
+    uint64_t launches = 0;
+    bool graphs_ok = true;
+    std::map<uint32_t, cudaGraphExec_t> graphs;
+    std::vector<uint32_t> conn_ld;
+
+    ~bsnn_sim() {
+        for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+        if (arena) cudaFree(arena);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+template <class F>
+bsnn_status guarded(bsnn_sim* sim, F&& f) {
+    try {
+        if (sim) {
+            DeviceGuard g(sim->device);
+            f();
+        } else {
+            f();
+        }
+        return BSNN_OK;
+    } catch (const ApiError& e) {
+        if (sim) sim->err = e.what();
+        g_thread_error = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        if (sim) sim->err = e.what();
+        g_thread_error = e.what();
+        return BSNN_ERR_RUNTIME;
+    }
+}
+
+void require(bool cond, bsnn_status code, const std::string& msg) {
+    if (!cond) throw ApiError(code, msg);
+}
+
+void require_building(const bsnn_sim* s) {
+    require(!s->finalized, BSNN_ERR_STATE, "components cannot be added after the simulation has started");
+}
+
+float exp_neg_mean_of(float mean) { return static_cast<float>(std::exp(-static_cast<double>(mean))); }
+
+// ------------------------------------------------------------------------------------------
+// Planning: neuron ownership, per-CTA segments/blocks/rows, slot lists.
+struct Plan {
+    std::vector<DCta> ctas;
+    std::vector<DSeg> segs;
+    std::vector<DBlk> blks;
+    std::vector<DRowMeta> rows;
+    std::vector<uint32_t> rows_begin;
+    std::vector<uint32_t> red_list;
+    uint32_t red_begin[2][kMaxGroups]{}, red_end[2][kMaxGroups]{};
+    uint32_t n_slots = 0, max_rows = 1, max_own = 1, max_items = 1;
+};
+
+int group_of_host(const bsnn_sim* s, uint32_t j) {
+    for (size_t g = 0; g < s->groups.size(); ++g) {
+        const auto& p = s->groups[g].p;
+        if (j >= p.offset && j - p.offset < p.num_neurons) return static_cast<int>(g);
+    }
+    return -1;
+}
+
+Plan build_plan(const bsnn_sim* s, uint32_t n_ctas) {
+    Plan P;
+    const uint32_t N = s->N;
+    // Per-neuron cost of its outgoing rows: one weight read, plus write and (normalised) re-read
+    // for plastic rows.
+    std::vector<double> cost(N, 1.0);
+    for (uint32_t j = 0; j < N; ++j) {
+        const int g = group_of_host(s, j);
+        if (g < 0) continue;
+        for (size_t c = 0; c < s->conns.size(); ++c) {
+            const auto& C = s->conns[c];
+            if (static_cast<int>(C.pre) != g) continue;
+            double w = 1.0;
+            for (const auto& pl : s->plasts)
+                if (pl.conn == c) w += pl.kind == BSNN_PLASTICITY_TRIPLET ? 2.0 : 1.0;
+            cost[j] += w * round_up(s->groups[C.post].p.num_neurons, 4);
+        }
+    }
+    std::vector<double> prefix(N + 1, 0.0);
+    for (uint32_t j = 0; j < N; ++j) prefix[j + 1] = prefix[j] + cost[j];
+    const double total = prefix[N];
+    std::vector<uint32_t> bounds(n_ctas + 1, 0);
+    bounds[n_ctas] = N;
+    for (uint32_t c = 1; c < n_ctas; ++c) {
+        const double target = total * c / n_ctas;
+        uint32_t j = static_cast<uint32_t>(std::lower_bound(prefix.begin(), prefix.end(), target) - prefix.begin());
+        j = std::min(std::max(j, bounds[c - 1] + (N - bounds[c - 1] > n_ctas - c ? 1u : 0u)), N);
+        bounds[c] = j;
+    }
+    for (uint32_t c = 1; c <= n_ctas; ++c) bounds[c] = std::max(bounds[c], bounds[c - 1]);
+
+    // Slot bookkeeping: slot of (cta, target), and which (target, group) each CTA feeds.
+    std::vector<std::vector<uint32_t>> red(2 * kMaxGroups);
+    for (uint32_t c = 0; c < n_ctas; ++c) {
+        DCta cta{};
+        cta.n0 = bounds[c];
+        cta.n1 = bounds[c + 1];
+        cta.seg_begin = static_cast<uint32_t>(P.segs.size());
+        P.rows_begin.push_back(static_cast<uint32_t>(P.rows.size()));
+        const uint32_t row_base = static_cast<uint32_t>(P.rows.size());
+        int32_t slot_of_target[2] = {-1, -1};
+        uint32_t item = 0;
+        for (uint32_t T = 0; T < 2; ++T) {
+            for (uint32_t q = 0; q < s->groups.size(); ++q) {
+                DSeg seg{};
+                seg.target = T;
+                seg.post_g = q;
+                seg.blk_begin = static_cast<uint32_t>(P.blks.size());
+                for (uint32_t ci = 0; ci < s->conns.size(); ++ci) {
+                    const auto& C = s->conns[ci];
+                    const auto& gp = s->groups[C.pre].p;
+                    const uint32_t target = gp.is_inhibitory ? kTargetInh : kTargetExc;
+                    if (target != T || C.post != q) continue;
+                    const uint32_t a = std::max(cta.n0, gp.offset);
+                    const uint32_t b = std::min(cta.n1, gp.offset + gp.num_neurons);
+                    if (a >= b) continue;
+                    DBlk blk{};
+                    blk.conn = ci;
+                    blk.row_begin = a - gp.offset;
+                    blk.row_end = b - gp.offset;
+                    blk.srow = static_cast<uint32_t>(P.rows.size()) - row_base;
+                    for (uint32_t pl = blk.row_begin; pl < blk.row_end; ++pl)
+                        P.rows.push_back(DRowMeta{ci, pl, gp.offset + pl});
+                    for (const auto& pl : s->plasts)
+                        if (pl.conn == ci && pl.kind == BSNN_PLASTICITY_TRIPLET) seg.normalized = 1;
+                    P.blks.push_back(blk);
+                }
+                seg.blk_end = static_cast<uint32_t>(P.blks.size());
+                if (seg.blk_end == seg.blk_begin) continue;
+                const auto& gq = s->groups[q].p;
+                seg.n_post = gq.num_neurons;
+                seg.units = round_up(gq.num_neurons, 4) / 4;
+                seg.item_begin = item;
+                item += round_up(seg.units, 32);
+                if (slot_of_target[T] < 0) slot_of_target[T] = static_cast<int32_t>(P.n_slots++);
+                seg.slot = static_cast<uint32_t>(slot_of_target[T]);
+                red[T * kMaxGroups + q].push_back(seg.slot);
+                P.segs.push_back(seg);
+            }
+        }
+        cta.seg_end = static_cast<uint32_t>(P.segs.size());
+        cta.n_rows = static_cast<uint32_t>(P.rows.size()) - row_base;
+        cta.n_items = item;
+        require(cta.seg_end - cta.seg_begin <= static_cast<uint32_t>(kMaxSegsPerCta), BSNN_ERR_INVALID_ARGUMENT,
+                "too many (target, post group) segments per CTA");
+        const uint32_t nblk = cta.seg_end > cta.seg_begin
+                                  ? P.segs[cta.seg_end - 1].blk_end - P.segs[cta.seg_begin].blk_begin
+                                  : 0u;
+        require(nblk <= static_cast<uint32_t>(kMaxBlksPerCta), BSNN_ERR_INVALID_ARGUMENT,
+                "too many connection blocks per CTA");
+        P.max_rows = std::max(P.max_rows, cta.n_rows);
+        P.max_own = std::max(P.max_own, cta.n1 - cta.n0);
+        P.max_items = std::max(P.max_items, cta.n_items);
+        P.ctas.push_back(cta);
+    }
+    for (uint32_t T = 0; T < 2; ++T)
+        for (uint32_t q = 0; q < kMaxGroups; ++q) {
+            P.red_begin[T][q] = static_cast<uint32_t>(P.red_list.size());
+            for (uint32_t sl : red[T * kMaxGroups + q]) P.red_list.push_back(sl);
+            P.red_end[T][q] = static_cast<uint32_t>(P.red_list.size());
+        }
+    if (P.red_list.empty()) P.red_list.push_back(0);
+    if (P.rows.empty()) P.rows.push_back(DRowMeta{0, 0, 0});
+    return P;
+}
+
+void finalize(bsnn_sim* s) {
+    if (s->finalized) return;
+    require(!s->groups.empty(), BSNN_ERR_STATE, "no neuron groups were added");
+    const uint32_t N = s->N;
+    DSim& h = s->h;
+    h = DSim{};
+    h.N = N;
+    h.n_groups = static_cast<uint32_t>(s->groups.size());
+    h.n_conns = static_cast<uint32_t>(s->conns.size());
+    h.n_plast = static_cast<uint32_t>(s->plasts.size());
+    h.n_mons = static_cast<uint32_t>(s->mons.size());
+
+    // Groups and their padded partial-sum columns.
+    uint32_t pcol = 0;
+    for (uint32_t g = 0; g < h.n_groups; ++g) {
+        const auto& p = s->groups[g].p;
+        DGroup& G = h.groups[g];
+        G.off = p.offset;
+        G.n = p.num_neurons;
+        G.pcol = pcol;
+        pcol += round_up(p.num_neurons, 4);
+        G.inhib = p.is_inhibitory ? 1u : 0u;
+        G.refractory_steps = p.refractory_steps;
+        G.has_bg_e = p.mean_background_excitatory_spikes > 0.0f;
+        G.has_bg_i = p.mean_background_inhibitory_spikes > 0.0f;
+        G.timestep = p.timestep;
+        G.g_leak = p.g_leak;
+        G.cap = p.membrane_capacitance;
+        G.delta_t = p.depolarization_slope_factor;
+        G.v_eff = p.v_effective_spike_threshold;
+        G.e_exc = p.v_excitatory_reversal;
+        G.e_inh = p.v_inhibitory_reversal;
+        G.v_th = p.v_threshold;
+        G.v_reset = p.v_reset;
+        G.v_rest = p.v_rest;
+        G.exp_neg_mean_e = exp_neg_mean_of(p.mean_background_excitatory_spikes);
+        G.exp_neg_mean_i = exp_neg_mean_of(p.mean_background_inhibitory_spikes);
+        G.bg_er_decay = p.background_excitatory_postsynaptic_r_trace_decay;
+        G.bg_ed_decay = p.background_excitatory_postsynaptic_d_trace_decay;
+        G.bg_ir_decay = p.background_inhibitory_postsynaptic_r_trace_decay;
+        G.bg_id_decay = p.background_inhibitory_postsynaptic_d_trace_decay;
+        G.bg_scale_e = p.background_excitatory_scaling_factor;
+        G.bg_scale_i = p.background_inhibitory_scaling_factor;
+    }
+    h.N_pad = std::max(pcol, 4u);
+
+    // Trace sets (shared by connections with the same presynaptic group and trace constants).
+    std::vector<int32_t> conn_ts(h.n_conns, -1);
+    for (uint32_t c = 0; c < h.n_conns; ++c) {
+        const auto& C = s->conns[c];
+        for (uint32_t t = 0; t < h.n_ts; ++t) {
+            const DTraceSet& T = h.ts[t];
+            if (T.group == C.pre && T.r_decay == C.r_decay && T.d_decay == C.d_decay && T.norm == C.norm) {
+                conn_ts[c] = static_cast<int32_t>(t);
+                break;
+            }
+        }
+        if (conn_ts[c] < 0) {
+            require(h.n_ts < static_cast<uint32_t>(kMaxTraceSets), BSNN_ERR_INVALID_ARGUMENT, "too many trace sets");
+            DTraceSet& T = h.ts[h.n_ts];
+            T.group = C.pre;
+            T.r_decay = C.r_decay;
+            T.d_decay = C.d_decay;
+            T.norm = C.norm;
+            DGroup& G = h.groups[C.pre];
+            require(G.n_ts < static_cast<uint32_t>(kMaxGroupRoles), BSNN_ERR_INVALID_ARGUMENT, "too many trace sets per group");
+            G.ts[G.n_ts++] = static_cast<int32_t>(h.n_ts);
+            conn_ts[c] = static_cast<int32_t>(h.n_ts++);
+        }
+    }
+
+    // Device arena layout.
+    Arena A;
+    const size_t fN = sizeof(float) * N;
+    size_t o_v = A.take(fN), o_ge = A.take(fN), o_gi = A.take(fN), o_is = A.take(fN);
+    size_t o_bge = A.take(fN), o_bgi = A.take(fN), o_ber = A.take(fN), o_bed = A.take(fN), o_bir = A.take(fN),
+           o_bid = A.take(fN);
+    size_t o_ref = A.take(sizeof(uint32_t) * N);
+    size_t o_spk0 = A.take(sizeof(uint32_t) * N), o_spk1 = A.take(sizeof(uint32_t) * N);
+    std::vector<size_t> o_ts(h.n_ts * 3);
+    for (uint32_t t = 0; t < h.n_ts; ++t) {
+        const size_t n = sizeof(float) * s->groups[h.ts[t].group].p.num_neurons;
+        o_ts[3 * t] = A.take(n);
+        o_ts[3 * t + 1] = A.take(n);
+        o_ts[3 * t + 2] = A.take(n);
+    }
+    std::vector<size_t> o_w(h.n_conns);
+    s->conn_ld.assign(h.n_conns, 0);
+    size_t wbytes = 0;
+    for (uint32_t c = 0; c < h.n_conns; ++c) {
+        const auto& C = s->conns[c];
+        const uint32_t n_pre = s->groups[C.pre].p.num_neurons, n_post = s->groups[C.post].p.num_neurons;
+        const uint32_t ld = round_up(n_post, 4);
+        s->conn_ld[c] = ld;
+        o_w[c] = A.take(sizeof(float) * static_cast<size_t>(n_pre) * ld);
+        wbytes += sizeof(float) * static_cast<size_t>(n_pre) * ld;
+    }
+    struct PlOff { size_t pre, post, tpre, tpost, rowA[2], rowB[2], colA[2], colB[2], pspk[2], sums; };
+    std::vector<PlOff> o_pl(h.n_plast);
+    for (uint32_t k = 0; k < h.n_plast; ++k) {
+        const auto& C = s->conns[s->plasts[k].conn];
+        const uint32_t n_pre = s->groups[C.pre].p.num_neurons, n_post = s->groups[C.post].p.num_neurons;
+        const size_t np = sizeof(float) * n_pre, nq = sizeof(float) * round_up(n_post, 4);
+        PlOff& o = o_pl[k];
+        o.pre = A.take(np); o.tpre = A.take(np); o.post = A.take(nq); o.tpost = A.take(nq);
+        for (int p = 0; p < 2; ++p) {
+            o.rowA[p] = A.take(np); o.rowB[p] = A.take(np);
+            o.colA[p] = A.take(nq); o.colB[p] = A.take(nq); o.pspk[p] = A.take(nq);
+        }
+        o.sums = A.take(np);
+    }
+    struct MonOff { size_t bits, vh, sel; };
+    std::vector<MonOff> o_mon(h.n_mons);
+    for (uint32_t m = 0; m < h.n_mons; ++m) {
+        const auto& M = s->mons[m];
+        const uint32_t ng = s->groups[M.group].p.num_neurons;
+        if (M.kind == kMonSpikes) {
+            o_mon[m].bits = A.take(sizeof(uint32_t) * static_cast<size_t>(M.interval) * ((ng + 31) / 32));
+        } else {
+            o_mon[m].vh = A.take(sizeof(float) * static_cast<size_t>(M.interval) * M.sel.size());
+            o_mon[m].sel = A.take(sizeof(int32_t) * ng);
+        }
+    }
+
+    // Work plan.
+    uint32_t n_ctas = static_cast<uint32_t>(s->sm_count);
+    if (const char* e = std::getenv("BSNN_CTAS")) n_ctas = std::max(1, std::atoi(e));
+    n_ctas = std::min<uint32_t>(n_ctas, std::max<uint32_t>(1u, (N + 3) / 4));
+    Plan P = build_plan(s, n_ctas);
+    h.n_ctas = n_ctas;
+    h.n_slots = std::max(P.n_slots, 1u);
+    h.max_rows = P.max_rows;
+    h.max_own = P.max_own;
+    std::memcpy(h.red_begin, P.red_begin, sizeof(P.red_begin));
+    std::memcpy(h.red_end, P.red_end, sizeof(P.red_end));
+    require(P.max_own <= static_cast<uint32_t>(kMaxThreads), BSNN_ERR_INVALID_ARGUMENT,
+            "network too large for one persistent grid (more than 1024 neurons per CTA)");
+    const uint32_t k_items = (P.max_items + kMaxThreads - 1) / kMaxThreads;
+    uint32_t block = round_up((P.max_items + k_items - 1) / k_items, 32);
+    block = std::max(block, round_up(P.max_own, 32));
+    block = std::min<uint32_t>(std::max<uint32_t>(block, 64), kMaxThreads);
+    if (const char* e = std::getenv("BSNN_BLOCK")) block = std::min<uint32_t>(kMaxThreads, round_up(std::max(32, std::atoi(e)), 32));
+    block = std::max(block, round_up(P.max_own, 32));
+    s->grid = n_ctas;
+    s->block = block;
+
+    size_t o_part = A.take(sizeof(float) * 2 * static_cast<size_t>(h.n_slots) * h.N_pad);
+    size_t o_red = A.take(sizeof(uint32_t) * P.red_list.size());
+    size_t o_ctas = A.take(sizeof(DCta) * P.ctas.size());
+    size_t o_segs = A.take(sizeof(DSeg) * std::max<size_t>(P.segs.size(), 1));
+    size_t o_blks = A.take(sizeof(DBlk) * std::max<size_t>(P.blks.size(), 1));
+    size_t o_rows = A.take(sizeof(DRowMeta) * P.rows.size());
+    size_t o_rowsb = A.take(sizeof(uint32_t) * P.rows_begin.size());
+
+    // Stimulus: merge all stimuli into one per-step CSR, each step's events sorted by neuron.
+    uint32_t stim_len = 0;
+    for (const auto& st : s->stims) stim_len = std::max<uint32_t>(stim_len, static_cast<uint32_t>(st.counts.size()));
+    std::vector<uint32_t> stim_off(stim_len + 1, 0), ev_neuron;
+    std::vector<float> ev_delta;
+    {
+        std::vector<size_t> cursor(s->stims.size(), 0);
+        std::vector<std::pair<uint32_t, float>> step_events;
+        for (uint32_t t = 0; t < stim_len; ++t) {
+            step_events.clear();
+            for (size_t k = 0; k < s->stims.size(); ++k) {
+                const auto& st = s->stims[k];
+                if (t >= st.counts.size()) continue;
+                for (uint32_t e = 0; e < st.counts[t]; ++e) {
+                    const size_t idx = cursor[k] + e;
+                    step_events.emplace_back(st.ids[idx] + st.offs[idx], st.deltas[idx]);
+                }
+                cursor[k] += st.counts[t];
+            }
+            std::stable_sort(step_events.begin(), step_events.end(),
+                             [](const auto& a, const auto& b) { return a.first < b.first; });
+            for (const auto& ev : step_events) {
+                ev_neuron.push_back(ev.first);
+                ev_delta.push_back(ev.second);
+            }
+            stim_off[t + 1] = static_cast<uint32_t>(ev_neuron.size());
+        }
+    }
+    size_t o_soff = A.take(sizeof(uint32_t) * stim_off.size());
+    size_t o_evn = A.take(sizeof(uint32_t) * std::max<size_t>(ev_neuron.size(), 1));
+    size_t o_evd = A.take(sizeof(float) * std::max<size_t>(ev_delta.size(), 1));
+    size_t o_rep = A.take(std::max<size_t>(s->replay.size(), 1));
+    size_t o_bar = A.take(sizeof(unsigned long long));
+    size_t o_err = A.take(sizeof(int32_t));
+    size_t o_sd = A.take(sizeof(unsigned long long));
+    size_t o_clk = A.take(sizeof(uint32_t));
+    size_t o_sim = A.take(sizeof(DSim));
+
+    cuda_check(cudaMalloc(&s->arena, A.size), "cudaMalloc arena");
+    s->arena_bytes = A.size;
+    s->weight_bytes = wbytes;
+    unsigned char* base = s->arena;
+    cuda_check(cudaMemsetAsync(base, 0, A.size, s->stream), "cudaMemset arena");
+    cuda_check(cudaStreamSynchronize(s->stream), "arena memset sync");
+    auto F = [&](size_t o) { return reinterpret_cast<float*>(base + o); };
+    auto U = [&](size_t o) { return reinterpret_cast<uint32_t*>(base + o); };
+
+    h.v = F(o_v); h.ge = F(o_ge); h.gi = F(o_gi); h.istim = F(o_is);
+    h.bg_ge = F(o_bge); h.bg_gi = F(o_bgi); h.bg_er = F(o_ber); h.bg_ed = F(o_bed); h.bg_ir = F(o_bir);
+    h.bg_id = F(o_bid);
+    h.refrac = U(o_ref);
+    h.spikes[0] = U(o_spk0);
+    h.spikes[1] = U(o_spk1);
+    for (uint32_t t = 0; t < h.n_ts; ++t) {
+        h.ts[t].r = F(o_ts[3 * t]);
+        h.ts[t].d = F(o_ts[3 * t + 1]);
+        h.ts[t].x = F(o_ts[3 * t + 2]);
+    }
+    std::vector<float> vinit(N, 0.0f);
+    for (const auto& g : s->groups)
+        for (uint32_t i = 0; i < g.p.num_neurons; ++i) vinit[g.p.offset + i] = g.p.v_rest;
+    cuda_check(cudaMemcpyAsync(h.v, vinit.data(), fN, cudaMemcpyHostToDevice, s->stream), "H2D v");
+
+    for (uint32_t c = 0; c < h.n_conns; ++c) {
+        const auto& C = s->conns[c];
+        DConn& D = h.conns[c];
+        D.pre_g = C.pre;
+        D.post_g = C.post;
+        D.pre_off = s->groups[C.pre].p.offset;
+        D.n_pre = s->groups[C.pre].p.num_neurons;
+        D.post_off = s->groups[C.post].p.offset;
+        D.n_post = s->groups[C.post].p.num_neurons;
+        D.ld = s->conn_ld[c];
+        D.units = D.ld / 4;
+        D.target = s->groups[C.pre].p.is_inhibitory ? kTargetInh : kTargetExc;
+        D.ts = conn_ts[c];
+        D.plast = -1;
+        D.w = F(o_w[c]);
+        std::vector<float> padded(static_cast<size_t>(D.n_pre) * D.ld, 0.0f);
+        for (uint32_t i = 0; i < D.n_pre; ++i)
+            std::memcpy(&padded[static_cast<size_t>(i) * D.ld], &C.w[static_cast<size_t>(i) * D.n_post],
+                        sizeof(float) * D.n_post);
+        cuda_check(cudaMemcpy(D.w, padded.data(), sizeof(float) * padded.size(), cudaMemcpyHostToDevice), "H2D w");
+    }
+    for (uint32_t k = 0; k < h.n_plast; ++k) {
+        const auto& PL = s->plasts[k];
+        DPlast& D = h.plast[k];
+        const PlOff& o = o_pl[k];
+        D.kind = PL.kind;
+        D.conn = PL.conn;
+        D.ltp_A = PL.p.ltp_A; D.ltd_A = PL.p.ltd_A; D.ltp_B = PL.p.ltp_B; D.ltd_B = PL.p.ltd_B;
+        D.pre_decay = PL.p.pre_trace_decay; D.post_decay = PL.p.post_trace_decay;
+        D.tpre_decay = PL.p.triplet_pre_trace_decay; D.tpost_decay = PL.p.triplet_post_trace_decay;
+        D.wmin = PL.p.weight_min; D.wmax = PL.p.weight_max;
+        D.pre = F(o.pre); D.post = F(o.post); D.tpre = F(o.tpre); D.tpost = F(o.tpost);
+        for (int p = 0; p < 2; ++p) {
+            D.rowA[p] = F(o.rowA[p]); D.rowB[p] = F(o.rowB[p]);
+            D.colA[p] = F(o.colA[p]); D.colB[p] = F(o.colB[p]); D.pspk[p] = U(o.pspk[p]);
+        }
+        D.sums = F(o.sums);
+        DConn& C = h.conns[PL.conn];
+        C.plast = static_cast<int32_t>(k);
+        DGroup& Gp = h.groups[C.pre_g];
+        DGroup& Gq = h.groups[C.post_g];
+        require(Gp.n_plast_pre < static_cast<uint32_t>(kMaxGroupRoles) && Gq.n_plast_post < static_cast<uint32_t>(kMaxGroupRoles),
+                BSNN_ERR_INVALID_ARGUMENT, "too many plasticities per group");
+        Gp.plast_pre[Gp.n_plast_pre++] = static_cast<int32_t>(k);
+        Gq.plast_post[Gq.n_plast_post++] = static_cast<int32_t>(k);
+        if (PL.kind == BSNN_PLASTICITY_TRIPLET) {
+            // TripletPlasticity::initialize_data (cpp_src/plasticities/triplet_plasticity.cpp:21-31):
+            // initial column sums (float, ascending pre), applied as row targets.
+            const auto& W = s->conns[PL.conn].w;
+            std::vector<float> sums(C.n_pre, 0.0f);
+            for (uint32_t q = 0; q < C.n_pre; ++q) {
+                float sum = 0.0f;
+                for (uint32_t i = 0; i < C.n_pre; ++i) sum += W[static_cast<size_t>(i) * C.n_post + q];
+                sums[q] = sum;
+            }
+            cuda_check(cudaMemcpy(D.sums, sums.data(), sizeof(float) * sums.size(), cudaMemcpyHostToDevice), "H2D sums");
+        }
+    }
+    for (uint32_t m = 0; m < h.n_mons; ++m) {
+        const auto& M = s->mons[m];
+        DMon& D = h.mons[m];
+        const uint32_t ng = s->groups[M.group].p.num_neurons;
+        D.kind = M.kind;
+        D.group = M.group;
+        D.interval = M.interval;
+        D.words = (ng + 31) / 32;
+        DGroup& G = h.groups[M.group];
+        require(G.n_mon < static_cast<uint32_t>(kMaxGroupRoles), BSNN_ERR_INVALID_ARGUMENT, "too many monitors per group");
+        G.mon[G.n_mon++] = static_cast<int32_t>(m);
+        if (M.kind == kMonSpikes) {
+            D.bits = U(o_mon[m].bits);
+        } else {
+            D.n_sel = static_cast<uint32_t>(M.sel.size());
+            D.vh = F(o_mon[m].vh);
+            D.sel_idx = reinterpret_cast<int32_t*>(base + o_mon[m].sel);
+            std::vector<int32_t> sel(ng, -1);
+            for (size_t k = 0; k < M.sel.size(); ++k)
+                if (sel[M.sel[k]] < 0) sel[M.sel[k]] = static_cast<int32_t>(k);
+            cuda_check(cudaMemcpy(D.sel_idx, sel.data(), sizeof(int32_t) * ng, cudaMemcpyHostToDevice), "H2D sel");
+        }
+    }
+
+    h.partials = F(o_part);
+    h.red_list = U(o_red);
+    h.ctas = reinterpret_cast<const DCta*>(base + o_ctas);
+    h.segs = reinterpret_cast<const DSeg*>(base + o_segs);
+    h.blks = reinterpret_cast<const DBlk*>(base + o_blks);
+    h.rows = reinterpret_cast<const DRowMeta*>(base + o_rows);
+    h.rows_begin = U(o_rowsb);
+    cuda_check(cudaMemcpy(base + o_red, P.red_list.data(), sizeof(uint32_t) * P.red_list.size(), cudaMemcpyHostToDevice), "H2D plan");
+    cuda_check(cudaMemcpy(base + o_ctas, P.ctas.data(), sizeof(DCta) * P.ctas.size(), cudaMemcpyHostToDevice), "H2D plan");
+    if (!P.segs.empty())
+        cuda_check(cudaMemcpy(base + o_segs, P.segs.data(), sizeof(DSeg) * P.segs.size(), cudaMemcpyHostToDevice), "H2D plan");
+    if (!P.blks.empty())
+        cuda_check(cudaMemcpy(base + o_blks, P.blks.data(), sizeof(DBlk) * P.blks.size(), cudaMemcpyHostToDevice), "H2D plan");
+    cuda_check(cudaMemcpy(base + o_rows, P.rows.data(), sizeof(DRowMeta) * P.rows.size(), cudaMemcpyHostToDevice), "H2D plan");
+    cuda_check(cudaMemcpy(base + o_rowsb, P.rows_begin.data(), sizeof(uint32_t) * P.rows_begin.size(), cudaMemcpyHostToDevice), "H2D plan");
+
+    h.stim_len = stim_len;
+    h.stim_off = U(o_soff);
+    h.ev_neuron = U(o_evn);
+    h.ev_delta = F(o_evd);
+    cuda_check(cudaMemcpy(base + o_soff, stim_off.data(), sizeof(uint32_t) * stim_off.size(), cudaMemcpyHostToDevice), "H2D stim");
+    if (!ev_neuron.empty()) {
+        cuda_check(cudaMemcpy(base + o_evn, ev_neuron.data(), sizeof(uint32_t) * ev_neuron.size(), cudaMemcpyHostToDevice), "H2D stim");
+        cuda_check(cudaMemcpy(base + o_evd, ev_delta.data(), sizeof(float) * ev_delta.size(), cudaMemcpyHostToDevice), "H2D stim");
+    }
+    h.noise_mode = s->noise_mode;
+    h.seed = static_cast<uint32_t>(s->desc.rng_seed);
+    h.replay = base + o_rep;
+    h.replay_steps = s->replay_steps;
+    if (!s->replay.empty())
+        cuda_check(cudaMemcpy(base + o_rep, s->replay.data(), s->replay.size(), cudaMemcpyHostToDevice), "H2D replay");
+    h.barrier = reinterpret_cast<unsigned long long*>(base + o_bar);
+    h.error = reinterpret_cast<int32_t*>(base + o_err);
+    h.steps_done = reinterpret_cast<unsigned long long*>(base + o_sd);
+    h.clock = U(o_clk);
+    s->d_sim = reinterpret_cast<DSim*>(base + o_sim);
+    cuda_check(cudaMemcpy(s->d_sim, &h, sizeof(DSim), cudaMemcpyHostToDevice), "H2D sim");
+
+    // Launch configuration.
+    uint32_t n_spike_mons = 0;
+    for (const auto& M : s->mons) n_spike_mons += M.kind == kMonSpikes ? 1u : 0u;
+    s->smem_bytes = (sizeof(float4) + sizeof(DRowMeta) + sizeof(uint32_t) + sizeof(float) * kMaxWarps) * h.max_rows +
+                    sizeof(float) * 2 * h.max_own + sizeof(uint32_t) * n_spike_mons * (h.max_own / 32 + 2);
+    cuda_check(cudaFuncSetAttribute(bsnn_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(s->smem_bytes)),
+               "cudaFuncSetAttribute smem");
+    int per_sm = 0;
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bsnn_step_kernel, static_cast<int>(s->block),
+                                                             s->smem_bytes),
+               "occupancy");
+    require(per_sm >= 1 && static_cast<long>(per_sm) * s->sm_count >= static_cast<long>(s->grid), BSNN_ERR_RUNTIME,
+            "persistent grid does not fit on the device");
+    cuda_check(cudaStreamSynchronize(s->stream), "finalize sync");
+    s->finalized = true;
+}
+
+void launch_direct(bsnn_sim* s, uint32_t n_steps) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(s->grid);
+    cfg.blockDim = dim3(s->block);
+    cfg.dynamicSmemBytes = s->smem_bytes;
+    cfg.stream = s->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cuda_check(cudaLaunchKernelEx(&cfg, bsnn_step_kernel, static_cast<const DSim*>(s->d_sim), n_steps),
+               "bsnn_step_kernel launch");
+    ++s->launches;
+}
+
+void launch_chunk(bsnn_sim* s, uint32_t n_steps) {
+    if (s->graphs_ok) {
+        auto it = s->graphs.find(n_steps);
+        if (it == s->graphs.end()) {
+            cudaGraph_t graph = nullptr;
+            cudaGraphExec_t exec = nullptr;
+            bool ok = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+            if (ok) {
+                cudaLaunchConfig_t cfg{};
+                cfg.gridDim = dim3(s->grid);
+                cfg.blockDim = dim3(s->block);
+                cfg.dynamicSmemBytes = s->smem_bytes;
+                cfg.stream = s->stream;
+                cudaLaunchAttribute attr[1];
+                attr[0].id = cudaLaunchAttributeCooperative;
+                attr[0].val.cooperative = 1;
+                cfg.attrs = attr;
+                cfg.numAttrs = 1;
+                const cudaError_t le = cudaLaunchKernelEx(&cfg, bsnn_step_kernel, static_cast<const DSim*>(s->d_sim), n_steps);
+                const cudaError_t ce = cudaStreamEndCapture(s->stream, &graph);
+                ok = le == cudaSuccess && ce == cudaSuccess && graph != nullptr &&
+                     cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+                if (graph) cudaGraphDestroy(graph);
+            }
+            if (!ok) {
+                cudaGetLastError();  // clear the capture failure; fall back to direct launches
+                s->graphs_ok = false;
+                launch_direct(s, n_steps);
+                return;
+            }
+            it = s->graphs.emplace(n_steps, exec).first;
+        }
+        cuda_check(cudaGraphLaunch(it->second, s->stream), "cudaGraphLaunch");
+        ++s->launches;
+        return;
+    }
+    launch_direct(s, n_steps);
+}
+
+void check_device_error(bsnn_sim* s) {
+    cuda_check(cudaStreamSynchronize(s->stream), "stream synchronize");
+    int32_t e = 0;
+    cuda_check(cudaMemcpy(&e, s->h.error, sizeof(e), cudaMemcpyDeviceToHost), "D2H error flag");
+    if (e != kErrNone) {
+        s->failed = true;
+        throw ApiError(BSNN_ERR_DEVICE_TIMEOUT, "device-side grid barrier timed out; simulation state is invalid");
+    }
+}
+
+void run_steps(bsnn_sim* s, uint32_t first_clock, uint32_t n) {
+    finalize(s);
+    require(!s->failed, BSNN_ERR_STATE, "simulation failed earlier (device timeout)");
+    if (n == 0) return;
+    if (first_clock != s->next_clock) {
+        bsnn_set_clock_kernel<<<1, 1, 0, s->stream>>>(s->h.clock, first_clock);
+        cuda_check(cudaGetLastError(), "set clock");
+    }
+    uint32_t left = n;
+    while (left > 0) {
+        const uint32_t chunk = std::min(left, s->steps_per_launch);
+        launch_chunk(s, chunk);
+        left -= chunk;
+    }
+    s->steps_done += n;
+    s->next_clock = first_clock + n;
+}
+
+// Field -> (device pointer, element count, element size).
+struct FieldRef {
+    void* ptr;
+    uint32_t len;
+};
+
+FieldRef field_ref(bsnn_sim* s, int32_t field, uint32_t index) {
+    const DSim& h = s->h;
+    const uint32_t N = s->N;
+    switch (field) {
+        case BSNN_FIELD_MEMBRANE_POTENTIALS: return {h.v, N};
+        case BSNN_FIELD_G_EXCITATORY: return {h.ge, N};
+        case BSNN_FIELD_G_INHIBITORY: return {h.gi, N};
+        case BSNN_FIELD_I_STIMULUS: return {h.istim, N};
+        case BSNN_FIELD_REFRACTORY_COUNTER: return {h.refrac, N};
+        case BSNN_FIELD_SPIKES: return {h.spikes[s->steps_done == 0 ? 0 : (s->steps_done - 1) & 1], N};
+        case BSNN_FIELD_BG_G_EXCITATORY: return {h.bg_ge, N};
+        case BSNN_FIELD_BG_G_INHIBITORY: return {h.bg_gi, N};
+        case BSNN_FIELD_BG_E_R_TRACES: return {h.bg_er, N};
+        case BSNN_FIELD_BG_E_D_TRACES: return {h.bg_ed, N};
+        case BSNN_FIELD_BG_I_R_TRACES: return {h.bg_ir, N};
+        case BSNN_FIELD_BG_I_D_TRACES: return {h.bg_id, N};
+        default: break;
+    }
+    if (field >= BSNN_FIELD_CONN_R_TRACES && field <= BSNN_FIELD_CONN_SUMMED) {
+        require(index < h.n_conns, BSNN_ERR_OUT_OF_RANGE, "connection index out of range");
+        const DTraceSet& T = h.ts[h.conns[index].ts];
+        const uint32_t n = h.conns[index].n_pre;
+        return {field == BSNN_FIELD_CONN_R_TRACES ? T.r : field == BSNN_FIELD_CONN_D_TRACES ? T.d : T.x, n};
+    }
+    if (field >= BSNN_FIELD_PLAST_PRE_TRACES && field <= BSNN_FIELD_PLAST_PRE_WEIGHT_SUMS) {
+        require(index < h.n_plast, BSNN_ERR_OUT_OF_RANGE, "plasticity index out of range");
+        const DPlast& P = h.plast[index];
+        const DConn& C = h.conns[P.conn];
+        switch (field) {
+            case BSNN_FIELD_PLAST_PRE_TRACES: return {P.pre, C.n_pre};
+            case BSNN_FIELD_PLAST_POST_TRACES: return {P.post, C.n_post};
+            case BSNN_FIELD_PLAST_TRIPLET_PRE: return {P.tpre, C.n_pre};
+            case BSNN_FIELD_PLAST_TRIPLET_POST: return {P.tpost, C.n_post};
+            default: return {P.sums, P.kind == kKindTriplet ? C.n_pre : 0u};
+        }
+    }
+    throw ApiError(BSNN_ERR_INVALID_ARGUMENT, "unknown field " + std::to_string(field));
+}
+
+}  // namespace
+
+// ============================================================================================
+extern "C" {
+
+BSNN_API const char* bsnn_version(void) { return "bsnn 0.1 (sm_100a persistent step kernel)"; }
+
+BSNN_API bsnn_status bsnn_create(const bsnn_state_desc* desc, bsnn_sim** out_sim) {
+    return guarded(nullptr, [&] {
+        require(desc && out_sim, BSNN_ERR_INVALID_ARGUMENT, "null argument");
+        require(desc->num_excitatory_neurons + static_cast<uint64_t>(desc->num_inhibitory_neurons) < (1ull << 31),
+                BSNN_ERR_INVALID_ARGUMENT, "too many neurons");
+        auto s = std::make_unique<bsnn_sim>();
+        s->desc = *desc;
+        if (s->desc.recording_interval_steps == 0) s->desc.recording_interval_steps = 10000;
+        s->N = desc->num_excitatory_neurons + desc->num_inhibitory_neurons;
+        s->device = desc->device;
+        int n_dev = 0;
+        cuda_check(cudaGetDeviceCount(&n_dev), "cudaGetDeviceCount");
+        require(desc->device >= 0 && desc->device < n_dev, BSNN_ERR_INVALID_ARGUMENT, "invalid CUDA device ordinal");
+        DeviceGuard g(s->device);
+        cudaDeviceProp prop{};
+        cuda_check(cudaGetDeviceProperties(&prop, s->device), "cudaGetDeviceProperties");
+        require(prop.cooperativeLaunch != 0, BSNN_ERR_RUNTIME, "device does not support cooperative launches");
+        s->sm_count = prop.multiProcessorCount;
+        cuda_check(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        *out_sim = s.release();
+    });
+}
+
+BSNN_API bsnn_status bsnn_destroy(bsnn_sim* sim) {
+    if (!sim) return BSNN_OK;
+    {
+        DeviceGuard g(sim->device);
+        if (sim->stream) cudaStreamSynchronize(sim->stream);
+        delete sim;
+    }
+    return BSNN_OK;
+}
+
+BSNN_API const char* bsnn_last_error(const bsnn_sim* sim) {
+    return sim ? sim->err.c_str() : g_thread_error.c_str();
+}
+
+BSNN_API bsnn_status bsnn_get_info(const bsnn_sim* sim, bsnn_info* out) {
+    if (!sim || !out) return BSNN_ERR_INVALID_ARGUMENT;
+    bsnn_info i{};
+    i.total_neurons = sim->N;
+    i.num_groups = static_cast<uint32_t>(sim->groups.size());
+    i.num_connections = static_cast<uint32_t>(sim->conns.size());
+    i.num_plasticities = static_cast<uint32_t>(sim->plasts.size());
+    i.num_monitors = static_cast<uint32_t>(sim->mons.size());
+    i.grid_ctas = sim->grid;
+    i.block_threads = sim->block;
+    i.steps_per_launch = sim->steps_per_launch;
+    i.steps_done = sim->steps_done;
+    i.device_bytes = sim->arena_bytes;
+    i.weight_bytes = sim->weight_bytes;
+    i.kernel_launches = sim->launches;
+    *out = i;
+    return BSNN_OK;
+}
+
+BSNN_API bsnn_status bsnn_add_neuron_group(bsnn_sim* sim, const bsnn_neuron_group_params* p, uint32_t* out_group) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        require_building(sim);
+        require(p != nullptr, BSNN_ERR_INVALID_ARGUMENT, "null params");
+        // GpuSimulationState::require_upload_bounds (gpu_simulation_state.cu:211-219)
+        require(p->offset <= sim->N && p->num_neurons <= sim->N - p->offset, BSNN_ERR_INVALID_ARGUMENT,
+                "neuron_group slice is out of bounds. offset=" + std::to_string(p->offset) +
+                    ", count=" + std::to_string(p->num_neurons) + ", total_neurons=" + std::to_string(sim->N));
+        require(sim->groups.size() < static_cast<size_t>(kMaxGroups), BSNN_ERR_INVALID_ARGUMENT, "too many neuron groups");
+        for (const auto& g : sim->groups) {
+            const bool disjoint = p->offset + p->num_neurons <= g.p.offset || g.p.offset + g.p.num_neurons <= p->offset;
+            require(disjoint, BSNN_ERR_INVALID_ARGUMENT, "neuron groups must not overlap");
+        }
+        require(p->num_neurons > 0, BSNN_ERR_INVALID_ARGUMENT, "neuron group must not be empty");
+        require(p->membrane_capacitance > 0.0f, BSNN_ERR_INVALID_ARGUMENT, "membrane_capacitance must be > 0");
+        require(p->mean_background_excitatory_spikes <= 80.0f && p->mean_background_inhibitory_spikes <= 80.0f,
+                BSNN_ERR_INVALID_ARGUMENT, "mean background spikes per step must be <= 80");
+        sim->groups.push_back(HostGroup{*p});
+        if (out_group) *out_group = static_cast<uint32_t>(sim->groups.size() - 1);
+    });
+}
+
+BSNN_API bsnn_status bsnn_add_connection(bsnn_sim* sim, uint32_t pre_group, uint32_t post_group, const float* weights,
+                                         const bsnn_connection_params* p, uint32_t* out_connection) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        require_building(sim);
+        require(weights && p, BSNN_ERR_INVALID_ARGUMENT, "null weights or params");
+        require(pre_group < sim->groups.size() && post_group < sim->groups.size(), BSNN_ERR_OUT_OF_RANGE,
+                "group index out of range");
+        // GpuSimulationState::lookup_weight_matrix_name (gpu_simulation_state.cu:231-236)
+        require(p->weight_matrix_idx < 4, BSNN_ERR_OUT_OF_RANGE,
+                "Invalid weight matrix index: " + std::to_string(p->weight_matrix_idx));
+        require(sim->conns.size() < static_cast<size_t>(kMaxConns), BSNN_ERR_INVALID_ARGUMENT, "too many connections");
+        for (const auto& c : sim->conns) {
+            require(c.p.weight_matrix_idx != p->weight_matrix_idx, BSNN_ERR_INVALID_ARGUMENT,
+                    "weight_matrix_idx already used by another connection");
+            require(!(c.pre == pre_group && c.post == post_group), BSNN_ERR_INVALID_ARGUMENT,
+                    "a connection between these groups already exists");
+        }
+        require(p->rise_time > 0.0f && p->decay_time > 0.0f, BSNN_ERR_INVALID_ARGUMENT, "rise_time and decay_time must be > 0");
+        const uint32_t n_pre = sim->groups[pre_group].p.num_neurons, n_post = sim->groups[post_group].p.num_neurons;
+        HostConn c;
+        c.pre = pre_group;
+        c.post = post_group;
+        c.p = *p;
+        const size_t n = static_cast<size_t>(n_pre) * n_post;
+        c.w.assign(weights, weights + n);
+        // GpuSimulationState::require_nonnegative_weights (gpu_simulation_state.cu:221-229)
+        for (size_t k = 0; k < n; ++k)
+            require(!(c.w[k] < 0.0f), BSNN_ERR_INVALID_ARGUMENT,
+                    "connection weight_matrix must be non-negative to preserve inhibitory routing contract");
+        // Connection::make_gpu_view (connection.cpp:46-47): decays in float on the host.
+        c.r_decay = std::exp(-1.0f * p->timestep / p->rise_time);
+        c.d_decay = std::exp(-1.0f * p->timestep / p->decay_time);
+        c.norm = p->postsynaptic_kernel_normalization_value;
+        sim->conns.push_back(std::move(c));
+        if (out_connection) *out_connection = static_cast<uint32_t>(sim->conns.size() - 1);
+    });
+}
+
+BSNN_API bsnn_status bsnn_add_stimulus(bsnn_sim* sim, const uint32_t* counts, uint32_t num_timesteps,
+                                       const uint32_t* ids, const uint32_t* offsets, const float* deltas,
+                                       uint32_t num_events) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        require_building(sim);
+        // GpuSimulationState::upload_stimulus_view (gpu_simulation_state.cu:172-186)
+        require(num_timesteps == sim->desc.total_simulation_length && num_events == sim->desc.num_stimulus_events,
+                BSNN_ERR_INVALID_ARGUMENT,
+                "upload_stimulus_view host data vectors must match gpu_view.num_stimulus_events and total_simulation_length");
+        require((counts || num_timesteps == 0) && ((ids && offsets && deltas) || num_events == 0),
+                BSNN_ERR_INVALID_ARGUMENT, "null stimulus arrays");
+        HostStim st;
+        st.counts.assign(counts, counts + num_timesteps);
+        st.ids.assign(ids, ids + num_events);
+        st.offs.assign(offsets, offsets + num_events);
+        st.deltas.assign(deltas, deltas + num_events);
+        uint64_t total = 0;
+        for (uint32_t c : st.counts) total += c;
+        // Stimulus::apply (stimulus.cpp:50-53) would throw when reaching the overflowing step.
+        require(total <= num_events, BSNN_ERR_RUNTIME, "Stimulus event indexing exceeded uploaded event buffers");
+        for (uint32_t e = 0; e < num_events; ++e)
+            require(static_cast<uint64_t>(st.ids[e]) + st.offs[e] < sim->N, BSNN_ERR_OUT_OF_RANGE,
+                    "stimulus event neuron out of range");
+        sim->stims.push_back(std::move(st));
+    });
+}
+
+BSNN_API bsnn_status bsnn_add_plasticity(bsnn_sim* sim, int32_t kind, uint32_t connection,
+                                         const bsnn_plasticity_params* p, uint32_t* out_plasticity) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        require_building(sim);
+        require(p != nullptr, BSNN_ERR_INVALID_ARGUMENT, "null params");
+        require(connection < sim->conns.size(), BSNN_ERR_OUT_OF_RANGE, "connection index out of range");
+        require(kind == BSNN_PLASTICITY_TRIPLET || kind == BSNN_PLASTICITY_ISTDP || kind == BSNN_PLASTICITY_STDP,
+                BSNN_ERR_INVALID_ARGUMENT, "unknown plasticity kind");
+        require(sim->plasts.size() < static_cast<size_t>(kMaxPlast), BSNN_ERR_INVALID_ARGUMENT, "too many plasticities");
+        require(p->plasticity_offset < std::max(sim->desc.num_plasticities, 1u), BSNN_ERR_OUT_OF_RANGE,
+                "plasticity_offset exceeds num_plasticities");
+        for (const auto& pl : sim->plasts)
+            require(pl.conn != connection, BSNN_ERR_INVALID_ARGUMENT, "connection already has a plasticity");
+        const auto& C = sim->conns[connection];
+        if (kind == BSNN_PLASTICITY_TRIPLET)
+            require(sim->groups[C.pre].p.num_neurons <= sim->groups[C.post].p.num_neurons, BSNN_ERR_INVALID_ARGUMENT,
+                    "triplet normalisation needs num_pre <= num_post");
+        // validate_plasticity_params (cpp_src/main_buryn.cpp:76-96)
+        require(p->pre_trace_decay >= 0.0f && p->pre_trace_decay <= 1.0f, BSNN_ERR_RUNTIME, "pre_trace_decay must be in [0, 1]");
+        require(p->post_trace_decay >= 0.0f && p->post_trace_decay <= 1.0f, BSNN_ERR_RUNTIME, "post_trace_decay must be in [0, 1]");
+        if (kind == BSNN_PLASTICITY_TRIPLET) {
+            require(p->triplet_pre_trace_decay >= 0.0f && p->triplet_pre_trace_decay <= 1.0f, BSNN_ERR_RUNTIME,
+                    "triplet_pre_trace_decay must be in [0, 1]");
+            require(p->triplet_post_trace_decay >= 0.0f && p->triplet_post_trace_decay <= 1.0f, BSNN_ERR_RUNTIME,
+                    "triplet_post_trace_decay must be in [0, 1]");
+        }
+        require(p->weight_min <= p->weight_max, BSNN_ERR_RUNTIME, "weight_min must be <= weight_max");
+        sim->plasts.push_back(HostPlast{kind, connection, *p});
+        if (out_plasticity) *out_plasticity = static_cast<uint32_t>(sim->plasts.size() - 1);
+    });
+}
+
+BSNN_API bsnn_status bsnn_add_spike_recorder(bsnn_sim* sim, uint32_t group, uint32_t interval, uint32_t* out_monitor) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        require_building(sim);
+        require(group < sim->groups.size(), BSNN_ERR_OUT_OF_RANGE, "group index out of range");
+        require(sim->mons.size() < static_cast<size_t>(kMaxMonitors), BSNN_ERR_INVALID_ARGUMENT, "too many monitors");
+        HostMon m;
+        m.kind = kMonSpikes;
+        m.group = group;
+        m.interval = interval ? interval : sim->desc.recording_interval_steps;
+        sim->mons.push_back(std::move(m));
+        if (out_monitor) *out_monitor = static_cast<uint32_t>(sim->mons.size() - 1);
+    });
+}
+
+BSNN_API bsnn_status bsnn_add_voltage_recorder(bsnn_sim* sim, uint32_t group, const uint32_t* ids, uint32_t n_ids,
+                                               uint32_t interval, uint32_t* out_monitor) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        require_building(sim);
+        require(group < sim->groups.size(), BSNN_ERR_OUT_OF_RANGE, "group index out of range");
+        require(sim->mons.size() < static_cast<size_t>(kMaxMonitors), BSNN_ERR_INVALID_ARGUMENT, "too many monitors");
+        const uint32_t ng = sim->groups[group].p.num_neurons;
+        HostMon m;
+        m.kind = kMonVoltage;
+        m.group = group;
+        m.interval = interval ? interval : sim->desc.recording_interval_steps;
+        // VoltageRecorder ctor (voltage_recorder.cpp:15-26)
+        if (n_ids == 0) {
+            m.sel.resize(ng);
+            std::iota(m.sel.begin(), m.sel.end(), 0u);
+        } else {
+            require(ids != nullptr, BSNN_ERR_INVALID_ARGUMENT, "null selected ids");
+            for (uint32_t k = 0; k < n_ids; ++k)
+                require(ids[k] < ng, BSNN_ERR_OUT_OF_RANGE,
+                        "Selected neuron ID " + std::to_string(ids[k]) + " is out of range for the neuron group.");
+            m.sel.assign(ids, ids + n_ids);
+        }
+        sim->mons.push_back(std::move(m));
+        if (out_monitor) *out_monitor = static_cast<uint32_t>(sim->mons.size() - 1);
+    });
+}
+
+BSNN_API bsnn_status bsnn_set_noise_mode(bsnn_sim* sim, int32_t mode) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        require_building(sim);
+        require(mode == BSNN_NOISE_PHILOX || mode == BSNN_NOISE_OFF || mode == BSNN_NOISE_REPLAY,
+                BSNN_ERR_INVALID_ARGUMENT, "unknown noise mode");
+        sim->noise_mode = mode;
+    });
+}
+
+BSNN_API bsnn_status bsnn_set_noise_replay(bsnn_sim* sim, const uint8_t* counts, uint32_t n_steps) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        require_building(sim);
+        require(counts != nullptr || n_steps == 0, BSNN_ERR_INVALID_ARGUMENT, "null counts");
+        sim->replay.assign(counts, counts + static_cast<size_t>(n_steps) * sim->N * 2);
+        sim->replay_steps = n_steps;
+        sim->noise_mode = BSNN_NOISE_REPLAY;
+    });
+}
+
+BSNN_API bsnn_status bsnn_step(bsnn_sim* sim, uint32_t clock_step) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] { run_steps(sim, clock_step, 1); });
+}
+
+BSNN_API bsnn_status bsnn_run(bsnn_sim* sim, uint32_t first_clock_step, uint32_t num_steps) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] { run_steps(sim, first_clock_step, num_steps); });
+}
+
+BSNN_API bsnn_status bsnn_synchronize(bsnn_sim* sim) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        if (!sim->finalized) return;
+        check_device_error(sim);
+    });
+}
+
+BSNN_API bsnn_status bsnn_get_stream(const bsnn_sim* sim, void** out_stream) {
+    if (!sim || !out_stream) return BSNN_ERR_INVALID_ARGUMENT;
+    *out_stream = sim->stream;
+    return BSNN_OK;
+}
+
+BSNN_API bsnn_status bsnn_set_steps_per_launch(bsnn_sim* sim, uint32_t steps) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        require(steps >= 1 && steps <= 65536, BSNN_ERR_INVALID_ARGUMENT, "steps per launch must be in [1, 65536]");
+        sim->steps_per_launch = steps;
+    });
+}
+
+BSNN_API bsnn_status bsnn_read_state(bsnn_sim* sim, int32_t field, uint32_t index, uint32_t offset, uint32_t count,
+                                     void* host_out) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        finalize(sim);
+        check_device_error(sim);
+        const FieldRef f = field_ref(sim, field, index);
+        require(offset <= f.len && count <= f.len - offset, BSNN_ERR_OUT_OF_RANGE, "read out of range");
+        require(host_out != nullptr || count == 0, BSNN_ERR_INVALID_ARGUMENT, "null output");
+        if (count)
+            cuda_check(cudaMemcpy(host_out, static_cast<char*>(f.ptr) + 4ull * offset, 4ull * count, cudaMemcpyDeviceToHost),
+                       "D2H state");
+    });
+}
+
+BSNN_API bsnn_status bsnn_write_state(bsnn_sim* sim, int32_t field, uint32_t index, uint32_t offset, uint32_t count,
+                                      const void* host_in) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        finalize(sim);
+        check_device_error(sim);
+        require(field != BSNN_FIELD_SPIKES && field != BSNN_FIELD_PLAST_PRE_WEIGHT_SUMS, BSNN_ERR_INVALID_ARGUMENT,
+                "field is not writable");
+        const FieldRef f = field_ref(sim, field, index);
+        require(offset <= f.len && count <= f.len - offset, BSNN_ERR_OUT_OF_RANGE, "write out of range");
+        require(host_in != nullptr || count == 0, BSNN_ERR_INVALID_ARGUMENT, "null input");
+        if (count)
+            cuda_check(cudaMemcpy(static_cast<char*>(f.ptr) + 4ull * offset, host_in, 4ull * count, cudaMemcpyHostToDevice),
+                       "H2D state");
+    });
+}
+
+BSNN_API bsnn_status bsnn_read_weights(bsnn_sim* sim, uint32_t connection, float* host_out) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        finalize(sim);
+        check_device_error(sim);
+        require(connection < sim->h.n_conns, BSNN_ERR_OUT_OF_RANGE, "connection index out of range");
+        require(host_out != nullptr, BSNN_ERR_INVALID_ARGUMENT, "null output");
+        const DConn& C = sim->h.conns[connection];
+        cuda_check(cudaMemcpy2D(host_out, sizeof(float) * C.n_post, C.w, sizeof(float) * C.ld, sizeof(float) * C.n_post,
+                                C.n_pre, cudaMemcpyDeviceToHost),
+                   "D2H weights");
+    });
+}
+
+BSNN_API bsnn_status bsnn_read_spike_bits(bsnn_sim* sim, uint32_t monitor, uint32_t* host_out, int32_t flush) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        finalize(sim);
+        check_device_error(sim);
+        require(monitor < sim->h.n_mons && sim->h.mons[monitor].kind == kMonSpikes, BSNN_ERR_OUT_OF_RANGE,
+                "not a spike recorder");
+        const DMon& M = sim->h.mons[monitor];
+        const size_t bytes = sizeof(uint32_t) * static_cast<size_t>(M.interval) * M.words;
+        cuda_check(cudaMemcpy(host_out, M.bits, bytes, cudaMemcpyDeviceToHost), "D2H spike ring");
+        if (flush) cuda_check(cudaMemsetAsync(M.bits, 0, bytes, sim->stream), "flush spike ring");
+    });
+}
+
+BSNN_API bsnn_status bsnn_read_spike_history(bsnn_sim* sim, uint32_t monitor, uint32_t* host_out, int32_t flush) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        finalize(sim);
+        check_device_error(sim);
+        require(monitor < sim->h.n_mons && sim->h.mons[monitor].kind == kMonSpikes, BSNN_ERR_OUT_OF_RANGE,
+                "not a spike recorder");
+        const DMon& M = sim->h.mons[monitor];
+        const uint32_t ng = sim->groups[M.group].p.num_neurons;
+        std::vector<uint32_t> bits(static_cast<size_t>(M.interval) * M.words);
+        cuda_check(cudaMemcpy(bits.data(), M.bits, sizeof(uint32_t) * bits.size(), cudaMemcpyDeviceToHost), "D2H spike ring");
+        if (flush) cuda_check(cudaMemsetAsync(M.bits, 0, sizeof(uint32_t) * bits.size(), sim->stream), "flush spike ring");
+        for (uint32_t i = 0; i < ng; ++i)
+            for (uint32_t slot = 0; slot < M.interval; ++slot)
+                host_out[static_cast<size_t>(i) * M.interval + slot] =
+                    (bits[static_cast<size_t>(slot) * M.words + (i >> 5)] >> (i & 31u)) & 1u;
+    });
+}
+
+BSNN_API bsnn_status bsnn_read_voltage_history(bsnn_sim* sim, uint32_t monitor, float* host_out, int32_t flush) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        finalize(sim);
+        check_device_error(sim);
+        require(monitor < sim->h.n_mons && sim->h.mons[monitor].kind == kMonVoltage, BSNN_ERR_OUT_OF_RANGE,
+                "not a voltage recorder");
+        const DMon& M = sim->h.mons[monitor];
+        const auto& sel = sim->mons[monitor].sel;
+        std::vector<float> vh(static_cast<size_t>(M.interval) * M.n_sel);
+        cuda_check(cudaMemcpy(vh.data(), M.vh, sizeof(float) * vh.size(), cudaMemcpyDeviceToHost), "D2H voltage ring");
+        if (flush) cuda_check(cudaMemsetAsync(M.vh, 0, sizeof(float) * vh.size(), sim->stream), "flush voltage ring");
+        // first occurrence of each selected neuron holds its column
+        std::vector<int32_t> first(sim->groups[M.group].p.num_neurons, -1);
+        for (size_t k = 0; k < sel.size(); ++k)
+            if (first[sel[k]] < 0) first[sel[k]] = static_cast<int32_t>(k);
+        for (size_t k = 0; k < sel.size(); ++k) {
+            const uint32_t col = static_cast<uint32_t>(first[sel[k]]);
+            for (uint32_t slot = 0; slot < M.interval; ++slot)
+                host_out[k * M.interval + slot] = vh[static_cast<size_t>(slot) * M.n_sel + col];
+        }
+    });
+}
+
+BSNN_API bsnn_status bsnn_get_device_pointer(const bsnn_sim* sim, int32_t field, uint32_t index, void** out) {
+    if (!sim || !out) return BSNN_ERR_INVALID_ARGUMENT;
+    bsnn_sim* s = const_cast<bsnn_sim*>(sim);
+    return guarded(s, [&] {
+        finalize(s);
+        *out = field_ref(s, field, index).ptr;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,275 @@
+/*
+ * bsnn.h -- C-ABI of libbsnn, the B200-native (sm_100a) engine for the per-step hot path of the
+ * paulazoo/example-cuda-spiking-nn simulator ("buryn").
+ *
+ * The entry points below replace the reference's component constructors and its step loop:
+ * the host builds a network with the same parameter PODs the reference uses
+ * (NeuronGroupParams, ConnectionParams, PlasticityParams: identical field names, order and
+ * layout), then advances it with bsnn_step / bsnn_run, which execute exactly what
+ * System::step_the_clock (cpp_src/core/system.cpp:43-63) executes: neuron evolve, the four
+ * propagations, stimulus, plasticity and monitor historicize, fused into one persistent
+ * sm_100a kernel per call.
+ *
+ * Conventions
+ *  - Every call returns a bsnn_status; on failure bsnn_last_error(sim) (or bsnn_last_error(NULL)
+ *    for failures before a sim exists) holds a message.  The status codes map onto the
+ *    exception types the reference throws (cpp_src/gpu_core/cuda_utils.h:10-20).
+ *  - Plain pointers and sizes only; all host arrays are copied in at the call.
+ *  - Calls on one bsnn_sim are not thread-safe; different sims may be driven from different
+ *    host threads.  Each sim owns one CUDA stream.
+ *  - Neuron indices are global ("offset + local id") exactly as in the reference's
+ *    GpuSimulationState, where the excitatory group sits at offset 0 and the inhibitory group
+ *    at offset num_excitatory_neurons.
+ */
+#ifndef BSNN_H
+#define BSNN_H
+
+#include <stdbool.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define BSNN_API __attribute__((visibility("default")))
+#else
+#define BSNN_API
+#endif
+
+typedef struct bsnn_sim bsnn_sim; /* opaque; one simulated network on one GPU */
+
+typedef int32_t bsnn_status;
+#define BSNN_OK 0
+#define BSNN_ERR_INVALID_ARGUMENT 1 /* reference: std::invalid_argument                          */
+#define BSNN_ERR_OUT_OF_RANGE 2     /* reference: std::out_of_range                               */
+#define BSNN_ERR_RUNTIME 3          /* reference: std::runtime_error                              */
+#define BSNN_ERR_CUDA 4             /* reference: cuda_check -> std::runtime_error                */
+#define BSNN_ERR_DEVICE_TIMEOUT 5   /* a bounded device-side wait gave up (kernel returned early) */
+#define BSNN_ERR_STATE 6            /* call made in the wrong lifecycle state                     */
+
+/* Plasticity kinds (TripletPlasticity / IstdpPlasticity / StdpPlasticity classes). */
+#define BSNN_PLASTICITY_TRIPLET 1 /* cpp_src/plasticities/triplet_plasticity.h:10-27 (normalising form) */
+#define BSNN_PLASTICITY_ISTDP 2   /* cpp_src/plasticities/istdp_plasticity.h:14-27                     */
+#define BSNN_PLASTICITY_STDP 3    /* cpp_src/plasticities/stdp_plasticity.h:14-27                      */
+
+/* Background-noise source for the per-neuron Poisson shot noise. */
+#define BSNN_NOISE_PHILOX 0 /* counter-based Philox4x32-10 keyed by (rng_seed, neuron, step)         */
+#define BSNN_NOISE_OFF 1    /* all Poisson counts are 0 (same as mean_background_* == 0)             */
+#define BSNN_NOISE_REPLAY 2 /* counts supplied by bsnn_set_noise_replay (e.g. recorded elsewhere)    */
+
+/* Fields for bsnn_read_state / bsnn_write_state. */
+#define BSNN_FIELD_MEMBRANE_POTENTIALS 1     /* float [N_total]                                        */
+#define BSNN_FIELD_G_EXCITATORY 2            /* float [N_total]                                        */
+#define BSNN_FIELD_G_INHIBITORY 3            /* float [N_total]                                        */
+#define BSNN_FIELD_I_STIMULUS 4              /* float [N_total]                                        */
+#define BSNN_FIELD_REFRACTORY_COUNTER 5      /* uint32 [N_total]                                       */
+#define BSNN_FIELD_SPIKES 6                  /* uint32 [N_total] (0/1)                                 */
+#define BSNN_FIELD_BG_G_EXCITATORY 7         /* float [N_total]                                        */
+#define BSNN_FIELD_BG_G_INHIBITORY 8         /* float [N_total]                                        */
+#define BSNN_FIELD_BG_E_R_TRACES 9           /* float [N_total]                                        */
+#define BSNN_FIELD_BG_E_D_TRACES 10          /* float [N_total]                                        */
+#define BSNN_FIELD_BG_I_R_TRACES 11          /* float [N_total]                                        */
+#define BSNN_FIELD_BG_I_D_TRACES 12          /* float [N_total]                                        */
+#define BSNN_FIELD_CONN_R_TRACES 13          /* float [N_pre] of connection `index`                    */
+#define BSNN_FIELD_CONN_D_TRACES 14          /* float [N_pre] of connection `index`                    */
+#define BSNN_FIELD_CONN_SUMMED 15            /* float [N_pre] x = d - r of connection `index`          */
+#define BSNN_FIELD_PLAST_PRE_TRACES 16       /* float [N_pre] of plasticity `index`                    */
+#define BSNN_FIELD_PLAST_POST_TRACES 17      /* float [N_post] of plasticity `index`                   */
+#define BSNN_FIELD_PLAST_TRIPLET_PRE 18      /* float [N_pre] of plasticity `index`                    */
+#define BSNN_FIELD_PLAST_TRIPLET_POST 19     /* float [N_post] of plasticity `index`                   */
+#define BSNN_FIELD_PLAST_PRE_WEIGHT_SUMS 20  /* float [N_pre] normalisation targets of plasticity     */
+
+/*
+ * Parameter PODs.  Field names, order and types are those of the reference structs, so a
+ * reference NeuronGroupParams / ConnectionParams / PlasticityParams object can be passed by
+ * address.  (The reference gives C++ default member initialisers; C has none, so the C++
+ * facade in this package supplies the same defaults.)
+ */
+
+/* cpp_src/neuron_groups/neuron_group_params.h:7-31 */
+typedef struct bsnn_neuron_group_params {
+    float timestep;
+    float g_leak;
+    float membrane_capacitance;
+    float depolarization_slope_factor;
+    float v_effective_spike_threshold;
+    float v_excitatory_reversal;
+    float v_inhibitory_reversal;
+    float v_threshold;
+    float v_reset;
+    float v_rest;
+    uint32_t refractory_steps;
+    bool is_inhibitory;
+    float mean_background_excitatory_spikes;
+    float mean_background_inhibitory_spikes;
+    float background_excitatory_postsynaptic_r_trace_decay;
+    float background_excitatory_postsynaptic_d_trace_decay;
+    float background_inhibitory_postsynaptic_r_trace_decay;
+    float background_inhibitory_postsynaptic_d_trace_decay;
+    float background_excitatory_scaling_factor;
+    float background_inhibitory_scaling_factor;
+    uint32_t offset;
+    uint32_t num_neurons;
+} bsnn_neuron_group_params;
+
+/* cpp_src/connections/connection_params.h:7-14 */
+typedef struct bsnn_connection_params {
+    float timestep;
+    float decay_time;
+    float rise_time;
+    float postsynaptic_kernel_normalization_value;
+    uint32_t weight_matrix_idx;
+} bsnn_connection_params;
+
+/* cpp_src/plasticities/plasticity_params.h:7-20 */
+typedef struct bsnn_plasticity_params {
+    float ltp_A;
+    float ltd_A;
+    float ltp_B;
+    float ltd_B;
+    float pre_trace_decay;
+    float post_trace_decay;
+    float triplet_pre_trace_decay;
+    float triplet_post_trace_decay;
+    float weight_min;
+    float weight_max;
+    uint32_t plasticity_offset;
+} bsnn_plasticity_params;
+
+/* Constructor arguments of GpuSimulationState (cpp_src/gpu_core/gpu_simulation_state.h:21-25)
+ * plus the two globals of cpp_src/core/buryn_definitions.h:11-13 the reference reads. */
+typedef struct bsnn_state_desc {
+    uint32_t total_simulation_length;
+    uint32_t num_excitatory_neurons;
+    uint32_t num_inhibitory_neurons;
+    uint32_t num_stimulus_events;
+    uint32_t num_plasticities;
+    uint32_t recording_interval_steps; /* buryn::recording_interval_steps; 0 means 10000 */
+    int32_t rng_seed;                  /* buryn::rng_seed */
+    int32_t device;                    /* CUDA device ordinal */
+} bsnn_state_desc;
+
+typedef struct bsnn_info {
+    uint32_t total_neurons;
+    uint32_t num_groups;
+    uint32_t num_connections;
+    uint32_t num_plasticities;
+    uint32_t num_monitors;
+    uint32_t grid_ctas;        /* persistent CTAs (one per SM)                          */
+    uint32_t block_threads;    /* threads per CTA                                       */
+    uint32_t steps_per_launch; /* steps one persistent launch covers inside bsnn_run    */
+    uint64_t steps_done;       /* steps executed so far (the stimulus / noise cursor)   */
+    uint64_t device_bytes;     /* bytes held in the device arena                        */
+    uint64_t weight_bytes;     /* bytes of weight storage                               */
+    uint64_t kernel_launches;  /* persistent-kernel launches issued so far              */
+} bsnn_info;
+
+/* ---- lifecycle --------------------------------------------------------------------------- */
+
+/* Replaces GpuSimulationState::GpuSimulationState (cpp_src/gpu_core/gpu_simulation_state.cu:8-28). */
+BSNN_API bsnn_status bsnn_create(const bsnn_state_desc* desc, bsnn_sim** out_sim);
+/* Replaces GpuSimulationState::~GpuSimulationState (cpp_src/gpu_core/gpu_simulation_state.cu:31-33). */
+BSNN_API bsnn_status bsnn_destroy(bsnn_sim* sim);
+/* Message of the last failed call on `sim` (or of the calling thread when sim == NULL). */
+BSNN_API const char* bsnn_last_error(const bsnn_sim* sim);
+BSNN_API bsnn_status bsnn_get_info(const bsnn_sim* sim, bsnn_info* out);
+/* Version string of the library build. */
+BSNN_API const char* bsnn_version(void);
+
+/* ---- components (each mirrors one reference constructor) --------------------------------- */
+
+/* NeuronGroup::NeuronGroup (cpp_src/neuron_groups/neuron_group.cpp:4-17): uploads v = v_rest and
+ * zero for every other per-neuron field of the slice [offset, offset + num_neurons). */
+BSNN_API bsnn_status bsnn_add_neuron_group(bsnn_sim* sim, const bsnn_neuron_group_params* params,
+                                           uint32_t* out_group);
+
+/* Connection::Connection (cpp_src/connections/connection.cpp:3-23): `weights` is the
+ * pre x post matrix in row-major order (weights[pre * num_post + post]), as
+ * Connection::initialize_data flattens it (cpp_src/connections/connection.cpp:27-42).
+ * Negative weights are rejected (gpu_simulation_state.cu:221-229). */
+BSNN_API bsnn_status bsnn_add_connection(bsnn_sim* sim, uint32_t pre_group, uint32_t post_group,
+                                         const float* weights, const bsnn_connection_params* params,
+                                         uint32_t* out_connection);
+
+/* Stimulus::Stimulus (cpp_src/stimuli/stimulus.cpp:3-17): per-step event counts and the flat,
+ * time-ordered event arrays; events add `delta` to i_stimulus[offset + id]. */
+BSNN_API bsnn_status bsnn_add_stimulus(bsnn_sim* sim, const uint32_t* timestep_event_count,
+                                       uint32_t num_timesteps, const uint32_t* neuron_ids,
+                                       const uint32_t* post_group_offsets, const float* amplitude_changes,
+                                       uint32_t num_events);
+
+/* TripletPlasticity / IstdpPlasticity / StdpPlasticity constructors
+ * (cpp_src/plasticities/triplet_plasticity.cpp:3-12, istdp_plasticity.cpp:3-12,
+ * stdp_plasticity.cpp:3-12).  For the triplet rule the normalisation targets are the initial
+ * column sums of the weight matrix (triplet_plasticity.cpp:21-31). */
+BSNN_API bsnn_status bsnn_add_plasticity(bsnn_sim* sim, int32_t kind, uint32_t connection,
+                                         const bsnn_plasticity_params* params, uint32_t* out_plasticity);
+
+/* SpikeRecorder::SpikeRecorder (cpp_src/monitors/spike_recorder.cpp:3-14): a device ring of
+ * `recording_interval_steps` slots holding the group's spikes of each step. */
+BSNN_API bsnn_status bsnn_add_spike_recorder(bsnn_sim* sim, uint32_t group, uint32_t recording_interval_steps,
+                                             uint32_t* out_monitor);
+
+/* VoltageRecorder::VoltageRecorder (cpp_src/monitors/voltage_recorder.cpp:3-28): ring of the
+ * selected neurons' membrane potentials (an empty selection records the whole group). */
+BSNN_API bsnn_status bsnn_add_voltage_recorder(bsnn_sim* sim, uint32_t group, const uint32_t* selected_neurons,
+                                               uint32_t num_selected, uint32_t recording_interval_steps,
+                                               uint32_t* out_monitor);
+
+/* ---- noise ---------------------------------------------------------------------------------- */
+
+BSNN_API bsnn_status bsnn_set_noise_mode(bsnn_sim* sim, int32_t mode);
+/* counts[(s * N_total + neuron) * 2 + channel] for steps s = 0 .. num_steps-1 counted from the
+ * sim's first step; channel 0 = excitatory, 1 = inhibitory.  Steps past num_steps draw 0. */
+BSNN_API bsnn_status bsnn_set_noise_replay(bsnn_sim* sim, const uint8_t* counts, uint32_t num_steps);
+
+/* ---- the hot path --------------------------------------------------------------------------- */
+
+/* System::step_the_clock(clock_step) (cpp_src/core/system.cpp:43-63): one step of every phase.
+ * Returns after the work is queued; errors of the kernel surface at the next synchronising
+ * call (bsnn_synchronize, reads). */
+BSNN_API bsnn_status bsnn_step(bsnn_sim* sim, uint32_t clock_step);
+/* The step loop of System::run (cpp_src/core/system.cpp:65-84) without its callbacks and
+ * recording: steps first_clock_step .. first_clock_step + num_steps - 1, as CUDA-graph replays
+ * of the persistent kernel. */
+BSNN_API bsnn_status bsnn_run(bsnn_sim* sim, uint32_t first_clock_step, uint32_t num_steps);
+/* Waits for queued work and reports a device-side error (barrier timeout) if one occurred. */
+BSNN_API bsnn_status bsnn_synchronize(bsnn_sim* sim);
+/* The sim's CUDA stream (a cudaStream_t), for callers that time or order work around it. */
+BSNN_API bsnn_status bsnn_get_stream(const bsnn_sim* sim, void** out_stream);
+/* Steps per persistent launch used by bsnn_run (default 1000; 1..65536). */
+BSNN_API bsnn_status bsnn_set_steps_per_launch(bsnn_sim* sim, uint32_t steps);
+
+/* ---- state access (GpuSimulationState download helpers) ------------------------------------ */
+
+/* Copies `count` elements starting at `offset` of a field (BSNN_FIELD_*) to host memory.
+ * `index` selects the connection / plasticity for the per-component fields. */
+BSNN_API bsnn_status bsnn_read_state(bsnn_sim* sim, int32_t field, uint32_t index, uint32_t offset,
+                                     uint32_t count, void* host_out);
+/* Overwrites elements of a per-neuron field (test set-up; same fields as bsnn_read_state). */
+BSNN_API bsnn_status bsnn_write_state(bsnn_sim* sim, int32_t field, uint32_t index, uint32_t offset,
+                                      uint32_t count, const void* host_in);
+/* GpuSimulationState::download_weight_matrix (cpp_src/gpu_core/gpu_simulation_state.cu:287-306):
+ * row-major pre x post matrix of a connection. */
+BSNN_API bsnn_status bsnn_read_weights(bsnn_sim* sim, uint32_t connection, float* host_out);
+/* GpuSimulationState::download_and_flush_spike_history (gpu_simulation_state.cu:239-261):
+ * writes the spike ring of a spike recorder in the reference layout
+ * host_out[neuron * interval + slot] (0/1) and, when `flush` is non-zero, zeroes the ring. */
+BSNN_API bsnn_status bsnn_read_spike_history(bsnn_sim* sim, uint32_t monitor, uint32_t* host_out, int32_t flush);
+/* Same ring as packed bits, time-major: host_out[slot * words + w], words = ceil(N_group / 32);
+ * bit b of word w is neuron 32 * w + b of the group.  This is what the device stores. */
+BSNN_API bsnn_status bsnn_read_spike_bits(bsnn_sim* sim, uint32_t monitor, uint32_t* host_out, int32_t flush);
+/* GpuSimulationState::download_and_flush_membrane_potential_history (gpu_simulation_state.cu:263-285),
+ * restricted to the recorder's selected neurons: host_out[k * interval + slot] for the k-th
+ * selected neuron. */
+BSNN_API bsnn_status bsnn_read_voltage_history(bsnn_sim* sim, uint32_t monitor, float* host_out, int32_t flush);
+/* Device address of a field (for the C++ facade's *View structs); read-only use. */
+BSNN_API bsnn_status bsnn_get_device_pointer(const bsnn_sim* sim, int32_t field, uint32_t index, void** out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BSNN_H */
