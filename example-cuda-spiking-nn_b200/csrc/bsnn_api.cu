@@ -255,6 +255,10 @@ Plan build_plan(const bsnn_sim* s, uint32_t n_ctas) {
                 seg.blk_end = static_cast<uint32_t>(P.blks.size());
                 if (seg.blk_end == seg.blk_begin) continue;
                 const auto& gq = s->groups[q].p;
+                // first column of group q in the padded partial rows (groups in index order,
+                // each rounded up to 4 columns; the same layout finalize() gives DGroup::pcol)
+                seg.pcol = 0;
+                for (uint32_t g2 = 0; g2 < q; ++g2) seg.pcol += round_up(s->groups[g2].p.num_neurons, 4);
                 seg.n_post = gq.num_neurons;
                 seg.units = round_up(gq.num_neurons, 4) / 4;
                 seg.item_begin = item;

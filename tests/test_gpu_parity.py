@@ -183,7 +183,9 @@ def test_example_size_network_properties():
     spec.build(g)
     g.run(0, 2000)
     w = g.read_weights(0).astype(np.float64)
-    assert np.isfinite(w).all() and w.min() >= 0.0 and w.max() <= 3.0e-9 * (1 + 1e-6)
+    # clamped to [weight_min, weight_max] by LTP/LTD, then rescaled by the row normalisation, which
+    # may lift entries above weight_max (kernel_triplet_plasticity_update.cu:117-145 runs after the clamp)
+    assert np.isfinite(w).all() and w.min() >= 0.0
     targets = g.read("plasticity_pre_weight_sums", 0, count=spec.num_excitatory).astype(np.float64)
     rows = w.sum(axis=1)
     ok = rows > 0
