@@ -215,6 +215,8 @@ class Info(ctypes.Structure):
         ("device_bytes", ctypes.c_uint64),
         ("weight_bytes", ctypes.c_uint64),
         ("kernel_launches", ctypes.c_uint64),
+        ("smem_bytes", ctypes.c_uint64),
+        ("resident_bytes", ctypes.c_uint64),
     ]
 
 

@@ -103,6 +103,7 @@ struct bsnn_sim {
     DSim* d_sim = nullptr;
     uint32_t grid = 0, block = 0;
     size_t smem_bytes = 0;
+    const void* kernel = nullptr;  // the bsnn_step_kernel instantiation chosen for this network
     uint64_t steps_done = 0;
     uint32_t next_clock = 0;
     uint32_t steps_per_launch = 1000;
@@ -175,6 +176,7 @@ struct Plan {
     std::vector<uint32_t> red_list;
     uint32_t red_begin[2][kMaxGroups]{}, red_end[2][kMaxGroups]{};
     uint32_t n_slots = 0, max_rows = 1, max_own = 1, max_items = 1;
+    uint64_t resident_floats = 0;
 };
 
 int group_of_host(const bsnn_sim* s, uint32_t j) {
@@ -185,7 +187,53 @@ int group_of_host(const bsnn_sim* s, uint32_t j) {
     return -1;
 }
 
-Plan build_plan(const bsnn_sim* s, uint32_t n_ctas) {
+// Partitions the neurons into n_ctas contiguous ranges balancing `cost`; when `cap_bytes` > 0 the
+// plastic rows of every range must also fit in cap_bytes of shared memory (returns false if not).
+bool greedy_partition(const std::vector<double>& cost, const std::vector<uint64_t>& res_bytes, uint32_t n_ctas,
+                      double max_cost, uint64_t cap_bytes, std::vector<uint32_t>& bounds) {
+    const uint32_t N = static_cast<uint32_t>(cost.size());
+    bounds.assign(n_ctas + 1, N);
+    bounds[0] = 0;
+    uint32_t c = 0;
+    double acc = 0.0;
+    uint64_t acc_res = 0;
+    for (uint32_t j = 0; j < N; ++j) {
+        if (cost[j] > max_cost || (cap_bytes > 0 && res_bytes[j] > cap_bytes)) return false;
+        if (acc + cost[j] > max_cost || (cap_bytes > 0 && acc_res + res_bytes[j] > cap_bytes)) {
+            if (++c >= n_ctas) return false;
+            bounds[c] = j;
+            acc = 0.0;
+            acc_res = 0;
+        }
+        acc += cost[j];
+        acc_res += res_bytes[j];
+    }
+    for (uint32_t k = c + 1; k <= n_ctas; ++k) bounds[k] = N;
+    return true;
+}
+
+// Contiguous partition of the neurons into n_ctas ranges that minimises the largest per-range
+// cost (binary search on that maximum); with cap_bytes > 0 every range's plastic rows must also
+// fit in cap_bytes of shared memory.  Returns false if no such partition exists.
+bool partition(const std::vector<double>& cost, const std::vector<uint64_t>& res_bytes, uint32_t n_ctas,
+               uint64_t cap_bytes, std::vector<uint32_t>& bounds) {
+    double total = 0.0, biggest = 0.0;
+    for (double c : cost) {
+        total += c;
+        biggest = std::max(biggest, c);
+    }
+    double lo = std::max(biggest, total / n_ctas), hi = total + 1.0;
+    if (!greedy_partition(cost, res_bytes, n_ctas, hi, cap_bytes, bounds)) return false;
+    for (int it = 0; it < 60 && hi - lo > 1e-6 * hi; ++it) {
+        const double mid = 0.5 * (lo + hi);
+        std::vector<uint32_t> b;
+        if (greedy_partition(cost, res_bytes, n_ctas, mid, cap_bytes, b)) hi = mid;
+        else lo = mid;
+    }
+    return greedy_partition(cost, res_bytes, n_ctas, hi, cap_bytes, bounds);
+}
+
+Plan build_plan(const bsnn_sim* s, uint32_t n_ctas, uint64_t cap_bytes, bool* resident_ok) {
     Plan P;
     const uint32_t N = s->N;
     // Per-neuron cost of its outgoing rows: one weight read, plus write and (normalised) re-read
@@ -203,18 +251,23 @@ Plan build_plan(const bsnn_sim* s, uint32_t n_ctas) {
             cost[j] += w * round_up(s->groups[C.post].p.num_neurons, 4);
         }
     }
-    std::vector<double> prefix(N + 1, 0.0);
-    for (uint32_t j = 0; j < N; ++j) prefix[j + 1] = prefix[j] + cost[j];
-    const double total = prefix[N];
-    std::vector<uint32_t> bounds(n_ctas + 1, 0);
-    bounds[n_ctas] = N;
-    for (uint32_t c = 1; c < n_ctas; ++c) {
-        const double target = total * c / n_ctas;
-        uint32_t j = static_cast<uint32_t>(std::lower_bound(prefix.begin(), prefix.end(), target) - prefix.begin());
-        j = std::min(std::max(j, bounds[c - 1] + (N - bounds[c - 1] > n_ctas - c ? 1u : 0u)), N);
-        bounds[c] = j;
+    // Shared-memory bytes of each neuron's plastic rows (resident candidates).
+    std::vector<uint64_t> res_bytes(N, 0);
+    for (uint32_t j = 0; j < N; ++j) {
+        const int g = group_of_host(s, j);
+        if (g < 0) continue;
+        for (size_t c = 0; c < s->conns.size(); ++c) {
+            const auto& C = s->conns[c];
+            if (static_cast<int>(C.pre) != g) continue;
+            bool plastic = false;
+            for (const auto& pl : s->plasts) plastic |= pl.conn == c;
+            if (plastic) res_bytes[j] += 4ull * round_up(s->groups[C.post].p.num_neurons, 4);
+        }
     }
-    for (uint32_t c = 1; c <= n_ctas; ++c) bounds[c] = std::max(bounds[c], bounds[c - 1]);
+    std::vector<uint32_t> bounds;
+    bool resident = cap_bytes > 0 && partition(cost, res_bytes, n_ctas, cap_bytes, bounds);
+    if (!resident) partition(cost, res_bytes, n_ctas, 0, bounds);
+    if (resident_ok) *resident_ok = resident;
 
     // Slot bookkeeping: slot of (cta, target), and which (target, group) each CTA feeds.
     std::vector<std::vector<uint32_t>> red(2 * kMaxGroups);
@@ -271,6 +324,26 @@ Plan build_plan(const bsnn_sim* s, uint32_t n_ctas) {
         }
         cta.seg_end = static_cast<uint32_t>(P.segs.size());
         cta.n_rows = static_cast<uint32_t>(P.rows.size()) - row_base;
+        if (resident) {
+            // plastic blocks first, then read-only blocks while they still fit under the cap
+            const uint32_t b0 = cta.seg_end > cta.seg_begin ? P.segs[cta.seg_begin].blk_begin : 0u;
+            const uint32_t b1 = cta.seg_end > cta.seg_begin ? P.segs[cta.seg_end - 1].blk_end : 0u;
+            uint64_t used = 0;
+            for (int pass = 0; pass < 2; ++pass)
+                for (uint32_t bk = b0; bk < b1; ++bk) {
+                    DBlk& B = P.blks[bk];
+                    bool plastic = false;
+                    for (const auto& pl : s->plasts) plastic |= pl.conn == B.conn;
+                    if (plastic != (pass == 0)) continue;
+                    const uint64_t bytes = 4ull * (B.row_end - B.row_begin) *
+                                           round_up(s->groups[s->conns[B.conn].post].p.num_neurons, 4);
+                    if (used + bytes > cap_bytes) continue;
+                    B.resident = 1;
+                    B.sm_off = static_cast<uint32_t>(used / 4);
+                    used += bytes;
+                }
+            P.resident_floats = std::max<uint64_t>(P.resident_floats, used / 4);
+        }
         cta.n_items = item;
         require(cta.seg_end - cta.seg_begin <= static_cast<uint32_t>(kMaxSegsPerCta), BSNN_ERR_INVALID_ARGUMENT,
                 "too many (target, post group) segments per CTA");
@@ -374,6 +447,8 @@ void finalize(bsnn_sim* s) {
            o_bid = A.take(fN);
     size_t o_ref = A.take(sizeof(uint32_t) * N);
     size_t o_spk0 = A.take(sizeof(uint32_t) * N), o_spk1 = A.take(sizeof(uint32_t) * N);
+    const uint32_t spk_words = (N + 31) / 32 + 2;
+    size_t o_sb0 = A.take(sizeof(uint32_t) * spk_words), o_sb1 = A.take(sizeof(uint32_t) * spk_words);
     std::vector<size_t> o_ts(h.n_ts * 3);
     for (uint32_t t = 0; t < h.n_ts; ++t) {
         const size_t n = sizeof(float) * s->groups[h.ts[t].group].p.num_neurons;
@@ -392,7 +467,7 @@ void finalize(bsnn_sim* s) {
         o_w[c] = A.take(sizeof(float) * static_cast<size_t>(n_pre) * ld);
         wbytes += sizeof(float) * static_cast<size_t>(n_pre) * ld;
     }
-    struct PlOff { size_t pre, post, tpre, tpost, rowA[2], rowB[2], colA[2], colB[2], pspk[2], sums; };
+    struct PlOff { size_t pre, post, tpre, tpost, colA[2], colB[2], sums; };
     std::vector<PlOff> o_pl(h.n_plast);
     for (uint32_t k = 0; k < h.n_plast; ++k) {
         const auto& C = s->conns[s->plasts[k].conn];
@@ -401,8 +476,7 @@ void finalize(bsnn_sim* s) {
         PlOff& o = o_pl[k];
         o.pre = A.take(np); o.tpre = A.take(np); o.post = A.take(nq); o.tpost = A.take(nq);
         for (int p = 0; p < 2; ++p) {
-            o.rowA[p] = A.take(np); o.rowB[p] = A.take(np);
-            o.colA[p] = A.take(nq); o.colB[p] = A.take(nq); o.pspk[p] = A.take(nq);
+            o.colA[p] = A.take(nq); o.colB[p] = A.take(nq);
         }
         o.sums = A.take(np);
     }
@@ -423,7 +497,38 @@ void finalize(bsnn_sim* s) {
     uint32_t n_ctas = static_cast<uint32_t>(s->sm_count);
     if (const char* e = std::getenv("BSNN_CTAS")) n_ctas = std::max(1, std::atoi(e));
     n_ctas = std::min<uint32_t>(n_ctas, std::max<uint32_t>(1u, (N + 3) / 4));
-    Plan P = build_plan(s, n_ctas);
+    // Shared memory: the largest opt-in dynamic allocation minus the kernel's static shared data.
+    int optin = 0;
+    cuda_check(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device), "smem attr");
+    cudaFuncAttributes fa{};
+    cuda_check(cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(&bsnn_step_kernel)), "func attr");
+    uint32_t n_spike_mons = 0;
+    for (const auto& M : s->mons) n_spike_mons += M.kind == kMonSpikes ? 1u : 0u;
+    auto smem_of = [&](const Plan& pl, uint32_t resident_floats) {
+        return smem_sizes(resident_floats, pl.max_rows, pl.max_own, spk_words, n_spike_mons, h.n_groups, h.n_ts,
+                          h.n_conns, h.n_plast, h.n_mons, static_cast<uint32_t>(pl.red_list.size()))
+            .total;
+    };
+    const int64_t smem_limit = static_cast<int64_t>(optin) - static_cast<int64_t>(fa.sharedSizeBytes) - 128;
+    // Plastic weight rows stay resident in shared memory for a whole launch when every CTA's
+    // share fits; otherwise all rows stream from global memory (L2 / HBM).
+    bool use_resident = true;
+    if (const char* e = std::getenv("BSNN_RESIDENT")) use_resident = std::atoi(e) != 0;
+    Plan P;
+    bool resident_ok = false;
+    if (use_resident) {
+        int64_t cap = smem_limit - 8192;
+        for (int attempt = 0; attempt < 8 && cap > 16384; ++attempt) {
+            P = build_plan(s, n_ctas, static_cast<uint64_t>(cap), &resident_ok);
+            if (!resident_ok) break;
+            const int64_t need = static_cast<int64_t>(smem_of(P, static_cast<uint32_t>(P.resident_floats)));
+            if (need <= smem_limit) break;
+            cap -= need - smem_limit + 256;
+            resident_ok = false;
+        }
+    }
+    if (!resident_ok) P = build_plan(s, n_ctas, 0, nullptr);
+    h.resident_floats = resident_ok ? static_cast<uint32_t>(P.resident_floats) : 0u;
     h.n_ctas = n_ctas;
     h.n_slots = std::max(P.n_slots, 1u);
     h.max_rows = P.max_rows;
@@ -431,15 +536,19 @@ void finalize(bsnn_sim* s) {
     std::memcpy(h.red_begin, P.red_begin, sizeof(P.red_begin));
     std::memcpy(h.red_end, P.red_end, sizeof(P.red_end));
     require(P.max_own <= static_cast<uint32_t>(kMaxThreads), BSNN_ERR_INVALID_ARGUMENT,
-            "network too large for one persistent grid (more than 1024 neurons per CTA)");
-    const uint32_t k_items = (P.max_items + kMaxThreads - 1) / kMaxThreads;
+            "network too large for one persistent grid (more than 512 neurons per CTA)");
+    // Threads per CTA: the work items (32-aligned 4-column units of each segment) spread evenly
+    // over at most kMaxThreads threads.
+    const uint32_t max_threads = static_cast<uint32_t>(kMaxThreads);
+    const uint32_t k_items = (P.max_items + max_threads - 1) / max_threads;
     uint32_t block = round_up((P.max_items + k_items - 1) / k_items, 32);
     block = std::max(block, round_up(P.max_own, 32));
-    block = std::min<uint32_t>(std::max<uint32_t>(block, 64), kMaxThreads);
-    if (const char* e = std::getenv("BSNN_BLOCK")) block = std::min<uint32_t>(kMaxThreads, round_up(std::max(32, std::atoi(e)), 32));
+    block = std::min<uint32_t>(std::max<uint32_t>(block, 64), max_threads);
+    if (const char* e = std::getenv("BSNN_BLOCK")) block = std::min<uint32_t>(max_threads, round_up(std::max(32, std::atoi(e)), 32));
     block = std::max(block, round_up(P.max_own, 32));
     s->grid = n_ctas;
     s->block = block;
+    s->kernel = reinterpret_cast<const void*>(&bsnn_step_kernel);
 
     size_t o_part = A.take(sizeof(float) * 2 * static_cast<size_t>(h.n_slots) * h.N_pad);
     size_t o_red = A.take(sizeof(uint32_t) * P.red_list.size());
@@ -485,6 +594,7 @@ void finalize(bsnn_sim* s) {
     size_t o_err = A.take(sizeof(int32_t));
     size_t o_sd = A.take(sizeof(unsigned long long));
     size_t o_clk = A.take(sizeof(uint32_t));
+    size_t o_pns = A.take(sizeof(unsigned long long) * 8 * std::max<uint32_t>(s->sm_count, 1));
     size_t o_sim = A.take(sizeof(DSim));
 
     cuda_check(cudaMalloc(&s->arena, A.size), "cudaMalloc arena");
@@ -502,6 +612,9 @@ void finalize(bsnn_sim* s) {
     h.refrac = U(o_ref);
     h.spikes[0] = U(o_spk0);
     h.spikes[1] = U(o_spk1);
+    h.spk_bits[0] = U(o_sb0);
+    h.spk_bits[1] = U(o_sb1);
+    h.spk_words = spk_words;
     for (uint32_t t = 0; t < h.n_ts; ++t) {
         h.ts[t].r = F(o_ts[3 * t]);
         h.ts[t].d = F(o_ts[3 * t + 1]);
@@ -545,8 +658,7 @@ void finalize(bsnn_sim* s) {
         D.wmin = PL.p.weight_min; D.wmax = PL.p.weight_max;
         D.pre = F(o.pre); D.post = F(o.post); D.tpre = F(o.tpre); D.tpost = F(o.tpost);
         for (int p = 0; p < 2; ++p) {
-            D.rowA[p] = F(o.rowA[p]); D.rowB[p] = F(o.rowB[p]);
-            D.colA[p] = F(o.colA[p]); D.colB[p] = F(o.colB[p]); D.pspk[p] = U(o.pspk[p]);
+            D.colA[p] = F(o.colA[p]); D.colB[p] = F(o.colB[p]);
         }
         D.sums = F(o.sums);
         DConn& C = h.conns[PL.conn];
@@ -596,6 +708,7 @@ void finalize(bsnn_sim* s) {
 
     h.partials = F(o_part);
     h.red_list = U(o_red);
+    h.n_red = static_cast<uint32_t>(P.red_list.size());
     h.ctas = reinterpret_cast<const DCta*>(base + o_ctas);
     h.segs = reinterpret_cast<const DSeg*>(base + o_segs);
     h.blks = reinterpret_cast<const DBlk*>(base + o_blks);
@@ -629,19 +742,17 @@ void finalize(bsnn_sim* s) {
     h.error = reinterpret_cast<int32_t*>(base + o_err);
     h.steps_done = reinterpret_cast<unsigned long long*>(base + o_sd);
     h.clock = U(o_clk);
+    h.phase_ns = reinterpret_cast<unsigned long long*>(base + o_pns);
     s->d_sim = reinterpret_cast<DSim*>(base + o_sim);
     cuda_check(cudaMemcpy(s->d_sim, &h, sizeof(DSim), cudaMemcpyHostToDevice), "H2D sim");
 
     // Launch configuration.
-    uint32_t n_spike_mons = 0;
-    for (const auto& M : s->mons) n_spike_mons += M.kind == kMonSpikes ? 1u : 0u;
-    s->smem_bytes = (sizeof(float4) + sizeof(DRowMeta) + sizeof(uint32_t) + sizeof(float) * kMaxWarps) * h.max_rows +
-                    sizeof(float) * 2 * h.max_own + sizeof(uint32_t) * n_spike_mons * (h.max_own / 32 + 2);
-    cuda_check(cudaFuncSetAttribute(bsnn_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    s->smem_bytes = smem_of(P, h.resident_floats);
+    cuda_check(cudaFuncSetAttribute(s->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(s->smem_bytes)),
                "cudaFuncSetAttribute smem");
     int per_sm = 0;
-    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bsnn_step_kernel, static_cast<int>(s->block),
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, s->kernel, static_cast<int>(s->block),
                                                              s->smem_bytes),
                "occupancy");
     require(per_sm >= 1 && static_cast<long>(per_sm) * s->sm_count >= static_cast<long>(s->grid), BSNN_ERR_RUNTIME,
@@ -661,8 +772,9 @@ void launch_direct(bsnn_sim* s, uint32_t n_steps) {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    cuda_check(cudaLaunchKernelEx(&cfg, bsnn_step_kernel, static_cast<const DSim*>(s->d_sim), n_steps),
-               "bsnn_step_kernel launch");
+    const DSim* arg0 = s->d_sim;
+    void* args[2] = {&arg0, &n_steps};
+    cuda_check(cudaLaunchKernelExC(&cfg, s->kernel, args), "bsnn_step_kernel launch");
     ++s->launches;
 }
 
@@ -684,7 +796,9 @@ void launch_chunk(bsnn_sim* s, uint32_t n_steps) {
                 attr[0].val.cooperative = 1;
                 cfg.attrs = attr;
                 cfg.numAttrs = 1;
-                const cudaError_t le = cudaLaunchKernelEx(&cfg, bsnn_step_kernel, static_cast<const DSim*>(s->d_sim), n_steps);
+                const DSim* arg0 = s->d_sim;
+                void* args[2] = {&arg0, &n_steps};
+                const cudaError_t le = cudaLaunchKernelExC(&cfg, s->kernel, args);
                 const cudaError_t ce = cudaStreamEndCapture(s->stream, &graph);
                 ok = le == cudaSuccess && ce == cudaSuccess && graph != nullptr &&
                      cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
@@ -837,6 +951,8 @@ BSNN_API bsnn_status bsnn_get_info(const bsnn_sim* sim, bsnn_info* out) {
     i.device_bytes = sim->arena_bytes;
     i.weight_bytes = sim->weight_bytes;
     i.kernel_launches = sim->launches;
+    i.smem_bytes = sim->smem_bytes;
+    i.resident_bytes = 4ull * sim->h.resident_floats;
     *out = i;
     return BSNN_OK;
 }
@@ -1173,3 +1289,17 @@ BSNN_API bsnn_status bsnn_get_device_pointer(const bsnn_sim* sim, int32_t field,
 }
 
 }  // extern "C"
+
+#ifdef BSNN_PHASE_TIMING
+// Profiling builds only: SM clock cycles each CTA spent per phase (0 partial reduction, 1 neuron
+// update, 2 row table, 3 normalisation pass, 4 weight pass, 5 grid barrier), accumulated since
+// creation; out[cta * 8 + phase] for the first grid_ctas CTAs.
+extern "C" BSNN_API bsnn_status bsnn_debug_phase_ns(bsnn_sim* sim, unsigned long long* out) {
+    if (!sim || !out) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        check_device_error(sim);
+        cuda_check(cudaMemcpy(out, sim->h.phase_ns, 8 * sizeof(unsigned long long) * sim->grid, cudaMemcpyDeviceToHost),
+                   "D2H");
+    });
+}
+#endif

@@ -20,10 +20,10 @@ constexpr int kMaxConns = 16;
 constexpr int kMaxTraceSets = 16;
 constexpr int kMaxPlast = 16;
 constexpr int kMaxMonitors = 16;
-constexpr int kMaxGroupRoles = 8;  // trace sets / plasticities a group takes part in
+constexpr int kMaxGroupRoles = 4;  // trace sets / plasticities / monitors per group and role
 constexpr int kMaxSegsPerCta = 2 * kMaxGroups;
 constexpr int kMaxBlksPerCta = kMaxConns;
-constexpr int kMaxThreads = 1024;
+constexpr int kMaxThreads = 256;  // threads per CTA (up to 255 registers per thread, no spills)
 constexpr int kMaxWarps = kMaxThreads / 32;
 
 enum : int32_t { kTargetExc = 0, kTargetInh = 1 };
@@ -74,8 +74,9 @@ struct DConn {
 };
 
 // PlasticityView (cpp_src/plasticities/plasticity_view.h:8-38) plus per-step factor buffers.
-// Row factors (per presynaptic neuron) and column factors (per postsynaptic neuron) are formed
-// once per step by the neuron that owns them, so that every weight update is
+// Row factors (per presynaptic neuron, kept in the owning CTA's shared memory) and column factors
+// (per postsynaptic neuron, parity buffers here) are formed once per step by the neuron that owns
+// them, so that every weight update is
 //   LTP: w = clamp(fma(rowA, colA, w))   if the post neuron spiked
 //   LTD: w = clamp(fma(colB, rowB, w))   if the pre neuron spiked
 // which is the reference's delta expression with its factors grouped the way it computes them.
@@ -89,11 +90,8 @@ struct DPlast {
     float* post;   // [n_post]
     float* tpre;   // [n_pre]  triplet traces (triplet rule only)
     float* tpost;  // [n_post]
-    float* rowA[2];     // [n_pre] parity buffers
-    float* rowB[2];
     float* colA[2];     // [units*4] parity buffers (padded)
     float* colB[2];
-    uint32_t* pspk[2];  // [units*4] post spiked at that step (padded with 0)
     float* sums;        // [n_pre] normalisation targets (triplet)
 };
 
@@ -117,7 +115,9 @@ struct DSeg {  // all rows of this CTA that add into (target, post group)
 };
 struct DBlk {  // rows [row_begin, row_end) (presynaptic local index) of one connection
     uint32_t conn, row_begin, row_end;
-    uint32_t srow;  // index of row_begin in the CTA's row table
+    uint32_t srow;      // index of row_begin in the CTA's row table
+    uint32_t resident;  // rows held in shared memory for the whole launch
+    uint32_t sm_off;    // float offset of row_begin in the resident region
 };
 struct DCta {
     uint32_t n0, n1;  // owned neurons (phase A) == owned presynaptic rows (phase B)
@@ -133,6 +133,7 @@ struct DSim {
     uint32_t N, N_pad;
     uint32_t n_groups, n_conns, n_ts, n_plast, n_mons;
     uint32_t n_ctas, n_slots, max_rows, max_own;
+    uint32_t resident_floats;  // shared-memory floats reserved for resident weight rows (per CTA)
     DGroup groups[kMaxGroups];
     DTraceSet ts[kMaxTraceSets];
     DConn conns[kMaxConns];
@@ -144,9 +145,12 @@ struct DSim {
     float *bg_ge, *bg_gi, *bg_er, *bg_ed, *bg_ir, *bg_id;
     uint32_t* refrac;
     uint32_t* spikes[2];  // parity buffers; the last step's are the canonical spikes
+    uint32_t* spk_bits[2];  // parity buffers: network-wide spike bitmask of a step [spk_words]
+    uint32_t spk_words;     // ceil(N / 32) + 2 (one spare word for 64-bit funnel reads)
 
     float* partials;  // [2][n_slots][N_pad]
     uint32_t* red_list;  // slot lists per (target, group)
+    uint32_t n_red;      // entries of red_list
     uint32_t red_begin[2][kMaxGroups], red_end[2][kMaxGroups];
 
     const DCta* ctas;
@@ -170,7 +174,7 @@ struct DSim {
     int32_t* error;
     unsigned long long* steps_done;  // internal step counter (stimulus / noise cursor)
     uint32_t* clock;                 // clock_step of the next step
-    uint32_t* has_partials;          // unused by the kernel; reserved
+    unsigned long long* phase_ns;    // [8] per-phase time of CTA 0 (profiling builds only)
 };
 
 }  // namespace bsnn

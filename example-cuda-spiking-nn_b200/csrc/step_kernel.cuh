@@ -34,6 +34,8 @@ namespace bsnn {
 
 constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;  // 2 s
 constexpr unsigned kFull = 0xffffffffu;
+constexpr int kRowBatch = 4;     // rows whose weights one thread loads before using them (plastic rows)
+constexpr int kStreamBatch = 4;  // same for read-only rows
 
 __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
     unsigned long long v;
@@ -138,76 +140,211 @@ __device__ __forceinline__ bool grid_barrier(const DSim* S, int* s_ok) {
     return *s_ok != 0;
 }
 
-struct SmemLayout {
-    DRowMeta* meta;     // [max_rows]
-    float4* row;        // [max_rows] {x, rowA, rowB, scale}
-    uint32_t* rowflag;  // [max_rows] bit0: presynaptic neuron spiked at the step being applied
-    float* part;        // [kMaxWarps][max_rows] per-warp row sums for the normalisation
-    float* dot;         // [2][max_own]
-    uint32_t* bits;     // [n_spike_monitors][max_own/32 + 2]
+// Optional phase timing (profiling builds only, -DBSNN_PHASE_TIMING): thread 0 of every CTA adds
+// the SM clock cycles spent in each phase to S->phase_ns[cta * 8 + phase].
+#ifdef BSNN_PHASE_TIMING
+#define BSNN_TMARK(slot)                                                                   \
+    do {                                                                                   \
+        if (threadIdx.x == 0) {                                                            \
+            const unsigned long long now_ = static_cast<unsigned long long>(clock64());    \
+            S->phase_ns[blockIdx.x * 8u + (slot)] += now_ - t_mark_;                        \
+            t_mark_ = now_;                                                                \
+        }                                                                                  \
+    } while (0)
+#else
+#define BSNN_TMARK(slot) \
+    do {                 \
+    } while (0)
+#endif
+
+
+// Shared-memory copies of the launch-invariant descriptors, so every phase dereferences shared
+// memory instead of chaining dependent global loads through DSim.
+struct Desc {
+    const DGroup* groups;
+    const DTraceSet* ts;
+    const DConn* conns;
+    const DPlast* plast;
+    const DMon* mons;
+    const uint32_t* red_list;
+    uint32_t n_groups, n_mons, n_plast, N;
+    int32_t noise_mode;
+    uint32_t seed, stim_len, replay_steps;
+    uint32_t goff[kMaxGroups], gn[kMaxGroups];
+    uint32_t bitbase[kMaxMonitors];
+    uint32_t red_begin[2][kMaxGroups], red_end[2][kMaxGroups];
 };
 
-__device__ __forceinline__ int group_of(const uint32_t* s_goff, const uint32_t* s_gn, uint32_t n_groups, uint32_t j) {
-    for (uint32_t g = 0; g < n_groups; ++g)
-        if (j - s_goff[g] < s_gn[g]) return static_cast<int>(g);
+// Values produced and consumed by the same CTA stay in shared memory: x of the own neurons, the
+// plasticity row factors (double-buffered by step parity: the neuron phase of step t writes them
+// while the weight pass of step t still reads step t-1's) and the own neurons' spike bits.
+struct SmemLayout {
+    float* wres;        // resident weight rows, S->resident_floats floats (16-byte aligned)
+    float4* row;        // [max_rows] {x, rowA, rowB, scale}
+    DRowMeta* meta;     // [max_rows]
+    uint32_t* rowflag;  // [max_rows] presynaptic neuron spiked at the step being applied
+    float* rowtgt;      // [max_rows] triplet normalisation target of the row
+    uint32_t* sbits;    // [spk_words] spike bitmask of the step whose plasticity is being applied
+    uint32_t* gbits;    // [2][max_own/32 + 2] this CTA's spike bits, by step parity
+    float* xown;        // [n_ts][max_own] x = d - r of the own neurons (this step)
+    float2* rowfac;     // [2][n_plast][max_own] {rowA, rowB} of the own neurons, by step parity
+    float* dot;         // [2][max_own]
+    float* red;         // [warps][2][max_own] per-warp partial-sum reduction scratch
+    uint32_t* bits;     // [n_spike_monitors][max_own/32 + 2]
+    unsigned char* desc;  // descriptor copies (DGroup, DTraceSet, DConn, DPlast, DMon, slot lists)
+};
+
+__host__ __device__ __forceinline__ size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+// Byte layout of the dynamic shared memory; the host sizes the launch with the same function.
+struct SmemSizes {
+    size_t wres, row, meta, rowflag, rowtgt, sbits, gbits, xown, rowfac, dot, redscr, bits, groups, ts, conns, plast,
+        mons, red, total;
+};
+__host__ __device__ __forceinline__ SmemSizes smem_sizes(uint32_t resident_floats, uint32_t max_rows, uint32_t max_own,
+                                                         uint32_t spk_words, uint32_t n_spike_mons, uint32_t n_groups,
+                                                         uint32_t n_ts, uint32_t n_conns, uint32_t n_plast,
+                                                         uint32_t n_mons, uint32_t n_red) {
+    SmemSizes z;
+    z.wres = align16(sizeof(float) * static_cast<size_t>(resident_floats));
+    z.row = align16(sizeof(float4) * max_rows);
+    z.meta = align16(sizeof(DRowMeta) * max_rows);
+    z.rowflag = align16(sizeof(uint32_t) * max_rows);
+    z.rowtgt = align16(sizeof(float) * max_rows);
+    z.sbits = align16(sizeof(uint32_t) * spk_words);
+    z.gbits = align16(sizeof(uint32_t) * 2 * (max_own / 32 + 2));
+    z.xown = align16(sizeof(float) * n_ts * max_own);
+    z.rowfac = align16(sizeof(float2) * 2 * n_plast * max_own);
+    z.dot = align16(sizeof(float) * 2 * max_own);
+    z.redscr = align16(sizeof(float) * 2 * kMaxWarps * max_own);
+    z.bits = align16(sizeof(uint32_t) * n_spike_mons * (max_own / 32 + 2));
+    z.groups = align16(sizeof(DGroup) * n_groups);
+    z.ts = align16(sizeof(DTraceSet) * n_ts);
+    z.conns = align16(sizeof(DConn) * n_conns);
+    z.plast = align16(sizeof(DPlast) * n_plast);
+    z.mons = align16(sizeof(DMon) * n_mons);
+    z.red = align16(sizeof(uint32_t) * n_red);
+    z.total = z.wres + z.row + z.meta + z.rowflag + z.rowtgt + z.sbits + z.gbits + z.xown + z.rowfac + z.dot + z.redscr +
+              z.bits + z.groups + z.ts + z.conns + z.plast + z.mons + z.red;
+    return z;
+}
+
+__device__ __forceinline__ int group_of(const Desc& D, uint32_t j) {
+    for (uint32_t g = 0; g < D.n_groups; ++g)
+        if (j - D.goff[g] < D.gn[g]) return static_cast<int>(g);
     return -1;
 }
 
 // Phase A1 / finalize: dot[T][i] = sum over the slots listed for (T, group of neuron n0+i) of the
-// parity-`par` partial sums at that neuron's column.  Warp per (neuron, target), lanes stride the
-// slot list, xor-butterfly: a fixed summation order.
-__device__ __forceinline__ void reduce_partials(const DSim* S, const DCta& cta, uint32_t par, const SmemLayout& sm,
-                                                uint32_t max_own, const uint32_t* s_goff, const uint32_t* s_gn) {
+// parity-`par` partial sums at that neuron's column.  Lanes take consecutive neurons (coalesced
+// reads of a slot row), warps take every nwarps-th slot of the list; the per-warp sums are then
+// added in warp order.  A fixed summation order.
+__device__ __forceinline__ void reduce_partials(const DSim* S, const Desc& D, const DCta& cta, uint32_t par,
+                                             const SmemLayout& sm, uint32_t max_own) {
     const uint32_t n_own = cta.n1 - cta.n0;
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u, nwarps = blockDim.x >> 5;
     const float* part = S->partials + static_cast<size_t>(par) * S->n_slots * S->N_pad;
-    for (uint32_t pr = warp; pr < 2u * n_own; pr += nwarps) {
-        const uint32_t i = pr >> 1, T = pr & 1u, j = cta.n0 + i;
-        const int g = group_of(s_goff, s_gn, S->n_groups, j);
-        float s = 0.0f;
-        if (g >= 0) {
-            const uint32_t b = S->red_begin[T][g], e = S->red_end[T][g];
-            const uint32_t col = S->groups[g].pcol + (j - s_goff[g]);
-            for (uint32_t k = b + lane; k < e; k += 32u)
-                s += __ldcg(part + static_cast<size_t>(S->red_list[k]) * S->N_pad + col);
-        }
+    const uint32_t npad = S->N_pad;
+    for (uint32_t g = 0; g < D.n_groups; ++g) {
+        const uint32_t goff = D.goff[g], gend = goff + D.gn[g];
+        const uint32_t a = cta.n0 > goff ? cta.n0 : goff, b = cta.n1 < gend ? cta.n1 : gend;
+        if (a >= b) continue;
+        const uint32_t pcol = D.groups[g].pcol;
+        for (uint32_t T = 0; T < 2; ++T) {
+            const uint32_t lb = D.red_begin[T][g], le = D.red_end[T][g];
+            for (uint32_t j0 = a; j0 < b; j0 += 32u) {
+                const uint32_t j = j0 + lane;
+                float s = 0.0f;
+                if (j < b) {
+                    const float* col = part + pcol + (j - goff);
+                    // 8 independent loads in flight per batch; the adds keep list order
+                    for (uint32_t k0 = lb + warp; k0 < le; k0 += 8u * nwarps) {
+                        float v[8];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
-        if (lane == 0) sm.dot[T * max_own + i] = s;
+                        for (int q = 0; q < 8; ++q) {
+                            const uint32_t k = k0 + q * nwarps;
+                            v[q] = k < le ? __ldcg(col + static_cast<size_t>(D.red_list[k]) * npad) : 0.0f;
+                        }
+#pragma unroll
+                        for (int q = 0; q < 8; ++q)
+                            if (k0 + q * nwarps < le) s += v[q];
+                    }
+                    sm.red[(warp * 2u + T) * max_own + (j - cta.n0)] = s;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (uint32_t e = threadIdx.x; e < 2u * n_own; e += blockDim.x) {
+        const uint32_t T = e / n_own, i = e % n_own;
+        float s = 0.0f;
+        for (uint32_t w = 0; w < nwarps; ++w) s += sm.red[(w * 2u + T) * max_own + i];
+        sm.dot[T * max_own + i] = s;
     }
 }
 
-// Phase A2: one thread per owned neuron.
-__device__ __forceinline__ void neuron_phase(const DSim* S, const DCta& cta, unsigned long long t, uint32_t clock,
-                                             uint32_t par, bool has_dot, const SmemLayout& sm, uint32_t max_own,
-                                             const uint32_t* s_goff, const uint32_t* s_gn, const uint32_t* s_bitbase) {
+// Phase A2: one thread per owned neuron.  All of the neuron's inputs are loaded first, then the
+// reference's per-step arithmetic runs, then everything is stored.
+__device__ __forceinline__ void neuron_phase(const DSim* S, const Desc& D, const DCta& cta, unsigned long long t,
+                                          uint32_t clock, uint32_t par, bool has_dot, const SmemLayout& sm,
+                                          uint32_t max_own) {
     const uint32_t i = threadIdx.x;
     if (i >= cta.n1 - cta.n0) return;
     const uint32_t j = cta.n0 + i;
-    const int g = group_of(s_goff, s_gn, S->n_groups, j);
+    const int g = group_of(D, j);
     if (g < 0) return;
-    const DGroup& G = S->groups[g];
+    const DGroup& G = D.groups[g];
     const uint32_t loc = j - G.off;
 
-    // Conductances seen by this step's evolve: background of the previous step plus the
-    // previous step's propagation (cublasSgemv y = A x + y, kernel_connection_propagate.cu:79-94).
+    // ---- loads ----
     float ge_used = S->ge[j], gi_used = S->gi[j];
+    const float er0 = S->bg_er[j], ir0 = S->bg_ir[j], ed0 = S->bg_ed[j], id0 = S->bg_id[j];
+    float istim = S->istim[j];
+    float v = S->v[j];
+    uint32_t refrac = S->refrac[j];
+    constexpr int kR = kMaxGroupRoles;  // role slots, all loaded up front into registers
+    float ts_r[kR], ts_d[kR], pre0[kR], tpre0[kR], post0[kR], tpost0[kR];
+#pragma unroll
+    for (int k = 0; k < kR; ++k) {
+        if (k < static_cast<int>(G.n_ts)) {
+            const DTraceSet& TS = D.ts[G.ts[k]];
+            ts_r[k] = TS.r[loc];
+            ts_d[k] = TS.d[loc];
+        }
+        if (k < static_cast<int>(G.n_plast_pre)) {
+            const DPlast& P = D.plast[G.plast_pre[k]];
+            pre0[k] = P.pre[loc];
+            tpre0[k] = P.kind == kKindTriplet ? P.tpre[loc] : 0.0f;
+        }
+        if (k < static_cast<int>(G.n_plast_post)) {
+            const DPlast& P = D.plast[G.plast_post[k]];
+            post0[k] = P.post[loc];
+            tpost0[k] = P.kind == kKindTriplet ? P.tpost[loc] : 0.0f;
+        }
+    }
+    uint32_t ev_lo = 0, ev_hi = 0;
+    if (t < D.stim_len) {
+        ev_lo = S->stim_off[t];
+        ev_hi = S->stim_off[t + 1];
+    }
     if (has_dot) {
+        // background of the previous step plus the previous step's propagation
+        // (cublasSgemv y = A x + y, kernel_connection_propagate.cu:79-94)
         ge_used = ge_used + sm.dot[i];
         gi_used = gi_used + sm.dot[max_own + i];
     }
 
-    // kernel_update_background_conductances (kernel_neuron_group_evolve.cu:11-83)
-    float er = flush_tiny(S->bg_er[j] * G.bg_er_decay);
-    float ir = flush_tiny(S->bg_ir[j] * G.bg_ir_decay);
-    float ed = flush_tiny(S->bg_ed[j] * G.bg_ed_decay);
-    float id = flush_tiny(S->bg_id[j] * G.bg_id_decay);
+    // ---- kernel_update_background_conductances (kernel_neuron_group_evolve.cu:11-83) ----
+    float er = flush_tiny(er0 * G.bg_er_decay);
+    float ir = flush_tiny(ir0 * G.bg_ir_decay);
+    float ed = flush_tiny(ed0 * G.bg_ed_decay);
+    float id = flush_tiny(id0 * G.bg_id_decay);
     uint32_t ne = 0, ni = 0;
-    if (S->noise_mode == kNoisePhilox) {
-        if (G.has_bg_e) ne = poisson_knuth(G.exp_neg_mean_e, S->seed, j, t, 0u);
-        if (G.has_bg_i) ni = poisson_knuth(G.exp_neg_mean_i, S->seed, j, t, 1u);
-    } else if (S->noise_mode == kNoiseReplay && t < S->replay_steps) {
-        const size_t base = (static_cast<size_t>(t) * S->N + j) * 2u;
+    if (D.noise_mode == kNoisePhilox) {
+        if (G.has_bg_e) ne = poisson_knuth(G.exp_neg_mean_e, D.seed, j, t, 0u);
+        if (G.has_bg_i) ni = poisson_knuth(G.exp_neg_mean_i, D.seed, j, t, 1u);
+    } else if (D.noise_mode == kNoiseReplay && t < D.replay_steps) {
+        const size_t base = (static_cast<size_t>(t) * D.N + j) * 2u;
         ne = S->replay[base];
         ni = S->replay[base + 1];
     }
@@ -223,18 +360,9 @@ __device__ __forceinline__ void neuron_phase(const DSim* S, const DCta& cta, uns
         id += inc;
     }
     const float bg_gi = (id - ir) * G.bg_scale_i;
-    S->bg_er[j] = er;
-    S->bg_ed[j] = ed;
-    S->bg_ir[j] = ir;
-    S->bg_id[j] = id;
-    S->bg_ge[j] = bg_ge;
-    S->bg_gi[j] = bg_gi;
 
-    // kernel_neuron_group_evolve (kernel_neuron_group_evolve.cu:85-130)
-    float istim = S->istim[j];
+    // ---- kernel_neuron_group_evolve (kernel_neuron_group_evolve.cu:85-130) ----
     uint32_t spike = 0;
-    float v = S->v[j];
-    uint32_t refrac = S->refrac[j];
     if (refrac > 0) {
         --refrac;
         v = G.v_reset;
@@ -255,24 +383,32 @@ __device__ __forceinline__ void neuron_phase(const DSim* S, const DCta& cta, uns
             v = v_next;
         }
     }
+
+    // ---- stores ----
+    S->bg_er[j] = er;
+    S->bg_ed[j] = ed;
+    S->bg_ir[j] = ir;
+    S->bg_id[j] = id;
+    S->bg_ge[j] = bg_ge;
+    S->bg_gi[j] = bg_gi;
     S->v[j] = v;
     S->refrac[j] = refrac;
     S->ge[j] = bg_ge;  // reset for the next propagation (kernel_neuron_group_evolve.cu:126-129)
     S->gi[j] = bg_gi;
     S->spikes[par][j] = spike;
+    if (spike) atomicOr(&sm.gbits[par * (max_own / 32u + 2u) + (j >> 5) - (cta.n0 >> 5)], 1u << (j & 31u));
 
     // Stimulus::apply / kernel_stimulus_apply (stimulus.cpp:46-60, kernel_stimulus_apply.cu:7-21):
     // events of this step land after the evolve read i_stimulus, so they act from the next step.
-    if (t < S->stim_len) {
-        uint32_t lo = S->stim_off[t], hi = S->stim_off[t + 1];
+    if (ev_lo < ev_hi) {
+        uint32_t lo = ev_lo, hi = ev_hi;
         while (lo < hi) {  // lower_bound of j in the step's events (sorted by neuron)
             const uint32_t mid = (lo + hi) >> 1;
             if (S->ev_neuron[mid] < j) lo = mid + 1;
             else hi = mid;
         }
-        const uint32_t end = S->stim_off[t + 1];
         bool any = false;
-        for (uint32_t k = lo; k < end && S->ev_neuron[k] == j; ++k) {
+        for (uint32_t k = lo; k < ev_hi && S->ev_neuron[k] == j; ++k) {
             istim = istim + S->ev_delta[k];
             any = true;
         }
@@ -280,10 +416,14 @@ __device__ __forceinline__ void neuron_phase(const DSim* S, const DCta& cta, uns
     }
 
     // Connection traces (kernel_connection_propagate.cu:8-46): decay d, decay r, +norm on spike.
-    for (uint32_t k = 0; k < G.n_ts; ++k) {
-        const DTraceSet& TS = S->ts[G.ts[k]];
-        float d = flush_tiny(TS.d[loc] * TS.d_decay);
-        float r = flush_tiny(TS.r[loc] * TS.r_decay);
+#pragma unroll
+    for (int k = 0; k < kR; ++k) {
+        if (k >= static_cast<int>(G.n_ts)) break;
+        const DTraceSet& TS = D.ts[G.ts[k]];
+        const float r_in = ts_r[k];
+        const float d_in = ts_d[k];
+        float d = flush_tiny(d_in * TS.d_decay);
+        float r = flush_tiny(r_in * TS.r_decay);
         if (spike == 1) {
             r += TS.norm;
             d += TS.norm;
@@ -291,16 +431,21 @@ __device__ __forceinline__ void neuron_phase(const DSim* S, const DCta& cta, uns
         TS.r[loc] = r;
         TS.d[loc] = d;
         TS.x[loc] = d - r;
+        sm.xown[static_cast<uint32_t>(G.ts[k]) * max_own + i] = d - r;
     }
 
     // Plasticity traces as presynaptic neuron: decay (the value the weight update uses), row
     // factors for that update, then the spike increment (kernel_*_plasticity_update.cu).
-    for (uint32_t k = 0; k < G.n_plast_pre; ++k) {
-        const DPlast& P = S->plast[G.plast_pre[k]];
-        const float pre = flush_tiny(P.pre[loc] * P.pre_decay);
+#pragma unroll
+    for (int k = 0; k < kR; ++k) {
+        if (k >= static_cast<int>(G.n_plast_pre)) break;
+        const DPlast& P = D.plast[G.plast_pre[k]];
+        const float pre_in = pre0[k];
+        const float pre = flush_tiny(pre_in * P.pre_decay);
         float rowA, rowB;
         if (P.kind == kKindTriplet) {
-            const float tpre = flush_tiny(P.tpre[loc] * P.tpre_decay);
+            const float tpre_in = tpre0[k];
+            const float tpre = flush_tiny(tpre_in * P.tpre_decay);
             rowA = pre;
             rowB = P.ltd_A + (P.ltd_B * tpre);
             P.tpre[loc] = spike == 1 ? tpre + 1.0f : tpre;
@@ -308,17 +453,20 @@ __device__ __forceinline__ void neuron_phase(const DSim* S, const DCta& cta, uns
             rowA = pre;
             rowB = -1.0f * P.ltd_A;
         }
-        P.rowA[par][loc] = rowA;
-        P.rowB[par][loc] = rowB;
+        sm.rowfac[(par * D.n_plast + static_cast<uint32_t>(G.plast_pre[k])) * max_own + i] = make_float2(rowA, rowB);
         P.pre[loc] = spike == 1 ? pre + 1.0f : pre;
     }
     // ... and as postsynaptic neuron: column factors.
-    for (uint32_t k = 0; k < G.n_plast_post; ++k) {
-        const DPlast& P = S->plast[G.plast_post[k]];
-        const float post = flush_tiny(P.post[loc] * P.post_decay);
+#pragma unroll
+    for (int k = 0; k < kR; ++k) {
+        if (k >= static_cast<int>(G.n_plast_post)) break;
+        const DPlast& P = D.plast[G.plast_post[k]];
+        const float post_in = post0[k];
+        const float post = flush_tiny(post_in * P.post_decay);
         float colA, colB;
         if (P.kind == kKindTriplet) {
-            const float tpost = flush_tiny(P.tpost[loc] * P.tpost_decay);
+            const float tpost_in = tpost0[k];
+            const float tpost = flush_tiny(tpost_in * P.tpost_decay);
             colA = P.ltp_A + (P.ltp_B * tpost);
             colB = -1.0f * post;
             P.tpost[loc] = spike == 1 ? tpost + 1.0f : tpost;
@@ -331,18 +479,17 @@ __device__ __forceinline__ void neuron_phase(const DSim* S, const DCta& cta, uns
         }
         P.colA[par][loc] = colA;
         P.colB[par][loc] = colB;
-        P.pspk[par][loc] = spike;
         P.post[loc] = spike == 1 ? post + 1.0f : post;
     }
 
     // Monitors (kernel_historicize_spikes.cu:7-21, kernel_historicize_membrane_potentials.cu:7-21).
     for (uint32_t k = 0; k < G.n_mon; ++k) {
         const int m = G.mon[k];
-        const DMon& M = S->mons[m];
+        const DMon& M = D.mons[m];
         if (M.kind == kMonSpikes) {
             if (spike) {
                 const uint32_t w0 = (cta.n0 > G.off ? cta.n0 - G.off : 0u) >> 5;
-                atomicOr(&sm.bits[s_bitbase[m] + ((loc >> 5) - w0)], 1u << (loc & 31u));
+                atomicOr(&sm.bits[D.bitbase[m] + ((loc >> 5) - w0)], 1u << (loc & 31u));
             }
         } else {
             const int32_t col = M.sel_idx[loc];
@@ -353,12 +500,31 @@ __device__ __forceinline__ void neuron_phase(const DSim* S, const DCta& cta, uns
 
 // Writes this CTA's spike bits of each spike monitor into the ring slot of `clock`.  Each CTA
 // clears and sets only the bits of its own neurons, so the word updates of different CTAs commute.
-__device__ __forceinline__ void flush_spike_bits(const DSim* S, const DCta& cta, uint32_t clock,
-                                                 const SmemLayout& sm, const uint32_t* s_bitbase) {
-    for (uint32_t m = 0; m < S->n_mons; ++m) {
-        const DMon& M = S->mons[m];
+__device__ __forceinline__ void merge_bits(uint32_t* word, uint32_t mask, uint32_t bits) {
+    const uint32_t clear = mask & ~bits;
+    if (clear) atomicAnd(word, ~clear);
+    if (bits) atomicOr(word, bits);
+}
+
+__device__ __forceinline__ uint32_t range_mask(uint32_t w, uint32_t w0, uint32_t w1, uint32_t a, uint32_t b_end) {
+    const uint32_t lo = w == w0 ? (a & 31u) : 0u;
+    const uint32_t hi = w == w1 ? ((b_end - 1) & 31u) : 31u;
+    return (hi == 31u ? 0xffffffffu : ((1u << (hi + 1u)) - 1u)) & ~((1u << lo) - 1u);
+}
+
+__device__ __forceinline__ void flush_spike_bits(const DSim* S, const Desc& D, const DCta& cta, uint32_t clock,
+                                              uint32_t par, const SmemLayout& sm) {
+    // the network-wide spike bitmask of this step (read by every CTA's next weight pass)
+    if (cta.n1 > cta.n0) {
+        const uint32_t w0 = cta.n0 >> 5, w1 = (cta.n1 - 1) >> 5;
+        for (uint32_t w = w0 + threadIdx.x; w <= w1; w += blockDim.x)
+            merge_bits(S->spk_bits[par] + w, range_mask(w, w0, w1, cta.n0, cta.n1),
+                       sm.gbits[par * (S->max_own / 32u + 2u) + w - w0]);
+    }
+    for (uint32_t m = 0; m < D.n_mons; ++m) {
+        const DMon& M = D.mons[m];
         if (M.kind != kMonSpikes) continue;
-        const DGroup& G = S->groups[M.group];
+        const DGroup& G = D.groups[M.group];
         const uint32_t a = cta.n0 > G.off ? cta.n0 - G.off : 0u;
         const uint32_t b_end = cta.n1 - G.off < G.n ? cta.n1 - G.off : G.n;
         if (cta.n1 <= G.off || a >= b_end) continue;
@@ -367,7 +533,7 @@ __device__ __forceinline__ void flush_spike_bits(const DSim* S, const DCta& cta,
             const uint32_t lo = w == w0 ? (a & 31u) : 0u;
             const uint32_t hi = w == w1 ? ((b_end - 1) & 31u) : 31u;
             const uint32_t mask = (hi == 31u ? 0xffffffffu : ((1u << (hi + 1u)) - 1u)) & ~((1u << lo) - 1u);
-            const uint32_t bits = sm.bits[s_bitbase[m] + (w - w0)] & mask;
+            const uint32_t bits = sm.bits[D.bitbase[m] + (w - w0)] & mask;
             uint32_t* word = M.bits + static_cast<size_t>(clock % M.interval) * M.words + w;
             const uint32_t clear = mask & ~bits;
             if (clear) atomicAnd(word, ~clear);
@@ -376,20 +542,25 @@ __device__ __forceinline__ void flush_spike_bits(const DSim* S, const DCta& cta,
     }
 }
 
-// Per-row data for phase B: x of this step, and the pending plasticity's row factors.
-__device__ __forceinline__ void build_rows(const DSim* S, const DCta& cta, bool pending, uint32_t ppar,
-                                           const SmemLayout& sm, bool with_x) {
+// Per-row data for phase B (x of this step, the pending plasticity's row factors, the presynaptic
+// spike) and the staged network-wide spike bitmask of the step whose plasticity is pending.
+__device__ __forceinline__ void build_rows(const DSim* S, const Desc& D, const DCta& cta, bool pending, uint32_t ppar,
+                                        const SmemLayout& sm, bool with_x) {
+    if (pending)
+        for (uint32_t w = threadIdx.x; w < S->spk_words; w += blockDim.x) sm.sbits[w] = __ldcg(S->spk_bits[ppar] + w);
+    const uint32_t max_own = S->max_own, n_gbits = max_own / 32u + 2u;
     for (uint32_t r = threadIdx.x; r < cta.n_rows; r += blockDim.x) {
         const DRowMeta meta = sm.meta[r];
-        const DConn& C = S->conns[meta.conn];
+        const DConn& C = D.conns[meta.conn];
+        const uint32_t i = meta.j - cta.n0;  // rows belong to this CTA's own neurons
         float4 row = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
         uint32_t flag = 0;
-        if (with_x) row.x = __ldcg(S->ts[C.ts].x + meta.pl);
+        if (with_x) row.x = sm.xown[static_cast<uint32_t>(C.ts) * max_own + i];
         if (pending && C.plast >= 0) {
-            const DPlast& P = S->plast[C.plast];
-            row.y = __ldcg(P.rowA[ppar] + meta.pl);
-            row.z = __ldcg(P.rowB[ppar] + meta.pl);
-            flag = __ldcg(S->spikes[ppar] + meta.j) == 1u ? 1u : 0u;
+            const float2 f = sm.rowfac[(ppar * D.n_plast + static_cast<uint32_t>(C.plast)) * max_own + i];
+            row.y = f.x;
+            row.z = f.y;
+            flag = (sm.gbits[ppar * n_gbits + (meta.j >> 5) - (cta.n0 >> 5)] >> (meta.j & 31u)) & 1u;
         }
         sm.row[r] = row;
         sm.rowflag[r] = flag;
@@ -397,7 +568,6 @@ __device__ __forceinline__ void build_rows(const DSim* S, const DCta& cta, bool 
 }
 
 __device__ __forceinline__ float4 ld_col4(const float* p) { return __ldcg(reinterpret_cast<const float4*>(p)); }
-__device__ __forceinline__ uint4 ld_col4u(const uint32_t* p) { return __ldcg(reinterpret_cast<const uint4*>(p)); }
 
 // The reference's per-element plasticity sequence: LTP clamp (if post spiked), then LTD clamp
 // (if pre spiked), skipping the diagonal of group-local indices.
@@ -410,6 +580,32 @@ __device__ __forceinline__ float plastic_update(float w, uint32_t q, uint32_t pl
     return w;
 }
 
+// Post spikes of the 4 columns of unit u (postsynaptic group at global offset `post_off`) from the
+// staged bitmask, as a 4-bit mask.
+__device__ __forceinline__ uint32_t post_mask(const uint32_t* sbits, uint32_t post_off, uint32_t u, uint32_t n_post) {
+    const uint32_t idx = post_off + 4u * u;
+    const uint32_t w = idx >> 5, sh = idx & 31u;
+    const unsigned long long pair =
+        (static_cast<unsigned long long>(sbits[w + 1]) << 32) | static_cast<unsigned long long>(sbits[w]);
+    const uint32_t valid = n_post - 4u * u >= 4u ? 0xFu : ((1u << (n_post - 4u * u)) - 1u);
+    return static_cast<uint32_t>(pair >> sh) & valid;
+}
+
+// The pending plasticity update of the 4 weights of unit u of row pl when some spike touches them.
+// Spikes are rare, so this is out of line and loads its own factors.
+__device__ __noinline__ float4 update4_slow(float4 w4, uint32_t u, uint32_t pl, uint32_t pmask, uint32_t pre_spk,
+                                            float rowA, float rowB, const DPlast* P, uint32_t n_post, uint32_t ppar) {
+    const float4 cA = ld_col4(P->colA[ppar] + 4u * u);
+    const float4 cB = ld_col4(P->colB[ppar] + 4u * u);
+    const float wmin = P->wmin, wmax = P->wmax;
+    const uint32_t q = 4u * u;
+    w4.x = plastic_update(w4.x, q + 0u, pl, n_post, pmask & 1u, pre_spk, rowA, cA.x, cB.x, rowB, wmin, wmax);
+    w4.y = plastic_update(w4.y, q + 1u, pl, n_post, pmask & 2u, pre_spk, rowA, cA.y, cB.y, rowB, wmin, wmax);
+    w4.z = plastic_update(w4.z, q + 2u, pl, n_post, pmask & 4u, pre_spk, rowA, cA.z, cB.z, rowB, wmin, wmax);
+    w4.w = plastic_update(w4.w, q + 3u, pl, n_post, pmask & 8u, pre_spk, rowA, cA.w, cB.w, rowB, wmin, wmax);
+    return w4;
+}
+
 __device__ __forceinline__ int seg_of_item(const DSeg* s_seg, uint32_t n_seg, uint32_t it) {
     for (uint32_t s = 0; s < n_seg; ++s) {
         const uint32_t b = s_seg[s].item_begin;
@@ -418,80 +614,140 @@ __device__ __forceinline__ int seg_of_item(const DSeg* s_seg, uint32_t n_seg, ui
     return -1;
 }
 
-// Pass 1 of the triplet normalisation: each warp sums, per normalised row, the updated weights
-// of its 32 units into its own slot sm.part[warp][row] (no atomics; fixed order).
-__device__ __forceinline__ void norm_pass1(const DSim* S, const DCta& cta, uint32_t ppar, const SmemLayout& sm,
-                                           const DSeg* s_seg, const DBlk* s_blk, uint32_t n_seg, uint32_t max_rows) {
-    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-    for (uint32_t r = threadIdx.x; r < cta.n_rows; r += blockDim.x)
-        for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) sm.part[w * max_rows + r] = 0.0f;
-    __syncthreads();
-    for (uint32_t it0 = 0; it0 < cta.n_items; it0 += blockDim.x) {
-        const uint32_t it = it0 + threadIdx.x;
-        const int s = seg_of_item(s_seg, n_seg, it - lane);  // warp-uniform
-        if (s < 0 || !s_seg[s].normalized) continue;
-        const DSeg& SG = s_seg[s];
-        const uint32_t u = it - SG.item_begin;
-        const bool valid = u < SG.units;
-        for (uint32_t bk = SG.blk_begin; bk < SG.blk_end; ++bk) {
-            const DBlk& B = s_blk[bk];
-            const DConn& C = S->conns[B.conn];
-            if (C.plast < 0 || S->plast[C.plast].kind != kKindTriplet) continue;
-            const DPlast& P = S->plast[C.plast];
-            float4 cA = make_float4(0.f, 0.f, 0.f, 0.f), cB = cA;
-            uint4 ps = make_uint4(0u, 0u, 0u, 0u);
-            if (valid) {
-                cA = ld_col4(P.colA[ppar] + 4u * u);
-                cB = ld_col4(P.colB[ppar] + 4u * u);
-                ps = ld_col4u(P.pspk[ppar] + 4u * u);
-            }
-            const float* wrow = C.w + 4u * u;
-            for (uint32_t pl = B.row_begin, r = B.srow; pl < B.row_end; ++pl, ++r) {
-                float sum = 0.0f;
-                if (valid) {
-                    const float4 rw = sm.row[r];
-                    const uint32_t pre_spk = sm.rowflag[r];
-                    float4 w4 = *reinterpret_cast<const float4*>(wrow + static_cast<size_t>(pl) * C.ld);
-                    const uint32_t q = 4u * u;
-                    w4.x = plastic_update(w4.x, q + 0u, pl, C.n_post, ps.x, pre_spk, rw.y, cA.x, cB.x, rw.z, P.wmin, P.wmax);
-                    w4.y = plastic_update(w4.y, q + 1u, pl, C.n_post, ps.y, pre_spk, rw.y, cA.y, cB.y, rw.z, P.wmin, P.wmax);
-                    w4.z = plastic_update(w4.z, q + 2u, pl, C.n_post, ps.z, pre_spk, rw.y, cA.z, cB.z, rw.z, P.wmin, P.wmax);
-                    w4.w = plastic_update(w4.w, q + 3u, pl, C.n_post, ps.w, pre_spk, rw.y, cA.w, cB.w, rw.z, P.wmin, P.wmax);
-                    sum = (w4.x + w4.y) + (w4.z + w4.w);
-                }
+// 16-byte weight accesses: shared memory (resident rows, 32-bit shared addresses) or global.
+__device__ __forceinline__ float4 lds4(uint32_t a) {
+    float4 v;
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ void sts4(uint32_t a, float4 v) {
+    asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(a), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w));
+}
+__device__ __forceinline__ uint32_t saddr(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+// Pass 1 of the triplet normalisation, one warp per row: each lane sums its units of the updated
+// row (units lane, lane+32, ...), then an xor-butterfly; lane 0 forms target / sum.
+__device__ __forceinline__ void norm_rows(const DSim* S, const Desc& D, uint32_t ppar, const SmemLayout& sm,
+                                       const DBlk* s_blk, uint32_t nblk) {
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u, nwarps = blockDim.x >> 5;
+    uint32_t k = 0;  // running index over the CTA's normalised rows
+    for (uint32_t bk = 0; bk < nblk; ++bk) {
+        const DBlk B = s_blk[bk];
+        const DConn& C = D.conns[B.conn];
+        if (C.plast < 0 || D.plast[C.plast].kind != kKindTriplet) continue;
+        const DPlast* P = &D.plast[C.plast];
+        const uint32_t nrows = B.row_end - B.row_begin, units = C.units, ld = C.ld, n_post = C.n_post;
+        const uint32_t post_off = C.post_off;
+        // first row of this block handled by this warp
+        const uint32_t first = (warp + nwarps - (k % nwarps)) % nwarps;
+        for (uint32_t i = first; i < nrows; i += nwarps) {
+            const uint32_t pl = B.row_begin + i, r = B.srow + i;
+            const float4 rw = sm.row[r];
+            const uint32_t pre_spk = sm.rowflag[r];
+            float sum = 0.0f;
+            if (B.resident) {
+                const uint32_t base = saddr(sm.wres + B.sm_off) + 4u * ld * i;
+                for (uint32_t u0 = 0; u0 < units; u0 += 128u) {
+                    float4 wb[4];
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
-                if (lane == 0) sm.part[warp * max_rows + r] += sum;
+                    for (int b = 0; b < 4; ++b) {
+                        const uint32_t u = u0 + lane + 32u * b;
+                        wb[b] = u < units ? lds4(base + 16u * u) : make_float4(0.f, 0.f, 0.f, 0.f);
+                    }
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        const uint32_t u = u0 + lane + 32u * b;
+                        if (u >= units) continue;
+                        float4 w4 = wb[b];
+                        const uint32_t pm = post_mask(sm.sbits, post_off, u, n_post);
+                        if (pre_spk | pm) w4 = update4_slow(w4, u, pl, pm, pre_spk, rw.y, rw.z, P, n_post, ppar);
+                        sum += (w4.x + w4.y) + (w4.z + w4.w);
+                    }
+                }
+            } else {
+                const float* wrow = C.w + static_cast<size_t>(pl) * ld;
+                for (uint32_t u0 = 0; u0 < units; u0 += 128u) {
+                    float4 wb[4];
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        const uint32_t u = u0 + lane + 32u * b;
+                        wb[b] = u < units ? ld_col4(wrow + 4u * u) : make_float4(0.f, 0.f, 0.f, 0.f);
+                    }
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        const uint32_t u = u0 + lane + 32u * b;
+                        if (u >= units) continue;
+                        float4 w4 = wb[b];
+                        const uint32_t pm = post_mask(sm.sbits, post_off, u, n_post);
+                        if (pre_spk | pm) w4 = update4_slow(w4, u, pl, pm, pre_spk, rw.y, rw.z, P, n_post, ppar);
+                        sum += (w4.x + w4.y) + (w4.z + w4.w);
+                    }
+                }
             }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
+            if (lane == 0) sm.row[r].w = sum <= 0.0f ? 1.0f : __fdiv_rn(sm.rowtgt[r], sum);
         }
+        k += nrows;
     }
-    __syncthreads();
-    // Row scale = target / current sum; rows with sum <= 0 are left unscaled (scale 1 is exact).
-    for (uint32_t s = 0; s < n_seg; ++s) {
-        if (!s_seg[s].normalized) continue;
-        for (uint32_t bk = s_seg[s].blk_begin; bk < s_seg[s].blk_end; ++bk) {
-            const DBlk& B = s_blk[bk];
-            const DConn& C = S->conns[B.conn];
-            if (C.plast < 0 || S->plast[C.plast].kind != kKindTriplet) continue;
-            const DPlast& P = S->plast[C.plast];
-            for (uint32_t pl = B.row_begin + threadIdx.x; pl < B.row_end; pl += blockDim.x) {
-                const uint32_t r = B.srow + (pl - B.row_begin);
-                float sum = 0.0f;
-                for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) sum += sm.part[w * max_rows + r];
-                const float scale = sum <= 0.0f ? 1.0f : __fdiv_rn(P.sums[pl], sum);
-                sm.row[r].w = scale;
-            }
-        }
-    }
-    __syncthreads();
 }
 
-// Pass 2: update + normalise + store the pending plasticity, and (if `accumulate`) the GEMV
-// partial sums of this step, written to the parity-`par` partial slots.
-__device__ __forceinline__ void weight_pass(const DSim* S, const DCta& cta, bool pending, uint32_t ppar,
-                                            bool accumulate, uint32_t par, const SmemLayout& sm, const DSeg* s_seg,
-                                            const DBlk* s_blk, uint32_t n_seg) {
+// Pass 2 over the rows of one block for unit u: apply + normalise + store the pending plasticity
+// (plastic rows) and accumulate this step's GEMV partial sums.
+template <bool RESIDENT, bool PLASTIC>
+__device__ __forceinline__ float4 block_rows(const DBlk& B, const DConn& C, const DPlast* P, uint32_t u,
+                                             uint32_t pmask, uint32_t ppar, const SmemLayout& sm, bool accumulate,
+                                             float4 acc) {
+    const uint32_t nrows = B.row_end - B.row_begin, ld = C.ld, n_post = C.n_post;
+    const uint32_t sbase = RESIDENT ? saddr(sm.wres + B.sm_off) + 16u * u : 0u;
+    float* gbase = RESIDENT ? nullptr : C.w + static_cast<size_t>(B.row_begin) * ld + 4u * u;
+    const float4* rowp = sm.row + B.srow;
+    const uint32_t* flagp = sm.rowflag + B.srow;
+    constexpr int kB = RESIDENT ? 4 : 8;
+    for (uint32_t i0 = 0; i0 < nrows; i0 += kB) {
+        float4 wb[kB];
+#pragma unroll
+        for (int b = 0; b < kB; ++b) {
+            if (i0 + b < nrows) {
+                if constexpr (RESIDENT) wb[b] = lds4(sbase + 4u * ld * (i0 + b));
+                else wb[b] = ld_col4(gbase + static_cast<size_t>(i0 + b) * ld);
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < kB; ++b) {
+            if (i0 + b >= nrows) break;
+            const uint32_t i = i0 + b;
+            const float4 rw = rowp[i];
+            float4 w4 = wb[b];
+            if constexpr (PLASTIC) {
+                const uint32_t pre_spk = flagp[i];
+                if (pre_spk | pmask)
+                    w4 = update4_slow(w4, u, B.row_begin + i, pmask, pre_spk, rw.y, rw.z, P, n_post, ppar);
+                w4.x *= rw.w;
+                w4.y *= rw.w;
+                w4.z *= rw.w;
+                w4.w *= rw.w;
+                if constexpr (RESIDENT) sts4(sbase + 4u * ld * i, w4);
+                else __stcg(reinterpret_cast<float4*>(gbase + static_cast<size_t>(i) * ld), w4);
+            }
+            if (accumulate) {
+                acc.x = fmaf(w4.x, rw.x, acc.x);
+                acc.y = fmaf(w4.y, rw.x, acc.y);
+                acc.z = fmaf(w4.z, rw.x, acc.z);
+                acc.w = fmaf(w4.w, rw.x, acc.w);
+            }
+        }
+    }
+    return acc;
+}
+
+// Pass 2: each thread owns work items (one 4-column unit of one segment) and walks all of the
+// segment's rows; per item the partial sums go to the parity-`par` slot of this CTA.
+__device__ __forceinline__ void weight_pass(const DSim* S, const Desc& D, const DCta& cta, bool pending, uint32_t ppar,
+                                         bool accumulate, uint32_t par, const SmemLayout& sm, const DSeg* s_seg,
+                                         const DBlk* s_blk, uint32_t n_seg) {
     float* part_out = S->partials + static_cast<size_t>(par) * S->n_slots * S->N_pad;
+    const uint32_t npad = S->N_pad;
     for (uint32_t it0 = 0; it0 < cta.n_items; it0 += blockDim.x) {
         const uint32_t it = it0 + threadIdx.x;
         const int s = seg_of_item(s_seg, n_seg, it);
@@ -502,58 +758,55 @@ __device__ __forceinline__ void weight_pass(const DSim* S, const DCta& cta, bool
         float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
         bool touched = false;
         for (uint32_t bk = SG.blk_begin; bk < SG.blk_end; ++bk) {
-            const DBlk& B = s_blk[bk];
-            const DConn& C = S->conns[B.conn];
+            const DBlk B = s_blk[bk];
+            const DConn& C = D.conns[B.conn];
             const bool plastic = pending && C.plast >= 0;
             if (!plastic && !accumulate) continue;
             touched = true;
-            float* wrow = C.w + 4u * u;
             if (plastic) {
-                const DPlast& P = S->plast[C.plast];
-                const float4 cA = ld_col4(P.colA[ppar] + 4u * u);
-                const float4 cB = ld_col4(P.colB[ppar] + 4u * u);
-                const uint4 ps = ld_col4u(P.pspk[ppar] + 4u * u);
-                const uint32_t q = 4u * u;
-                for (uint32_t pl = B.row_begin, r = B.srow; pl < B.row_end; ++pl, ++r) {
-                    const float4 rw = sm.row[r];
-                    const uint32_t pre_spk = sm.rowflag[r];
-                    float4* wp = reinterpret_cast<float4*>(wrow + static_cast<size_t>(pl) * C.ld);
-                    float4 w4 = *wp;
-                    w4.x = plastic_update(w4.x, q + 0u, pl, C.n_post, ps.x, pre_spk, rw.y, cA.x, cB.x, rw.z, P.wmin, P.wmax) * rw.w;
-                    w4.y = plastic_update(w4.y, q + 1u, pl, C.n_post, ps.y, pre_spk, rw.y, cA.y, cB.y, rw.z, P.wmin, P.wmax) * rw.w;
-                    w4.z = plastic_update(w4.z, q + 2u, pl, C.n_post, ps.z, pre_spk, rw.y, cA.z, cB.z, rw.z, P.wmin, P.wmax) * rw.w;
-                    w4.w = plastic_update(w4.w, q + 3u, pl, C.n_post, ps.w, pre_spk, rw.y, cA.w, cB.w, rw.z, P.wmin, P.wmax) * rw.w;
-                    *wp = w4;
-                    if (accumulate) {
-                        acc.x = fmaf(w4.x, rw.x, acc.x);
-                        acc.y = fmaf(w4.y, rw.x, acc.y);
-                        acc.z = fmaf(w4.z, rw.x, acc.z);
-                        acc.w = fmaf(w4.w, rw.x, acc.w);
-                    }
-                }
+                const DPlast* P = &D.plast[C.plast];
+                const uint32_t pm = post_mask(sm.sbits, C.post_off, u, C.n_post);
+                acc = B.resident ? block_rows<true, true>(B, C, P, u, pm, ppar, sm, accumulate, acc)
+                                 : block_rows<false, true>(B, C, P, u, pm, ppar, sm, accumulate, acc);
             } else {
-                for (uint32_t pl = B.row_begin, r = B.srow; pl < B.row_end; ++pl, ++r) {
-                    const float x = sm.row[r].x;
-                    const float4 w4 = *reinterpret_cast<const float4*>(wrow + static_cast<size_t>(pl) * C.ld);
-                    acc.x = fmaf(w4.x, x, acc.x);
-                    acc.y = fmaf(w4.y, x, acc.y);
-                    acc.z = fmaf(w4.z, x, acc.z);
-                    acc.w = fmaf(w4.w, x, acc.w);
-                }
+                acc = B.resident ? block_rows<true, false>(B, C, nullptr, u, 0u, ppar, sm, true, acc)
+                                 : block_rows<false, false>(B, C, nullptr, u, 0u, ppar, sm, true, acc);
             }
         }
         if (accumulate && touched)
-            *reinterpret_cast<float4*>(part_out + static_cast<size_t>(SG.slot) * S->N_pad + SG.pcol + 4u * u) = acc;
+            *reinterpret_cast<float4*>(part_out + static_cast<size_t>(SG.slot) * npad + SG.pcol + 4u * u) = acc;
     }
+}
+
+// Copies the resident rows of this CTA between global memory and shared memory.
+__device__ __forceinline__ void move_resident(const Desc& D, const DBlk* s_blk, uint32_t nblk, const SmemLayout& sm,
+                                           bool to_smem) {
+    for (uint32_t bk = 0; bk < nblk; ++bk) {
+        const DBlk& B = s_blk[bk];
+        if (!B.resident) continue;
+        const DConn& C = D.conns[B.conn];
+        const uint32_t n4 = (B.row_end - B.row_begin) * (C.ld / 4u);
+        float4* g = reinterpret_cast<float4*>(C.w + static_cast<size_t>(B.row_begin) * C.ld);
+        const uint32_t sh = saddr(sm.wres + B.sm_off);
+        if (to_smem)
+            for (uint32_t i = threadIdx.x; i < n4; i += blockDim.x) sts4(sh + 16u * i, __ldcg(g + i));
+        else
+            for (uint32_t i = threadIdx.x; i < n4; i += blockDim.x) __stcg(g + i, lds4(sh + 16u * i));
+    }
+}
+
+__device__ __forceinline__ void copy_words(void* dst, const void* src, size_t bytes) {
+    uint32_t* d = static_cast<uint32_t*>(dst);
+    const uint32_t* s = static_cast<const uint32_t*>(src);
+    for (size_t k = threadIdx.x; k < bytes / 4; k += blockDim.x) d[k] = s[k];
 }
 
 __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* __restrict__ S, uint32_t n_steps) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ Desc s_d;
     __shared__ DCta s_cta;
     __shared__ DSeg s_seg[kMaxSegsPerCta];
     __shared__ DBlk s_blk[kMaxBlksPerCta];
-    __shared__ uint32_t s_goff[kMaxGroups], s_gn[kMaxGroups];
-    __shared__ uint32_t s_bitbase[kMaxMonitors];
     __shared__ unsigned long long s_t0;
     __shared__ uint32_t s_clock0;
     __shared__ int s_ok;
@@ -561,35 +814,93 @@ __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* _
     __shared__ uint32_t s_blk_base, s_nblk;
 
     const uint32_t max_rows = S->max_rows, max_own = S->max_own;
+    uint32_t n_spike_mons = 0;
+    for (uint32_t m = 0; m < S->n_mons; ++m) n_spike_mons += S->mons[m].kind == kMonSpikes ? 1u : 0u;
+    const SmemSizes z = smem_sizes(S->resident_floats, max_rows, max_own, S->spk_words, n_spike_mons, S->n_groups,
+                                   S->n_ts, S->n_conns, S->n_plast, S->n_mons, S->n_red);
     SmemLayout sm;
     {
         unsigned char* p = smem_raw;
+        sm.wres = reinterpret_cast<float*>(p);
+        p += z.wres;
         sm.row = reinterpret_cast<float4*>(p);
-        p += sizeof(float4) * max_rows;
+        p += z.row;
         sm.meta = reinterpret_cast<DRowMeta*>(p);
-        p += sizeof(DRowMeta) * max_rows;
+        p += z.meta;
         sm.rowflag = reinterpret_cast<uint32_t*>(p);
-        p += sizeof(uint32_t) * max_rows;
-        sm.part = reinterpret_cast<float*>(p);
-        p += sizeof(float) * kMaxWarps * max_rows;
+        p += z.rowflag;
+        sm.rowtgt = reinterpret_cast<float*>(p);
+        p += z.rowtgt;
+        sm.sbits = reinterpret_cast<uint32_t*>(p);
+        p += z.sbits;
+        sm.gbits = reinterpret_cast<uint32_t*>(p);
+        p += z.gbits;
+        sm.xown = reinterpret_cast<float*>(p);
+        p += z.xown;
+        sm.rowfac = reinterpret_cast<float2*>(p);
+        p += z.rowfac;
         sm.dot = reinterpret_cast<float*>(p);
-        p += sizeof(float) * 2 * max_own;
+        p += z.dot;
+        sm.red = reinterpret_cast<float*>(p);
+        p += z.redscr;
         sm.bits = reinterpret_cast<uint32_t*>(p);
+        p += z.bits;
+        sm.desc = p;
     }
-
+    // Descriptor copies.
+    {
+        unsigned char* p = sm.desc;
+        copy_words(p, S->groups, sizeof(DGroup) * S->n_groups);
+        p += z.groups;
+        copy_words(p, S->ts, sizeof(DTraceSet) * S->n_ts);
+        p += z.ts;
+        copy_words(p, S->conns, sizeof(DConn) * S->n_conns);
+        p += z.conns;
+        copy_words(p, S->plast, sizeof(DPlast) * S->n_plast);
+        p += z.plast;
+        copy_words(p, S->mons, sizeof(DMon) * S->n_mons);
+        p += z.mons;
+        copy_words(p, S->red_list, sizeof(uint32_t) * S->n_red);
+    }
     if (threadIdx.x == 0) {
-        s_cta = S->ctas[blockIdx.x];
-        s_t0 = *S->steps_done;
-        s_clock0 = *S->clock;
-        uint32_t base = 0, has_norm = 0;
+        unsigned char* p = sm.desc;
+        s_d.groups = reinterpret_cast<const DGroup*>(p);
+        p += z.groups;
+        s_d.ts = reinterpret_cast<const DTraceSet*>(p);
+        p += z.ts;
+        s_d.conns = reinterpret_cast<const DConn*>(p);
+        p += z.conns;
+        s_d.plast = reinterpret_cast<const DPlast*>(p);
+        p += z.plast;
+        s_d.mons = reinterpret_cast<const DMon*>(p);
+        p += z.mons;
+        s_d.red_list = reinterpret_cast<const uint32_t*>(p);
+        s_d.n_groups = S->n_groups;
+        s_d.n_mons = S->n_mons;
+        s_d.n_plast = S->n_plast;
+        s_d.N = S->N;
+        s_d.noise_mode = S->noise_mode;
+        s_d.seed = S->seed;
+        s_d.stim_len = S->stim_len;
+        s_d.replay_steps = S->replay_steps;
+        uint32_t base = 0;
         for (uint32_t m = 0; m < S->n_mons; ++m) {
-            s_bitbase[m] = base;
+            s_d.bitbase[m] = base;
             if (S->mons[m].kind == kMonSpikes) base += max_own / 32u + 2u;
         }
         for (uint32_t g = 0; g < S->n_groups; ++g) {
-            s_goff[g] = S->groups[g].off;
-            s_gn[g] = S->groups[g].n;
+            s_d.goff[g] = S->groups[g].off;
+            s_d.gn[g] = S->groups[g].n;
         }
+        for (uint32_t T = 0; T < 2; ++T)
+            for (uint32_t g = 0; g < kMaxGroups; ++g) {
+                s_d.red_begin[T][g] = S->red_begin[T][g];
+                s_d.red_end[T][g] = S->red_end[T][g];
+            }
+        s_cta = S->ctas[blockIdx.x];
+        s_t0 = *S->steps_done;
+        s_clock0 = *S->clock;
+        uint32_t has_norm = 0;
         // Segments index the global block list; rebase them onto this CTA's copy in s_blk.
         const uint32_t blk_base = s_cta.seg_end > s_cta.seg_begin ? S->segs[s_cta.seg_begin].blk_begin : 0u;
         uint32_t nblk = 0;
@@ -606,6 +917,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* _
         s_nblk = nblk;
     }
     __syncthreads();
+    const Desc& D = s_d;
     const DCta cta = s_cta;
     const uint32_t n_seg = cta.seg_end - cta.seg_begin;
     for (uint32_t b = threadIdx.x; b < s_nblk; b += blockDim.x) s_blk[b] = S->blks[s_blk_base + b];
@@ -613,49 +925,77 @@ __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* _
         const DRowMeta* rows = S->rows + S->rows_begin[blockIdx.x];
         for (uint32_t r = threadIdx.x; r < cta.n_rows; r += blockDim.x) sm.meta[r] = rows[r];
     }
-    uint32_t n_bits_words = 0;
-    for (uint32_t m = 0; m < S->n_mons; ++m)
-        if (S->mons[m].kind == kMonSpikes) n_bits_words += max_own / 32u + 2u;
+    const uint32_t n_bits_words = n_spike_mons * (max_own / 32u + 2u);
+    const uint32_t n_gbits = max_own / 32u + 2u;
+    __syncthreads();
+    move_resident(D, s_blk, s_nblk, sm, true);
+    // triplet normalisation targets of this CTA's rows (constant for the launch)
+    for (uint32_t r = threadIdx.x; r < cta.n_rows; r += blockDim.x) {
+        const DRowMeta meta = sm.meta[r];
+        const DConn& C = D.conns[meta.conn];
+        sm.rowtgt[r] = C.plast >= 0 && D.plast[C.plast].kind == kKindTriplet ? __ldcg(D.plast[C.plast].sums + meta.pl)
+                                                                              : 0.0f;
+    }
     __syncthreads();
 
     const unsigned long long t0 = s_t0;
     const uint32_t clock0 = s_clock0;
     bool ok = true;
+#ifdef BSNN_PHASE_TIMING
+    unsigned long long t_mark_ = static_cast<unsigned long long>(clock64());
+#endif
     for (uint32_t k = 0; k < n_steps; ++k) {
         const unsigned long long t = t0 + k;
         const uint32_t clock = clock0 + k;
         const uint32_t par = static_cast<uint32_t>(t & 1ull), ppar = par ^ 1u;
         const bool pending = k > 0;  // the previous step's plasticity and partials are outstanding
 
-        if (pending) reduce_partials(S, cta, ppar, sm, max_own, s_goff, s_gn);
+        if (pending) reduce_partials(S, D, cta, ppar, sm, max_own);
         for (uint32_t w = threadIdx.x; w < n_bits_words; w += blockDim.x) sm.bits[w] = 0u;
+        for (uint32_t w = threadIdx.x; w < n_gbits; w += blockDim.x) sm.gbits[par * n_gbits + w] = 0u;
         __syncthreads();
-        neuron_phase(S, cta, t, clock, par, pending, sm, max_own, s_goff, s_gn, s_bitbase);
+        BSNN_TMARK(0);
+        neuron_phase(S, D, cta, t, clock, par, pending, sm, max_own);
         __syncthreads();
-        flush_spike_bits(S, cta, clock, sm, s_bitbase);
-        build_rows(S, cta, pending, ppar, sm, true);
+        BSNN_TMARK(1);
+        flush_spike_bits(S, D, cta, clock, par, sm);
+        build_rows(S, D, cta, pending, ppar, sm, true);
         __syncthreads();
-        if (pending && s_has_norm) norm_pass1(S, cta, ppar, sm, s_seg, s_blk, n_seg, max_rows);
-        weight_pass(S, cta, pending, ppar, true, par, sm, s_seg, s_blk, n_seg);
+        BSNN_TMARK(2);
+        if (pending && s_has_norm) {
+            norm_rows(S, D, ppar, sm, s_blk, s_nblk);
+            __syncthreads();
+        }
+        BSNN_TMARK(3);
+        weight_pass(S, D, cta, pending, ppar, true, par, sm, s_seg, s_blk, n_seg);
+        __syncthreads();
+        BSNN_TMARK(4);
         if (!grid_barrier(S, &s_ok)) {
             ok = false;
             break;
         }
+        BSNN_TMARK(5);
     }
     if (!ok) return;
 
-    // Finalize: apply the last step's plasticity and fold its propagation into g.
+    // Finalize: apply the last step's plasticity, write resident rows back, and fold the last
+    // propagation into g.
     const unsigned long long t_last = t0 + n_steps - 1ull;
     const uint32_t lpar = static_cast<uint32_t>(t_last & 1ull);
-    build_rows(S, cta, true, lpar, sm, false);
+    build_rows(S, D, cta, true, lpar, sm, false);
     __syncthreads();
-    if (s_has_norm) norm_pass1(S, cta, lpar, sm, s_seg, s_blk, n_seg, max_rows);
-    weight_pass(S, cta, true, lpar, false, lpar, sm, s_seg, s_blk, n_seg);
-    reduce_partials(S, cta, lpar, sm, max_own, s_goff, s_gn);
+    if (s_has_norm) {
+        norm_rows(S, D, lpar, sm, s_blk, s_nblk);
+        __syncthreads();
+    }
+    weight_pass(S, D, cta, true, lpar, false, lpar, sm, s_seg, s_blk, n_seg);
+    __syncthreads();
+    move_resident(D, s_blk, s_nblk, sm, false);
+    reduce_partials(S, D, cta, lpar, sm, max_own);
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < cta.n1 - cta.n0; i += blockDim.x) {
         const uint32_t j = cta.n0 + i;
-        if (group_of(s_goff, s_gn, S->n_groups, j) < 0) continue;
+        if (group_of(D, j) < 0) continue;
         S->ge[j] = S->ge[j] + sm.dot[i];
         S->gi[j] = S->gi[j] + sm.dot[max_own + i];
     }

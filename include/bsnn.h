@@ -164,6 +164,8 @@ typedef struct bsnn_info {
     uint64_t device_bytes;     /* bytes held in the device arena                        */
     uint64_t weight_bytes;     /* bytes of weight storage                               */
     uint64_t kernel_launches;  /* persistent-kernel launches issued so far              */
+    uint64_t smem_bytes;       /* dynamic shared memory per CTA                         */
+    uint64_t resident_bytes;   /* weight bytes per CTA kept in shared memory per launch */
 } bsnn_info;
 
 /* ---- lifecycle --------------------------------------------------------------------------- */
