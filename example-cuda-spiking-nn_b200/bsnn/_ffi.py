@@ -220,6 +220,29 @@ class Info(ctypes.Structure):
     ]
 
 
+class ConnectionView(ctypes.Structure):
+    """ConnectionView (cpp_src/connections/connection_view.h:8-31): device pointers of one connection."""
+    _fields_ = [
+        ("postsynaptic_r_trace_decay", ctypes.c_float),
+        ("postsynaptic_d_trace_decay", ctypes.c_float),
+        ("postsynaptic_kernel_normalization_value", ctypes.c_float),
+        ("pre_group_is_inhibtory", ctypes.c_bool),
+        ("weight_matrix_idx", ctypes.c_uint32),
+        ("pre_group_offset", ctypes.c_uint32),
+        ("post_group_offset", ctypes.c_uint32),
+        ("pre_group_num_neurons", ctypes.c_uint32),
+        ("post_group_num_neurons", ctypes.c_uint32),
+        ("weight_matrix", ctypes.c_void_p),
+        ("postsynaptic_r_traces", ctypes.c_void_p),
+        ("postsynaptic_d_traces", ctypes.c_void_p),
+        ("summed_postsynaptic_conductances", ctypes.c_void_p),
+        ("post_group_g_excitatory", ctypes.c_void_p),
+        ("post_group_g_inhibitory", ctypes.c_void_p),
+        ("spikes", ctypes.c_void_p),
+        ("cublas_handle", ctypes.c_void_p),
+    ]
+
+
 # Exported symbols and their signatures (every entry point declared in include/bsnn.h).
 _P = ctypes.c_void_p
 _U32 = ctypes.c_uint32
@@ -252,6 +275,7 @@ SIGNATURES = {
     "bsnn_read_spike_bits": (_I32, [_P, _U32, _UP, _I32]),
     "bsnn_read_voltage_history": (_I32, [_P, _U32, _FP, _I32]),
     "bsnn_get_device_pointer": (_I32, [_P, _I32, _U32, ctypes.POINTER(_P)]),
+    "bsnn_connection_propagate": (_I32, [ctypes.POINTER(ConnectionView), _P]),
 }
 
 _lib = None

@@ -12,8 +12,8 @@ import ctypes
 import numpy as np
 
 from . import _ffi
-from ._ffi import (FIELD, UINT_FIELDS, ConnectionParams, Info, NeuronGroupParams, PlasticityParams, StateDesc,
-                   error_for)
+from ._ffi import (FIELD, UINT_FIELDS, ConnectionParams, ConnectionView, Info, NeuronGroupParams, PlasticityParams,
+                   StateDesc, error_for)
 
 
 def _ptr(a: np.ndarray, ctype):
@@ -195,3 +195,13 @@ class Simulation:
         p = ctypes.c_void_p()
         self._check(self._lib.bsnn_get_device_pointer(self._h, FIELD[name], index, ctypes.byref(p)))
         return p.value or 0
+
+
+def connection_propagate(view: ConnectionView, stream: int = 0, library=None):
+    """kernel_connection_propagate_launch (cpp_src/connections/kernel_connection_propagate.cu:64-111) on
+    caller-owned device buffers described by `view`; queued on `stream` (a cudaStream_t address, 0 =
+    legacy default stream).  Raises the BsnnError subclass of the returned status."""
+    lib = library if library is not None else _ffi.load_library()
+    st = lib.bsnn_connection_propagate(ctypes.byref(view), ctypes.c_void_p(stream or None))
+    if st != 0:
+        raise error_for(st, lib.bsnn_last_error(None).decode())

@@ -22,6 +22,7 @@
 
 #include "../../include/bsnn.h"
 #include "bsnn_device.cuh"
+#include "propagate.cuh"
 #include "step_kernel.cuh"
 
 using namespace bsnn;
@@ -1285,6 +1286,26 @@ BSNN_API bsnn_status bsnn_get_device_pointer(const bsnn_sim* sim, int32_t field,
     return guarded(s, [&] {
         finalize(s);
         *out = field_ref(s, field, index).ptr;
+    });
+}
+
+BSNN_API bsnn_status bsnn_connection_propagate(const bsnn_connection_view* view, void* stream) {
+    return guarded(nullptr, [&] {
+        const char* bad = prop::check_view(view);
+        require(bad == nullptr, BSNN_ERR_INVALID_ARGUMENT, bad ? bad : "");
+        int dev = 0, sms = 0;
+        cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+        cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
+        const uint32_t n_post = view->post_group_num_neurons;
+        const uint32_t splits = prop::choose_splits(view->pre_group_num_neurons, n_post, sms);
+        auto st = static_cast<cudaStream_t>(stream);
+        float* scratch = nullptr;
+        cuda_check(cudaMallocAsync(reinterpret_cast<void**>(&scratch), sizeof(float) * splits * size_t(n_post), st),
+                   "cudaMallocAsync (propagate scratch)");
+        const cudaError_t launched = prop::enqueue(view, splits, scratch, st);
+        const cudaError_t freed = cudaFreeAsync(scratch, st);
+        cuda_check(launched, "connection propagate launch");
+        cuda_check(freed, "cudaFreeAsync (propagate scratch)");
     });
 }
 

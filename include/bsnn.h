@@ -270,6 +270,46 @@ BSNN_API bsnn_status bsnn_read_voltage_history(bsnn_sim* sim, uint32_t monitor, 
 /* Device address of a field (for the C++ facade's *View structs); read-only use. */
 BSNN_API bsnn_status bsnn_get_device_pointer(const bsnn_sim* sim, int32_t field, uint32_t index, void** out);
 
+/* ---- one connection on caller-owned device buffers ------------------------------------------ */
+
+/* cpp_src/connections/connection_view.h:8-31, same field names, order and layout, so the address of
+ * a reference ConnectionView can be passed as is.  The pointers are device pointers into the
+ * caller's buffers: weight_matrix is row-major [pre][post], the trace arrays and `spikes` are
+ * [pre_group_num_neurons] (the reference points `spikes` at d_spikes + pre_group_offset,
+ * connection.cpp:85), and the conductance arrays are [post_group_num_neurons].  The offsets and
+ * weight_matrix_idx are bookkeeping and are not read; cublas_handle is ignored. */
+typedef struct bsnn_connection_view {
+    float postsynaptic_r_trace_decay;
+    float postsynaptic_d_trace_decay;
+    float postsynaptic_kernel_normalization_value;
+    bool pre_group_is_inhibtory;
+    uint32_t weight_matrix_idx;
+    uint32_t pre_group_offset;
+    uint32_t post_group_offset;
+    uint32_t pre_group_num_neurons;
+    uint32_t post_group_num_neurons;
+    float* weight_matrix;
+    float* postsynaptic_r_traces;
+    float* postsynaptic_d_traces;
+    float* summed_postsynaptic_conductances;
+    float* post_group_g_excitatory;
+    float* post_group_g_inhibitory;
+    uint32_t* spikes;
+    void* cublas_handle;
+} bsnn_connection_view;
+
+/* kernel_connection_propagate_launch (cpp_src/connections/kernel_connection_propagate.cu:64-111):
+ * decays the r and d traces, adds the normalisation value on a presynaptic spike, writes
+ * x = d - r into summed_postsynaptic_conductances, then adds W^T x into post_group_g_inhibitory
+ * when the presynaptic group is inhibitory, else into post_group_g_excitatory (the cublasSgemv
+ * with alpha = beta = 1).  Runs on the current CUDA device; `stream` is a cudaStream_t (NULL =
+ * the legacy default stream).  The work is queued and the call returns: where the reference
+ * blocks on cudaDeviceSynchronize, synchronise the stream.  GEMV scratch of splits x N_post
+ * floats comes from cudaMallocAsync on `stream` and is freed in stream order.  Errors: null view
+ * or pointer, or an empty connection -> BSNN_ERR_INVALID_ARGUMENT; failed launch -> BSNN_ERR_CUDA
+ * (message in bsnn_last_error(NULL)). */
+BSNN_API bsnn_status bsnn_connection_propagate(const bsnn_connection_view* view, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

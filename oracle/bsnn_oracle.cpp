@@ -756,4 +756,25 @@ BSNN_API uint32_t or_poisson(float exp_neg_mean, uint32_t seed, uint32_t neuron,
     return poisson_knuth(exp_neg_mean, seed, neuron, step, channel);
 }
 
+BSNN_API void or_connection_propagate(float r_decay, float d_decay, float norm, uint32_t n_pre, uint32_t n_post,
+                                      const float* w, float* r, float* d, float* x, float* g,
+                                      const uint32_t* spikes) {
+    for (uint32_t i = 0; i < n_pre; ++i) {  // kernel_connection_decay_d_traces (:22-33)
+        float t = d[i] * d_decay; if (t < 1e-30f) t = 0.0f; d[i] = t;
+    }
+    for (uint32_t i = 0; i < n_pre; ++i) {  // kernel_connection_decay_r_traces (:8-20)
+        float t = r[i] * r_decay; if (t < 1e-30f) t = 0.0f; r[i] = t;
+    }
+    for (uint32_t i = 0; i < n_pre; ++i) {  // kernel_connection_update_conductances_with_spikes (:35-46)
+        if (spikes[i] == 1) { r[i] += norm; d[i] += norm; }
+        x[i] = d[i] - r[i];
+    }
+    parallel_for(n_post, [&](uint32_t q) {  // cublasSgemv, alpha = beta = 1 (:79-94)
+        double acc = 0.0;
+        for (uint32_t i = 0; i < n_pre; ++i)
+            acc += static_cast<double>(w[static_cast<size_t>(i) * n_post + q]) * static_cast<double>(x[i]);
+        g[q] = static_cast<float>(acc) + g[q];
+    });
+}
+
 }  // extern "C"

@@ -71,6 +71,13 @@ BSNN_API int32_t or_last_noise_counts(or_sim* s, uint8_t* out);
 BSNN_API void or_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 BSNN_API uint32_t or_poisson(float exp_neg_mean, uint32_t seed, uint32_t neuron, uint64_t step, uint32_t channel);
 
+/* One connection's propagation on host arrays (kernel_connection_propagate_launch,
+ * cpp_src/connections/kernel_connection_propagate.cu:8-46, 64-111): r, d and x [n_pre] are updated
+ * in place and g [n_post] += W^T x with W row-major [n_pre][n_post], dot products in double. */
+BSNN_API void or_connection_propagate(float r_decay, float d_decay, float norm, uint32_t n_pre, uint32_t n_post,
+                                      const float* w, float* r, float* d, float* x, float* g,
+                                      const uint32_t* spikes);
+
 #ifdef __cplusplus
 }
 #endif

@@ -55,6 +55,7 @@ def load():
         "or_read_weights_f64": (I32, [P, U32, P]), "or_write_weights": (I32, [P, U32, P]), "or_read_spike_history": (I32, [P, U32, P, I32]),
         "or_read_voltage_history": (I32, [P, U32, P, I32]), "or_last_noise_counts": (I32, [P, P]),
         "or_philox4x32_10": (None, [P, P, P]), "or_poisson": (U32, [ctypes.c_float, U32, U32, ctypes.c_uint64, U32]),
+        "or_connection_propagate": (None, [ctypes.c_float, ctypes.c_float, ctypes.c_float, U32, U32, P, P, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -75,6 +76,17 @@ def philox4x32_10(counter, key):
 
 def poisson(exp_neg_mean, seed, neuron, step, channel):
     return load().or_poisson(exp_neg_mean, seed, neuron, step, channel)
+
+
+def connection_propagate(r_decay, d_decay, norm, w, r, d, x, g, spikes):
+    """One connection's propagation on numpy arrays, updated in place (r, d, x [n_pre] float32,
+    g [n_post] float32, w [n_pre, n_post] float32, spikes [n_pre] uint32)."""
+    n_pre, n_post = w.shape
+    arrs = [np.ascontiguousarray(w, np.float32)]
+    for a, dt in ((r, np.float32), (d, np.float32), (x, np.float32), (g, np.float32), (spikes, np.uint32)):
+        assert a.dtype == dt and a.flags.c_contiguous
+    load().or_connection_propagate(r_decay, d_decay, norm, n_pre, n_post, _vp(arrs[0]), _vp(r), _vp(d), _vp(x),
+                                   _vp(g), _vp(spikes))
 
 
 def _vp(a: np.ndarray):

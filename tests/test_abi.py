@@ -48,6 +48,24 @@ def test_struct_layouts_match_reference_field_order():
     assert ctypes.sizeof(NeuronGroupParams) == 88
     assert ctypes.sizeof(ConnectionParams) == 20
     assert ctypes.sizeof(PlasticityParams) == 44
+    # ConnectionView: 3 floats, bool, 5 uint32, 8 pointers (connection_view.h:8-31)
+    from bsnn._ffi import ConnectionView
+    assert ConnectionView.pre_group_is_inhibtory.offset == 12 and ConnectionView.weight_matrix_idx.offset == 16
+    assert ConnectionView.weight_matrix.offset == 40 and ConnectionView.cublas_handle.offset == 96
+    assert ctypes.sizeof(ConnectionView) == 104
+
+
+def test_connection_propagate_rejects_bad_views_before_touching_a_device():
+    import bsnn
+    lib = bsnn.load_library()
+    assert lib.bsnn_connection_propagate(None, None) == 1  # BSNN_ERR_INVALID_ARGUMENT
+    assert b"null view" in lib.bsnn_last_error(None)
+    empty = bsnn.ConnectionView()
+    with pytest.raises(bsnn.InvalidArgument, match="empty connection"):
+        bsnn.connection_propagate(empty)
+    nulls = bsnn.ConnectionView(pre_group_num_neurons=4, post_group_num_neurons=3)
+    with pytest.raises(bsnn.InvalidArgument, match="null device pointer"):
+        bsnn.connection_propagate(nulls)
 
 
 @pytest.mark.skipif(gpu_available(), reason="checks the no-GPU failure path")

@@ -181,3 +181,30 @@ def test_stimulus_overflow_is_rejected(oracle_mod):
     o.run(0, 3)
     with pytest.raises(RuntimeError):
         o.step(3)
+
+
+def test_connection_propagate_restatement(oracle_mod):
+    """or_connection_propagate against numpy: trace arithmetic bit-exact in float32, the GEMV
+    within double-precision rounding of a float64 matrix-vector product."""
+    rng = np.random.default_rng(11)
+    n_pre, n_post = 37, 29
+    w = rng.uniform(0, 2, (n_pre, n_post)).astype(np.float32)
+    r = rng.uniform(0, 1, n_pre).astype(np.float32)
+    d = rng.uniform(0, 1, n_pre).astype(np.float32)
+    r[:3] = 1e-31  # decays below the 1e-30 flush threshold
+    x = np.zeros(n_pre, np.float32)
+    g = rng.uniform(0, 1, n_post).astype(np.float32)
+    spikes = (rng.random(n_pre) < 0.3).astype(np.uint32)
+    rd, dd, norm = np.float32(0.9), np.float32(0.97), np.float32(1.25)
+    want_d = d * dd
+    want_d[want_d < np.float32(1e-30)] = 0
+    want_r = r * rd
+    want_r[want_r < np.float32(1e-30)] = 0
+    want_r = np.where(spikes == 1, want_r + norm, want_r).astype(np.float32)
+    want_d = np.where(spikes == 1, want_d + norm, want_d).astype(np.float32)
+    want_x = want_d - want_r
+    want_g = (w.astype(np.float64).T @ want_x.astype(np.float64)).astype(np.float32) + g
+    oracle_mod.connection_propagate(rd, dd, norm, w, r, d, x, g, spikes)
+    assert np.array_equal(r, want_r) and np.array_equal(d, want_d) and np.array_equal(x, want_x)
+    assert r[0] == 0 or spikes[0] == 1
+    np.testing.assert_allclose(g, want_g, rtol=1e-6)
