@@ -223,8 +223,9 @@ def run_bsnn(args, rank, world):
     value = sim_seconds / (t_ms / 1e3)
     steps_per_s = K * S * world / (t_ms / 1e3)
     per_launch_ms = t_ms / max(1, launches)
+    clock_steps_per_launch = K * S / max(1, launches)
     bytes_step = algorithmic_bytes_per_step(spec)
-    achieved = bytes_step * STEPS_PER_LAUNCH / (per_launch_ms / 1e3) / 1e9
+    achieved = bytes_step * clock_steps_per_launch / (per_launch_ms / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
     traffic = None
     if PROFILE_TRAFFIC.exists():
@@ -255,7 +256,7 @@ def run_bsnn(args, rank, world):
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_kind,
-                     "bytes_per_clock_step": bytes_step, "clock_steps_per_launch": STEPS_PER_LAUNCH,
+                     "bytes_per_clock_step": bytes_step, "clock_steps_per_launch": clock_steps_per_launch,
                      "launch_ms": per_launch_ms,
                      "note": "working set (~40 MB) is L2-resident, so frac of HBM peak can exceed 1"},
         "clocks": clocks.summary(),
