@@ -276,6 +276,7 @@ SIGNATURES = {
     "bsnn_read_voltage_history": (_I32, [_P, _U32, _FP, _I32]),
     "bsnn_get_device_pointer": (_I32, [_P, _I32, _U32, ctypes.POINTER(_P)]),
     "bsnn_connection_propagate": (_I32, [ctypes.POINTER(ConnectionView), _P]),
+    "bsnn_connection_propagate_noalloc": (_I32, [ctypes.POINTER(ConnectionView), _P]),
 }
 
 _lib = None

@@ -23,6 +23,7 @@
 #include "../../include/bsnn.h"
 #include "bsnn_device.cuh"
 #include "propagate.cuh"
+#include "propagate_static.cuh"
 #include "step_kernel.cuh"
 
 using namespace bsnn;
@@ -1306,6 +1307,25 @@ BSNN_API bsnn_status bsnn_connection_propagate(const bsnn_connection_view* view,
         const cudaError_t freed = cudaFreeAsync(scratch, st);
         cuda_check(launched, "connection propagate launch");
         cuda_check(freed, "cudaFreeAsync (propagate scratch)");
+    });
+}
+
+BSNN_API bsnn_status bsnn_connection_propagate_noalloc(const bsnn_connection_view* view, void* stream) {
+    return guarded(nullptr, [&] {
+        const char* bad = prop::check_view(view);
+        require(bad == nullptr, BSNN_ERR_INVALID_ARGUMENT, bad ? bad : "");
+        const uint32_t n_post = view->post_group_num_neurons;
+        require(n_post <= prop::kStaticScratchFloats, BSNN_ERR_OUT_OF_RANGE,
+                "post_group_num_neurons " + std::to_string(n_post) +
+                    " exceeds the static propagate scratch limit of " + std::to_string(prop::kStaticScratchFloats));
+        int dev = 0, sms = 0;
+        cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+        cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
+        float* scratch = nullptr;
+        cuda_check(prop::static_scratch(dev, &scratch), "static propagate scratch set-up (cudaGetSymbolAddress)");
+        const uint32_t splits = prop::static_splits(view->pre_group_num_neurons, n_post, sms);
+        cuda_check(prop::enqueue(view, splits, scratch, static_cast<cudaStream_t>(stream)),
+                   "connection propagate launch");
     });
 }
 

@@ -310,6 +310,20 @@ typedef struct bsnn_connection_view {
  * (message in bsnn_last_error(NULL)). */
 BSNN_API bsnn_status bsnn_connection_propagate(const bsnn_connection_view* view, void* stream);
 
+/* No counterpart in the reference.  The same work and result as bsnn_connection_propagate, but the
+ * call allocates no device memory: the GEMV scratch is a fixed module-scope device array of
+ * 1,048,576 floats (4 MiB) per device, so post_group_num_neurons above 1,048,576 is rejected with
+ * BSNN_ERR_OUT_OF_RANGE before anything is queued.  It is for callers that must not allocate per
+ * call, e.g. a step loop inside an application whose device memory is already claimed by its own
+ * caching allocator (PyTorch's), where a cudaMallocAsync can fail or grow a pool mid-run.
+ *  - The first call on each device does a one-time set-up with that device current (looking up the
+ *    array's device address with cudaGetSymbolAddress, which may load this library's device code);
+ *    make that first call before any stream capture.  A failed set-up returns BSNN_ERR_CUDA.
+ *  - Nothing has to start at zero: each call writes every scratch value it reads.
+ *  - All calls on one device share the array: calls that overlap in time (on different streams or
+ *    from different host threads) race and give wrong results.  Order them (one stream, or events). */
+BSNN_API bsnn_status bsnn_connection_propagate_noalloc(const bsnn_connection_view* view, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
