@@ -162,6 +162,18 @@ def cpu_baseline(spec, seconds: float):
             "sample": f"{n} clock steps of {spec.name} (FP32 oracle, {threads} threads), {el:.1f} s"}
 
 
+def reduce_over_ranks(t_ms: float, events: int, spikes: int, device):
+    """Whole-job figures of N independent replicas: the slowest rank's device time (max) and the
+    summed event and spike counts.  `device` is where the process group's backend keeps tensors
+    (a CUDA device for NCCL, "cpu" for gloo)."""
+    import torch
+    t = torch.tensor([t_ms], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ev = torch.tensor([float(events), float(spikes)], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(ev)
+    return float(t.item()), int(ev[0].item()), int(ev[1].item())
+
+
 def run_bsnn(args, rank, world):
     import torch
 
@@ -212,12 +224,7 @@ def run_bsnn(args, rank, world):
     info1 = sim.info()
     t_ms = float(sum(times_ms))
     if world > 1:
-        t = torch.tensor([t_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        t_ms = float(t.item())
-        ev = torch.tensor([float(events), float(spikes)], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(ev)
-        events, spikes = int(ev[0].item()), int(ev[1].item())
+        t_ms, events, spikes = reduce_over_ranks(t_ms, events, spikes, dev)
     launches = int(info1.kernel_launches - info0.kernel_launches)
     sim_seconds = K * S * DT * world
     value = sim_seconds / (t_ms / 1e3)

@@ -1,0 +1,68 @@
+"""The N > 1 bench path on CPU: two gloo ranks run the whole-job reduction of independent
+replicas (max of the device times, sum of the event counts) and the reference arm prints from
+rank 0 only."""
+from __future__ import annotations
+
+import os
+import socket
+import subprocess
+import sys
+
+import pytest
+import torch.multiprocessing as mp
+
+from conftest import ROOT
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank(rank, world, port, results):
+    import datetime
+
+    import torch
+    sys.path.insert(0, str(ROOT))
+    import bench
+    torch.distributed.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                                         world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        t_ms = [12.5, 30.25][rank]
+        out = bench.reduce_over_ranks(t_ms, events=100 * (rank + 1), spikes=7 + rank, device="cpu")
+        results[rank] = out
+    finally:
+        torch.distributed.destroy_process_group()
+
+
+def test_replica_reduction_two_gloo_ranks():
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as mgr:
+        results = mgr.dict()
+        port = _free_port()
+        procs = [ctx.Process(target=_rank, args=(r, 2, port, results)) for r in range(2)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(120)
+            assert p.exitcode == 0
+        assert dict(results) == {0: (30.25, 300, 15), 1: (30.25, 300, 15)}
+
+
+@pytest.mark.parametrize("rank,expect_line", [(0, True), (1, False)])
+def test_reference_arm_prints_on_rank_zero_only(rank, expect_line):
+    env = dict(os.environ, RANK=str(rank), WORLD_SIZE="2", LOCAL_RANK=str(rank), CUDA_VISIBLE_DEVICES="")
+    if rank != 0:
+        res = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--gpus", "2"],
+                             env=env, capture_output=True, text=True, timeout=120)
+        assert res.returncode == 0 and res.stdout.strip() == ""
+    else:
+        # rank 0 runs the bounded CPU sample (no GPU here); keep it short
+        res = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--gpus", "2",
+                              "--workload", "small_plastic_500", "--cpu-seconds", "0.5"],
+                             env=env, capture_output=True, text=True, timeout=300)
+        assert res.returncode == 0, res.stderr[-2000:]
+        import json
+        line = json.loads(res.stdout.strip().splitlines()[-1])
+        assert line["impl"] == "reference" and line["value"] > 0 and line["cpu_baseline"]["kind"] == "port"
