@@ -506,9 +506,26 @@ void finalize(bsnn_sim* s) {
     cuda_check(cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(&bsnn_step_kernel)), "func attr");
     uint32_t n_spike_mons = 0;
     for (const auto& M : s->mons) n_spike_mons += M.kind == kMonSpikes ? 1u : 0u;
+    // Per-group role counts that size the shared-memory neuron state.
+    {
+        std::vector<uint32_t> n_pre(h.n_groups, 0), n_post(h.n_groups, 0), n_vmon(h.n_groups, 0);
+        for (const auto& PL : s->plasts) {
+            ++n_pre[s->conns[PL.conn].pre];
+            ++n_post[s->conns[PL.conn].post];
+        }
+        for (const auto& M : s->mons)
+            if (M.kind != kMonSpikes) ++n_vmon[M.group];
+        for (uint32_t g = 0; g < h.n_groups; ++g) {
+            h.ns_ts = std::max(h.ns_ts, h.groups[g].n_ts);
+            h.ns_pre = std::max(h.ns_pre, n_pre[g]);
+            h.ns_post = std::max(h.ns_post, n_post[g]);
+            h.ns_mon = std::max(h.ns_mon, n_vmon[g]);
+        }
+    }
+    const uint32_t ns_fields = ns_layout(h.ns_ts, h.ns_pre, h.ns_post, h.ns_mon).fields;
     auto smem_of = [&](const Plan& pl, uint32_t resident_floats) {
         return smem_sizes(resident_floats, pl.max_rows, pl.max_own, spk_words, n_spike_mons, h.n_groups, h.n_ts,
-                          h.n_conns, h.n_plast, h.n_mons, static_cast<uint32_t>(pl.red_list.size()))
+                          h.n_conns, h.n_plast, h.n_mons, static_cast<uint32_t>(pl.red_list.size()), ns_fields)
             .total;
     };
     const int64_t smem_limit = static_cast<int64_t>(optin) - static_cast<int64_t>(fa.sharedSizeBytes) - 128;

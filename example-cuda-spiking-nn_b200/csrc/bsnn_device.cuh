@@ -2,7 +2,9 @@
 //
 // One DSim lives in device memory per bsnn_sim.  All per-neuron state is structure-of-arrays
 // over the global neuron index (the reference's GpuSimulationState layout,
-// cpp_src/gpu_core/gpu_simulation_state.cu:35-86).  What differs from the reference:
+// cpp_src/gpu_core/gpu_simulation_state.cu:35-86); between launches it is canonical there, and
+// during a launch each CTA keeps its own neurons' copy in shared memory.  What differs from the
+// reference:
 //  * weight matrices are row-major [pre][ld] with ld = num_post rounded up to 4 floats, so every
 //    row starts on a 16-byte boundary and is read with 128-bit loads;
 //  * values that other CTAs read inside one persistent launch (spikes, plasticity column and
@@ -134,6 +136,9 @@ struct DSim {
     uint32_t n_groups, n_conns, n_ts, n_plast, n_mons;
     uint32_t n_ctas, n_slots, max_rows, max_own;
     uint32_t resident_floats;  // shared-memory floats reserved for resident weight rows (per CTA)
+    // Largest per-group role counts (trace sets, plasticities as pre / post side, voltage
+    // monitors): they size the per-neuron state each CTA keeps in shared memory during a launch.
+    uint32_t ns_ts, ns_pre, ns_post, ns_mon;
     DGroup groups[kMaxGroups];
     DTraceSet ts[kMaxTraceSets];
     DConn conns[kMaxConns];

@@ -3,8 +3,12 @@
 // One cooperative launch runs `n_steps` consecutive calls of System::step_the_clock
 // (cpp_src/core/system.cpp:43-63) with ONE grid-wide barrier per step.  Each CTA owns a
 // contiguous range of neurons; it updates them as neurons (phase A) and streams their outgoing
-// weight rows as presynaptic rows (phase B):
+// weight rows as presynaptic rows (phase B).  The own neurons' state stays in shared memory for
+// the whole launch; global memory carries only what other CTAs read (GEMV partial sums, the
+// spike bitmask, plasticity column factors) and the monitor rings.
 //
+//   inputs (one batch of loads): the previous step's GEMV partials of the own neurons, the
+//                           network spike bitmask of the previous step, the step's stimulus range
 //   phase A (own neurons): g = g_base + sum of the previous step's GEMV partials (fixed order)
 //                           -> background Poisson shot noise      (kernel_neuron_group_evolve.cu:11-83)
 //                           -> conductance-EIF Euler step, spike   (kernel_neuron_group_evolve.cu:85-130)
@@ -12,6 +16,8 @@
 //                           -> difference-of-exponentials traces   (kernel_connection_propagate.cu:8-46)
 //                           -> plasticity trace decay/increment    (kernel_*_plasticity_update.cu)
 //                           -> monitor ring buffers                (kernel_historicize_*.cu)
+//                           while the remaining warps compute the triplet row-normalisation sums
+//                           of the previous step's update
 //   phase B (own rows):    the previous step's plasticity weight update (+ row normalisation),
 //                           fused with this step's propagation GEMV (the cublasSgemv of
 //                           kernel_connection_propagate.cu:79-94): each weight is read once,
@@ -22,8 +28,8 @@
 // Deferring step t's plasticity into step t+1's phase B is exact: between the two the
 // reference touches the weights only to read them in step t+1's propagation, which phase B
 // performs after the update.  At the end of a launch a finalize pass applies the pending
-// plasticity and reduces the pending partials, so between launches the device state is the
-// reference's state after step_the_clock.
+// plasticity, reduces the pending partials and writes the neuron state back, so between
+// launches the device state is the reference's state after step_the_clock.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -104,17 +110,21 @@ __device__ __forceinline__ float clamp_w(float w, float wmin, float wmax) {
     return w;
 }
 
-// Grid-wide barrier over the persistent CTAs: monotonically increasing 64-bit arrival counter,
-// release/acquire at gpu scope.  Bounded: after kBarrierTimeoutNs (or when another CTA has
-// already given up) it records kErrBarrierTimeout and returns false so the kernel can exit.
-__device__ __forceinline__ bool grid_barrier(const DSim* S, int* s_ok) {
+__device__ __forceinline__ void red_release_add_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Grid-wide barrier over the persistent CTAs on a monotonically increasing 64-bit arrival counter.
+// After the CTA-wide sync, thread 0 arrives with a gpu-scope release reduction (no return value
+// to wait for) and spins with gpu-scope acquire loads until the counter reaches `target`, the
+// count at which every CTA has arrived; the closing CTA-wide sync extends the acquire to the
+// whole CTA.  Bounded: after kBarrierTimeoutNs (or when another CTA has already given up) it
+// records kErrBarrierTimeout and returns false so the kernel can exit.
+__device__ __forceinline__ bool grid_barrier(const DSim* S, unsigned long long target, int* s_ok) {
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
-        __threadfence();
-        const unsigned long long n = gridDim.x;
-        const unsigned long long old = atomicAdd(S->barrier, 1ull);
-        const unsigned long long target = (old / n + 1ull) * n;
+        red_release_add_u64(S->barrier, 1ull);
         unsigned long long t_start = 0;
         uint32_t spins = 0;
         while (static_cast<long long>(ld_acquire_u64(S->barrier) - target) < 0) {
@@ -133,7 +143,6 @@ __device__ __forceinline__ bool grid_barrier(const DSim* S, int* s_ok) {
                 }
             }
         }
-        __threadfence();
         *s_ok = ok;
     }
     __syncthreads();
@@ -188,23 +197,43 @@ struct SmemLayout {
     uint32_t* gbits;    // [2][max_own/32 + 2] this CTA's spike bits, by step parity
     float* xown;        // [n_ts][max_own] x = d - r of the own neurons (this step)
     float2* rowfac;     // [2][n_plast][max_own] {rowA, rowB} of the own neurons, by step parity
-    float* dot;         // [2][max_own]
+    float* ns;          // [ns_fields][max_own] state of the own neurons (kNs* fields below)
     float* red;         // [warps][2][max_own] per-warp partial-sum reduction scratch
     uint32_t* bits;     // [n_spike_monitors][max_own/32 + 2]
     unsigned char* desc;  // descriptor copies (DGroup, DTraceSet, DConn, DPlast, DMon, slot lists)
 };
 
+// Fields of the shared-memory neuron state: fixed ones, then two per trace set (r, d), two per
+// plasticity on the presynaptic side (pre, triplet pre), two per plasticity on the postsynaptic
+// side (post, triplet post) and one per voltage monitor (the neuron's ring column, or -1).
+enum : uint32_t {
+    kNsV = 0, kNsGe, kNsGi, kNsIstim, kNsEr, kNsEd, kNsIr, kNsId, kNsBgGe, kNsBgGi, kNsRefrac, kNsSpike,
+    kNsFixed
+};
+struct NsLayout {
+    uint32_t ts, pre, post, mon, fields;
+};
+__host__ __device__ __forceinline__ NsLayout ns_layout(uint32_t n_ts, uint32_t n_pre, uint32_t n_post, uint32_t n_mon) {
+    NsLayout L;
+    L.ts = kNsFixed;
+    L.pre = L.ts + 2u * n_ts;
+    L.post = L.pre + 2u * n_pre;
+    L.mon = L.post + 2u * n_post;
+    L.fields = L.mon + n_mon;
+    return L;
+}
+
 __host__ __device__ __forceinline__ size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
 // Byte layout of the dynamic shared memory; the host sizes the launch with the same function.
 struct SmemSizes {
-    size_t wres, row, meta, rowflag, rowtgt, sbits, gbits, xown, rowfac, dot, redscr, bits, groups, ts, conns, plast,
+    size_t wres, row, meta, rowflag, rowtgt, sbits, gbits, xown, rowfac, ns, redscr, bits, groups, ts, conns, plast,
         mons, red, total;
 };
 __host__ __device__ __forceinline__ SmemSizes smem_sizes(uint32_t resident_floats, uint32_t max_rows, uint32_t max_own,
                                                          uint32_t spk_words, uint32_t n_spike_mons, uint32_t n_groups,
                                                          uint32_t n_ts, uint32_t n_conns, uint32_t n_plast,
-                                                         uint32_t n_mons, uint32_t n_red) {
+                                                         uint32_t n_mons, uint32_t n_red, uint32_t ns_fields) {
     SmemSizes z;
     z.wres = align16(sizeof(float) * static_cast<size_t>(resident_floats));
     z.row = align16(sizeof(float4) * max_rows);
@@ -215,7 +244,7 @@ __host__ __device__ __forceinline__ SmemSizes smem_sizes(uint32_t resident_float
     z.gbits = align16(sizeof(uint32_t) * 2 * (max_own / 32 + 2));
     z.xown = align16(sizeof(float) * n_ts * max_own);
     z.rowfac = align16(sizeof(float2) * 2 * n_plast * max_own);
-    z.dot = align16(sizeof(float) * 2 * max_own);
+    z.ns = align16(sizeof(float) * ns_fields * max_own);
     z.redscr = align16(sizeof(float) * 2 * kMaxWarps * max_own);
     z.bits = align16(sizeof(uint32_t) * n_spike_mons * (max_own / 32 + 2));
     z.groups = align16(sizeof(DGroup) * n_groups);
@@ -224,7 +253,7 @@ __host__ __device__ __forceinline__ SmemSizes smem_sizes(uint32_t resident_float
     z.plast = align16(sizeof(DPlast) * n_plast);
     z.mons = align16(sizeof(DMon) * n_mons);
     z.red = align16(sizeof(uint32_t) * n_red);
-    z.total = z.wres + z.row + z.meta + z.rowflag + z.rowtgt + z.sbits + z.gbits + z.xown + z.rowfac + z.dot + z.redscr +
+    z.total = z.wres + z.row + z.meta + z.rowflag + z.rowtgt + z.sbits + z.gbits + z.xown + z.rowfac + z.ns + z.redscr +
               z.bits + z.groups + z.ts + z.conns + z.plast + z.mons + z.red;
     return z;
 }
@@ -235,59 +264,72 @@ __device__ __forceinline__ int group_of(const Desc& D, uint32_t j) {
     return -1;
 }
 
-// Phase A1 / finalize: dot[T][i] = sum over the slots listed for (T, group of neuron n0+i) of the
-// parity-`par` partial sums at that neuron's column.  Lanes take consecutive neurons (coalesced
-// reads of a slot row), warps take every nwarps-th slot of the list; the per-warp sums are then
-// added in warp order.  A fixed summation order.
-__device__ __forceinline__ void reduce_partials(const DSim* S, const Desc& D, const DCta& cta, uint32_t par,
-                                             const SmemLayout& sm, uint32_t max_own) {
-    const uint32_t n_own = cta.n1 - cta.n0;
+// The previous step's GEMV partial sums at the own neurons' columns, summed per warp:
+// red[warp][T][i] = sum over the entries k = warp, warp + nwarps, ... of the slot list of
+// (T, group of neuron n0+i), in list order; dot_of() then adds the warps in warp order, so the
+// summation order is fixed.  Lanes take consecutive neurons (coalesced reads of a slot row).  Both
+// targets' loads of a 16-entry batch are issued before any is used, so for up to 16 * nwarps
+// slots per target the whole reduction costs one round trip to L2.
+__device__ __forceinline__ void load_partials(const DSim* S, const Desc& D, const DCta& cta, uint32_t par,
+                                              const SmemLayout& sm, uint32_t max_own) {
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u, nwarps = blockDim.x >> 5;
     const float* part = S->partials + static_cast<size_t>(par) * S->n_slots * S->N_pad;
     const uint32_t npad = S->N_pad;
+    constexpr int kQ = 16;
     for (uint32_t g = 0; g < D.n_groups; ++g) {
         const uint32_t goff = D.goff[g], gend = goff + D.gn[g];
         const uint32_t a = cta.n0 > goff ? cta.n0 : goff, b = cta.n1 < gend ? cta.n1 : gend;
         if (a >= b) continue;
         const uint32_t pcol = D.groups[g].pcol;
-        for (uint32_t T = 0; T < 2; ++T) {
-            const uint32_t lb = D.red_begin[T][g], le = D.red_end[T][g];
-            for (uint32_t j0 = a; j0 < b; j0 += 32u) {
-                const uint32_t j = j0 + lane;
-                float s = 0.0f;
-                if (j < b) {
-                    const float* col = part + pcol + (j - goff);
-                    // 8 independent loads in flight per batch; the adds keep list order
-                    for (uint32_t k0 = lb + warp; k0 < le; k0 += 8u * nwarps) {
-                        float v[8];
+        const uint32_t lb0 = D.red_begin[0][g], le0 = D.red_end[0][g];
+        const uint32_t lb1 = D.red_begin[1][g], le1 = D.red_end[1][g];
+        for (uint32_t j0 = a; j0 < b; j0 += 32u) {
+            const uint32_t j = j0 + lane;
+            const bool valid = j < b;
+            const float* col = part + pcol + (j - goff);
+            float s0 = 0.0f, s1 = 0.0f;
+            for (uint32_t m0 = 0; lb0 + warp + m0 * nwarps < le0 || lb1 + warp + m0 * nwarps < le1; m0 += kQ) {
+                float v0[kQ], v1[kQ];
 #pragma unroll
-                        for (int q = 0; q < 8; ++q) {
-                            const uint32_t k = k0 + q * nwarps;
-                            v[q] = k < le ? __ldcg(col + static_cast<size_t>(D.red_list[k]) * npad) : 0.0f;
-                        }
-#pragma unroll
-                        for (int q = 0; q < 8; ++q)
-                            if (k0 + q * nwarps < le) s += v[q];
-                    }
-                    sm.red[(warp * 2u + T) * max_own + (j - cta.n0)] = s;
+                for (int q = 0; q < kQ; ++q) {
+                    const uint32_t k = lb0 + warp + (m0 + q) * nwarps;
+                    v0[q] = valid && k < le0 ? __ldcg(col + static_cast<size_t>(D.red_list[k]) * npad) : 0.0f;
                 }
+#pragma unroll
+                for (int q = 0; q < kQ; ++q) {
+                    const uint32_t k = lb1 + warp + (m0 + q) * nwarps;
+                    v1[q] = valid && k < le1 ? __ldcg(col + static_cast<size_t>(D.red_list[k]) * npad) : 0.0f;
+                }
+#pragma unroll
+                for (int q = 0; q < kQ; ++q)
+                    if (lb0 + warp + (m0 + q) * nwarps < le0) s0 += v0[q];
+#pragma unroll
+                for (int q = 0; q < kQ; ++q)
+                    if (lb1 + warp + (m0 + q) * nwarps < le1) s1 += v1[q];
+            }
+            if (valid) {
+                sm.red[(warp * 2u + 0u) * max_own + (j - cta.n0)] = s0;
+                sm.red[(warp * 2u + 1u) * max_own + (j - cta.n0)] = s1;
             }
         }
     }
-    __syncthreads();
-    for (uint32_t e = threadIdx.x; e < 2u * n_own; e += blockDim.x) {
-        const uint32_t T = e / n_own, i = e % n_own;
-        float s = 0.0f;
-        for (uint32_t w = 0; w < nwarps; ++w) s += sm.red[(w * 2u + T) * max_own + i];
-        sm.dot[T * max_own + i] = s;
-    }
 }
 
-// Phase A2: one thread per owned neuron.  All of the neuron's inputs are loaded first, then the
-// reference's per-step arithmetic runs, then everything is stored.
+// Sum of the per-warp partial sums of own neuron i for target T, in warp order.
+__device__ __forceinline__ float dot_of(const SmemLayout& sm, uint32_t T, uint32_t i, uint32_t max_own,
+                                        uint32_t nwarps) {
+    float s = 0.0f;
+    for (uint32_t w = 0; w < nwarps; ++w) s += sm.red[(w * 2u + T) * max_own + i];
+    return s;
+}
+
+// Phase A: one thread per owned neuron (threads 0 .. n_own-1).  The neuron's state is read from
+// and written back to the shared-memory copy; global memory receives only the plasticity column
+// factors (read by other CTAs) and the voltage rings.  The reference's per-step arithmetic runs
+// statement by statement.
 __device__ __forceinline__ void neuron_phase(const DSim* S, const Desc& D, const DCta& cta, unsigned long long t,
                                           uint32_t clock, uint32_t par, bool has_dot, const SmemLayout& sm,
-                                          uint32_t max_own) {
+                                          uint32_t max_own, const NsLayout& L, uint32_t ev_lo, uint32_t ev_hi) {
     const uint32_t i = threadIdx.x;
     if (i >= cta.n1 - cta.n0) return;
     const uint32_t j = cta.n0 + i;
@@ -295,43 +337,21 @@ __device__ __forceinline__ void neuron_phase(const DSim* S, const Desc& D, const
     if (g < 0) return;
     const DGroup& G = D.groups[g];
     const uint32_t loc = j - G.off;
+    float* ns = sm.ns + i;
+    const uint32_t MO = max_own;
 
-    // ---- loads ----
-    float ge_used = S->ge[j], gi_used = S->gi[j];
-    const float er0 = S->bg_er[j], ir0 = S->bg_ir[j], ed0 = S->bg_ed[j], id0 = S->bg_id[j];
-    float istim = S->istim[j];
-    float v = S->v[j];
-    uint32_t refrac = S->refrac[j];
-    constexpr int kR = kMaxGroupRoles;  // role slots, all loaded up front into registers
-    float ts_r[kR], ts_d[kR], pre0[kR], tpre0[kR], post0[kR], tpost0[kR];
-#pragma unroll
-    for (int k = 0; k < kR; ++k) {
-        if (k < static_cast<int>(G.n_ts)) {
-            const DTraceSet& TS = D.ts[G.ts[k]];
-            ts_r[k] = TS.r[loc];
-            ts_d[k] = TS.d[loc];
-        }
-        if (k < static_cast<int>(G.n_plast_pre)) {
-            const DPlast& P = D.plast[G.plast_pre[k]];
-            pre0[k] = P.pre[loc];
-            tpre0[k] = P.kind == kKindTriplet ? P.tpre[loc] : 0.0f;
-        }
-        if (k < static_cast<int>(G.n_plast_post)) {
-            const DPlast& P = D.plast[G.plast_post[k]];
-            post0[k] = P.post[loc];
-            tpost0[k] = P.kind == kKindTriplet ? P.tpost[loc] : 0.0f;
-        }
-    }
-    uint32_t ev_lo = 0, ev_hi = 0;
-    if (t < D.stim_len) {
-        ev_lo = S->stim_off[t];
-        ev_hi = S->stim_off[t + 1];
-    }
+    // ---- loads (shared memory) ----
+    float ge_used = ns[kNsGe * MO], gi_used = ns[kNsGi * MO];
+    const float er0 = ns[kNsEr * MO], ir0 = ns[kNsIr * MO], ed0 = ns[kNsEd * MO], id0 = ns[kNsId * MO];
+    float istim = ns[kNsIstim * MO];
+    float v = ns[kNsV * MO];
+    uint32_t refrac = __float_as_uint(ns[kNsRefrac * MO]);
     if (has_dot) {
         // background of the previous step plus the previous step's propagation
         // (cublasSgemv y = A x + y, kernel_connection_propagate.cu:79-94)
-        ge_used = ge_used + sm.dot[i];
-        gi_used = gi_used + sm.dot[max_own + i];
+        const uint32_t nwarps = blockDim.x >> 5;
+        ge_used = ge_used + dot_of(sm, 0u, i, MO, nwarps);
+        gi_used = gi_used + dot_of(sm, 1u, i, MO, nwarps);
     }
 
     // ---- kernel_update_background_conductances (kernel_neuron_group_evolve.cu:11-83) ----
@@ -385,17 +405,17 @@ __device__ __forceinline__ void neuron_phase(const DSim* S, const Desc& D, const
     }
 
     // ---- stores ----
-    S->bg_er[j] = er;
-    S->bg_ed[j] = ed;
-    S->bg_ir[j] = ir;
-    S->bg_id[j] = id;
-    S->bg_ge[j] = bg_ge;
-    S->bg_gi[j] = bg_gi;
-    S->v[j] = v;
-    S->refrac[j] = refrac;
-    S->ge[j] = bg_ge;  // reset for the next propagation (kernel_neuron_group_evolve.cu:126-129)
-    S->gi[j] = bg_gi;
-    S->spikes[par][j] = spike;
+    ns[kNsEr * MO] = er;
+    ns[kNsEd * MO] = ed;
+    ns[kNsIr * MO] = ir;
+    ns[kNsId * MO] = id;
+    ns[kNsBgGe * MO] = bg_ge;
+    ns[kNsBgGi * MO] = bg_gi;
+    ns[kNsV * MO] = v;
+    ns[kNsRefrac * MO] = __uint_as_float(refrac);
+    ns[kNsGe * MO] = bg_ge;  // reset for the next propagation (kernel_neuron_group_evolve.cu:126-129)
+    ns[kNsGi * MO] = bg_gi;
+    ns[kNsSpike * MO] = __uint_as_float(spike);
     if (spike) atomicOr(&sm.gbits[par * (max_own / 32u + 2u) + (j >> 5) - (cta.n0 >> 5)], 1u << (j & 31u));
 
     // Stimulus::apply / kernel_stimulus_apply (stimulus.cpp:46-60, kernel_stimulus_apply.cu:7-21):
@@ -407,69 +427,61 @@ __device__ __forceinline__ void neuron_phase(const DSim* S, const Desc& D, const
             if (S->ev_neuron[mid] < j) lo = mid + 1;
             else hi = mid;
         }
-        bool any = false;
-        for (uint32_t k = lo; k < ev_hi && S->ev_neuron[k] == j; ++k) {
-            istim = istim + S->ev_delta[k];
-            any = true;
-        }
-        if (any) S->istim[j] = istim;
+        for (uint32_t k = lo; k < ev_hi && S->ev_neuron[k] == j; ++k) istim = istim + S->ev_delta[k];
+        ns[kNsIstim * MO] = istim;
     }
 
     // Connection traces (kernel_connection_propagate.cu:8-46): decay d, decay r, +norm on spike.
 #pragma unroll
-    for (int k = 0; k < kR; ++k) {
+    for (int k = 0; k < kMaxGroupRoles; ++k) {
         if (k >= static_cast<int>(G.n_ts)) break;
         const DTraceSet& TS = D.ts[G.ts[k]];
-        const float r_in = ts_r[k];
-        const float d_in = ts_d[k];
-        float d = flush_tiny(d_in * TS.d_decay);
-        float r = flush_tiny(r_in * TS.r_decay);
+        float* f = ns + (L.ts + 2u * k) * MO;
+        float d = flush_tiny(f[MO] * TS.d_decay);
+        float r = flush_tiny(f[0] * TS.r_decay);
         if (spike == 1) {
             r += TS.norm;
             d += TS.norm;
         }
-        TS.r[loc] = r;
-        TS.d[loc] = d;
-        TS.x[loc] = d - r;
+        f[0] = r;
+        f[MO] = d;
         sm.xown[static_cast<uint32_t>(G.ts[k]) * max_own + i] = d - r;
     }
 
     // Plasticity traces as presynaptic neuron: decay (the value the weight update uses), row
     // factors for that update, then the spike increment (kernel_*_plasticity_update.cu).
 #pragma unroll
-    for (int k = 0; k < kR; ++k) {
+    for (int k = 0; k < kMaxGroupRoles; ++k) {
         if (k >= static_cast<int>(G.n_plast_pre)) break;
         const DPlast& P = D.plast[G.plast_pre[k]];
-        const float pre_in = pre0[k];
-        const float pre = flush_tiny(pre_in * P.pre_decay);
+        float* f = ns + (L.pre + 2u * k) * MO;
+        const float pre = flush_tiny(f[0] * P.pre_decay);
         float rowA, rowB;
         if (P.kind == kKindTriplet) {
-            const float tpre_in = tpre0[k];
-            const float tpre = flush_tiny(tpre_in * P.tpre_decay);
+            const float tpre = flush_tiny(f[MO] * P.tpre_decay);
             rowA = pre;
             rowB = P.ltd_A + (P.ltd_B * tpre);
-            P.tpre[loc] = spike == 1 ? tpre + 1.0f : tpre;
+            f[MO] = spike == 1 ? tpre + 1.0f : tpre;
         } else {
             rowA = pre;
             rowB = -1.0f * P.ltd_A;
         }
         sm.rowfac[(par * D.n_plast + static_cast<uint32_t>(G.plast_pre[k])) * max_own + i] = make_float2(rowA, rowB);
-        P.pre[loc] = spike == 1 ? pre + 1.0f : pre;
+        f[0] = spike == 1 ? pre + 1.0f : pre;
     }
-    // ... and as postsynaptic neuron: column factors.
+    // ... and as postsynaptic neuron: column factors, which other CTAs read.
 #pragma unroll
-    for (int k = 0; k < kR; ++k) {
+    for (int k = 0; k < kMaxGroupRoles; ++k) {
         if (k >= static_cast<int>(G.n_plast_post)) break;
         const DPlast& P = D.plast[G.plast_post[k]];
-        const float post_in = post0[k];
-        const float post = flush_tiny(post_in * P.post_decay);
+        float* f = ns + (L.post + 2u * k) * MO;
+        const float post = flush_tiny(f[0] * P.post_decay);
         float colA, colB;
         if (P.kind == kKindTriplet) {
-            const float tpost_in = tpost0[k];
-            const float tpost = flush_tiny(tpost_in * P.tpost_decay);
+            const float tpost = flush_tiny(f[MO] * P.tpost_decay);
             colA = P.ltp_A + (P.ltp_B * tpost);
             colB = -1.0f * post;
-            P.tpost[loc] = spike == 1 ? tpost + 1.0f : tpost;
+            f[MO] = spike == 1 ? tpost + 1.0f : tpost;
         } else if (P.kind == kKindIstdp) {
             colA = P.ltp_A;
             colB = post - P.ltd_B;
@@ -479,10 +491,11 @@ __device__ __forceinline__ void neuron_phase(const DSim* S, const Desc& D, const
         }
         P.colA[par][loc] = colA;
         P.colB[par][loc] = colB;
-        P.post[loc] = spike == 1 ? post + 1.0f : post;
+        f[0] = spike == 1 ? post + 1.0f : post;
     }
 
     // Monitors (kernel_historicize_spikes.cu:7-21, kernel_historicize_membrane_potentials.cu:7-21).
+    uint32_t vk = 0;  // voltage monitors seen so far (their ring columns are ns fields)
     for (uint32_t k = 0; k < G.n_mon; ++k) {
         const int m = G.mon[k];
         const DMon& M = D.mons[m];
@@ -492,8 +505,95 @@ __device__ __forceinline__ void neuron_phase(const DSim* S, const Desc& D, const
                 atomicOr(&sm.bits[D.bitbase[m] + ((loc >> 5) - w0)], 1u << (loc & 31u));
             }
         } else {
-            const int32_t col = M.sel_idx[loc];
+            const int32_t col = __float_as_int(ns[(L.mon + vk) * MO]);
+            ++vk;
             if (col >= 0) M.vh[static_cast<size_t>(clock % M.interval) * M.n_sel + col] = v;
+        }
+    }
+}
+
+// Copies the own neurons' state between global memory and the shared-memory copy (launch
+// prologue: to_smem; finalize: back, with the pending propagation added to g and x = d - r).
+__device__ __forceinline__ void move_neuron_state(const DSim* S, const Desc& D, const DCta& cta, const SmemLayout& sm,
+                                               uint32_t max_own, const NsLayout& L, bool to_smem, uint32_t spar,
+                                               bool add_dot) {
+    const uint32_t MO = max_own, nwarps = blockDim.x >> 5;
+    for (uint32_t i = threadIdx.x; i < cta.n1 - cta.n0; i += blockDim.x) {
+        const uint32_t j = cta.n0 + i;
+        const int g = group_of(D, j);
+        if (g < 0) continue;
+        const DGroup& G = D.groups[g];
+        const uint32_t loc = j - G.off;
+        float* ns = sm.ns + i;
+        if (to_smem) {
+            ns[kNsV * MO] = S->v[j];
+            ns[kNsGe * MO] = S->ge[j];
+            ns[kNsGi * MO] = S->gi[j];
+            ns[kNsIstim * MO] = S->istim[j];
+            ns[kNsEr * MO] = S->bg_er[j];
+            ns[kNsEd * MO] = S->bg_ed[j];
+            ns[kNsIr * MO] = S->bg_ir[j];
+            ns[kNsId * MO] = S->bg_id[j];
+            ns[kNsBgGe * MO] = S->bg_ge[j];
+            ns[kNsBgGi * MO] = S->bg_gi[j];
+            ns[kNsRefrac * MO] = __uint_as_float(S->refrac[j]);
+            ns[kNsSpike * MO] = 0.0f;
+        } else {
+            S->v[j] = ns[kNsV * MO];
+            S->ge[j] = add_dot ? ns[kNsGe * MO] + dot_of(sm, 0u, i, MO, nwarps) : ns[kNsGe * MO];
+            S->gi[j] = add_dot ? ns[kNsGi * MO] + dot_of(sm, 1u, i, MO, nwarps) : ns[kNsGi * MO];
+            S->istim[j] = ns[kNsIstim * MO];
+            S->bg_er[j] = ns[kNsEr * MO];
+            S->bg_ed[j] = ns[kNsEd * MO];
+            S->bg_ir[j] = ns[kNsIr * MO];
+            S->bg_id[j] = ns[kNsId * MO];
+            S->bg_ge[j] = ns[kNsBgGe * MO];
+            S->bg_gi[j] = ns[kNsBgGi * MO];
+            S->refrac[j] = __float_as_uint(ns[kNsRefrac * MO]);
+            S->spikes[spar][j] = __float_as_uint(ns[kNsSpike * MO]);
+        }
+        for (uint32_t k = 0; k < G.n_ts; ++k) {
+            const DTraceSet& TS = D.ts[G.ts[k]];
+            float* f = ns + (L.ts + 2u * k) * MO;
+            if (to_smem) {
+                f[0] = TS.r[loc];
+                f[MO] = TS.d[loc];
+            } else {
+                TS.r[loc] = f[0];
+                TS.d[loc] = f[MO];
+                TS.x[loc] = f[MO] - f[0];
+            }
+        }
+        for (uint32_t k = 0; k < G.n_plast_pre; ++k) {
+            const DPlast& P = D.plast[G.plast_pre[k]];
+            float* f = ns + (L.pre + 2u * k) * MO;
+            if (to_smem) {
+                f[0] = P.pre[loc];
+                f[MO] = P.kind == kKindTriplet ? P.tpre[loc] : 0.0f;
+            } else {
+                P.pre[loc] = f[0];
+                if (P.kind == kKindTriplet) P.tpre[loc] = f[MO];
+            }
+        }
+        for (uint32_t k = 0; k < G.n_plast_post; ++k) {
+            const DPlast& P = D.plast[G.plast_post[k]];
+            float* f = ns + (L.post + 2u * k) * MO;
+            if (to_smem) {
+                f[0] = P.post[loc];
+                f[MO] = P.kind == kKindTriplet ? P.tpost[loc] : 0.0f;
+            } else {
+                P.post[loc] = f[0];
+                if (P.kind == kKindTriplet) P.tpost[loc] = f[MO];
+            }
+        }
+        if (to_smem) {
+            uint32_t vk = 0;
+            for (uint32_t k = 0; k < G.n_mon; ++k) {
+                const DMon& M = D.mons[G.mon[k]];
+                if (M.kind == kMonSpikes) continue;
+                ns[(L.mon + vk) * MO] = __int_as_float(M.sel_idx[loc]);
+                ++vk;
+            }
         }
     }
 }
@@ -542,20 +642,18 @@ __device__ __forceinline__ void flush_spike_bits(const DSim* S, const Desc& D, c
     }
 }
 
-// Per-row data for phase B (x of this step, the pending plasticity's row factors, the presynaptic
-// spike) and the staged network-wide spike bitmask of the step whose plasticity is pending.
-__device__ __forceinline__ void build_rows(const DSim* S, const Desc& D, const DCta& cta, bool pending, uint32_t ppar,
-                                        const SmemLayout& sm, bool with_x) {
-    if (pending)
-        for (uint32_t w = threadIdx.x; w < S->spk_words; w += blockDim.x) sm.sbits[w] = __ldcg(S->spk_bits[ppar] + w);
-    const uint32_t max_own = S->max_own, n_gbits = max_own / 32u + 2u;
+// Per-row data of the pending plasticity update for phase B and the normalisation pass: the row
+// factors and the presynaptic spike of the step being applied (both from shared memory); the
+// row scale starts at 1 and x at 0.
+__device__ __forceinline__ void rows_pending(const Desc& D, const DCta& cta, bool pending, uint32_t ppar,
+                                          const SmemLayout& sm, uint32_t max_own) {
+    const uint32_t n_gbits = max_own / 32u + 2u;
     for (uint32_t r = threadIdx.x; r < cta.n_rows; r += blockDim.x) {
         const DRowMeta meta = sm.meta[r];
         const DConn& C = D.conns[meta.conn];
         const uint32_t i = meta.j - cta.n0;  // rows belong to this CTA's own neurons
         float4 row = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
         uint32_t flag = 0;
-        if (with_x) row.x = sm.xown[static_cast<uint32_t>(C.ts) * max_own + i];
         if (pending && C.plast >= 0) {
             const float2 f = sm.rowfac[(ppar * D.n_plast + static_cast<uint32_t>(C.plast)) * max_own + i];
             row.y = f.x;
@@ -565,6 +663,20 @@ __device__ __forceinline__ void build_rows(const DSim* S, const Desc& D, const D
         sm.row[r] = row;
         sm.rowflag[r] = flag;
     }
+}
+
+// x = d - r of this step into the row table (after the neuron phase).
+__device__ __forceinline__ void rows_x(const Desc& D, const DCta& cta, const SmemLayout& sm, uint32_t max_own) {
+    for (uint32_t r = threadIdx.x; r < cta.n_rows; r += blockDim.x) {
+        const DRowMeta meta = sm.meta[r];
+        const DConn& C = D.conns[meta.conn];
+        sm.row[r].x = sm.xown[static_cast<uint32_t>(C.ts) * max_own + (meta.j - cta.n0)];
+    }
+}
+
+// Stages the network-wide spike bitmask of step parity `spar` in shared memory.
+__device__ __forceinline__ void stage_spike_bits(const DSim* S, uint32_t spar, const SmemLayout& sm) {
+    for (uint32_t w = threadIdx.x; w < S->spk_words; w += blockDim.x) sm.sbits[w] = __ldcg(S->spk_bits[spar] + w);
 }
 
 __device__ __forceinline__ float4 ld_col4(const float* p) { return __ldcg(reinterpret_cast<const float4*>(p)); }
@@ -625,11 +737,12 @@ __device__ __forceinline__ void sts4(uint32_t a, float4 v) {
 }
 __device__ __forceinline__ uint32_t saddr(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
 
-// Pass 1 of the triplet normalisation, one warp per row: each lane sums its units of the updated
-// row (units lane, lane+32, ...), then an xor-butterfly; lane 0 forms target / sum.
+// Pass 1 of the triplet normalisation, one warp per row on warps [w_first, w_first + nwarps): each
+// lane sums its units of the updated row (units lane, lane+32, ...), then an xor-butterfly; lane 0
+// forms target / sum.
 __device__ __forceinline__ void norm_rows(const DSim* S, const Desc& D, uint32_t ppar, const SmemLayout& sm,
-                                       const DBlk* s_blk, uint32_t nblk) {
-    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u, nwarps = blockDim.x >> 5;
+                                       const DBlk* s_blk, uint32_t nblk, uint32_t w_first, uint32_t nwarps) {
+    const uint32_t warp = (threadIdx.x >> 5) - w_first, lane = threadIdx.x & 31u;
     uint32_t k = 0;  // running index over the CTA's normalised rows
     for (uint32_t bk = 0; bk < nblk; ++bk) {
         const DBlk B = s_blk[bk];
@@ -807,17 +920,19 @@ __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* _
     __shared__ DCta s_cta;
     __shared__ DSeg s_seg[kMaxSegsPerCta];
     __shared__ DBlk s_blk[kMaxBlksPerCta];
-    __shared__ unsigned long long s_t0;
+    __shared__ unsigned long long s_t0, s_bar0;
     __shared__ uint32_t s_clock0;
     __shared__ int s_ok;
     __shared__ uint32_t s_has_norm;
     __shared__ uint32_t s_blk_base, s_nblk;
+    __shared__ uint32_t s_ev[2];
 
     const uint32_t max_rows = S->max_rows, max_own = S->max_own;
     uint32_t n_spike_mons = 0;
     for (uint32_t m = 0; m < S->n_mons; ++m) n_spike_mons += S->mons[m].kind == kMonSpikes ? 1u : 0u;
+    const NsLayout L = ns_layout(S->ns_ts, S->ns_pre, S->ns_post, S->ns_mon);
     const SmemSizes z = smem_sizes(S->resident_floats, max_rows, max_own, S->spk_words, n_spike_mons, S->n_groups,
-                                   S->n_ts, S->n_conns, S->n_plast, S->n_mons, S->n_red);
+                                   S->n_ts, S->n_conns, S->n_plast, S->n_mons, S->n_red, L.fields);
     SmemLayout sm;
     {
         unsigned char* p = smem_raw;
@@ -839,8 +954,8 @@ __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* _
         p += z.xown;
         sm.rowfac = reinterpret_cast<float2*>(p);
         p += z.rowfac;
-        sm.dot = reinterpret_cast<float*>(p);
-        p += z.dot;
+        sm.ns = reinterpret_cast<float*>(p);
+        p += z.ns;
         sm.red = reinterpret_cast<float*>(p);
         p += z.redscr;
         sm.bits = reinterpret_cast<uint32_t*>(p);
@@ -900,6 +1015,11 @@ __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* _
         s_cta = S->ctas[blockIdx.x];
         s_t0 = *S->steps_done;
         s_clock0 = *S->clock;
+        // Every launch completes all of its barriers, so between launches the arrival counter is a
+        // multiple of the grid size; CTAs of this launch that already arrived at its first barrier
+        // (fewer than the grid size, since this CTA has not) do not change the rounded-down value.
+        const unsigned long long n = gridDim.x;
+        s_bar0 = ld_acquire_u64(S->barrier) / n * n;
         uint32_t has_norm = 0;
         // Segments index the global block list; rebase them onto this CTA's copy in s_blk.
         const uint32_t blk_base = s_cta.seg_end > s_cta.seg_begin ? S->segs[s_cta.seg_begin].blk_begin : 0u;
@@ -920,6 +1040,11 @@ __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* _
     const Desc& D = s_d;
     const DCta cta = s_cta;
     const uint32_t n_seg = cta.seg_end - cta.seg_begin;
+    const uint32_t nwarps = blockDim.x >> 5;
+    const uint32_t n_own = cta.n1 - cta.n0;
+    const uint32_t neuron_warps = (n_own + 31u) / 32u;
+    // The normalisation pass runs beside the neuron phase on the warps the neurons leave free.
+    const bool norm_beside = neuron_warps < nwarps;
     for (uint32_t b = threadIdx.x; b < s_nblk; b += blockDim.x) s_blk[b] = S->blks[s_blk_base + b];
     {
         const DRowMeta* rows = S->rows + S->rows_begin[blockIdx.x];
@@ -929,6 +1054,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* _
     const uint32_t n_gbits = max_own / 32u + 2u;
     __syncthreads();
     move_resident(D, s_blk, s_nblk, sm, true);
+    move_neuron_state(S, D, cta, sm, max_own, L, true, 0u, false);
     // triplet normalisation targets of this CTA's rows (constant for the launch)
     for (uint32_t r = threadIdx.x; r < cta.n_rows; r += blockDim.x) {
         const DRowMeta meta = sm.meta[r];
@@ -938,7 +1064,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* _
     }
     __syncthreads();
 
-    const unsigned long long t0 = s_t0;
+    const unsigned long long t0 = s_t0, bar0 = s_bar0;
     const uint32_t clock0 = s_clock0;
     bool ok = true;
 #ifdef BSNN_PHASE_TIMING
@@ -950,27 +1076,54 @@ __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* _
         const uint32_t par = static_cast<uint32_t>(t & 1ull), ppar = par ^ 1u;
         const bool pending = k > 0;  // the previous step's plasticity and partials are outstanding
 
-        if (pending) reduce_partials(S, D, cta, ppar, sm, max_own);
-        for (uint32_t w = threadIdx.x; w < n_bits_words; w += blockDim.x) sm.bits[w] = 0u;
-        for (uint32_t w = threadIdx.x; w < n_gbits; w += blockDim.x) sm.gbits[par * n_gbits + w] = 0u;
+        // Global inputs of the step, issued together: the spike bitmask of the previous step, the
+        // stimulus range of this step and the previous step's partial sums.
+        const uint32_t tid = threadIdx.x, nthr = blockDim.x, spk_words = S->spk_words;
+        uint32_t sb0 = 0, sb1 = 0, ev_lo = 0, ev_hi = 0;
+        if (pending) {
+            if (tid < spk_words) sb0 = __ldcg(S->spk_bits[ppar] + tid);
+            if (tid + nthr < spk_words) sb1 = __ldcg(S->spk_bits[ppar] + tid + nthr);
+        }
+        if (tid == 0 && t < D.stim_len) {
+            ev_lo = __ldg(S->stim_off + t);
+            ev_hi = __ldg(S->stim_off + t + 1);
+        }
+        if (pending) load_partials(S, D, cta, ppar, sm, max_own);
+        if (pending) {
+            if (tid < spk_words) sm.sbits[tid] = sb0;
+            if (tid + nthr < spk_words) sm.sbits[tid + nthr] = sb1;
+            for (uint32_t w = tid + 2u * nthr; w < spk_words; w += nthr) sm.sbits[w] = __ldcg(S->spk_bits[ppar] + w);
+        }
+        if (tid == 0) {
+            s_ev[0] = ev_lo;
+            s_ev[1] = ev_hi;
+        }
+        rows_pending(D, cta, pending, ppar, sm, max_own);
+        for (uint32_t w = tid; w < n_bits_words; w += nthr) sm.bits[w] = 0u;
+        for (uint32_t w = tid; w < n_gbits; w += nthr) sm.gbits[par * n_gbits + w] = 0u;
         __syncthreads();
         BSNN_TMARK(0);
-        neuron_phase(S, D, cta, t, clock, par, pending, sm, max_own);
+        const bool norm_now = pending && s_has_norm;
+        if (tid < 32u * neuron_warps) {
+            neuron_phase(S, D, cta, t, clock, par, pending, sm, max_own, L, s_ev[0], s_ev[1]);
+        } else if (norm_now && norm_beside) {
+            norm_rows(S, D, ppar, sm, s_blk, s_nblk, neuron_warps, nwarps - neuron_warps);
+        }
         __syncthreads();
         BSNN_TMARK(1);
-        flush_spike_bits(S, D, cta, clock, par, sm);
-        build_rows(S, D, cta, pending, ppar, sm, true);
-        __syncthreads();
-        BSNN_TMARK(2);
-        if (pending && s_has_norm) {
-            norm_rows(S, D, ppar, sm, s_blk, s_nblk);
+        if (norm_now && !norm_beside) {
+            norm_rows(S, D, ppar, sm, s_blk, s_nblk, 0u, nwarps);
             __syncthreads();
         }
+        flush_spike_bits(S, D, cta, clock, par, sm);
+        rows_x(D, cta, sm, max_own);
+        __syncthreads();
+        BSNN_TMARK(2);
         BSNN_TMARK(3);
         weight_pass(S, D, cta, pending, ppar, true, par, sm, s_seg, s_blk, n_seg);
         __syncthreads();
         BSNN_TMARK(4);
-        if (!grid_barrier(S, &s_ok)) {
+        if (!grid_barrier(S, bar0 + (k + 1ull) * gridDim.x, &s_ok)) {
             ok = false;
             break;
         }
@@ -978,27 +1131,23 @@ __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* _
     }
     if (!ok) return;
 
-    // Finalize: apply the last step's plasticity, write resident rows back, and fold the last
-    // propagation into g.
+    // Finalize: apply the last step's plasticity, write resident rows and the neuron state back,
+    // and fold the last propagation into g.
     const unsigned long long t_last = t0 + n_steps - 1ull;
     const uint32_t lpar = static_cast<uint32_t>(t_last & 1ull);
-    build_rows(S, D, cta, true, lpar, sm, false);
+    stage_spike_bits(S, lpar, sm);
+    rows_pending(D, cta, true, lpar, sm, max_own);
     __syncthreads();
     if (s_has_norm) {
-        norm_rows(S, D, lpar, sm, s_blk, s_nblk);
+        norm_rows(S, D, lpar, sm, s_blk, s_nblk, 0u, nwarps);
         __syncthreads();
     }
     weight_pass(S, D, cta, true, lpar, false, lpar, sm, s_seg, s_blk, n_seg);
     __syncthreads();
     move_resident(D, s_blk, s_nblk, sm, false);
-    reduce_partials(S, D, cta, lpar, sm, max_own);
+    load_partials(S, D, cta, lpar, sm, max_own);
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < cta.n1 - cta.n0; i += blockDim.x) {
-        const uint32_t j = cta.n0 + i;
-        if (group_of(D, j) < 0) continue;
-        S->ge[j] = S->ge[j] + sm.dot[i];
-        S->gi[j] = S->gi[j] + sm.dot[max_own + i];
-    }
+    move_neuron_state(S, D, cta, sm, max_own, L, false, lpar, true);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         *S->steps_done = t0 + n_steps;
         *S->clock = clock0 + n_steps;
