@@ -190,9 +190,11 @@ int group_of_host(const bsnn_sim* s, uint32_t j) {
 }
 
 // Partitions the neurons into n_ctas contiguous ranges balancing `cost`; when `cap_bytes` > 0 the
-// plastic rows of every range must also fit in cap_bytes of shared memory (returns false if not).
-bool greedy_partition(const std::vector<double>& cost, const std::vector<uint64_t>& res_bytes, uint32_t n_ctas,
-                      double max_cost, uint64_t cap_bytes, std::vector<uint32_t>& bounds) {
+// plastic rows of every range must also fit in cap_bytes of shared memory, and neurons flagged in
+// `cut` must start a range (returns false if not possible).
+bool greedy_partition(const std::vector<double>& cost, const std::vector<uint64_t>& res_bytes,
+                      const std::vector<char>& cut, uint32_t n_ctas, double max_cost, uint64_t cap_bytes,
+                      std::vector<uint32_t>& bounds) {
     const uint32_t N = static_cast<uint32_t>(cost.size());
     bounds.assign(n_ctas + 1, N);
     bounds[0] = 0;
@@ -201,7 +203,8 @@ bool greedy_partition(const std::vector<double>& cost, const std::vector<uint64_
     uint64_t acc_res = 0;
     for (uint32_t j = 0; j < N; ++j) {
         if (cost[j] > max_cost || (cap_bytes > 0 && res_bytes[j] > cap_bytes)) return false;
-        if (acc + cost[j] > max_cost || (cap_bytes > 0 && acc_res + res_bytes[j] > cap_bytes)) {
+        if ((cut[j] && j > 0 && acc > 0.0) || acc + cost[j] > max_cost ||
+            (cap_bytes > 0 && acc_res + res_bytes[j] > cap_bytes)) {
             if (++c >= n_ctas) return false;
             bounds[c] = j;
             acc = 0.0;
@@ -216,23 +219,25 @@ bool greedy_partition(const std::vector<double>& cost, const std::vector<uint64_
 
 // Contiguous partition of the neurons into n_ctas ranges that minimises the largest per-range
 // cost (binary search on that maximum); with cap_bytes > 0 every range's plastic rows must also
-// fit in cap_bytes of shared memory.  Returns false if no such partition exists.
-bool partition(const std::vector<double>& cost, const std::vector<uint64_t>& res_bytes, uint32_t n_ctas,
-               uint64_t cap_bytes, std::vector<uint32_t>& bounds) {
+// fit in cap_bytes of shared memory, and every range holds neurons of one group only (a range
+// that spans two groups carries both groups' work and slows the whole grid).  Returns false if
+// no such partition exists.
+bool partition(const std::vector<double>& cost, const std::vector<uint64_t>& res_bytes, const std::vector<char>& cut,
+               uint32_t n_ctas, uint64_t cap_bytes, std::vector<uint32_t>& bounds) {
     double total = 0.0, biggest = 0.0;
     for (double c : cost) {
         total += c;
         biggest = std::max(biggest, c);
     }
     double lo = std::max(biggest, total / n_ctas), hi = total + 1.0;
-    if (!greedy_partition(cost, res_bytes, n_ctas, hi, cap_bytes, bounds)) return false;
+    if (!greedy_partition(cost, res_bytes, cut, n_ctas, hi, cap_bytes, bounds)) return false;
     for (int it = 0; it < 60 && hi - lo > 1e-6 * hi; ++it) {
         const double mid = 0.5 * (lo + hi);
         std::vector<uint32_t> b;
-        if (greedy_partition(cost, res_bytes, n_ctas, mid, cap_bytes, b)) hi = mid;
+        if (greedy_partition(cost, res_bytes, cut, n_ctas, mid, cap_bytes, b)) hi = mid;
         else lo = mid;
     }
-    return greedy_partition(cost, res_bytes, n_ctas, hi, cap_bytes, bounds);
+    return greedy_partition(cost, res_bytes, cut, n_ctas, hi, cap_bytes, bounds);
 }
 
 Plan build_plan(const bsnn_sim* s, uint32_t n_ctas, uint64_t cap_bytes, bool* resident_ok) {
@@ -267,8 +272,13 @@ Plan build_plan(const bsnn_sim* s, uint32_t n_ctas, uint64_t cap_bytes, bool* re
         }
     }
     std::vector<uint32_t> bounds;
-    bool resident = cap_bytes > 0 && partition(cost, res_bytes, n_ctas, cap_bytes, bounds);
-    if (!resident) partition(cost, res_bytes, n_ctas, 0, bounds);
+    std::vector<char> cut(N, 0), no_cut(N, 0);
+    for (const auto& g : s->groups)
+        if (g.p.offset < N) cut[g.p.offset] = 1;
+    bool resident = cap_bytes > 0 && (partition(cost, res_bytes, cut, n_ctas, cap_bytes, bounds) ||
+                                      partition(cost, res_bytes, no_cut, n_ctas, cap_bytes, bounds));
+    if (!resident && !partition(cost, res_bytes, cut, n_ctas, 0, bounds))
+        partition(cost, res_bytes, no_cut, n_ctas, 0, bounds);
     if (resident_ok) *resident_ok = resident;
 
     // Slot bookkeeping: slot of (cta, target), and which (target, group) each CTA feeds.

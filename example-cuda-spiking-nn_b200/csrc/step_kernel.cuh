@@ -102,6 +102,8 @@ __device__ __forceinline__ uint32_t poisson_knuth(float exp_neg_mean, uint32_t s
     return k;
 }
 
+__device__ __forceinline__ float4 ld_col4(const float* p) { return __ldcg(reinterpret_cast<const float4*>(p)); }
+
 __device__ __forceinline__ float flush_tiny(float t) { return t < 1e-30f ? 0.0f : t; }
 
 __device__ __forceinline__ float clamp_w(float w, float wmin, float wmax) {
@@ -120,24 +122,25 @@ __device__ __forceinline__ void red_release_add_u64(unsigned long long* p, unsig
 // count at which every CTA has arrived; the closing CTA-wide sync extends the acquire to the
 // whole CTA.  Bounded: after kBarrierTimeoutNs (or when another CTA has already given up) it
 // records kErrBarrierTimeout and returns false so the kernel can exit.
-__device__ __forceinline__ bool grid_barrier(const DSim* S, unsigned long long target, int* s_ok) {
+__device__ __forceinline__ bool grid_barrier(unsigned long long* barrier, int32_t* error, unsigned long long target,
+                                             int* s_ok) {
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
-        red_release_add_u64(S->barrier, 1ull);
+        red_release_add_u64(barrier, 1ull);
         unsigned long long t_start = 0;
         uint32_t spins = 0;
-        while (static_cast<long long>(ld_acquire_u64(S->barrier) - target) < 0) {
+        while (static_cast<long long>(ld_acquire_u64(barrier) - target) < 0) {
             if ((++spins & 255u) == 0u) {
                 const unsigned long long now = globaltimer_ns();
                 if (t_start == 0) {
                     t_start = now;
                 } else if (now - t_start > kBarrierTimeoutNs) {
-                    atomicExch(S->error, kErrBarrierTimeout);
+                    atomicExch(error, kErrBarrierTimeout);
                     ok = 0;
                     break;
                 }
-                if (ld_relaxed_s32(S->error) != kErrNone) {
+                if (ld_relaxed_s32(error) != kErrNone) {
                     ok = 0;
                     break;
                 }
@@ -150,13 +153,16 @@ __device__ __forceinline__ bool grid_barrier(const DSim* S, unsigned long long t
 }
 
 // Optional phase timing (profiling builds only, -DBSNN_PHASE_TIMING): thread 0 of every CTA adds
-// the SM clock cycles spent in each phase to S->phase_ns[cta * 8 + phase].
+// the SM clock cycles spent in each phase to a shared-memory tally (s_tally_[phase]) that the
+// kernel adds to S->phase_ns[cta * 8 + phase] when it ends: 3 partial-sum loads, 0 rest of the
+// step inputs, 6 plasticity updates, 1 neuron phase and normalisation, 2 spike bits and row x,
+// 4 weight pass, 5 grid barrier.
 #ifdef BSNN_PHASE_TIMING
 #define BSNN_TMARK(slot)                                                                   \
     do {                                                                                   \
         if (threadIdx.x == 0) {                                                            \
             const unsigned long long now_ = static_cast<unsigned long long>(clock64());    \
-            S->phase_ns[blockIdx.x * 8u + (slot)] += now_ - t_mark_;                        \
+            s_tally_[(slot)] += now_ - t_mark_;                                            \
             t_mark_ = now_;                                                                \
         }                                                                                  \
     } while (0)
@@ -182,6 +188,16 @@ struct Desc {
     uint32_t goff[kMaxGroups], gn[kMaxGroups];
     uint32_t bitbase[kMaxMonitors];
     uint32_t red_begin[2][kMaxGroups], red_end[2][kMaxGroups];
+    // DSim pointers and sizes the step loop uses (read from shared memory, not through DSim)
+    float* partials;
+    uint32_t n_slots, N_pad, spk_words, max_own;
+    uint32_t* spk_bits[2];
+    const uint32_t* stim_off;
+    const uint32_t* ev_neuron;
+    const float* ev_delta;
+    const uint8_t* replay;
+    unsigned long long* barrier;
+    int32_t* error;
 };
 
 // Values produced and consumed by the same CTA stay in shared memory: x of the own neurons, the
@@ -189,7 +205,7 @@ struct Desc {
 // while the weight pass of step t still reads step t-1's) and the own neurons' spike bits.
 struct SmemLayout {
     float* wres;        // resident weight rows, S->resident_floats floats (16-byte aligned)
-    float4* row;        // [max_rows] {x, rowA, rowB, scale}
+    float4* row;        // [max_rows] {x, scale, rowA, rowB}
     DRowMeta* meta;     // [max_rows]
     uint32_t* rowflag;  // [max_rows] presynaptic neuron spiked at the step being applied
     float* rowtgt;      // [max_rows] triplet normalisation target of the row
@@ -264,63 +280,84 @@ __device__ __forceinline__ int group_of(const Desc& D, uint32_t j) {
     return -1;
 }
 
-// The previous step's GEMV partial sums at the own neurons' columns, summed per warp:
-// red[warp][T][i] = sum over the entries k = warp, warp + nwarps, ... of the slot list of
-// (T, group of neuron n0+i), in list order; dot_of() then adds the warps in warp order, so the
-// summation order is fixed.  Lanes take consecutive neurons (coalesced reads of a slot row).  Both
-// targets' loads of a 16-entry batch are issued before any is used, so for up to 16 * nwarps
-// slots per target the whole reduction costs one round trip to L2.
+// The previous step's GEMV partial sums at the own neurons' columns: red[T][i] = sum over the
+// slots listed for (T, group of neuron n0+i) of that neuron's column.  One warp takes one quad of
+// 4 columns (quads start at multiples of 4 from the group's first column, which is 16-byte
+// aligned in the partial rows, so the first and last quad may include neighbours' columns that are
+// read and dropped); its lanes take the slot entries lane, lane + 32, ...
+// of the group's two lists taken as one sequence, each lane summing its entries in order, and an
+// xor-butterfly adds the lanes, so the summation order is fixed.  Up to 32 * kQ entries per quad
+// cost one round trip to L2.
 __device__ __forceinline__ void load_partials(const DSim* S, const Desc& D, const DCta& cta, uint32_t par,
                                               const SmemLayout& sm, uint32_t max_own) {
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u, nwarps = blockDim.x >> 5;
-    const float* part = S->partials + static_cast<size_t>(par) * S->n_slots * S->N_pad;
-    const uint32_t npad = S->N_pad;
-    constexpr int kQ = 16;
+    const float* part = D.partials + static_cast<size_t>(par) * D.n_slots * D.N_pad;
+    const uint32_t npad = D.N_pad;
+    constexpr int kQ = 8;
+    uint32_t qbase = 0;  // quads of earlier groups of this CTA, so that warps rotate over groups
     for (uint32_t g = 0; g < D.n_groups; ++g) {
         const uint32_t goff = D.goff[g], gend = goff + D.gn[g];
         const uint32_t a = cta.n0 > goff ? cta.n0 : goff, b = cta.n1 < gend ? cta.n1 : gend;
         if (a >= b) continue;
-        const uint32_t pcol = D.groups[g].pcol;
-        const uint32_t lb0 = D.red_begin[0][g], le0 = D.red_end[0][g];
-        const uint32_t lb1 = D.red_begin[1][g], le1 = D.red_end[1][g];
-        for (uint32_t j0 = a; j0 < b; j0 += 32u) {
-            const uint32_t j = j0 + lane;
-            const bool valid = j < b;
-            const float* col = part + pcol + (j - goff);
-            float s0 = 0.0f, s1 = 0.0f;
-            for (uint32_t m0 = 0; lb0 + warp + m0 * nwarps < le0 || lb1 + warp + m0 * nwarps < le1; m0 += kQ) {
-                float v0[kQ], v1[kQ];
+        const uint32_t qa = goff + ((a - goff) & ~3u);  // first column of the first quad
+        const uint32_t nq = (b - qa + 3u) / 4u;
+        const uint32_t lb0 = D.red_begin[0][g], n0 = D.red_end[0][g] - lb0;
+        const uint32_t lb1 = D.red_begin[1][g], n1 = D.red_end[1][g] - lb1;
+        const uint32_t n_all = n0 + n1;
+        const float* cols = part + D.groups[g].pcol + (qa - goff);
+        for (uint32_t qd = (warp + nwarps - qbase % nwarps) % nwarps; qd < nq; qd += nwarps) {
+            const float* col = cols + 4u * qd;
+            float4 s0 = make_float4(0.f, 0.f, 0.f, 0.f), s1 = s0;
+            for (uint32_t e0 = lane; e0 < n_all; e0 += 32u * kQ) {
+                float4 v[kQ];
 #pragma unroll
                 for (int q = 0; q < kQ; ++q) {
-                    const uint32_t k = lb0 + warp + (m0 + q) * nwarps;
-                    v0[q] = valid && k < le0 ? __ldcg(col + static_cast<size_t>(D.red_list[k]) * npad) : 0.0f;
+                    const uint32_t e = e0 + 32u * q;
+                    const uint32_t k = e < n0 ? lb0 + e : lb1 + (e - n0);
+                    v[q] = e < n_all ? ld_col4(col + static_cast<size_t>(D.red_list[k]) * npad)
+                                     : make_float4(0.f, 0.f, 0.f, 0.f);
                 }
 #pragma unroll
                 for (int q = 0; q < kQ; ++q) {
-                    const uint32_t k = lb1 + warp + (m0 + q) * nwarps;
-                    v1[q] = valid && k < le1 ? __ldcg(col + static_cast<size_t>(D.red_list[k]) * npad) : 0.0f;
+                    const uint32_t e = e0 + 32u * q;
+                    float4& acc = e < n0 ? s0 : s1;
+                    if (e < n_all) {
+                        acc.x += v[q].x;
+                        acc.y += v[q].y;
+                        acc.z += v[q].z;
+                        acc.w += v[q].w;
+                    }
                 }
-#pragma unroll
-                for (int q = 0; q < kQ; ++q)
-                    if (lb0 + warp + (m0 + q) * nwarps < le0) s0 += v0[q];
-#pragma unroll
-                for (int q = 0; q < kQ; ++q)
-                    if (lb1 + warp + (m0 + q) * nwarps < le1) s1 += v1[q];
             }
-            if (valid) {
-                sm.red[(warp * 2u + 0u) * max_own + (j - cta.n0)] = s0;
-                sm.red[(warp * 2u + 1u) * max_own + (j - cta.n0)] = s1;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                s0.x += __shfl_xor_sync(kFull, s0.x, o);
+                s0.y += __shfl_xor_sync(kFull, s0.y, o);
+                s0.z += __shfl_xor_sync(kFull, s0.z, o);
+                s0.w += __shfl_xor_sync(kFull, s0.w, o);
+                s1.x += __shfl_xor_sync(kFull, s1.x, o);
+                s1.y += __shfl_xor_sync(kFull, s1.y, o);
+                s1.z += __shfl_xor_sync(kFull, s1.z, o);
+                s1.w += __shfl_xor_sync(kFull, s1.w, o);
+            }
+            if (lane < 4u) {
+                const uint32_t j = qa + 4u * qd + lane;
+                if (j >= a && j < b) {
+                    const float t0 = lane == 0 ? s0.x : lane == 1 ? s0.y : lane == 2 ? s0.z : s0.w;
+                    const float t1 = lane == 0 ? s1.x : lane == 1 ? s1.y : lane == 2 ? s1.z : s1.w;
+                    sm.red[j - cta.n0] = t0;
+                    sm.red[max_own + (j - cta.n0)] = t1;
+                }
             }
         }
+        qbase += nq;
     }
 }
 
-// Sum of the per-warp partial sums of own neuron i for target T, in warp order.
+// The previous step's propagation into own neuron i for target T (after load_partials).
 __device__ __forceinline__ float dot_of(const SmemLayout& sm, uint32_t T, uint32_t i, uint32_t max_own,
                                         uint32_t nwarps) {
-    float s = 0.0f;
-    for (uint32_t w = 0; w < nwarps; ++w) s += sm.red[(w * 2u + T) * max_own + i];
-    return s;
+    return sm.red[T * max_own + i];
 }
 
 // Phase A: one thread per owned neuron (threads 0 .. n_own-1).  The neuron's state is read from
@@ -365,8 +402,8 @@ __device__ __forceinline__ void neuron_phase(const DSim* S, const Desc& D, const
         if (G.has_bg_i) ni = poisson_knuth(G.exp_neg_mean_i, D.seed, j, t, 1u);
     } else if (D.noise_mode == kNoiseReplay && t < D.replay_steps) {
         const size_t base = (static_cast<size_t>(t) * D.N + j) * 2u;
-        ne = S->replay[base];
-        ni = S->replay[base + 1];
+        ne = D.replay[base];
+        ni = D.replay[base + 1];
     }
     if (ne > 0u) {
         const float inc = static_cast<float>(ne);
@@ -424,10 +461,10 @@ __device__ __forceinline__ void neuron_phase(const DSim* S, const Desc& D, const
         uint32_t lo = ev_lo, hi = ev_hi;
         while (lo < hi) {  // lower_bound of j in the step's events (sorted by neuron)
             const uint32_t mid = (lo + hi) >> 1;
-            if (S->ev_neuron[mid] < j) lo = mid + 1;
+            if (D.ev_neuron[mid] < j) lo = mid + 1;
             else hi = mid;
         }
-        for (uint32_t k = lo; k < ev_hi && S->ev_neuron[k] == j; ++k) istim = istim + S->ev_delta[k];
+        for (uint32_t k = lo; k < ev_hi && D.ev_neuron[k] == j; ++k) istim = istim + D.ev_delta[k];
         ns[kNsIstim * MO] = istim;
     }
 
@@ -618,8 +655,8 @@ __device__ __forceinline__ void flush_spike_bits(const DSim* S, const Desc& D, c
     if (cta.n1 > cta.n0) {
         const uint32_t w0 = cta.n0 >> 5, w1 = (cta.n1 - 1) >> 5;
         for (uint32_t w = w0 + threadIdx.x; w <= w1; w += blockDim.x)
-            merge_bits(S->spk_bits[par] + w, range_mask(w, w0, w1, cta.n0, cta.n1),
-                       sm.gbits[par * (S->max_own / 32u + 2u) + w - w0]);
+            merge_bits(D.spk_bits[par] + w, range_mask(w, w0, w1, cta.n0, cta.n1),
+                       sm.gbits[par * (D.max_own / 32u + 2u) + w - w0]);
     }
     for (uint32_t m = 0; m < D.n_mons; ++m) {
         const DMon& M = D.mons[m];
@@ -644,7 +681,7 @@ __device__ __forceinline__ void flush_spike_bits(const DSim* S, const Desc& D, c
 
 // Per-row data of the pending plasticity update for phase B and the normalisation pass: the row
 // factors and the presynaptic spike of the step being applied (both from shared memory); the
-// row scale starts at 1 and x at 0.
+// row scale starts at 1 and x at 0 (row = {x, scale, rowA, rowB}).
 __device__ __forceinline__ void rows_pending(const Desc& D, const DCta& cta, bool pending, uint32_t ppar,
                                           const SmemLayout& sm, uint32_t max_own) {
     const uint32_t n_gbits = max_own / 32u + 2u;
@@ -652,12 +689,12 @@ __device__ __forceinline__ void rows_pending(const Desc& D, const DCta& cta, boo
         const DRowMeta meta = sm.meta[r];
         const DConn& C = D.conns[meta.conn];
         const uint32_t i = meta.j - cta.n0;  // rows belong to this CTA's own neurons
-        float4 row = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+        float4 row = make_float4(0.0f, 1.0f, 0.0f, 0.0f);
         uint32_t flag = 0;
         if (pending && C.plast >= 0) {
             const float2 f = sm.rowfac[(ppar * D.n_plast + static_cast<uint32_t>(C.plast)) * max_own + i];
-            row.y = f.x;
-            row.z = f.y;
+            row.z = f.x;
+            row.w = f.y;
             flag = (sm.gbits[ppar * n_gbits + (meta.j >> 5) - (cta.n0 >> 5)] >> (meta.j & 31u)) & 1u;
         }
         sm.row[r] = row;
@@ -675,11 +712,10 @@ __device__ __forceinline__ void rows_x(const Desc& D, const DCta& cta, const Sme
 }
 
 // Stages the network-wide spike bitmask of step parity `spar` in shared memory.
-__device__ __forceinline__ void stage_spike_bits(const DSim* S, uint32_t spar, const SmemLayout& sm) {
-    for (uint32_t w = threadIdx.x; w < S->spk_words; w += blockDim.x) sm.sbits[w] = __ldcg(S->spk_bits[spar] + w);
+__device__ __forceinline__ void stage_spike_bits(const Desc& D, uint32_t spar, const SmemLayout& sm) {
+    for (uint32_t w = threadIdx.x; w < D.spk_words; w += blockDim.x) sm.sbits[w] = __ldcg(D.spk_bits[spar] + w);
 }
 
-__device__ __forceinline__ float4 ld_col4(const float* p) { return __ldcg(reinterpret_cast<const float4*>(p)); }
 
 // The reference's per-element plasticity sequence: LTP clamp (if post spiked), then LTD clamp
 // (if pre spiked), skipping the diagonal of group-local indices.
@@ -690,32 +726,6 @@ __device__ __forceinline__ float plastic_update(float w, uint32_t q, uint32_t pl
     if (post_spk) w = clamp_w(fmaf(rowA, colA, w), wmin, wmax);
     if (pre_spk) w = clamp_w(fmaf(colB, rowB, w), wmin, wmax);
     return w;
-}
-
-// Post spikes of the 4 columns of unit u (postsynaptic group at global offset `post_off`) from the
-// staged bitmask, as a 4-bit mask.
-__device__ __forceinline__ uint32_t post_mask(const uint32_t* sbits, uint32_t post_off, uint32_t u, uint32_t n_post) {
-    const uint32_t idx = post_off + 4u * u;
-    const uint32_t w = idx >> 5, sh = idx & 31u;
-    const unsigned long long pair =
-        (static_cast<unsigned long long>(sbits[w + 1]) << 32) | static_cast<unsigned long long>(sbits[w]);
-    const uint32_t valid = n_post - 4u * u >= 4u ? 0xFu : ((1u << (n_post - 4u * u)) - 1u);
-    return static_cast<uint32_t>(pair >> sh) & valid;
-}
-
-// The pending plasticity update of the 4 weights of unit u of row pl when some spike touches them.
-// Spikes are rare, so this is out of line and loads its own factors.
-__device__ __noinline__ float4 update4_slow(float4 w4, uint32_t u, uint32_t pl, uint32_t pmask, uint32_t pre_spk,
-                                            float rowA, float rowB, const DPlast* P, uint32_t n_post, uint32_t ppar) {
-    const float4 cA = ld_col4(P->colA[ppar] + 4u * u);
-    const float4 cB = ld_col4(P->colB[ppar] + 4u * u);
-    const float wmin = P->wmin, wmax = P->wmax;
-    const uint32_t q = 4u * u;
-    w4.x = plastic_update(w4.x, q + 0u, pl, n_post, pmask & 1u, pre_spk, rowA, cA.x, cB.x, rowB, wmin, wmax);
-    w4.y = plastic_update(w4.y, q + 1u, pl, n_post, pmask & 2u, pre_spk, rowA, cA.y, cB.y, rowB, wmin, wmax);
-    w4.z = plastic_update(w4.z, q + 2u, pl, n_post, pmask & 4u, pre_spk, rowA, cA.z, cB.z, rowB, wmin, wmax);
-    w4.w = plastic_update(w4.w, q + 3u, pl, n_post, pmask & 8u, pre_spk, rowA, cA.w, cB.w, rowB, wmin, wmax);
-    return w4;
 }
 
 __device__ __forceinline__ int seg_of_item(const DSeg* s_seg, uint32_t n_seg, uint32_t it) {
@@ -737,157 +747,259 @@ __device__ __forceinline__ void sts4(uint32_t a, float4 v) {
 }
 __device__ __forceinline__ uint32_t saddr(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
 
-// Pass 1 of the triplet normalisation, one warp per row on warps [w_first, w_first + nwarps): each
-// lane sums its units of the updated row (units lane, lane+32, ...), then an xor-butterfly; lane 0
-// forms target / sum.
-__device__ __forceinline__ void norm_rows(const DSim* S, const Desc& D, uint32_t ppar, const SmemLayout& sm,
-                                       const DBlk* s_blk, uint32_t nblk, uint32_t w_first, uint32_t nwarps) {
+// Address of weight (row i of block B, column q), in shared memory for resident blocks.
+__device__ __forceinline__ float* weight_ptr(const DBlk& B, const DConn& C, const SmemLayout& sm, uint32_t i,
+                                             uint32_t q) {
+    return B.resident ? sm.wres + B.sm_off + static_cast<size_t>(i) * C.ld + q
+                      : C.w + static_cast<size_t>(B.row_begin + i) * C.ld + q;
+}
+
+// The pending plasticity update of step parity `ppar`, applied in place and only where a spike
+// touches a weight (spikes are sparse, so this pass is event-driven):
+//   column pass: every weight in the column of a postsynaptic neuron that spiked, in rows whose
+//                presynaptic neuron did not spike: LTP;
+//   row pass:    every weight in the row of a presynaptic neuron that spiked: LTP where the
+//                postsynaptic neuron spiked, then LTD.
+// The two passes touch disjoint weights, so each weight gets the reference's LTP-then-LTD
+// sequence exactly once.  The column factors come from the owners' parity buffers in global
+// memory, the row factors from the row table.
+__device__ __forceinline__ void apply_updates(const Desc& D, const DBlk* s_blk, uint32_t nblk, uint32_t ppar,
+                                           const SmemLayout& sm) {
+    const uint32_t tid = threadIdx.x, nthr = blockDim.x, warp = tid >> 5, lane = tid & 31u, nwarps = nthr >> 5;
+    for (uint32_t bk = 0; bk < nblk; ++bk) {
+        const DBlk B = s_blk[bk];
+        const DConn& C = D.conns[B.conn];
+        if (C.plast < 0) continue;
+        const DPlast& P = D.plast[C.plast];
+        const uint32_t nrows = B.row_end - B.row_begin, n_post = C.n_post, post_off = C.post_off;
+        const float* colA = P.colA[ppar];
+        const float* colB = P.colB[ppar];
+        // column pass: threads scan the bitmask words of the postsynaptic group
+        const uint32_t w0 = post_off >> 5, w1 = (post_off + n_post - 1u) >> 5;
+        for (uint32_t w = w0 + tid; w <= w1; w += nthr) {
+            uint32_t bits = sm.sbits[w];
+            if (w == w0) bits &= 0xffffffffu << (post_off & 31u);
+            if (w == w1) bits &= 0xffffffffu >> (31u - ((post_off + n_post - 1u) & 31u));
+            while (bits) {
+                const uint32_t b = __ffs(bits) - 1u;
+                bits &= bits - 1u;
+                const uint32_t q = 32u * w + b - post_off;
+                const float cA = __ldcg(colA + q), cB = __ldcg(colB + q);
+                for (uint32_t i = 0; i < nrows; ++i) {
+                    const uint32_t r = B.srow + i;
+                    if (sm.rowflag[r]) continue;  // the row pass owns this weight
+                    float* wp = weight_ptr(B, C, sm, i, q);
+                    const float4 rw = sm.row[r];
+                    *wp = plastic_update(*wp, q, B.row_begin + i, n_post, 1u, 0u, rw.z, cA, cB, rw.w, P.wmin, P.wmax);
+                }
+            }
+        }
+        // row pass: one warp per spiking row, lanes over the columns
+        for (uint32_t i = warp; i < nrows; i += nwarps) {
+            const uint32_t r = B.srow + i;
+            if (!sm.rowflag[r]) continue;
+            const float4 rw = sm.row[r];
+            for (uint32_t q = lane; q < n_post; q += 32u) {
+                const uint32_t g = post_off + q;
+                const uint32_t post_spk = (sm.sbits[g >> 5] >> (g & 31u)) & 1u;
+                float* wp = weight_ptr(B, C, sm, i, q);
+                *wp = plastic_update(*wp, q, B.row_begin + i, n_post, post_spk, 1u, rw.z, __ldcg(colA + q),
+                                     __ldcg(colB + q), rw.w, P.wmin, P.wmax);
+            }
+        }
+    }
+}
+
+// Sum of `lane`'s units (lane, lane+32, ...) of two rows at once, each as (x + y) + (z + w) per
+// unit in unit order; `two` = false sums the first row only.
+template <bool RESIDENT>
+__device__ __forceinline__ void row_pair_sums(const float* g0, const float* g1, uint32_t s0, uint32_t s1,
+                                              uint32_t units, uint32_t lane, bool two, float& sum0, float& sum1) {
+    sum0 = 0.0f;
+    sum1 = 0.0f;
+    for (uint32_t u0 = 0; u0 < units; u0 += 128u) {
+        float4 a[4], b[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t u = u0 + lane + 32u * k;
+            const bool in = u < units;
+            if constexpr (RESIDENT) {
+                a[k] = in ? lds4(s0 + 16u * u) : make_float4(0.f, 0.f, 0.f, 0.f);
+                b[k] = in && two ? lds4(s1 + 16u * u) : make_float4(0.f, 0.f, 0.f, 0.f);
+            } else {
+                a[k] = in ? ld_col4(g0 + 4u * u) : make_float4(0.f, 0.f, 0.f, 0.f);
+                b[k] = in && two ? ld_col4(g1 + 4u * u) : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (u0 + lane + 32u * k >= units) continue;
+            sum0 += (a[k].x + a[k].y) + (a[k].z + a[k].w);
+            sum1 += (b[k].x + b[k].y) + (b[k].z + b[k].w);
+        }
+    }
+}
+
+// Pass 1 of the triplet normalisation (after apply_updates), on warps [w_first, w_first + nwarps):
+// each warp takes two rows at a time; each lane sums its units of the updated rows, then an
+// xor-butterfly; lane 0 forms target / sum.
+__device__ __forceinline__ void norm_rows(const Desc& D, const SmemLayout& sm, const DBlk* s_blk, uint32_t nblk,
+                                       uint32_t w_first, uint32_t nwarps) {
     const uint32_t warp = (threadIdx.x >> 5) - w_first, lane = threadIdx.x & 31u;
     uint32_t k = 0;  // running index over the CTA's normalised rows
     for (uint32_t bk = 0; bk < nblk; ++bk) {
         const DBlk B = s_blk[bk];
         const DConn& C = D.conns[B.conn];
         if (C.plast < 0 || D.plast[C.plast].kind != kKindTriplet) continue;
-        const DPlast* P = &D.plast[C.plast];
-        const uint32_t nrows = B.row_end - B.row_begin, units = C.units, ld = C.ld, n_post = C.n_post;
-        const uint32_t post_off = C.post_off;
-        // first row of this block handled by this warp
+        const uint32_t nrows = B.row_end - B.row_begin, units = C.units, ld = C.ld;
+        // first row of this block handled by this warp; then every nwarps-th, two at a time
         const uint32_t first = (warp + nwarps - (k % nwarps)) % nwarps;
-        for (uint32_t i = first; i < nrows; i += nwarps) {
-            const uint32_t pl = B.row_begin + i, r = B.srow + i;
-            const float4 rw = sm.row[r];
-            const uint32_t pre_spk = sm.rowflag[r];
-            float sum = 0.0f;
+        for (uint32_t i = first; i < nrows; i += 2u * nwarps) {
+            const uint32_t i2 = i + nwarps;
+            const bool two = i2 < nrows;
+            float sum0, sum1;
             if (B.resident) {
-                const uint32_t base = saddr(sm.wres + B.sm_off) + 4u * ld * i;
-                for (uint32_t u0 = 0; u0 < units; u0 += 128u) {
-                    float4 wb[4];
-#pragma unroll
-                    for (int b = 0; b < 4; ++b) {
-                        const uint32_t u = u0 + lane + 32u * b;
-                        wb[b] = u < units ? lds4(base + 16u * u) : make_float4(0.f, 0.f, 0.f, 0.f);
-                    }
-#pragma unroll
-                    for (int b = 0; b < 4; ++b) {
-                        const uint32_t u = u0 + lane + 32u * b;
-                        if (u >= units) continue;
-                        float4 w4 = wb[b];
-                        const uint32_t pm = post_mask(sm.sbits, post_off, u, n_post);
-                        if (pre_spk | pm) w4 = update4_slow(w4, u, pl, pm, pre_spk, rw.y, rw.z, P, n_post, ppar);
-                        sum += (w4.x + w4.y) + (w4.z + w4.w);
-                    }
-                }
+                const uint32_t base = saddr(sm.wres + B.sm_off);
+                row_pair_sums<true>(nullptr, nullptr, base + 4u * ld * i, base + 4u * ld * (two ? i2 : i), units, lane,
+                                    two, sum0, sum1);
             } else {
-                const float* wrow = C.w + static_cast<size_t>(pl) * ld;
-                for (uint32_t u0 = 0; u0 < units; u0 += 128u) {
-                    float4 wb[4];
-#pragma unroll
-                    for (int b = 0; b < 4; ++b) {
-                        const uint32_t u = u0 + lane + 32u * b;
-                        wb[b] = u < units ? ld_col4(wrow + 4u * u) : make_float4(0.f, 0.f, 0.f, 0.f);
-                    }
-#pragma unroll
-                    for (int b = 0; b < 4; ++b) {
-                        const uint32_t u = u0 + lane + 32u * b;
-                        if (u >= units) continue;
-                        float4 w4 = wb[b];
-                        const uint32_t pm = post_mask(sm.sbits, post_off, u, n_post);
-                        if (pre_spk | pm) w4 = update4_slow(w4, u, pl, pm, pre_spk, rw.y, rw.z, P, n_post, ppar);
-                        sum += (w4.x + w4.y) + (w4.z + w4.w);
-                    }
-                }
+                const float* g = C.w + static_cast<size_t>(B.row_begin) * ld;
+                row_pair_sums<false>(g + static_cast<size_t>(i) * ld, g + static_cast<size_t>(two ? i2 : i) * ld, 0u, 0u,
+                                     units, lane, two, sum0, sum1);
             }
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
-            if (lane == 0) sm.row[r].w = sum <= 0.0f ? 1.0f : __fdiv_rn(sm.rowtgt[r], sum);
+            for (int o = 16; o > 0; o >>= 1) {
+                sum0 += __shfl_xor_sync(kFull, sum0, o);
+                sum1 += __shfl_xor_sync(kFull, sum1, o);
+            }
+            if (lane == 0) {
+                const uint32_t r = B.srow + i;
+                sm.row[r].y = sum0 <= 0.0f ? 1.0f : __fdiv_rn(sm.rowtgt[r], sum0);
+                if (two) {
+                    const uint32_t r2 = B.srow + i2;
+                    sm.row[r2].y = sum1 <= 0.0f ? 1.0f : __fdiv_rn(sm.rowtgt[r2], sum1);
+                }
+            }
         }
         k += nrows;
     }
 }
 
-// Pass 2 over the rows of one block for unit u: apply + normalise + store the pending plasticity
-// (plastic rows) and accumulate this step's GEMV partial sums.
-template <bool RESIDENT, bool PLASTIC>
-__device__ __forceinline__ float4 block_rows(const DBlk& B, const DConn& C, const DPlast* P, uint32_t u,
-                                             uint32_t pmask, uint32_t ppar, const SmemLayout& sm, bool accumulate,
-                                             float4 acc) {
-    const uint32_t nrows = B.row_end - B.row_begin, ld = C.ld, n_post = C.n_post;
-    const uint32_t sbase = RESIDENT ? saddr(sm.wres + B.sm_off) + 16u * u : 0u;
-    float* gbase = RESIDENT ? nullptr : C.w + static_cast<size_t>(B.row_begin) * ld + 4u * u;
-    const float4* rowp = sm.row + B.srow;
-    const uint32_t* flagp = sm.rowflag + B.srow;
-    constexpr int kB = RESIDENT ? 4 : 8;
+// Pass 2 over the rows of one block for NU units of the same block: normalise + store the updated
+// weights (SCALE: rows of a triplet plasticity) and accumulate this step's GEMV partial sums.
+// Each unit's rows are visited in row order, so NU only interleaves independent chains.
+template <bool RESIDENT, bool SCALE, int NU>
+__device__ __forceinline__ void block_rows(const DBlk& B, const DConn& C, const uint32_t (&u)[NU],
+                                           const SmemLayout& sm, bool accumulate, float4 (&acc)[NU]) {
+    const uint32_t nrows = B.row_end - B.row_begin, ld = C.ld;
+    uint32_t sbase[NU];
+    float* gbase[NU];
+#pragma unroll
+    for (int n = 0; n < NU; ++n) {
+        sbase[n] = RESIDENT ? saddr(sm.wres + B.sm_off) + 16u * u[n] : 0u;
+        gbase[n] = RESIDENT ? nullptr : C.w + static_cast<size_t>(B.row_begin) * ld + 4u * u[n];
+    }
+    const float2* rowp = reinterpret_cast<const float2*>(sm.row + B.srow);  // {x, scale} of each row
+    constexpr int kB = 4;
     for (uint32_t i0 = 0; i0 < nrows; i0 += kB) {
-        float4 wb[kB];
+        float4 wb[NU][kB];
 #pragma unroll
         for (int b = 0; b < kB; ++b) {
             if (i0 + b < nrows) {
-                if constexpr (RESIDENT) wb[b] = lds4(sbase + 4u * ld * (i0 + b));
-                else wb[b] = ld_col4(gbase + static_cast<size_t>(i0 + b) * ld);
+#pragma unroll
+                for (int n = 0; n < NU; ++n) {
+                    if constexpr (RESIDENT) wb[n][b] = lds4(sbase[n] + 4u * ld * (i0 + b));
+                    else wb[n][b] = ld_col4(gbase[n] + static_cast<size_t>(i0 + b) * ld);
+                }
             }
         }
 #pragma unroll
         for (int b = 0; b < kB; ++b) {
             if (i0 + b >= nrows) break;
             const uint32_t i = i0 + b;
-            const float4 rw = rowp[i];
-            float4 w4 = wb[b];
-            if constexpr (PLASTIC) {
-                const uint32_t pre_spk = flagp[i];
-                if (pre_spk | pmask)
-                    w4 = update4_slow(w4, u, B.row_begin + i, pmask, pre_spk, rw.y, rw.z, P, n_post, ppar);
-                w4.x *= rw.w;
-                w4.y *= rw.w;
-                w4.z *= rw.w;
-                w4.w *= rw.w;
-                if constexpr (RESIDENT) sts4(sbase + 4u * ld * i, w4);
-                else __stcg(reinterpret_cast<float4*>(gbase + static_cast<size_t>(i) * ld), w4);
-            }
-            if (accumulate) {
-                acc.x = fmaf(w4.x, rw.x, acc.x);
-                acc.y = fmaf(w4.y, rw.x, acc.y);
-                acc.z = fmaf(w4.z, rw.x, acc.z);
-                acc.w = fmaf(w4.w, rw.x, acc.w);
+            const float2 rw = rowp[2u * i];
+#pragma unroll
+            for (int n = 0; n < NU; ++n) {
+                float4 w4 = wb[n][b];
+                if constexpr (SCALE) {
+                    w4.x *= rw.y;
+                    w4.y *= rw.y;
+                    w4.z *= rw.y;
+                    w4.w *= rw.y;
+                    if constexpr (RESIDENT) sts4(sbase[n] + 4u * ld * i, w4);
+                    else __stcg(reinterpret_cast<float4*>(gbase[n] + static_cast<size_t>(i) * ld), w4);
+                }
+                if (accumulate) {
+                    acc[n].x = fmaf(w4.x, rw.x, acc[n].x);
+                    acc[n].y = fmaf(w4.y, rw.x, acc[n].y);
+                    acc[n].z = fmaf(w4.z, rw.x, acc[n].z);
+                    acc[n].w = fmaf(w4.w, rw.x, acc[n].w);
+                }
             }
         }
     }
-    return acc;
+}
+
+// All blocks of segment SG for NU of its units; the partial sums go to the segment's slot.
+// `pending` = a triplet normalisation of the previous step is to be applied.
+template <int NU>
+__device__ __forceinline__ void segment_units(const Desc& D, const DSeg& SG, const DBlk* s_blk, const uint32_t (&u)[NU],
+                                              bool pending, bool accumulate, const SmemLayout& sm, float* part_out,
+                                              uint32_t npad) {
+    float4 acc[NU];
+#pragma unroll
+    for (int n = 0; n < NU; ++n) acc[n] = make_float4(0.f, 0.f, 0.f, 0.f);
+    bool touched = false;
+    for (uint32_t bk = SG.blk_begin; bk < SG.blk_end; ++bk) {
+        const DBlk B = s_blk[bk];
+        const DConn& C = D.conns[B.conn];
+        const bool scale = pending && C.plast >= 0 && D.plast[C.plast].kind == kKindTriplet;
+        if (!scale && !accumulate) continue;
+        touched = true;
+        if (scale) {
+            if (B.resident) block_rows<true, true, NU>(B, C, u, sm, accumulate, acc);
+            else block_rows<false, true, NU>(B, C, u, sm, accumulate, acc);
+        } else {
+            if (B.resident) block_rows<true, false, NU>(B, C, u, sm, true, acc);
+            else block_rows<false, false, NU>(B, C, u, sm, true, acc);
+        }
+    }
+    if (accumulate && touched) {
+#pragma unroll
+        for (int n = 0; n < NU; ++n)
+            *reinterpret_cast<float4*>(part_out + static_cast<size_t>(SG.slot) * npad + SG.pcol + 4u * u[n]) = acc[n];
+    }
 }
 
 // Pass 2: each thread owns work items (one 4-column unit of one segment) and walks all of the
-// segment's rows; per item the partial sums go to the parity-`par` slot of this CTA.
-__device__ __forceinline__ void weight_pass(const DSim* S, const Desc& D, const DCta& cta, bool pending, uint32_t ppar,
-                                         bool accumulate, uint32_t par, const SmemLayout& sm, const DSeg* s_seg,
-                                         const DBlk* s_blk, uint32_t n_seg) {
-    float* part_out = S->partials + static_cast<size_t>(par) * S->n_slots * S->N_pad;
-    const uint32_t npad = S->N_pad;
-    for (uint32_t it0 = 0; it0 < cta.n_items; it0 += blockDim.x) {
-        const uint32_t it = it0 + threadIdx.x;
-        const int s = seg_of_item(s_seg, n_seg, it);
-        if (s < 0) continue;
-        const DSeg& SG = s_seg[s];
-        const uint32_t u = it - SG.item_begin;
-        if (u >= SG.units) continue;
-        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-        bool touched = false;
-        for (uint32_t bk = SG.blk_begin; bk < SG.blk_end; ++bk) {
-            const DBlk B = s_blk[bk];
-            const DConn& C = D.conns[B.conn];
-            const bool plastic = pending && C.plast >= 0;
-            if (!plastic && !accumulate) continue;
-            touched = true;
-            if (plastic) {
-                const DPlast* P = &D.plast[C.plast];
-                const uint32_t pm = post_mask(sm.sbits, C.post_off, u, C.n_post);
-                acc = B.resident ? block_rows<true, true>(B, C, P, u, pm, ppar, sm, accumulate, acc)
-                                 : block_rows<false, true>(B, C, P, u, pm, ppar, sm, accumulate, acc);
-            } else {
-                acc = B.resident ? block_rows<true, false>(B, C, nullptr, u, 0u, ppar, sm, true, acc)
-                                 : block_rows<false, false>(B, C, nullptr, u, 0u, ppar, sm, true, acc);
+// segment's rows; per item the partial sums go to the parity-`par` slot of this CTA.  With
+// kPairedUnits a thread's items it and it + blockDim of the same segment are processed together
+// (off: at 256 threads the paired loop does not fit the register file without spills).
+constexpr bool kPairedUnits = false;
+__device__ __forceinline__ void weight_pass(const DSim* S, const Desc& D, const DCta& cta, bool pending, bool accumulate,
+                                         uint32_t par, const SmemLayout& sm, const DSeg* s_seg, const DBlk* s_blk,
+                                         uint32_t n_seg) {
+    float* part_out = D.partials + static_cast<size_t>(par) * D.n_slots * D.N_pad;
+    const uint32_t npad = D.N_pad, nthr = blockDim.x;
+    for (uint32_t it0 = 0; it0 < cta.n_items; it0 += 2u * nthr) {
+        const uint32_t ia = it0 + threadIdx.x, ib = ia + nthr;
+        const int sa = seg_of_item(s_seg, n_seg, ia);
+        const int sb = seg_of_item(s_seg, n_seg, ib);
+        const bool va = sa >= 0 && ia - s_seg[sa].item_begin < s_seg[sa].units;
+        const bool vb = sb >= 0 && ib - s_seg[sb].item_begin < s_seg[sb].units;
+        if (kPairedUnits && va && vb && sa == sb) {
+            const uint32_t u2[2] = {ia - s_seg[sa].item_begin, ib - s_seg[sa].item_begin};
+            segment_units<2>(D, s_seg[sa], s_blk, u2, pending, accumulate, sm, part_out, npad);
+        } else {
+            if (va) {
+                const uint32_t u1[1] = {ia - s_seg[sa].item_begin};
+                segment_units<1>(D, s_seg[sa], s_blk, u1, pending, accumulate, sm, part_out, npad);
+            }
+            if (vb) {
+                const uint32_t u1[1] = {ib - s_seg[sb].item_begin};
+                segment_units<1>(D, s_seg[sb], s_blk, u1, pending, accumulate, sm, part_out, npad);
             }
         }
-        if (accumulate && touched)
-            *reinterpret_cast<float4*>(part_out + static_cast<size_t>(SG.slot) * npad + SG.pcol + 4u * u) = acc;
     }
 }
 
@@ -926,15 +1038,19 @@ __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* _
     __shared__ uint32_t s_has_norm;
     __shared__ uint32_t s_blk_base, s_nblk;
     __shared__ uint32_t s_ev[2];
+    // Shared-memory copies of the layout and the work plan: phases re-read them from shared memory
+    // instead of keeping them in registers for the whole launch.
+    __shared__ SmemLayout sm;
+    __shared__ NsLayout s_L;
 
     const uint32_t max_rows = S->max_rows, max_own = S->max_own;
     uint32_t n_spike_mons = 0;
     for (uint32_t m = 0; m < S->n_mons; ++m) n_spike_mons += S->mons[m].kind == kMonSpikes ? 1u : 0u;
-    const NsLayout L = ns_layout(S->ns_ts, S->ns_pre, S->ns_post, S->ns_mon);
+    const NsLayout L0 = ns_layout(S->ns_ts, S->ns_pre, S->ns_post, S->ns_mon);
     const SmemSizes z = smem_sizes(S->resident_floats, max_rows, max_own, S->spk_words, n_spike_mons, S->n_groups,
-                                   S->n_ts, S->n_conns, S->n_plast, S->n_mons, S->n_red, L.fields);
-    SmemLayout sm;
-    {
+                                   S->n_ts, S->n_conns, S->n_plast, S->n_mons, S->n_red, L0.fields);
+    if (threadIdx.x == 0) {
+        s_L = L0;
         unsigned char* p = smem_raw;
         sm.wres = reinterpret_cast<float*>(p);
         p += z.wres;
@@ -962,6 +1078,8 @@ __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* _
         p += z.bits;
         sm.desc = p;
     }
+    __syncthreads();
+    const NsLayout& L = s_L;
     // Descriptor copies.
     {
         unsigned char* p = sm.desc;
@@ -998,6 +1116,19 @@ __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* _
         s_d.seed = S->seed;
         s_d.stim_len = S->stim_len;
         s_d.replay_steps = S->replay_steps;
+        s_d.partials = S->partials;
+        s_d.n_slots = S->n_slots;
+        s_d.N_pad = S->N_pad;
+        s_d.spk_words = S->spk_words;
+        s_d.max_own = max_own;
+        s_d.spk_bits[0] = S->spk_bits[0];
+        s_d.spk_bits[1] = S->spk_bits[1];
+        s_d.stim_off = S->stim_off;
+        s_d.ev_neuron = S->ev_neuron;
+        s_d.ev_delta = S->ev_delta;
+        s_d.replay = S->replay;
+        s_d.barrier = S->barrier;
+        s_d.error = S->error;
         uint32_t base = 0;
         for (uint32_t m = 0; m < S->n_mons; ++m) {
             s_d.bitbase[m] = base;
@@ -1038,7 +1169,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* _
     }
     __syncthreads();
     const Desc& D = s_d;
-    const DCta cta = s_cta;
+    const DCta& cta = s_cta;
     const uint32_t n_seg = cta.seg_end - cta.seg_begin;
     const uint32_t nwarps = blockDim.x >> 5;
     const uint32_t n_own = cta.n1 - cta.n0;
@@ -1068,6 +1199,9 @@ __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* _
     const uint32_t clock0 = s_clock0;
     bool ok = true;
 #ifdef BSNN_PHASE_TIMING
+    __shared__ unsigned long long s_tally_[8];
+    if (threadIdx.x == 0)
+        for (int i = 0; i < 8; ++i) s_tally_[i] = 0;
     unsigned long long t_mark_ = static_cast<unsigned long long>(clock64());
 #endif
     for (uint32_t k = 0; k < n_steps; ++k) {
@@ -1078,21 +1212,22 @@ __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* _
 
         // Global inputs of the step, issued together: the spike bitmask of the previous step, the
         // stimulus range of this step and the previous step's partial sums.
-        const uint32_t tid = threadIdx.x, nthr = blockDim.x, spk_words = S->spk_words;
+        const uint32_t tid = threadIdx.x, nthr = blockDim.x, spk_words = D.spk_words;
         uint32_t sb0 = 0, sb1 = 0, ev_lo = 0, ev_hi = 0;
         if (pending) {
-            if (tid < spk_words) sb0 = __ldcg(S->spk_bits[ppar] + tid);
-            if (tid + nthr < spk_words) sb1 = __ldcg(S->spk_bits[ppar] + tid + nthr);
+            if (tid < spk_words) sb0 = __ldcg(D.spk_bits[ppar] + tid);
+            if (tid + nthr < spk_words) sb1 = __ldcg(D.spk_bits[ppar] + tid + nthr);
         }
         if (tid == 0 && t < D.stim_len) {
-            ev_lo = __ldg(S->stim_off + t);
-            ev_hi = __ldg(S->stim_off + t + 1);
+            ev_lo = __ldg(D.stim_off + t);
+            ev_hi = __ldg(D.stim_off + t + 1);
         }
         if (pending) load_partials(S, D, cta, ppar, sm, max_own);
+        BSNN_TMARK(3);
         if (pending) {
             if (tid < spk_words) sm.sbits[tid] = sb0;
             if (tid + nthr < spk_words) sm.sbits[tid + nthr] = sb1;
-            for (uint32_t w = tid + 2u * nthr; w < spk_words; w += nthr) sm.sbits[w] = __ldcg(S->spk_bits[ppar] + w);
+            for (uint32_t w = tid + 2u * nthr; w < spk_words; w += nthr) sm.sbits[w] = __ldcg(D.spk_bits[ppar] + w);
         }
         if (tid == 0) {
             s_ev[0] = ev_lo;
@@ -1103,46 +1238,56 @@ __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* _
         for (uint32_t w = tid; w < n_gbits; w += nthr) sm.gbits[par * n_gbits + w] = 0u;
         __syncthreads();
         BSNN_TMARK(0);
+        if (pending) {
+            apply_updates(D, s_blk, s_nblk, ppar, sm);
+            __syncthreads();
+        }
+        BSNN_TMARK(6);
         const bool norm_now = pending && s_has_norm;
         if (tid < 32u * neuron_warps) {
             neuron_phase(S, D, cta, t, clock, par, pending, sm, max_own, L, s_ev[0], s_ev[1]);
         } else if (norm_now && norm_beside) {
-            norm_rows(S, D, ppar, sm, s_blk, s_nblk, neuron_warps, nwarps - neuron_warps);
+            norm_rows(D, sm, s_blk, s_nblk, neuron_warps, nwarps - neuron_warps);
         }
         __syncthreads();
         BSNN_TMARK(1);
         if (norm_now && !norm_beside) {
-            norm_rows(S, D, ppar, sm, s_blk, s_nblk, 0u, nwarps);
+            norm_rows(D, sm, s_blk, s_nblk, 0u, nwarps);
             __syncthreads();
         }
         flush_spike_bits(S, D, cta, clock, par, sm);
         rows_x(D, cta, sm, max_own);
         __syncthreads();
         BSNN_TMARK(2);
-        BSNN_TMARK(3);
-        weight_pass(S, D, cta, pending, ppar, true, par, sm, s_seg, s_blk, n_seg);
+        weight_pass(S, D, cta, pending, true, par, sm, s_seg, s_blk, n_seg);
         __syncthreads();
         BSNN_TMARK(4);
-        if (!grid_barrier(S, bar0 + (k + 1ull) * gridDim.x, &s_ok)) {
+        if (!grid_barrier(D.barrier, D.error, bar0 + (k + 1ull) * gridDim.x, &s_ok)) {
             ok = false;
             break;
         }
         BSNN_TMARK(5);
     }
+#ifdef BSNN_PHASE_TIMING
+    if (threadIdx.x == 0)
+        for (int i = 0; i < 8; ++i) S->phase_ns[blockIdx.x * 8u + i] += s_tally_[i];
+#endif
     if (!ok) return;
 
     // Finalize: apply the last step's plasticity, write resident rows and the neuron state back,
     // and fold the last propagation into g.
     const unsigned long long t_last = t0 + n_steps - 1ull;
     const uint32_t lpar = static_cast<uint32_t>(t_last & 1ull);
-    stage_spike_bits(S, lpar, sm);
+    stage_spike_bits(D, lpar, sm);
     rows_pending(D, cta, true, lpar, sm, max_own);
     __syncthreads();
+    apply_updates(D, s_blk, s_nblk, lpar, sm);
+    __syncthreads();
     if (s_has_norm) {
-        norm_rows(S, D, lpar, sm, s_blk, s_nblk, 0u, nwarps);
+        norm_rows(D, sm, s_blk, s_nblk, 0u, nwarps);
         __syncthreads();
     }
-    weight_pass(S, D, cta, true, lpar, false, lpar, sm, s_seg, s_blk, n_seg);
+    weight_pass(S, D, cta, true, false, lpar, sm, s_seg, s_blk, n_seg);
     __syncthreads();
     move_resident(D, s_blk, s_nblk, sm, false);
     load_partials(S, D, cta, lpar, sm, max_own);
