@@ -112,6 +112,12 @@ __device__ __forceinline__ float clamp_w(float w, float wmin, float wmax) {
     return w;
 }
 
+// Barrier among `threads` threads (a multiple of 32) of the CTA on hardware barrier `id` (> 0;
+// barrier 0 is __syncthreads).
+__device__ __forceinline__ void named_barrier_sync(uint32_t id, uint32_t threads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+}
+
 __device__ __forceinline__ void red_release_add_u64(unsigned long long* p, unsigned long long v) {
     asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
@@ -155,8 +161,8 @@ __device__ __forceinline__ bool grid_barrier(unsigned long long* barrier, int32_
 // Optional phase timing (profiling builds only, -DBSNN_PHASE_TIMING): thread 0 of every CTA adds
 // the SM clock cycles spent in each phase to a shared-memory tally (s_tally_[phase]) that the
 // kernel adds to S->phase_ns[cta * 8 + phase] when it ends: 3 partial-sum loads, 0 rest of the
-// step inputs, 6 plasticity updates, 1 neuron phase and normalisation, 2 spike bits and row x,
-// 4 weight pass, 5 grid barrier.
+// step inputs, 1 neuron phase beside the plasticity update and normalisation, 2 spike bits and
+// row x, 4 weight pass, 5 grid barrier.
 #ifdef BSNN_PHASE_TIMING
 #define BSNN_TMARK(slot)                                                                   \
     do {                                                                                   \
@@ -763,9 +769,10 @@ __device__ __forceinline__ float* weight_ptr(const DBlk& B, const DConn& C, cons
 // The two passes touch disjoint weights, so each weight gets the reference's LTP-then-LTD
 // sequence exactly once.  The column factors come from the owners' parity buffers in global
 // memory, the row factors from the row table.
+// Runs on warps [w_first, w_first + nwarps) of the CTA.
 __device__ __forceinline__ void apply_updates(const Desc& D, const DBlk* s_blk, uint32_t nblk, uint32_t ppar,
-                                           const SmemLayout& sm) {
-    const uint32_t tid = threadIdx.x, nthr = blockDim.x, warp = tid >> 5, lane = tid & 31u, nwarps = nthr >> 5;
+                                           const SmemLayout& sm, uint32_t w_first, uint32_t nwarps) {
+    const uint32_t tid = threadIdx.x - 32u * w_first, nthr = 32u * nwarps, warp = tid >> 5, lane = tid & 31u;
     for (uint32_t bk = 0; bk < nblk; ++bk) {
         const DBlk B = s_blk[bk];
         const DConn& C = D.conns[B.conn];
@@ -900,7 +907,7 @@ __device__ __forceinline__ void block_rows(const DBlk& B, const DConn& C, const 
         gbase[n] = RESIDENT ? nullptr : C.w + static_cast<size_t>(B.row_begin) * ld + 4u * u[n];
     }
     const float2* rowp = reinterpret_cast<const float2*>(sm.row + B.srow);  // {x, scale} of each row
-    constexpr int kB = 4;
+    constexpr int kB = (RESIDENT || SCALE) ? 4 : 8;
     for (uint32_t i0 = 0; i0 < nrows; i0 += kB) {
         float4 wb[NU][kB];
 #pragma unroll
@@ -1238,23 +1245,34 @@ __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* _
         for (uint32_t w = tid; w < n_gbits; w += nthr) sm.gbits[par * n_gbits + w] = 0u;
         __syncthreads();
         BSNN_TMARK(0);
-        if (pending) {
-            apply_updates(D, s_blk, s_nblk, ppar, sm);
-            __syncthreads();
-        }
-        BSNN_TMARK(6);
         const bool norm_now = pending && s_has_norm;
-        if (tid < 32u * neuron_warps) {
-            neuron_phase(S, D, cta, t, clock, par, pending, sm, max_own, L, s_ev[0], s_ev[1]);
-        } else if (norm_now && norm_beside) {
-            norm_rows(D, sm, s_blk, s_nblk, neuron_warps, nwarps - neuron_warps);
-        }
-        __syncthreads();
-        BSNN_TMARK(1);
-        if (norm_now && !norm_beside) {
-            norm_rows(D, sm, s_blk, s_nblk, 0u, nwarps);
+        if (norm_beside) {
+            // The neuron phase on the first warps; the plasticity update and then the normalisation
+            // sums on the others (they touch no data of the neuron phase).
+            if (tid < 32u * neuron_warps) {
+                neuron_phase(S, D, cta, t, clock, par, pending, sm, max_own, L, s_ev[0], s_ev[1]);
+            } else if (pending) {
+                const uint32_t nw = nwarps - neuron_warps;
+                apply_updates(D, s_blk, s_nblk, ppar, sm, neuron_warps, nw);
+                if (norm_now) {
+                    named_barrier_sync(1u, 32u * nw);
+                    norm_rows(D, sm, s_blk, s_nblk, neuron_warps, nw);
+                }
+            }
             __syncthreads();
+        } else {
+            if (pending) {
+                apply_updates(D, s_blk, s_nblk, ppar, sm, 0u, nwarps);
+                __syncthreads();
+            }
+            neuron_phase(S, D, cta, t, clock, par, pending, sm, max_own, L, s_ev[0], s_ev[1]);
+            __syncthreads();
+            if (norm_now) {
+                norm_rows(D, sm, s_blk, s_nblk, 0u, nwarps);
+                __syncthreads();
+            }
         }
+        BSNN_TMARK(1);
         flush_spike_bits(S, D, cta, clock, par, sm);
         rows_x(D, cta, sm, max_own);
         __syncthreads();
@@ -1281,7 +1299,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* _
     stage_spike_bits(D, lpar, sm);
     rows_pending(D, cta, true, lpar, sm, max_own);
     __syncthreads();
-    apply_updates(D, s_blk, s_nblk, lpar, sm);
+    apply_updates(D, s_blk, s_nblk, lpar, sm, 0u, nwarps);
     __syncthreads();
     if (s_has_norm) {
         norm_rows(D, sm, s_blk, s_nblk, 0u, nwarps);
