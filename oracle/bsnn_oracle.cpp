@@ -651,6 +651,19 @@ BSNN_API int32_t or_run(or_sim* s, uint32_t first, uint32_t n) {
     });
 }
 
+BSNN_API int32_t or_skip_steps(or_sim* s, uint32_t n) {
+    return with_sim(s, [&](auto& sim) {
+        for (uint32_t k = 0; k < n; ++k) {
+            for (auto& st : sim.stims) {
+                if (st.cursor_t >= st.counts.size()) continue;
+                st.cursor_e += st.counts[st.cursor_t];
+                ++st.cursor_t;
+            }
+            ++sim.steps_done;
+        }
+    });
+}
+
 BSNN_API int32_t or_read_state(or_sim* s, int32_t field, uint32_t index, uint32_t offset, uint32_t count, void* out) {
     return with_sim(s, [&](auto& sim) {
         if (field == BSNN_FIELD_REFRACTORY_COUNTER || field == BSNN_FIELD_SPIKES) {

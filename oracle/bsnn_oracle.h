@@ -51,6 +51,9 @@ BSNN_API int32_t or_set_noise_mode(or_sim* s, int32_t mode);
 BSNN_API int32_t or_set_noise_replay(or_sim* s, const uint8_t* counts, uint32_t n_steps);
 BSNN_API int32_t or_step(or_sim* s, uint32_t clock_step);
 BSNN_API int32_t or_run(or_sim* s, uint32_t first_clock_step, uint32_t n_steps);
+/* Advances the step counter and the stimulus cursors by n steps without simulating them (for
+ * tests that copy a device state into the oracle at step n). */
+BSNN_API int32_t or_skip_steps(or_sim* s, uint32_t n);
 /* Same field codes as bsnn_read_state; values converted to float (uint32 fields as uint32). */
 BSNN_API int32_t or_read_state(or_sim* s, int32_t field, uint32_t index, uint32_t offset, uint32_t count,
                                void* out);

@@ -49,7 +49,7 @@ def load():
         "or_add_stimulus": (I32, [P, P, U32, P, P, P, U32]), "or_add_plasticity": (I32, [P, I32, U32, P, P]),
         "or_add_spike_recorder": (I32, [P, U32, U32, P]), "or_add_voltage_recorder": (I32, [P, U32, P, U32, U32, P]),
         "or_set_noise_mode": (I32, [P, I32]), "or_set_noise_replay": (I32, [P, P, U32]),
-        "or_step": (I32, [P, U32]), "or_run": (I32, [P, U32, U32]),
+        "or_step": (I32, [P, U32]), "or_run": (I32, [P, U32, U32]), "or_skip_steps": (I32, [P, U32]),
         "or_read_state": (I32, [P, I32, U32, U32, U32, P]), "or_read_state_f64": (I32, [P, I32, U32, U32, U32, P]),
         "or_write_state": (I32, [P, I32, U32, U32, U32, P]), "or_read_weights": (I32, [P, U32, P]),
         "or_read_weights_f64": (I32, [P, U32, P]), "or_write_weights": (I32, [P, U32, P]), "or_read_spike_history": (I32, [P, U32, P, I32]),
@@ -186,6 +186,10 @@ class OracleSimulation:
 
     def synchronize(self):
         pass
+
+    def skip_steps(self, n):
+        """Advances the step counter and stimulus cursors by n steps without simulating them."""
+        self._check(self._lib.or_skip_steps(self._h, n))
 
     def _len(self, name, index):
         if name.startswith("connection_"):

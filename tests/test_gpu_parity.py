@@ -76,6 +76,26 @@ def test_resync_single_step_parity_long_run(plasticity):
         compare_state(g, o, spec, RTOL, tag=f"resync block {block}")
 
 
+@pytest.mark.parametrize("plasticity", [("triplet", "istdp", "stdp")])
+def test_resync_parity_with_rows_streamed_from_global_memory(monkeypatch, plasticity):
+    """The same single-step parity with shared-memory residency switched off, so every weight row
+    (plastic ones included) is read, updated and written in global memory."""
+    monkeypatch.setenv("BSNN_RESIDENT", "0")
+    spec = bsnn.random_network(128, 32, steps=800, seed=12, plasticity=plasticity)
+    g, o = make_pair(spec)
+    done = 0
+    for block in range(4):
+        g.run(done, 151)
+        o.run(done, 151)
+        done += 151
+        assert g.info().resident_bytes == 0
+        copy_state(g, o, spec)
+        g.step(done)
+        o.step(done)
+        done += 1
+        compare_state(g, o, spec, RTOL, tag=f"streamed rows, resync block {block}")
+
+
 def test_launch_split_is_bit_exact():
     spec = bsnn.random_network(100, 25, steps=500, seed=3)
     sims = []
@@ -204,6 +224,33 @@ def test_example_size_network_properties():
     g.step(2000)
     o.step(2000)
     compare_state(g, o, spec, RTOL, tag="example size")
+
+
+def test_large_network_properties_and_one_step_parity():
+    """Large size (8,100 E + 2,025 I, ~102.5 M dense synapses, 410 MB of FP32 weights; the plastic
+    rows no longer fit in shared memory and stream from L2/HBM): size-independent properties after
+    300 steps, then one step from a copy of the device state against the oracle."""
+    spec = bsnn.synthetic_network("large_plastic_10125", steps=400, weight_values="uniform")
+    g = bsnn.Simulation(spec.num_excitatory, spec.num_inhibitory, **spec.sim_kwargs())
+    spec.build(g)
+    g.run(0, 300)
+    w = g.read_weights(0).astype(np.float64)
+    assert np.isfinite(w).all() and w.min() >= 0.0
+    targets = g.read("plasticity_pre_weight_sums", 0, count=spec.num_excitatory).astype(np.float64)
+    rows = w.sum(axis=1)
+    ok = rows > 0
+    np.testing.assert_allclose(rows[ok], targets[ok], rtol=1e-4)
+    del w
+    v = g.read("membrane_potentials")
+    assert np.isfinite(v).all() and v.max() <= -0.04 + 1e-7
+    import oracle
+    o = oracle.OracleSimulation(spec.num_excitatory, spec.num_inhibitory, **spec.sim_kwargs())
+    spec.build(o)
+    o.skip_steps(300)
+    copy_state(g, o, spec)
+    g.step(300)
+    o.step(300)
+    compare_state(g, o, spec, RTOL, tag="large size")
 
 
 def test_errors_surface_as_reference_exceptions():
