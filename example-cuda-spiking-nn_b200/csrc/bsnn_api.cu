@@ -177,7 +177,7 @@ struct Plan {
     std::vector<uint32_t> rows_begin;
     std::vector<uint32_t> red_list;
     uint32_t red_begin[2][kMaxGroups]{}, red_end[2][kMaxGroups]{};
-    uint32_t n_slots = 0, max_rows = 1, max_own = 1, max_items = 1;
+    uint32_t n_slots = 0, max_rows = 1, max_own = 1, max_items = 1, max_trows = 0, n_chunks = 0;
     uint64_t resident_floats = 0;
 };
 
@@ -291,7 +291,7 @@ Plan build_plan(const bsnn_sim* s, uint32_t n_ctas, uint64_t cap_bytes, bool* re
         P.rows_begin.push_back(static_cast<uint32_t>(P.rows.size()));
         const uint32_t row_base = static_cast<uint32_t>(P.rows.size());
         int32_t slot_of_target[2] = {-1, -1};
-        uint32_t item = 0;
+        uint32_t item = 0, trows = 0;
         for (uint32_t T = 0; T < 2; ++T) {
             for (uint32_t q = 0; q < s->groups.size(); ++q) {
                 DSeg seg{};
@@ -356,6 +356,23 @@ Plan build_plan(const bsnn_sim* s, uint32_t n_ctas, uint64_t cap_bytes, bool* re
                 }
             P.resident_floats = std::max<uint64_t>(P.resident_floats, used / 4);
         }
+        // Streamed triplet blocks carry their row sums between steps (32-unit chunks per row).
+        {
+            const uint32_t b0 = cta.seg_end > cta.seg_begin ? P.segs[cta.seg_begin].blk_begin : 0u;
+            const uint32_t b1 = cta.seg_end > cta.seg_begin ? P.segs[cta.seg_end - 1].blk_end : 0u;
+            for (uint32_t bk = b0; bk < b1; ++bk) {
+                DBlk& B = P.blks[bk];
+                bool triplet = false;
+                for (const auto& pl : s->plasts) triplet |= pl.conn == B.conn && pl.kind == BSNN_PLASTICITY_TRIPLET;
+                if (!triplet || B.resident) continue;
+                for (uint32_t sg = cta.seg_begin; sg < cta.seg_end; ++sg)
+                    if (bk >= P.segs[sg].blk_begin && bk < P.segs[sg].blk_end) P.segs[sg].carried = 1;
+                B.trow = trows;
+                trows += B.row_end - B.row_begin;
+                const uint32_t units = round_up(s->groups[s->conns[B.conn].post].p.num_neurons, 4) / 4;
+                P.n_chunks = std::max(P.n_chunks, (units + 31) / 32);
+            }
+        }
         cta.n_items = item;
         require(cta.seg_end - cta.seg_begin <= static_cast<uint32_t>(kMaxSegsPerCta), BSNN_ERR_INVALID_ARGUMENT,
                 "too many (target, post group) segments per CTA");
@@ -365,6 +382,7 @@ Plan build_plan(const bsnn_sim* s, uint32_t n_ctas, uint64_t cap_bytes, bool* re
         require(nblk <= static_cast<uint32_t>(kMaxBlksPerCta), BSNN_ERR_INVALID_ARGUMENT,
                 "too many connection blocks per CTA");
         P.max_rows = std::max(P.max_rows, cta.n_rows);
+        P.max_trows = std::max(P.max_trows, trows);
         P.max_own = std::max(P.max_own, cta.n1 - cta.n0);
         P.max_items = std::max(P.max_items, cta.n_items);
         P.ctas.push_back(cta);
@@ -512,8 +530,10 @@ void finalize(bsnn_sim* s) {
     // Shared memory: the largest opt-in dynamic allocation minus the kernel's static shared data.
     int optin = 0;
     cuda_check(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device), "smem attr");
-    cudaFuncAttributes fa{};
-    cuda_check(cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(&bsnn_step_kernel)), "func attr");
+    cudaFuncAttributes fa{}, fa_carry{};
+    cuda_check(cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(&bsnn_step_kernel<false>)), "func attr");
+    cuda_check(cudaFuncGetAttributes(&fa_carry, reinterpret_cast<const void*>(&bsnn_step_kernel<true>)), "func attr");
+    fa.sharedSizeBytes = std::max(fa.sharedSizeBytes, fa_carry.sharedSizeBytes);
     uint32_t n_spike_mons = 0;
     for (const auto& M : s->mons) n_spike_mons += M.kind == kMonSpikes ? 1u : 0u;
     // Per-group role counts that size the shared-memory neuron state.
@@ -535,7 +555,8 @@ void finalize(bsnn_sim* s) {
     const uint32_t ns_fields = ns_layout(h.ns_ts, h.ns_pre, h.ns_post, h.ns_mon).fields;
     auto smem_of = [&](const Plan& pl, uint32_t resident_floats) {
         return smem_sizes(resident_floats, pl.max_rows, pl.max_own, spk_words, n_spike_mons, h.n_groups, h.n_ts,
-                          h.n_conns, h.n_plast, h.n_mons, static_cast<uint32_t>(pl.red_list.size()), ns_fields)
+                          h.n_conns, h.n_plast, h.n_mons, static_cast<uint32_t>(pl.red_list.size()), ns_fields,
+                          pl.max_trows * pl.n_chunks)
             .total;
     };
     const int64_t smem_limit = static_cast<int64_t>(optin) - static_cast<int64_t>(fa.sharedSizeBytes) - 128;
@@ -561,6 +582,8 @@ void finalize(bsnn_sim* s) {
     h.n_ctas = n_ctas;
     h.n_slots = std::max(P.n_slots, 1u);
     h.max_rows = P.max_rows;
+    h.max_trows = P.max_trows;
+    h.n_chunks = P.n_chunks;
     h.max_own = P.max_own;
     std::memcpy(h.red_begin, P.red_begin, sizeof(P.red_begin));
     std::memcpy(h.red_end, P.red_end, sizeof(P.red_end));
@@ -577,7 +600,9 @@ void finalize(bsnn_sim* s) {
     block = std::max(block, round_up(P.max_own, 32));
     s->grid = n_ctas;
     s->block = block;
-    s->kernel = reinterpret_cast<const void*>(&bsnn_step_kernel);
+    // Networks with streamed triplet rows carry row sums between steps (a kernel instance of its own).
+    s->kernel = P.max_trows > 0 ? reinterpret_cast<const void*>(&bsnn_step_kernel<true>)
+                                : reinterpret_cast<const void*>(&bsnn_step_kernel<false>);
 
     size_t o_part = A.take(sizeof(float) * 2 * static_cast<size_t>(h.n_slots) * h.N_pad);
     size_t o_red = A.take(sizeof(uint32_t) * P.red_list.size());

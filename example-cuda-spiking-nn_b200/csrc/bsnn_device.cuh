@@ -114,12 +114,14 @@ struct DSeg {  // all rows of this CTA that add into (target, post group)
     uint32_t slot;        // partial-sum slot this CTA writes for `target`
     uint32_t blk_begin, blk_end;
     uint32_t normalized;  // some block of this segment carries the triplet row normalisation
+    uint32_t carried;     // some triplet block of this segment streams from global memory
 };
 struct DBlk {  // rows [row_begin, row_end) (presynaptic local index) of one connection
     uint32_t conn, row_begin, row_end;
     uint32_t srow;      // index of row_begin in the CTA's row table
     uint32_t resident;  // rows held in shared memory for the whole launch
     uint32_t sm_off;    // float offset of row_begin in the resident region
+    uint32_t trow;      // index of row_begin among the CTA's triplet-normalised rows
 };
 struct DCta {
     uint32_t n0, n1;  // owned neurons (phase A) == owned presynaptic rows (phase B)
@@ -139,6 +141,8 @@ struct DSim {
     // Largest per-group role counts (trace sets, plasticities as pre / post side, voltage
     // monitors): they size the per-neuron state each CTA keeps in shared memory during a launch.
     uint32_t ns_ts, ns_pre, ns_post, ns_mon;
+    // Carried triplet row sums: most triplet rows of one CTA, and 32-unit chunks per row.
+    uint32_t max_trows, n_chunks;
     DGroup groups[kMaxGroups];
     DTraceSet ts[kMaxTraceSets];
     DConn conns[kMaxConns];

@@ -220,6 +220,7 @@ struct SmemLayout {
     float* xown;        // [n_ts][max_own] x = d - r of the own neurons (this step)
     float2* rowfac;     // [2][n_plast][max_own] {rowA, rowB} of the own neurons, by step parity
     float* ns;          // [ns_fields][max_own] state of the own neurons (kNs* fields below)
+    float* rsum;        // [max_trows][n_chunks] carried triplet row sums by 32-unit chunk
     float* red;         // [warps][2][max_own] per-warp partial-sum reduction scratch
     uint32_t* bits;     // [n_spike_monitors][max_own/32 + 2]
     unsigned char* desc;  // descriptor copies (DGroup, DTraceSet, DConn, DPlast, DMon, slot lists)
@@ -249,13 +250,14 @@ __host__ __device__ __forceinline__ size_t align16(size_t x) { return (x + 15) &
 
 // Byte layout of the dynamic shared memory; the host sizes the launch with the same function.
 struct SmemSizes {
-    size_t wres, row, meta, rowflag, rowtgt, sbits, gbits, xown, rowfac, ns, redscr, bits, groups, ts, conns, plast,
+    size_t wres, row, meta, rowflag, rowtgt, sbits, gbits, xown, rowfac, ns, rsum, redscr, bits, groups, ts, conns, plast,
         mons, red, total;
 };
 __host__ __device__ __forceinline__ SmemSizes smem_sizes(uint32_t resident_floats, uint32_t max_rows, uint32_t max_own,
                                                          uint32_t spk_words, uint32_t n_spike_mons, uint32_t n_groups,
                                                          uint32_t n_ts, uint32_t n_conns, uint32_t n_plast,
-                                                         uint32_t n_mons, uint32_t n_red, uint32_t ns_fields) {
+                                                         uint32_t n_mons, uint32_t n_red, uint32_t ns_fields,
+                                                         uint32_t rsum_floats) {
     SmemSizes z;
     z.wres = align16(sizeof(float) * static_cast<size_t>(resident_floats));
     z.row = align16(sizeof(float4) * max_rows);
@@ -267,6 +269,7 @@ __host__ __device__ __forceinline__ SmemSizes smem_sizes(uint32_t resident_float
     z.xown = align16(sizeof(float) * n_ts * max_own);
     z.rowfac = align16(sizeof(float2) * 2 * n_plast * max_own);
     z.ns = align16(sizeof(float) * ns_fields * max_own);
+    z.rsum = align16(sizeof(float) * rsum_floats);
     z.redscr = align16(sizeof(float) * 2 * kMaxWarps * max_own);
     z.bits = align16(sizeof(uint32_t) * n_spike_mons * (max_own / 32 + 2));
     z.groups = align16(sizeof(DGroup) * n_groups);
@@ -275,7 +278,7 @@ __host__ __device__ __forceinline__ SmemSizes smem_sizes(uint32_t resident_float
     z.plast = align16(sizeof(DPlast) * n_plast);
     z.mons = align16(sizeof(DMon) * n_mons);
     z.red = align16(sizeof(uint32_t) * n_red);
-    z.total = z.wres + z.row + z.meta + z.rowflag + z.rowtgt + z.sbits + z.gbits + z.xown + z.rowfac + z.ns + z.redscr +
+    z.total = z.wres + z.row + z.meta + z.rowflag + z.rowtgt + z.sbits + z.gbits + z.xown + z.rowfac + z.ns + z.rsum + z.redscr +
               z.bits + z.groups + z.ts + z.conns + z.plast + z.mons + z.red;
     return z;
 }
@@ -817,11 +820,26 @@ __device__ __forceinline__ void apply_updates(const Desc& D, const DBlk* s_blk, 
     }
 }
 
-// Sum of `lane`'s units (lane, lane+32, ...) of two rows at once, each as (x + y) + (z + w) per
-// unit in unit order; `two` = false sums the first row only.
-template <bool RESIDENT>
-__device__ __forceinline__ void row_pair_sums(const float* g0, const float* g1, uint32_t s0, uint32_t s1,
-                                              uint32_t units, uint32_t lane, bool two, float& sum0, float& sum1) {
+// For triplet rows streamed from global memory the row sums are carried from one step to the next
+// in 32-unit chunks, so the normalisation need not read every row again: rsum[tr][c] is the sum
+// over the units u = 32c .. 32c+31 of row tr (the CTA's tr-th streamed triplet row) of
+// (w.x + w.y) + (w.z + w.w), added over the lanes of a warp by an xor-butterfly.  The weight pass
+// produces them for the weights it has just stored; the next step's normalisation recomputes
+// only the chunks its plasticity update touched and adds the chunks of a row in a fixed order.
+// (Resident rows are summed from shared memory instead: reading them again is cheaper than the
+// butterflies.)
+__device__ __forceinline__ float unit_sum(float4 w) { return (w.x + w.y) + (w.z + w.w); }
+
+__device__ __forceinline__ float warp_sum(float p) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) p += __shfl_xor_sync(kFull, p, o);
+    return p;
+}
+
+// Sum of `lane`'s units (lane, lane+32, ...) of two resident rows at once, each as
+// (x + y) + (z + w) per unit in unit order; `two` = false sums the first row only.
+__device__ __forceinline__ void row_pair_sums(uint32_t s0, uint32_t s1, uint32_t units, uint32_t lane, bool two,
+                                              float& sum0, float& sum1) {
     sum0 = 0.0f;
     sum1 = 0.0f;
     for (uint32_t u0 = 0; u0 < units; u0 += 128u) {
@@ -830,183 +848,241 @@ __device__ __forceinline__ void row_pair_sums(const float* g0, const float* g1, 
         for (int k = 0; k < 4; ++k) {
             const uint32_t u = u0 + lane + 32u * k;
             const bool in = u < units;
-            if constexpr (RESIDENT) {
-                a[k] = in ? lds4(s0 + 16u * u) : make_float4(0.f, 0.f, 0.f, 0.f);
-                b[k] = in && two ? lds4(s1 + 16u * u) : make_float4(0.f, 0.f, 0.f, 0.f);
-            } else {
-                a[k] = in ? ld_col4(g0 + 4u * u) : make_float4(0.f, 0.f, 0.f, 0.f);
-                b[k] = in && two ? ld_col4(g1 + 4u * u) : make_float4(0.f, 0.f, 0.f, 0.f);
-            }
+            a[k] = in ? lds4(s0 + 16u * u) : make_float4(0.f, 0.f, 0.f, 0.f);
+            b[k] = in && two ? lds4(s1 + 16u * u) : make_float4(0.f, 0.f, 0.f, 0.f);
         }
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             if (u0 + lane + 32u * k >= units) continue;
-            sum0 += (a[k].x + a[k].y) + (a[k].z + a[k].w);
-            sum1 += (b[k].x + b[k].y) + (b[k].z + b[k].w);
+            sum0 += unit_sum(a[k]);
+            sum1 += unit_sum(b[k]);
         }
     }
 }
 
-// Pass 1 of the triplet normalisation (after apply_updates), on warps [w_first, w_first + nwarps):
-// each warp takes two rows at a time; each lane sums its units of the updated rows, then an
-// xor-butterfly; lane 0 forms target / sum.
+// Recomputes the carried chunk sums of row i of a streamed block B for the chunks c0 .. c0+7 set in
+// `need` (bit k = chunk c0 + k), eight butterflies at a time.
+__device__ __forceinline__ void chunk_sums8(const DBlk& B, const DConn& C, const SmemLayout& sm, uint32_t i,
+                                           uint32_t c0, uint32_t need, uint32_t lane, uint32_t n_chunks) {
+    const float* row = C.w + static_cast<size_t>(B.row_begin + i) * C.ld;
+    float p[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const uint32_t u = 32u * (c0 + k) + lane;
+        p[k] = ((need >> k) & 1u) && u < C.units ? unit_sum(ld_col4(row + 4u * u)) : 0.0f;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) p[k] += __shfl_xor_sync(kFull, p[k], o);
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if ((need >> k) & 1u) sm.rsum[(B.trow + i) * n_chunks + c0 + k] = p[k];
+    }
+}
+
+// Pass 1 of the triplet normalisation (after apply_updates), on warps [w_first, w_first + nwarps).
+// Resident rows: each warp sums two rows at a time, each lane its units, then an xor-butterfly.
+// Streamed rows: the carried chunk sums are used; the chunks the update touched are recomputed
+// first (all chunks of a row whose presynaptic neuron spiked; for a spiking postsynaptic neuron,
+// its chunk in every row), then the lanes add the chunks c = lane, lane + 32, ... in order and an
+// xor-butterfly adds the lanes.  Lane 0 forms target / sum.
+template <bool CARRY>
 __device__ __forceinline__ void norm_rows(const Desc& D, const SmemLayout& sm, const DBlk* s_blk, uint32_t nblk,
-                                       uint32_t w_first, uint32_t nwarps) {
+                                       uint32_t w_first, uint32_t nwarps, uint32_t n_chunks) {
     const uint32_t warp = (threadIdx.x >> 5) - w_first, lane = threadIdx.x & 31u;
     uint32_t k = 0;  // running index over the CTA's normalised rows
     for (uint32_t bk = 0; bk < nblk; ++bk) {
         const DBlk B = s_blk[bk];
         const DConn& C = D.conns[B.conn];
         if (C.plast < 0 || D.plast[C.plast].kind != kKindTriplet) continue;
-        const uint32_t nrows = B.row_end - B.row_begin, units = C.units, ld = C.ld;
-        // first row of this block handled by this warp; then every nwarps-th, two at a time
+        const uint32_t nrows = B.row_end - B.row_begin, units = C.units;
         const uint32_t first = (warp + nwarps - (k % nwarps)) % nwarps;
-        for (uint32_t i = first; i < nrows; i += 2u * nwarps) {
-            const uint32_t i2 = i + nwarps;
-            const bool two = i2 < nrows;
-            float sum0, sum1;
-            if (B.resident) {
-                const uint32_t base = saddr(sm.wres + B.sm_off);
-                row_pair_sums<true>(nullptr, nullptr, base + 4u * ld * i, base + 4u * ld * (two ? i2 : i), units, lane,
-                                    two, sum0, sum1);
-            } else {
-                const float* g = C.w + static_cast<size_t>(B.row_begin) * ld;
-                row_pair_sums<false>(g + static_cast<size_t>(i) * ld, g + static_cast<size_t>(two ? i2 : i) * ld, 0u, 0u,
-                                     units, lane, two, sum0, sum1);
-            }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                sum0 += __shfl_xor_sync(kFull, sum0, o);
-                sum1 += __shfl_xor_sync(kFull, sum1, o);
-            }
-            if (lane == 0) {
-                const uint32_t r = B.srow + i;
-                sm.row[r].y = sum0 <= 0.0f ? 1.0f : __fdiv_rn(sm.rowtgt[r], sum0);
-                if (two) {
-                    const uint32_t r2 = B.srow + i2;
-                    sm.row[r2].y = sum1 <= 0.0f ? 1.0f : __fdiv_rn(sm.rowtgt[r2], sum1);
+        k += nrows;
+        if (!CARRY || B.resident) {
+            const uint32_t base = saddr(sm.wres + B.sm_off), ld = C.ld;
+            for (uint32_t i = first; i < nrows; i += 2u * nwarps) {
+                const uint32_t i2 = i + nwarps;
+                const bool two = i2 < nrows;
+                float sum0, sum1;
+                row_pair_sums(base + 4u * ld * i, base + 4u * ld * (two ? i2 : i), units, lane, two, sum0, sum1);
+                sum0 = warp_sum(sum0);
+                sum1 = warp_sum(sum1);
+                if (lane == 0) {
+                    const uint32_t r = B.srow + i;
+                    sm.row[r].y = sum0 <= 0.0f ? 1.0f : __fdiv_rn(sm.rowtgt[r], sum0);
+                    if (two) {
+                        const uint32_t r2 = B.srow + i2;
+                        sm.row[r2].y = sum1 <= 0.0f ? 1.0f : __fdiv_rn(sm.rowtgt[r2], sum1);
+                    }
                 }
             }
+            continue;
         }
-        k += nrows;
+        const uint32_t nch = (units + 31u) / 32u;
+        // chunks holding a postsynaptic neuron that spiked (bit c % 32 of dirty<c / 32>; chunks past
+        // 128 are always recomputed)
+        uint32_t dirty0 = 0, dirty1 = 0, dirty2 = 0, dirty3 = 0;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const uint32_t c = lane + 32u * m;
+            bool d = false;
+            if (c < nch) {
+                const uint32_t q0 = 128u * c, q1 = q0 + 128u < C.n_post ? q0 + 128u : C.n_post;
+                const uint32_t g0 = C.post_off + q0, g1 = C.post_off + q1 - 1u;
+                for (uint32_t w = g0 >> 5; w <= (g1 >> 5); ++w) {
+                    uint32_t bits = sm.sbits[w];
+                    if (w == (g0 >> 5)) bits &= 0xffffffffu << (g0 & 31u);
+                    if (w == (g1 >> 5)) bits &= 0xffffffffu >> (31u - (g1 & 31u));
+                    d |= bits != 0u;
+                }
+            }
+            const uint32_t bal = __ballot_sync(kFull, d);
+            if (m == 0) dirty0 = bal;
+            else if (m == 1) dirty1 = bal;
+            else if (m == 2) dirty2 = bal;
+            else dirty3 = bal;
+        }
+        for (uint32_t i = first; i < nrows; i += nwarps) {
+            const uint32_t r = B.srow + i;
+            const bool all = sm.rowflag[r] != 0u;
+            for (uint32_t c0 = 0; c0 < nch; c0 += 8u) {
+                const uint32_t dm = c0 < 32u ? dirty0 : c0 < 64u ? dirty1 : c0 < 96u ? dirty2 : dirty3;
+                uint32_t need = all || c0 >= 128u ? 0xffu : (dm >> (c0 & 31u)) & 0xffu;
+                if (nch - c0 < 8u) need &= (1u << (nch - c0)) - 1u;
+                if (need) chunk_sums8(B, C, sm, i, c0, need, lane, n_chunks);
+            }
+            __syncwarp();
+            float s = 0.0f;
+            for (uint32_t c = lane; c < nch; c += 32u) s += sm.rsum[(B.trow + i) * n_chunks + c];
+            s = warp_sum(s);
+            if (lane == 0) sm.row[r].y = s <= 0.0f ? 1.0f : __fdiv_rn(sm.rowtgt[r], s);
+        }
     }
 }
 
-// Pass 2 over the rows of one block for NU units of the same block: normalise + store the updated
-// weights (SCALE: rows of a triplet plasticity) and accumulate this step's GEMV partial sums.
-// Each unit's rows are visited in row order, so NU only interleaves independent chains.
-template <bool RESIDENT, bool SCALE, int NU>
-__device__ __forceinline__ void block_rows(const DBlk& B, const DConn& C, const uint32_t (&u)[NU],
-                                           const SmemLayout& sm, bool accumulate, float4 (&acc)[NU]) {
+// Pass 2 over the rows of one block for unit u: normalise + store the updated weights (SCALE:
+// rows of a triplet plasticity with an update pending), accumulate this step's GEMV partial sums,
+// and (TRIP: rows of a triplet plasticity) leave the chunk sums of the stored weights in rsum.
+// All 32 lanes of a warp run this together on units 32c .. 32c+31 of one segment; lanes past the
+// segment's units (live = false) only take part in the chunk butterflies.
+template <bool RESIDENT, bool SCALE, bool TRIP>
+__device__ __forceinline__ float4 block_rows(const DBlk& B, const DConn& C, uint32_t u, bool live, const SmemLayout& sm,
+                                             bool accumulate, float4 acc, uint32_t n_chunks) {
     const uint32_t nrows = B.row_end - B.row_begin, ld = C.ld;
-    uint32_t sbase[NU];
-    float* gbase[NU];
-#pragma unroll
-    for (int n = 0; n < NU; ++n) {
-        sbase[n] = RESIDENT ? saddr(sm.wres + B.sm_off) + 16u * u[n] : 0u;
-        gbase[n] = RESIDENT ? nullptr : C.w + static_cast<size_t>(B.row_begin) * ld + 4u * u[n];
-    }
+    const uint32_t sbase = RESIDENT ? saddr(sm.wres + B.sm_off) + 16u * u : 0u;
+    float* gbase = RESIDENT ? nullptr : C.w + static_cast<size_t>(B.row_begin) * ld + 4u * u;
     const float2* rowp = reinterpret_cast<const float2*>(sm.row + B.srow);  // {x, scale} of each row
-    constexpr int kB = (RESIDENT || SCALE) ? 4 : 8;
+    const uint32_t lane = threadIdx.x & 31u, chunk = u / 32u;
+    constexpr int kB = (RESIDENT || SCALE || TRIP) ? 4 : 8;
     for (uint32_t i0 = 0; i0 < nrows; i0 += kB) {
-        float4 wb[NU][kB];
+        float4 wb[kB];
 #pragma unroll
         for (int b = 0; b < kB; ++b) {
             if (i0 + b < nrows) {
-#pragma unroll
-                for (int n = 0; n < NU; ++n) {
-                    if constexpr (RESIDENT) wb[n][b] = lds4(sbase[n] + 4u * ld * (i0 + b));
-                    else wb[n][b] = ld_col4(gbase[n] + static_cast<size_t>(i0 + b) * ld);
-                }
+                if constexpr (RESIDENT) wb[b] = lds4(sbase + 4u * ld * (i0 + b));
+                else wb[b] = ld_col4(gbase + static_cast<size_t>(i0 + b) * ld);
             }
         }
+        float p[kB];
 #pragma unroll
         for (int b = 0; b < kB; ++b) {
-            if (i0 + b >= nrows) break;
+            p[b] = 0.0f;
+            if (i0 + b >= nrows) continue;
             const uint32_t i = i0 + b;
             const float2 rw = rowp[2u * i];
+            float4 w4 = wb[b];
+            if constexpr (SCALE) {
+                w4.x *= rw.y;
+                w4.y *= rw.y;
+                w4.z *= rw.y;
+                w4.w *= rw.y;
+                if (live) {
+                    if constexpr (RESIDENT) sts4(sbase + 4u * ld * i, w4);
+                    else __stcg(reinterpret_cast<float4*>(gbase + static_cast<size_t>(i) * ld), w4);
+                }
+            }
+            if constexpr (TRIP) p[b] = live ? unit_sum(w4) : 0.0f;
+            if (accumulate) {
+                acc.x = fmaf(w4.x, rw.x, acc.x);
+                acc.y = fmaf(w4.y, rw.x, acc.y);
+                acc.z = fmaf(w4.z, rw.x, acc.z);
+                acc.w = fmaf(w4.w, rw.x, acc.w);
+            }
+        }
+        if constexpr (TRIP) {
 #pragma unroll
-            for (int n = 0; n < NU; ++n) {
-                float4 w4 = wb[n][b];
-                if constexpr (SCALE) {
-                    w4.x *= rw.y;
-                    w4.y *= rw.y;
-                    w4.z *= rw.y;
-                    w4.w *= rw.y;
-                    if constexpr (RESIDENT) sts4(sbase[n] + 4u * ld * i, w4);
-                    else __stcg(reinterpret_cast<float4*>(gbase[n] + static_cast<size_t>(i) * ld), w4);
-                }
-                if (accumulate) {
-                    acc[n].x = fmaf(w4.x, rw.x, acc[n].x);
-                    acc[n].y = fmaf(w4.y, rw.x, acc[n].y);
-                    acc[n].z = fmaf(w4.z, rw.x, acc[n].z);
-                    acc[n].w = fmaf(w4.w, rw.x, acc[n].w);
-                }
+            for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+                for (int b = 0; b < kB; ++b) p[b] += __shfl_xor_sync(kFull, p[b], o);
+            }
+            if (lane == 0) {
+#pragma unroll
+                for (int b = 0; b < kB; ++b)
+                    if (i0 + b < nrows) sm.rsum[(B.trow + i0 + b) * n_chunks + chunk] = p[b];
             }
         }
     }
+    return acc;
 }
 
-// All blocks of segment SG for NU of its units; the partial sums go to the segment's slot.
-// `pending` = a triplet normalisation of the previous step is to be applied.
-template <int NU>
-__device__ __forceinline__ void segment_units(const Desc& D, const DSeg& SG, const DBlk* s_blk, const uint32_t (&u)[NU],
-                                              bool pending, bool accumulate, const SmemLayout& sm, float* part_out,
-                                              uint32_t npad) {
-    float4 acc[NU];
-#pragma unroll
-    for (int n = 0; n < NU; ++n) acc[n] = make_float4(0.f, 0.f, 0.f, 0.f);
+// All blocks of segment SG for unit u; the partial sums go to the segment's slot.  `pending` = an
+// update of the previous step is to be applied (normalised triplet rows are rescaled and stored).
+// CARRY: the network has streamed triplet rows (a kernel instance of its own, so that networks
+// without them do not pay for the extra code).
+template <bool CARRY>
+__device__ __forceinline__ void segment_unit(const Desc& D, const DSeg& SG, const DBlk* s_blk, uint32_t u, bool live,
+                                             bool pending, bool accumulate, const SmemLayout& sm, float* part_out,
+                                             uint32_t npad, uint32_t n_chunks) {
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
     bool touched = false;
     for (uint32_t bk = SG.blk_begin; bk < SG.blk_end; ++bk) {
         const DBlk B = s_blk[bk];
         const DConn& C = D.conns[B.conn];
-        const bool scale = pending && C.plast >= 0 && D.plast[C.plast].kind == kKindTriplet;
+        const bool trip = C.plast >= 0 && D.plast[C.plast].kind == kKindTriplet;
+        const bool scale = pending && trip;
         if (!scale && !accumulate) continue;
         touched = true;
-        if (scale) {
-            if (B.resident) block_rows<true, true, NU>(B, C, u, sm, accumulate, acc);
-            else block_rows<false, true, NU>(B, C, u, sm, accumulate, acc);
+        if (CARRY && trip && accumulate && !B.resident) {
+            if (scale) {
+                acc = B.resident ? block_rows<true, true, true>(B, C, u, live, sm, true, acc, n_chunks)
+                                 : block_rows<false, true, true>(B, C, u, live, sm, true, acc, n_chunks);
+            } else {
+                acc = B.resident ? block_rows<true, false, true>(B, C, u, live, sm, true, acc, n_chunks)
+                                 : block_rows<false, false, true>(B, C, u, live, sm, true, acc, n_chunks);
+            }
+        } else if (scale) {
+            acc = B.resident ? block_rows<true, true, false>(B, C, u, live, sm, accumulate, acc, n_chunks)
+                             : block_rows<false, true, CARRY>(B, C, u, live, sm, accumulate, acc, n_chunks);
         } else {
-            if (B.resident) block_rows<true, false, NU>(B, C, u, sm, true, acc);
-            else block_rows<false, false, NU>(B, C, u, sm, true, acc);
+            acc = B.resident ? block_rows<true, false, false>(B, C, u, live, sm, true, acc, n_chunks)
+                             : block_rows<false, false, false>(B, C, u, live, sm, true, acc, n_chunks);
         }
     }
-    if (accumulate && touched) {
-#pragma unroll
-        for (int n = 0; n < NU; ++n)
-            *reinterpret_cast<float4*>(part_out + static_cast<size_t>(SG.slot) * npad + SG.pcol + 4u * u[n]) = acc[n];
-    }
+    if (accumulate && touched && live)
+        *reinterpret_cast<float4*>(part_out + static_cast<size_t>(SG.slot) * npad + SG.pcol + 4u * u) = acc;
 }
 
 // Pass 2: each thread owns work items (one 4-column unit of one segment) and walks all of the
-// segment's rows; per item the partial sums go to the parity-`par` slot of this CTA.  With
-// kPairedUnits a thread's items it and it + blockDim of the same segment are processed together
-// (off: at 256 threads the paired loop does not fit the register file without spills).
-constexpr bool kPairedUnits = false;
-__device__ __forceinline__ void weight_pass(const DSim* S, const Desc& D, const DCta& cta, bool pending, bool accumulate,
-                                         uint32_t par, const SmemLayout& sm, const DSeg* s_seg, const DBlk* s_blk,
-                                         uint32_t n_seg) {
+// segment's rows; per item the partial sums go to the parity-`par` slot of this CTA.  A warp's
+// 32 items always lie in one segment (segments start at multiples of 32 items).
+template <bool CARRY>
+__device__ __forceinline__ void weight_pass(const Desc& D, const DCta& cta, bool pending, bool accumulate, uint32_t par,
+                                         const SmemLayout& sm, const DSeg* s_seg, const DBlk* s_blk, uint32_t n_seg,
+                                         uint32_t n_chunks) {
     float* part_out = D.partials + static_cast<size_t>(par) * D.n_slots * D.N_pad;
-    const uint32_t npad = D.N_pad, nthr = blockDim.x;
-    for (uint32_t it0 = 0; it0 < cta.n_items; it0 += 2u * nthr) {
-        const uint32_t ia = it0 + threadIdx.x, ib = ia + nthr;
-        const int sa = seg_of_item(s_seg, n_seg, ia);
-        const int sb = seg_of_item(s_seg, n_seg, ib);
-        const bool va = sa >= 0 && ia - s_seg[sa].item_begin < s_seg[sa].units;
-        const bool vb = sb >= 0 && ib - s_seg[sb].item_begin < s_seg[sb].units;
-        if (kPairedUnits && va && vb && sa == sb) {
-            const uint32_t u2[2] = {ia - s_seg[sa].item_begin, ib - s_seg[sa].item_begin};
-            segment_units<2>(D, s_seg[sa], s_blk, u2, pending, accumulate, sm, part_out, npad);
-        } else {
-            if (va) {
-                const uint32_t u1[1] = {ia - s_seg[sa].item_begin};
-                segment_units<1>(D, s_seg[sa], s_blk, u1, pending, accumulate, sm, part_out, npad);
-            }
-            if (vb) {
-                const uint32_t u1[1] = {ib - s_seg[sb].item_begin};
-                segment_units<1>(D, s_seg[sb], s_blk, u1, pending, accumulate, sm, part_out, npad);
-            }
-        }
+    const uint32_t npad = D.N_pad;
+    for (uint32_t it0 = 0; it0 < cta.n_items; it0 += blockDim.x) {
+        const uint32_t it = it0 + threadIdx.x;
+        const int s = seg_of_item(s_seg, n_seg, it);
+        if (s < 0) continue;  // the whole warp
+        const DSeg& SG = s_seg[s];
+        const uint32_t u = it - SG.item_begin;
+        const bool live = u < SG.units;
+        if (!live && !(CARRY && SG.carried)) continue;  // only the chunk butterflies need every lane
+        segment_unit<CARRY>(D, SG, s_blk, live ? u : SG.units - 1u, live, pending, accumulate, sm, part_out, npad, n_chunks);
     }
 }
 
@@ -1033,6 +1109,7 @@ __device__ __forceinline__ void copy_words(void* dst, const void* src, size_t by
     for (size_t k = threadIdx.x; k < bytes / 4; k += blockDim.x) d[k] = s[k];
 }
 
+template <bool CARRY>
 __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* __restrict__ S, uint32_t n_steps) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ Desc s_d;
@@ -1055,7 +1132,8 @@ __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* _
     for (uint32_t m = 0; m < S->n_mons; ++m) n_spike_mons += S->mons[m].kind == kMonSpikes ? 1u : 0u;
     const NsLayout L0 = ns_layout(S->ns_ts, S->ns_pre, S->ns_post, S->ns_mon);
     const SmemSizes z = smem_sizes(S->resident_floats, max_rows, max_own, S->spk_words, n_spike_mons, S->n_groups,
-                                   S->n_ts, S->n_conns, S->n_plast, S->n_mons, S->n_red, L0.fields);
+                                   S->n_ts, S->n_conns, S->n_plast, S->n_mons, S->n_red, L0.fields,
+                                   S->max_trows * S->n_chunks);
     if (threadIdx.x == 0) {
         s_L = L0;
         unsigned char* p = smem_raw;
@@ -1079,6 +1157,8 @@ __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* _
         p += z.rowfac;
         sm.ns = reinterpret_cast<float*>(p);
         p += z.ns;
+        sm.rsum = reinterpret_cast<float*>(p);
+        p += z.rsum;
         sm.red = reinterpret_cast<float*>(p);
         p += z.redscr;
         sm.bits = reinterpret_cast<uint32_t*>(p);
@@ -1181,6 +1261,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* _
     const uint32_t nwarps = blockDim.x >> 5;
     const uint32_t n_own = cta.n1 - cta.n0;
     const uint32_t neuron_warps = (n_own + 31u) / 32u;
+    const uint32_t n_chunks = S->n_chunks;
     // The normalisation pass runs beside the neuron phase on the warps the neurons leave free.
     const bool norm_beside = neuron_warps < nwarps;
     for (uint32_t b = threadIdx.x; b < s_nblk; b += blockDim.x) s_blk[b] = S->blks[s_blk_base + b];
@@ -1256,7 +1337,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* _
                 apply_updates(D, s_blk, s_nblk, ppar, sm, neuron_warps, nw);
                 if (norm_now) {
                     named_barrier_sync(1u, 32u * nw);
-                    norm_rows(D, sm, s_blk, s_nblk, neuron_warps, nw);
+                    norm_rows<CARRY>(D, sm, s_blk, s_nblk, neuron_warps, nw, n_chunks);
                 }
             }
             __syncthreads();
@@ -1268,7 +1349,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* _
             neuron_phase(S, D, cta, t, clock, par, pending, sm, max_own, L, s_ev[0], s_ev[1]);
             __syncthreads();
             if (norm_now) {
-                norm_rows(D, sm, s_blk, s_nblk, 0u, nwarps);
+                norm_rows<CARRY>(D, sm, s_blk, s_nblk, 0u, nwarps, n_chunks);
                 __syncthreads();
             }
         }
@@ -1277,7 +1358,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* _
         rows_x(D, cta, sm, max_own);
         __syncthreads();
         BSNN_TMARK(2);
-        weight_pass(S, D, cta, pending, true, par, sm, s_seg, s_blk, n_seg);
+        weight_pass<CARRY>(D, cta, pending, true, par, sm, s_seg, s_blk, n_seg, n_chunks);
         __syncthreads();
         BSNN_TMARK(4);
         if (!grid_barrier(D.barrier, D.error, bar0 + (k + 1ull) * gridDim.x, &s_ok)) {
@@ -1302,10 +1383,10 @@ __global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* _
     apply_updates(D, s_blk, s_nblk, lpar, sm, 0u, nwarps);
     __syncthreads();
     if (s_has_norm) {
-        norm_rows(D, sm, s_blk, s_nblk, 0u, nwarps);
+        norm_rows<CARRY>(D, sm, s_blk, s_nblk, 0u, nwarps, n_chunks);
         __syncthreads();
     }
-    weight_pass(S, D, cta, true, false, lpar, sm, s_seg, s_blk, n_seg);
+    weight_pass<CARRY>(D, cta, true, false, lpar, sm, s_seg, s_blk, n_seg, n_chunks);
     __syncthreads();
     move_resident(D, s_blk, s_nblk, sm, false);
     load_partials(S, D, cta, lpar, sm, max_own);
