@@ -275,6 +275,11 @@ SIGNATURES = {
     "bsnn_read_spike_bits": (_I32, [_P, _U32, _UP, _I32]),
     "bsnn_read_voltage_history": (_I32, [_P, _U32, _FP, _I32]),
     "bsnn_get_device_pointer": (_I32, [_P, _I32, _U32, ctypes.POINTER(_P)]),
+    "bsnn_set_monitor_output": (_I32, [_P, _U32, ctypes.c_char_p]),
+    "bsnn_add_weight_recorder": (_I32, [_P, _U32, ctypes.c_char_p]),
+    "bsnn_record": (_I32, [_P, _U32]),
+    "bsnn_flush_records": (_I32, [_P]),
+    "bsnn_run_system": (_I32, [_P, _U32]),
     "bsnn_connection_propagate": (_I32, [ctypes.POINTER(ConnectionView), _P]),
     "bsnn_connection_propagate_noalloc": (_I32, [ctypes.POINTER(ConnectionView), _P]),
 }

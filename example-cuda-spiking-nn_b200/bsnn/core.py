@@ -191,6 +191,27 @@ class Simulation:
         self._check(self._lib.bsnn_read_voltage_history(self._h, monitor, _ptr(out, ctypes.c_float), int(flush)))
         return out
 
+    # -- recording to text files (Monitor::record) ------------------------------------------------
+    def set_monitor_output(self, monitor: int, path) -> None:
+        """Output file of a spike or voltage recorder (the reference's output_filepath)."""
+        self._check(self._lib.bsnn_set_monitor_output(self._h, monitor, str(path).encode()))
+
+    def add_weight_recorder(self, connection: int, path) -> None:
+        """WeightRecorder: weight triples at recorded clock steps that are multiples of 100,000."""
+        self._check(self._lib.bsnn_add_weight_recorder(self._h, connection, str(path).encode()))
+
+    def record(self, clock_step: int) -> None:
+        """Monitor::record(clock_step) of every recorder with an output."""
+        self._check(self._lib.bsnn_record(self._h, clock_step))
+
+    def flush_records(self) -> None:
+        """Waits until every queued record is written."""
+        self._check(self._lib.bsnn_flush_records(self._h))
+
+    def run_system(self, total_clock_steps: int) -> None:
+        """System::run without callbacks: steps 0 .. total-1, recording at multiples of the interval."""
+        self._check(self._lib.bsnn_run_system(self._h, total_clock_steps))
+
     def device_pointer(self, name: str, index: int = 0) -> int:
         p = ctypes.c_void_p()
         self._check(self._lib.bsnn_get_device_pointer(self._h, FIELD[name], index, ctypes.byref(p)))

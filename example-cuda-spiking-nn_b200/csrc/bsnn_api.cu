@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
 #include <map>
 #include <memory>
 #include <numeric>
@@ -24,6 +25,7 @@
 #include "bsnn_device.cuh"
 #include "propagate.cuh"
 #include "propagate_static.cuh"
+#include "records.h"
 #include "step_kernel.cuh"
 
 using namespace bsnn;
@@ -61,6 +63,12 @@ struct HostMon {
     int32_t kind;
     uint32_t group, interval;
     std::vector<uint32_t> sel;
+    std::string path;                        // output file (set by bsnn_set_monitor_output)
+    std::shared_ptr<std::ofstream> spike_out;  // spike recorder's open file
+};
+struct HostWeightRec {
+    uint32_t conn;
+    std::string path;
 };
 struct HostStim {
     std::vector<uint32_t> counts, ids, offs;
@@ -91,6 +99,8 @@ struct bsnn_sim {
     std::vector<HostConn> conns;
     std::vector<HostPlast> plasts;
     std::vector<HostMon> mons;
+    std::vector<HostWeightRec> wrecs;
+    std::unique_ptr<rec::Writer> writer;  // formats and writes recorded text off the stepping thread
     std::vector<HostStim> stims;
     int32_t noise_mode = BSNN_NOISE_PHILOX;
     std::vector<uint8_t> replay;
@@ -115,6 +125,9 @@ struct bsnn_sim {
     std::vector<uint32_t> conn_ld;
 
     ~bsnn_sim() {
+        writer.reset();  // finishes the queued writes
+        for (auto& m : mons)
+            if (m.spike_out) m.spike_out->flush();
         for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
         if (arena) cudaFree(arena);
         if (stream) cudaStreamDestroy(stream);
@@ -949,6 +962,74 @@ FieldRef field_ref(bsnn_sim* s, int32_t field, uint32_t index) {
 }  // namespace
 
 // ============================================================================================
+namespace {
+
+// Monitor::record(clock_step) for every recorder with an output (cpp_src/monitors/*.cpp): the
+// rings are copied to host memory and flushed here; the text is written by the writer thread.
+void record_all(bsnn_sim* s, uint32_t clock_step) {
+    finalize(s);
+    check_device_error(s);
+    if (!s->writer) s->writer = std::make_unique<rec::Writer>();
+    for (uint32_t m = 0; m < s->mons.size(); ++m) {
+        HostMon& hm = s->mons[m];
+        if (hm.path.empty()) continue;
+        const DMon& M = s->h.mons[m];
+        const uint32_t ng = s->groups[M.group].p.num_neurons, interval = M.interval;
+        if (M.kind == kMonSpikes) {
+            if (clock_step < interval) continue;  // spike_recorder.cpp:41-43
+            const size_t n = static_cast<size_t>(interval) * M.words;
+            auto bits = std::make_shared<std::vector<uint32_t>>(n);
+            cuda_check(cudaMemcpy(bits->data(), M.bits, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost), "D2H spike ring");
+            cuda_check(cudaMemsetAsync(M.bits, 0, sizeof(uint32_t) * n, s->stream), "flush spike ring");
+            auto out = hm.spike_out;
+            const uint32_t words = M.words;
+            s->writer->push([bits, out, words, ng, interval, clock_step] {
+                std::string text;
+                rec::spike_rows(text, bits->data(), words, ng, interval, clock_step);
+                if (out && out->good()) out->write(text.data(), static_cast<std::streamsize>(text.size()));
+            });
+        } else {
+            const size_t n = static_cast<size_t>(interval) * M.n_sel;
+            auto vh = std::make_shared<std::vector<float>>(n);
+            cuda_check(cudaMemcpy(vh->data(), M.vh, sizeof(float) * n, cudaMemcpyDeviceToHost), "D2H voltage ring");
+            cuda_check(cudaMemsetAsync(M.vh, 0, sizeof(float) * n, s->stream), "flush voltage ring");
+            // ring column of each selected neuron: its first occurrence in the selection
+            std::vector<int32_t> first(ng, -1);
+            auto col = std::make_shared<std::vector<uint32_t>>(hm.sel.size());
+            for (size_t k = 0; k < hm.sel.size(); ++k) {
+                if (first[hm.sel[k]] < 0) first[hm.sel[k]] = static_cast<int32_t>(k);
+                (*col)[k] = static_cast<uint32_t>(first[hm.sel[k]]);
+            }
+            auto sel = std::make_shared<std::vector<uint32_t>>(hm.sel);
+            const std::string path = hm.path;
+            const uint32_t n_cols = M.n_sel;
+            s->writer->push([vh, col, sel, path, n_cols, interval, clock_step] {
+                for (uint32_t slot = 0; slot < interval; ++slot) {  // voltage_recorder.cpp:60-76
+                    std::string text;
+                    rec::voltage_file(text, *sel, *col, vh->data(), n_cols, slot);
+                    rec::write_file(rec::step_path(path, clock_step - interval + slot + 1u), text);
+                }
+            });
+        }
+    }
+    for (const auto& wr : s->wrecs) {
+        if (clock_step % 100000u != 0u) continue;  // weight_recorder.cpp:26-28
+        const DConn& C = s->h.conns[wr.conn];
+        const size_t n = static_cast<size_t>(C.n_pre) * C.ld;
+        auto w = std::make_shared<std::vector<float>>(n);
+        cuda_check(cudaMemcpy(w->data(), C.w, sizeof(float) * n, cudaMemcpyDeviceToHost), "D2H weights");
+        const std::string path = wr.path;
+        const uint32_t n_pre = C.n_pre, n_post = C.n_post, ld = C.ld;
+        s->writer->push([w, path, n_pre, n_post, ld, clock_step] {
+            std::string text;
+            rec::weight_file(text, w->data(), n_pre, n_post, ld);
+            rec::write_file(rec::step_path(path, clock_step), text);
+        });
+    }
+}
+
+}  // namespace
+
 extern "C" {
 
 BSNN_API const char* bsnn_version(void) { return "bsnn 0.1 (sm_100a persistent step kernel)"; }
@@ -1339,6 +1420,66 @@ BSNN_API bsnn_status bsnn_get_device_pointer(const bsnn_sim* sim, int32_t field,
     return guarded(s, [&] {
         finalize(s);
         *out = field_ref(s, field, index).ptr;
+    });
+}
+
+BSNN_API bsnn_status bsnn_set_monitor_output(bsnn_sim* sim, uint32_t monitor, const char* path) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        require(monitor < sim->mons.size(), BSNN_ERR_OUT_OF_RANGE, "monitor index out of range");
+        require(path != nullptr && *path != '\0', BSNN_ERR_INVALID_ARGUMENT, "empty output path");
+        HostMon& m = sim->mons[monitor];
+        const std::string p(path);
+        if (m.kind == kMonSpikes) {
+            // SpikeRecorder ctor: the file is truncated and gets its header now (spike_recorder.cpp:3-28)
+            if (sim->writer) sim->writer->drain();
+            m.spike_out = std::make_shared<std::ofstream>(p, std::ios::out | std::ios::trunc | std::ios::binary);
+            if (m.spike_out->good()) *m.spike_out << "clock_step, neuron_ids\n";
+        } else {
+            // per-step file names are made by inserting "_step<N>" before ".txt" (voltage_recorder.cpp:62-64)
+            require(p.rfind(".txt") != std::string::npos, BSNN_ERR_OUT_OF_RANGE, "output path must contain \".txt\"");
+        }
+        m.path = p;
+    });
+}
+
+BSNN_API bsnn_status bsnn_add_weight_recorder(bsnn_sim* sim, uint32_t connection, const char* path) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        require(connection < sim->conns.size(), BSNN_ERR_OUT_OF_RANGE, "connection index out of range");
+        require(path != nullptr && std::string(path).rfind(".txt") != std::string::npos, BSNN_ERR_OUT_OF_RANGE,
+                "output path must contain \".txt\"");
+        sim->wrecs.push_back(HostWeightRec{connection, std::string(path)});
+    });
+}
+
+BSNN_API bsnn_status bsnn_record(bsnn_sim* sim, uint32_t clock_step) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] { record_all(sim, clock_step); });
+}
+
+BSNN_API bsnn_status bsnn_flush_records(bsnn_sim* sim) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        if (sim->writer) sim->writer->drain();
+        for (auto& m : sim->mons)
+            if (m.spike_out) m.spike_out->flush();
+    });
+}
+
+BSNN_API bsnn_status bsnn_run_system(bsnn_sim* sim, uint32_t total_clock_steps) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        const uint32_t interval = sim->desc.recording_interval_steps;
+        uint32_t step = 0;
+        while (step < total_clock_steps) {
+            // record after every step that is a multiple of the interval (system.cpp:71-76)
+            const uint64_t next = (static_cast<uint64_t>(step) + interval - 1u) / interval * interval;
+            const uint32_t end = static_cast<uint32_t>(std::min<uint64_t>(total_clock_steps, next + 1u));
+            run_steps(sim, step, end - step);
+            if (end == next + 1u) record_all(sim, static_cast<uint32_t>(next));
+            step = end;
+        }
     });
 }
 

@@ -270,6 +270,31 @@ BSNN_API bsnn_status bsnn_read_voltage_history(bsnn_sim* sim, uint32_t monitor, 
 /* Device address of a field (for the C++ facade's *View structs); read-only use. */
 BSNN_API bsnn_status bsnn_get_device_pointer(const bsnn_sim* sim, int32_t field, uint32_t index, void** out);
 
+/* ---- recording to text files (Monitor::record) --------------------------------------------- */
+
+/* Output file of a spike or voltage recorder: the output_filepath of SpikeRecorder /
+ * VoltageRecorder (cpp_src/monitors/spike_recorder.cpp:3-14, voltage_recorder.cpp:3-28).  A spike
+ * recorder's file is truncated now and gets the header "clock_step, neuron_ids"; a voltage recorder
+ * writes one file per recorded step, named by inserting "_step<N>" before the ".txt" that `path`
+ * must contain (else BSNN_ERR_OUT_OF_RANGE).  A file that cannot be opened is skipped, as the
+ * reference skips output when its stream is not good(). */
+BSNN_API bsnn_status bsnn_set_monitor_output(bsnn_sim* sim, uint32_t monitor, const char* path);
+/* WeightRecorder (cpp_src/monitors/weight_recorder.cpp:3-51): at recorded clock steps that are
+ * multiples of 100,000, writes "<path with _step<N>>" holding "pre_neuron_id, post_neuron_id,
+ * weight" and every (pre, post) triple, zeros included.  May be added at any time. */
+BSNN_API bsnn_status bsnn_add_weight_recorder(bsnn_sim* sim, uint32_t connection, const char* path);
+/* Monitor::record(clock_step) of every recorder with an output (spike_recorder.cpp:40-60,
+ * voltage_recorder.cpp:54-78, weight_recorder.cpp:25-51), in the reference's formats and labels:
+ * the rings are copied out and flushed before the call returns; the text is formatted and written
+ * by a writer thread of the sim, so stepping can continue meanwhile. */
+BSNN_API bsnn_status bsnn_record(bsnn_sim* sim, uint32_t clock_step);
+/* Waits until every record queued so far is written and flushed. */
+BSNN_API bsnn_status bsnn_flush_records(bsnn_sim* sim);
+/* System::run(total_clock_steps) (cpp_src/core/system.cpp:65-84) without step callbacks: clock
+ * steps 0 .. total-1, with bsnn_record after every step that is a multiple of the state's
+ * recording_interval_steps.  The reference's progress lines on stdout are not printed. */
+BSNN_API bsnn_status bsnn_run_system(bsnn_sim* sim, uint32_t total_clock_steps);
+
 /* ---- one connection on caller-owned device buffers ------------------------------------------ */
 
 /* cpp_src/connections/connection_view.h:8-31, same field names, order and layout, so the address of

@@ -14,6 +14,10 @@
 //   ref_harness <net.bin> time <warmup> <steps>
 //       times <steps> calls of System::step_the_clock (the hot path; Monitor::record's text
 //       output is not part of it) and prints one JSON line.
+//   ref_harness <net.bin> record <steps> <outdir>
+//       the step loop of System::run with the network's recorders (and a WeightRecorder per
+//       connection) writing their text files into <outdir>, plus the Poisson counts of every step
+//       in <outdir>/noise.bin, so the files can be reproduced with the noise replayed.
 #include <cuda_runtime.h>
 #include <curand_kernel.h>
 
@@ -21,6 +25,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
 #include <fstream>
 #include <memory>
 #include <stdexcept>
@@ -38,6 +43,7 @@
 #include "system.h"
 #include "triplet_plasticity.h"
 #include "voltage_recorder.h"
+#include "weight_recorder.h"
 
 namespace {
 
@@ -97,7 +103,10 @@ void d2h_append(std::ofstream& out, const T* dptr, size_t n) {
 int main(int argc, char** argv) {
     try {
         if (argc < 3) {
-            std::fprintf(stderr, "usage: %s net.bin dump <steps> <out.bin> <every> | time <warmup> <steps>\n", argv[0]);
+            std::fprintf(stderr,
+                         "usage: %s net.bin dump <steps> <out.bin> <every> | time <warmup> <steps> | "
+                         "record <steps> <outdir>\n",
+                         argv[0]);
             return 2;
         }
         Reader r(argv[1]);
@@ -162,20 +171,64 @@ int main(int argc, char** argv) {
             else if (kind == 2) system.add_plasticity(std::make_unique<IstdpPlasticity>(*conns[conn], p, state));
             else system.add_plasticity(std::make_unique<StdpPlasticity>(*conns[conn], p, state));
         }
+        // In record mode the recorders write their real files into <outdir> (spikes_m<k>.txt,
+        // voltage_m<k>.txt, weights_c<c>.txt); otherwise their output goes to /dev/null.
+        const std::string mode = argv[2];
+        const bool recording = mode == "record" && argc >= 5;
+        const std::string outdir = recording ? std::string(argv[4]) : std::string();
         static const std::string null_path = "/dev/null";
+        // VoltageRecorder keeps a reference to its path (voltage_recorder.h:40), so the strings
+        // must outlive the recorders.
+        std::deque<std::string> paths;
+        std::vector<Monitor*> monitors;
         const uint32_t n_mons = r.get<uint32_t>();
         for (uint32_t m = 0; m < n_mons; ++m) {
             const int32_t kind = r.get<int32_t>();
             const uint32_t group = r.get<uint32_t>();
             const uint32_t n_ids = r.get<uint32_t>();
             std::vector<uint32_t> sel = r.vec<uint32_t>(n_ids);
+            std::unique_ptr<Monitor> mon;
+            paths.push_back(recording ? outdir + (kind == 0 ? "/spikes_m" : "/voltage_m") + std::to_string(m) + ".txt"
+                                      : null_path);
             if (kind == 0)
-                system.add_monitor(std::make_unique<SpikeRecorder>(*groups[group], null_path, interval, state));
+                mon = std::make_unique<SpikeRecorder>(*groups[group], paths.back(), interval, state);
             else
-                system.add_monitor(std::make_unique<VoltageRecorder>(*groups[group], null_path, sel, interval, state));
+                mon = std::make_unique<VoltageRecorder>(*groups[group], paths.back(), sel, interval, state);
+            monitors.push_back(mon.get());
+            system.add_monitor(std::move(mon));
         }
+        if (recording)
+            for (uint32_t c = 0; c < n_conns; ++c) {
+                paths.push_back(outdir + "/weights_c" + std::to_string(c) + ".txt");
+                auto mon = std::make_unique<WeightRecorder>(*conns[c], paths.back(), state);
+                monitors.push_back(mon.get());
+                system.add_monitor(std::move(mon));
+            }
 
-        const std::string mode = argv[2];
+        if (recording) {
+            // The loop of System::run (cpp_src/core/system.cpp:65-84) with the Poisson counts of every
+            // step recorded (as in dump mode) into <outdir>/noise.bin: [steps][N][2] uint8.
+            const uint32_t steps = static_cast<uint32_t>(std::atoi(argv[3]));
+            uint8_t* d_counts = nullptr;
+            check(cudaMalloc(&d_counts, N * 2), "cudaMalloc counts");
+            check(cudaMemset(d_counts, 0, N * 2), "memset counts");
+            std::vector<uint8_t> all_counts, h_counts(N * 2);
+            for (uint32_t s = 0; s < steps; ++s) {
+                for (const auto& g : ginfo)
+                    peek_poisson_counts<<<(g.n + 255) / 256, 256>>>(state.d_neuron_rng_states(), g.offset, g.n,
+                                                                    g.mean_e, g.mean_i, d_counts);
+                check(cudaGetLastError(), "peek launch");
+                check(cudaMemcpy(h_counts.data(), d_counts, N * 2, cudaMemcpyDeviceToHost), "counts D2H");
+                all_counts.insert(all_counts.end(), h_counts.begin(), h_counts.end());
+                system.step_the_clock(s);
+                if (s % buryn::recording_interval_steps == 0)
+                    for (Monitor* mon : monitors) mon->record(s);
+            }
+            check(cudaFree(d_counts), "cudaFree");
+            std::ofstream nf(outdir + "/noise.bin", std::ios::binary);
+            nf.write(reinterpret_cast<const char*>(all_counts.data()), static_cast<std::streamsize>(all_counts.size()));
+            return 0;
+        }
         if (mode == "time") {
             const uint32_t warm = static_cast<uint32_t>(std::atoi(argv[3]));
             const uint32_t steps = static_cast<uint32_t>(std::atoi(argv[4]));

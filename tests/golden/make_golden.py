@@ -1,6 +1,6 @@
 """Records the golden fixtures of tests/golden/ from the reference's own CUDA implementation.
 
-    python tests/golden/make_golden.py [--out DIR]
+    python tests/golden/make_golden.py [--out DIR] [--only state|record]
 
 Needs a GPU and oracle/_ref/ref_harness (the reference's unmodified cpp_src components compiled
 for sm_100a by `make -C oracle ref`, linked with a driver that builds the network of a spec, calls
@@ -16,6 +16,10 @@ runs GOLDEN_STEPS steps and stores, in <name>.npz:
   pre_traces / post_traces  float32 [len(CHECK_STEPS), n_plast, N]
   weights_<c>  float32 [n_pre, n_post]  every connection's weights after the last step
   digest       sha256 of the network's inputs (specs.spec_digest)
+
+and, in record_random_120.npz, the text files the reference's SpikeRecorder, VoltageRecorder and
+WeightRecorder write over a System::run-style loop of RECORD_STEPS steps (ref_harness record
+mode), with that run's Poisson counts.
 
 Replaying `noise` makes every other input deterministic, so the oracle and the CUDA path can be
 compared with the reference step for step.
@@ -37,14 +41,14 @@ sys.path.insert(0, str(ROOT / "oracle"))
 sys.path.insert(0, str(HERE))
 
 import refnet  # noqa: E402
-from specs import CHECK_STEPS, GOLDEN_STEPS, golden_specs, spec_digest  # noqa: E402
+from specs import CHECK_STEPS, GOLDEN_STEPS, RECORD_STEPS, golden_specs, record_spec, spec_digest  # noqa: E402
 
 STATE_FIELDS = ["membrane_potentials", "g_excitatory", "g_inhibitory", "i_stimulus", "refractory_counter",
                 "background_g_excitatory", "background_g_inhibitory", "background_excitatory_r_traces",
                 "background_excitatory_d_traces", "background_inhibitory_r_traces", "background_inhibitory_d_traces"]
 
 
-def record(name, spec, out_dir: Path):
+def record_state(name, spec, out_dir: Path):
     with tempfile.TemporaryDirectory() as td:
         states, weights, noise = refnet.run_dump(spec, GOLDEN_STEPS, 1, td)
     steps = sorted(states)
@@ -72,16 +76,42 @@ def record(name, spec, out_dir: Path):
     print(f"{name}: {path.stat().st_size / 1e6:.2f} MB, {n_spk} spikes in {GOLDEN_STEPS} steps", flush=True)
 
 
+def record(spec, steps, out_dir: Path):
+    """The reference's recorder files of a System::run-style loop (ref_harness record mode): every
+    file's bytes as `file:<name>` (uint8) plus the Poisson counts of every step as `noise`."""
+    import subprocess
+    with tempfile.TemporaryDirectory() as td:
+        net = Path(td) / "net.bin"
+        files = Path(td) / "files"
+        files.mkdir()
+        refnet.write_network(spec, net)
+        subprocess.run([str(refnet.HARNESS), str(net), "record", str(steps), str(files)], check=True,
+                       stdout=subprocess.DEVNULL)
+        noise = np.fromfile(files / "noise.bin", np.uint8).reshape(steps, spec.num_neurons, 2)
+        arrays = {"noise": noise, "digest": np.array(spec_digest(spec)),
+                  "meta": np.array(json.dumps({"steps": steps, "interval": spec.recording_interval_steps}))}
+        for f in sorted(files.iterdir()):
+            if f.name != "noise.bin":
+                arrays["file:" + f.name] = np.frombuffer(f.read_bytes(), np.uint8)
+    path = out_dir / "record_random_120.npz"
+    np.savez_compressed(path, **arrays)
+    print(f"record_random_120: {path.stat().st_size / 1e6:.2f} MB, {len(arrays) - 3} files", flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=str(HERE))
+    ap.add_argument("--only", choices=["state", "record"], help="make one kind of fixture only")
     args = ap.parse_args()
     out = Path(args.out)
     out.mkdir(parents=True, exist_ok=True)
     if not refnet.HARNESS.exists():
         sys.exit(f"{refnet.HARNESS} is missing: build it with `make -C oracle ref`")
-    for name, spec in golden_specs().items():
-        record(name, spec, out)
+    if args.only != "record":
+        for name, spec in golden_specs().items():
+            record_state(name, spec, out)
+    if args.only != "state":
+        record(record_spec(), RECORD_STEPS, out)
 
 
 if __name__ == "__main__":

@@ -57,3 +57,21 @@ def spec_digest(spec) -> str:
     for m in spec.monitors:
         h.update(repr((m.kind, m.group, tuple(m.ids), m.interval)).encode())
     return h.hexdigest()
+
+
+RECORD_STEPS = 251  # System::run length of the recording fixture (records at steps 0, 50, ..., 250)
+
+
+def record_spec():
+    """The network of the recording fixture: the 96 E + 24 I random network with all three
+    plasticity rules, a recording interval of 50 steps and its stimulus pulse moved inside the
+    recorded steps; spike recorders on both groups, a voltage recorder on 8 E neurons."""
+    import bsnn
+    from bsnn import generation
+    r = bsnn.random_network(96, 24, steps=RECORD_STEPS + 1, seed=5, plasticity=("triplet", "istdp", "stdp"),
+                            stim_events=8)
+    r.recording_interval_steps = 50
+    ids = sorted(set(int(i) for i in r.stimulus[1]))
+    r.stimulus = generation.partial_group_multiple_square_waves(r.total_steps, ids, [0] * len(ids), [60], [140],
+                                                                [0.6e-9])
+    return r
