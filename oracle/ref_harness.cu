@@ -17,7 +17,8 @@
 //   ref_harness <net.bin> record <steps> <outdir>
 //       the step loop of System::run with the network's recorders (and a WeightRecorder per
 //       connection) writing their text files into <outdir>, plus the Poisson counts of every step
-//       in <outdir>/noise.bin, so the files can be reproduced with the noise replayed.
+//       in <outdir>/noise.bin, so the files can be reproduced with the noise replayed, and the
+//       final weights of every connection in <outdir>/weights_final_c<c>.bin.
 #include <cuda_runtime.h>
 #include <curand_kernel.h>
 
@@ -227,6 +228,11 @@ int main(int argc, char** argv) {
             check(cudaFree(d_counts), "cudaFree");
             std::ofstream nf(outdir + "/noise.bin", std::ios::binary);
             nf.write(reinterpret_cast<const char*>(all_counts.data()), static_cast<std::streamsize>(all_counts.size()));
+            for (uint32_t c = 0; c < n_conns; ++c) {  // final weights, raw float32 row-major
+                const std::vector<float> w = state.download_weight_matrix(conn_idx[c]);
+                std::ofstream wf(outdir + "/weights_final_c" + std::to_string(c) + ".bin", std::ios::binary);
+                wf.write(reinterpret_cast<const char*>(w.data()), static_cast<std::streamsize>(w.size() * sizeof(float)));
+            }
             return 0;
         }
         if (mode == "time") {

@@ -112,3 +112,29 @@ def read_dump(path, spec, steps):
     pos += 4
     noise = np.frombuffer(b, np.uint8, steps * N * 2, pos).copy().reshape(steps, N, 2)
     return states, weights, noise
+
+
+def run_record(spec, steps, outdir):
+    """ref_harness record mode: the reference's recorder files, the Poisson counts of every step
+    ([steps][N][2] uint8) and the final weights of every connection, all in `outdir`."""
+    outdir = Path(outdir)
+    outdir.mkdir(parents=True, exist_ok=True)
+    net = outdir / "net.bin"
+    write_network(spec, net)
+    subprocess.run([str(HARNESS), str(net), "record", str(steps), str(outdir)], check=True,
+                   stdout=subprocess.DEVNULL)
+    noise = np.fromfile(outdir / "noise.bin", np.uint8).reshape(steps, spec.num_neurons, 2)
+    weights = [np.fromfile(outdir / f"weights_final_c{c}.bin", np.float32).reshape(cn.weights.shape)
+               for c, cn in enumerate(spec.conns)]
+    return noise, weights
+
+
+def read_spike_rows(path):
+    """The rows of a SpikeRecorder file: {label: [neuron ids]}."""
+    rows = {}
+    with open(path) as f:
+        next(f)
+        for line in f:
+            label, _, ids = line.partition(", ")
+            rows[int(label)] = [int(x) for x in ids.split()]
+    return rows
