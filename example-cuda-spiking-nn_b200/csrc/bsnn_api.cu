@@ -600,11 +600,14 @@ void finalize(bsnn_sim* s) {
     h.max_own = P.max_own;
     std::memcpy(h.red_begin, P.red_begin, sizeof(P.red_begin));
     std::memcpy(h.red_end, P.red_end, sizeof(P.red_end));
-    require(P.max_own <= static_cast<uint32_t>(kMaxThreads), BSNN_ERR_INVALID_ARGUMENT,
-            "network too large for one persistent grid (more than 512 neurons per CTA)");
+    // Networks with streamed triplet rows carry row sums between steps (a kernel instance of its
+    // own, with a lower thread limit: it needs more registers).
+    const bool carry = P.max_trows > 0;
+    const uint32_t max_threads = static_cast<uint32_t>(carry ? kMaxThreads : kMaxThreadsPlain);
+    require(P.max_own <= max_threads, BSNN_ERR_INVALID_ARGUMENT,
+            "network too large for one persistent grid (more neurons per CTA than threads)");
     // Threads per CTA: the work items (32-aligned 4-column units of each segment) spread evenly
-    // over at most kMaxThreads threads.
-    const uint32_t max_threads = static_cast<uint32_t>(kMaxThreads);
+    // over at most max_threads threads.
     const uint32_t k_items = (P.max_items + max_threads - 1) / max_threads;
     uint32_t block = round_up((P.max_items + k_items - 1) / k_items, 32);
     block = std::max(block, round_up(P.max_own, 32));
@@ -613,9 +616,8 @@ void finalize(bsnn_sim* s) {
     block = std::max(block, round_up(P.max_own, 32));
     s->grid = n_ctas;
     s->block = block;
-    // Networks with streamed triplet rows carry row sums between steps (a kernel instance of its own).
-    s->kernel = P.max_trows > 0 ? reinterpret_cast<const void*>(&bsnn_step_kernel<true>)
-                                : reinterpret_cast<const void*>(&bsnn_step_kernel<false>);
+    s->kernel = carry ? reinterpret_cast<const void*>(&bsnn_step_kernel<true>)
+                      : reinterpret_cast<const void*>(&bsnn_step_kernel<false>);
 
     size_t o_part = A.take(sizeof(float) * 2 * static_cast<size_t>(h.n_slots) * h.N_pad);
     size_t o_red = A.take(sizeof(uint32_t) * P.red_list.size());

@@ -25,8 +25,11 @@ constexpr int kMaxMonitors = 16;
 constexpr int kMaxGroupRoles = 4;  // trace sets / plasticities / monitors per group and role
 constexpr int kMaxSegsPerCta = 2 * kMaxGroups;
 constexpr int kMaxBlksPerCta = kMaxConns;
-constexpr int kMaxThreads = 256;  // threads per CTA (up to 255 registers per thread, no spills)
-constexpr int kMaxWarps = kMaxThreads / 32;
+// Threads per CTA: the step-kernel instance that carries row sums needs up to 255 registers per
+// thread (256 threads); the other fits in 227 registers (288 threads, 9 warps).
+constexpr int kMaxThreads = 256;
+constexpr int kMaxThreadsPlain = 288;
+constexpr int kMaxWarps = kMaxThreadsPlain / 32;
 
 enum : int32_t { kTargetExc = 0, kTargetInh = 1 };
 enum : int32_t { kKindTriplet = 1, kKindIstdp = 2, kKindStdp = 3 };

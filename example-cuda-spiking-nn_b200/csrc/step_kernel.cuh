@@ -221,7 +221,7 @@ struct SmemLayout {
     float2* rowfac;     // [2][n_plast][max_own] {rowA, rowB} of the own neurons, by step parity
     float* ns;          // [ns_fields][max_own] state of the own neurons (kNs* fields below)
     float* rsum;        // [max_trows][n_chunks] carried triplet row sums by 32-unit chunk
-    float* red;         // [warps][2][max_own] per-warp partial-sum reduction scratch
+    float* red;         // [2][max_own] the previous step's propagation into the own neurons
     uint32_t* bits;     // [n_spike_monitors][max_own/32 + 2]
     unsigned char* desc;  // descriptor copies (DGroup, DTraceSet, DConn, DPlast, DMon, slot lists)
 };
@@ -270,7 +270,7 @@ __host__ __device__ __forceinline__ SmemSizes smem_sizes(uint32_t resident_float
     z.rowfac = align16(sizeof(float2) * 2 * n_plast * max_own);
     z.ns = align16(sizeof(float) * ns_fields * max_own);
     z.rsum = align16(sizeof(float) * rsum_floats);
-    z.redscr = align16(sizeof(float) * 2 * kMaxWarps * max_own);
+    z.redscr = align16(sizeof(float) * 2 * max_own);
     z.bits = align16(sizeof(uint32_t) * n_spike_mons * (max_own / 32 + 2));
     z.groups = align16(sizeof(DGroup) * n_groups);
     z.ts = align16(sizeof(DTraceSet) * n_ts);
@@ -1110,7 +1110,8 @@ __device__ __forceinline__ void copy_words(void* dst, const void* src, size_t by
 }
 
 template <bool CARRY>
-__global__ void __launch_bounds__(kMaxThreads, 1) bsnn_step_kernel(const DSim* __restrict__ S, uint32_t n_steps) {
+__global__ void __launch_bounds__(CARRY ? kMaxThreads : kMaxThreadsPlain, 1)
+    bsnn_step_kernel(const DSim* __restrict__ S, uint32_t n_steps) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ Desc s_d;
     __shared__ DCta s_cta;
