@@ -566,10 +566,10 @@ void finalize(bsnn_sim* s) {
         }
     }
     const uint32_t ns_fields = ns_layout(h.ns_ts, h.ns_pre, h.ns_post, h.ns_mon).fields;
-    auto smem_of = [&](const Plan& pl, uint32_t resident_floats) {
+    auto smem_of = [&](const Plan& pl, uint32_t resident_floats, uint32_t stage_rows) {
         return smem_sizes(resident_floats, pl.max_rows, pl.max_own, spk_words, n_spike_mons, h.n_groups, h.n_ts,
                           h.n_conns, h.n_plast, h.n_mons, static_cast<uint32_t>(pl.red_list.size()), ns_fields,
-                          pl.max_trows * pl.n_chunks)
+                          pl.max_trows * pl.n_chunks, kMaxWarps, stage_rows)
             .total;
     };
     const int64_t smem_limit = static_cast<int64_t>(optin) - static_cast<int64_t>(fa.sharedSizeBytes) - 128;
@@ -584,7 +584,7 @@ void finalize(bsnn_sim* s) {
         for (int attempt = 0; attempt < 8 && cap > 16384; ++attempt) {
             P = build_plan(s, n_ctas, static_cast<uint64_t>(cap), &resident_ok);
             if (!resident_ok) break;
-            const int64_t need = static_cast<int64_t>(smem_of(P, static_cast<uint32_t>(P.resident_floats)));
+            const int64_t need = static_cast<int64_t>(smem_of(P, static_cast<uint32_t>(P.resident_floats), 0u));
             if (need <= smem_limit) break;
             cap -= need - smem_limit + 256;
             resident_ok = false;
@@ -598,11 +598,25 @@ void finalize(bsnn_sim* s) {
     h.max_trows = P.max_trows;
     h.n_chunks = P.n_chunks;
     h.max_own = P.max_own;
-    std::memcpy(h.red_begin, P.red_begin, sizeof(P.red_begin));
-    std::memcpy(h.red_end, P.red_end, sizeof(P.red_end));
     // Networks with streamed triplet rows carry row sums between steps (a kernel instance of its
     // own, with a lower thread limit: it needs more registers).
     const bool carry = P.max_trows > 0;
+    // In that instance streamed rows go through per-warp double buffers in shared memory, filled
+    // by bulk asynchronous copies, when the room left after the plan holds them (the most rows
+    // per buffer that fit, up to 16).
+    {
+        uint32_t want = carry ? 16u : 0u;
+        if (const char* e = std::getenv("BSNN_STAGE"); e && carry)
+            want = std::min<uint32_t>(16u, static_cast<uint32_t>(std::max(0, std::atoi(e))));
+        h.stage_rows = 0;
+        for (uint32_t r = want; r >= 4u; r /= 2u)
+            if (static_cast<int64_t>(smem_of(P, h.resident_floats, r)) <= smem_limit) {
+                h.stage_rows = r;
+                break;
+            }
+    }
+    std::memcpy(h.red_begin, P.red_begin, sizeof(P.red_begin));
+    std::memcpy(h.red_end, P.red_end, sizeof(P.red_end));
     const uint32_t max_threads = static_cast<uint32_t>(carry ? kMaxThreads : kMaxThreadsPlain);
     require(P.max_own <= max_threads, BSNN_ERR_INVALID_ARGUMENT,
             "network too large for one persistent grid (more neurons per CTA than threads)");
@@ -816,7 +830,7 @@ void finalize(bsnn_sim* s) {
     cuda_check(cudaMemcpy(s->d_sim, &h, sizeof(DSim), cudaMemcpyHostToDevice), "H2D sim");
 
     // Launch configuration.
-    s->smem_bytes = smem_of(P, h.resident_floats);
+    s->smem_bytes = smem_of(P, h.resident_floats, h.stage_rows);
     cuda_check(cudaFuncSetAttribute(s->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(s->smem_bytes)),
                "cudaFuncSetAttribute smem");

@@ -35,7 +35,7 @@ enum : int32_t { kTargetExc = 0, kTargetInh = 1 };
 enum : int32_t { kKindTriplet = 1, kKindIstdp = 2, kKindStdp = 3 };
 enum : int32_t { kMonSpikes = 0, kMonVoltage = 1 };
 enum : int32_t { kNoisePhilox = 0, kNoiseOff = 1, kNoiseReplay = 2 };
-enum : int32_t { kErrNone = 0, kErrBarrierTimeout = 1 };
+enum : int32_t { kErrNone = 0, kErrBarrierTimeout = 1, kErrStageTimeout = 2 };
 
 // NeuronGroupView scalars (cpp_src/neuron_groups/neuron_group_view.h:8-49) plus derived values.
 struct DGroup {
@@ -146,6 +146,9 @@ struct DSim {
     uint32_t ns_ts, ns_pre, ns_post, ns_mon;
     // Carried triplet row sums: most triplet rows of one CTA, and 32-unit chunks per row.
     uint32_t max_trows, n_chunks;
+    // Streamed rows staged through shared memory by bulk asynchronous copies: rows per buffer
+    // (two buffers per warp), 0 = off (no shared memory left over).
+    uint32_t stage_rows;
     DGroup groups[kMaxGroups];
     DTraceSet ts[kMaxTraceSets];
     DConn conns[kMaxConns];

@@ -204,6 +204,7 @@ struct Desc {
     const uint8_t* replay;
     unsigned long long* barrier;
     int32_t* error;
+    uint32_t stage_rows;  // rows per staging buffer (0 = streamed rows are loaded directly)
 };
 
 // Values produced and consumed by the same CTA stay in shared memory: x of the own neurons, the
@@ -222,6 +223,9 @@ struct SmemLayout {
     float* ns;          // [ns_fields][max_own] state of the own neurons (kNs* fields below)
     float* rsum;        // [max_trows][n_chunks] carried triplet row sums by 32-unit chunk
     float* red;         // [2][max_own] the previous step's propagation into the own neurons
+    unsigned char* stage;  // [warps][2][stage_rows][512 B] staging buffers for streamed rows
+    uint64_t* stage_bar;   // [warps][2] their mbarriers
+    uint32_t* stage_phase; // [warps] parity of each buffer's next completion (bit b: buffer b)
     uint32_t* bits;     // [n_spike_monitors][max_own/32 + 2]
     unsigned char* desc;  // descriptor copies (DGroup, DTraceSet, DConn, DPlast, DMon, slot lists)
 };
@@ -250,14 +254,15 @@ __host__ __device__ __forceinline__ size_t align16(size_t x) { return (x + 15) &
 
 // Byte layout of the dynamic shared memory; the host sizes the launch with the same function.
 struct SmemSizes {
-    size_t wres, row, meta, rowflag, rowtgt, sbits, gbits, xown, rowfac, ns, rsum, redscr, bits, groups, ts, conns, plast,
-        mons, red, total;
+    size_t wres, row, meta, rowflag, rowtgt, sbits, gbits, xown, rowfac, ns, rsum, redscr, stage, bits, groups, ts,
+        conns, plast, mons, red, total;
 };
 __host__ __device__ __forceinline__ SmemSizes smem_sizes(uint32_t resident_floats, uint32_t max_rows, uint32_t max_own,
                                                          uint32_t spk_words, uint32_t n_spike_mons, uint32_t n_groups,
                                                          uint32_t n_ts, uint32_t n_conns, uint32_t n_plast,
                                                          uint32_t n_mons, uint32_t n_red, uint32_t ns_fields,
-                                                         uint32_t rsum_floats) {
+                                                         uint32_t rsum_floats, uint32_t stage_warps,
+                                                         uint32_t stage_rows) {
     SmemSizes z;
     z.wres = align16(sizeof(float) * static_cast<size_t>(resident_floats));
     z.row = align16(sizeof(float4) * max_rows);
@@ -271,6 +276,9 @@ __host__ __device__ __forceinline__ SmemSizes smem_sizes(uint32_t resident_float
     z.ns = align16(sizeof(float) * ns_fields * max_own);
     z.rsum = align16(sizeof(float) * rsum_floats);
     z.redscr = align16(sizeof(float) * 2 * max_own);
+    z.stage = stage_rows ? ((static_cast<size_t>(stage_warps) * 2u * stage_rows * 512u + 127u) & ~size_t(127)) +
+                               align16(static_cast<size_t>(stage_warps) * (2u * sizeof(uint64_t) + sizeof(uint32_t)))
+                         : 0;
     z.bits = align16(sizeof(uint32_t) * n_spike_mons * (max_own / 32 + 2));
     z.groups = align16(sizeof(DGroup) * n_groups);
     z.ts = align16(sizeof(DTraceSet) * n_ts);
@@ -278,7 +286,7 @@ __host__ __device__ __forceinline__ SmemSizes smem_sizes(uint32_t resident_float
     z.plast = align16(sizeof(DPlast) * n_plast);
     z.mons = align16(sizeof(DMon) * n_mons);
     z.red = align16(sizeof(uint32_t) * n_red);
-    z.total = z.wres + z.row + z.meta + z.rowflag + z.rowtgt + z.sbits + z.gbits + z.xown + z.rowfac + z.ns + z.rsum + z.redscr +
+    z.total = z.wres + z.row + z.meta + z.rowflag + z.rowtgt + z.sbits + z.gbits + z.xown + z.rowfac + z.ns + z.rsum + z.redscr + z.stage +
               z.bits + z.groups + z.ts + z.conns + z.plast + z.mons + z.red;
     return z;
 }
@@ -756,6 +764,42 @@ __device__ __forceinline__ void sts4(uint32_t a, float4 v) {
 }
 __device__ __forceinline__ uint32_t saddr(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
 
+// mbarrier and bulk asynchronous copy (global -> this CTA's shared memory, no multicast).
+constexpr unsigned long long kStageTimeoutNs = 2000000000ull;  // 2 s
+constexpr uint32_t kStageDead = 0x80000000u;  // staging gave up (stage_phase bit)
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return done != 0u;
+}
+// Bounded wait for the completion of phase `parity` of an mbarrier.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    while (!mbar_try_wait(bar, parity))
+        if (globaltimer_ns() - t0 > kStageTimeoutNs) return false;
+    return true;
+}
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
 // Address of weight (row i of block B, column q), in shared memory for resident blocks.
 __device__ __forceinline__ float* weight_ptr(const DBlk& B, const DConn& C, const SmemLayout& sm, uint32_t i,
                                              uint32_t q) {
@@ -1028,6 +1072,106 @@ __device__ __forceinline__ float4 block_rows(const DBlk& B, const DConn& C, uint
     return acc;
 }
 
+// block_rows for a streamed block whose rows are staged through shared memory: the warp's 32
+// units of a row (one contiguous run of up to 512 bytes) arrive by bulk asynchronous copies,
+// `stage_rows` rows per buffer, two buffers per warp, so the next batch streams in while the
+// current one is used.  Lane 0 (always a live lane) issues the copies; every lane waits on the
+// buffer's mbarrier (bounded: on timeout the error word is set and the pass gives up).  Returns
+// A timeout sets the error word and turns staging off for the warp.
+template <bool SCALE, bool TRIP>
+__device__ __forceinline__ void block_rows_staged(const Desc& D, const DBlk& B, const DConn& C, uint32_t u, bool live,
+                                                  unsigned mask, const SmemLayout& sm, bool accumulate, float4& acc,
+                                                  uint32_t n_chunks) {
+    const uint32_t nrows = B.row_end - B.row_begin, ld = C.ld, R = D.stage_rows;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, chunk = u / 32u;
+    uint32_t phase = sm.stage_phase[warp];
+    if (nrows == 0u || (phase & kStageDead)) return;
+    const uint32_t chunk_units = C.units - 32u * chunk < 32u ? C.units - 32u * chunk : 32u;
+    const uint32_t row_bytes = 16u * chunk_units;
+    const uint32_t buf0 = saddr(sm.stage) + warp * 2u * R * 512u;
+    const uint32_t bar0 = saddr(sm.stage_bar + 2u * warp);
+    const float* src0 = C.w + static_cast<size_t>(B.row_begin) * ld + 4u * 32u * chunk;
+    const float2* rowp = reinterpret_cast<const float2*>(sm.row + B.srow);
+    float* gbase = C.w + static_cast<size_t>(B.row_begin) * ld + 4u * u;
+    const uint32_t nb = (nrows + R - 1u) / R;
+    auto issue = [&](uint32_t k) {
+        if (lane == 0) {
+            const uint32_t r0 = k * R, r1 = r0 + R < nrows ? r0 + R : nrows;
+            const uint32_t bar = bar0 + 8u * (k & 1u), dst = buf0 + (k & 1u) * R * 512u;
+            mbar_expect_tx(bar, (r1 - r0) * row_bytes);
+            for (uint32_t r = r0; r < r1; ++r)
+                bulk_load(dst + (r - r0) * 512u, src0 + static_cast<size_t>(r) * ld, row_bytes, bar);
+        }
+    };
+    issue(0);
+    if (nb > 1u) issue(1);
+    for (uint32_t k = 0; k < nb; ++k) {
+        const uint32_t b = k & 1u;
+        const bool got = mbar_wait(bar0 + 8u * b, (phase >> b) & 1u);
+        if (!__all_sync(mask, got)) {
+            // Give up on staging for the rest of the launch: the batches in flight (this one and
+            // the next) land (bounded) and later calls return at once; the host sees the error.
+            if (lane == 0) atomicExch(D.error, kErrStageTimeout);
+            if (!got) mbar_wait(bar0 + 8u * b, (phase >> b) & 1u);
+            if (k + 1u < nb) mbar_wait(bar0 + 8u * (b ^ 1u), (phase >> (b ^ 1u)) & 1u);
+            phase |= kStageDead;
+            break;
+        }
+        phase ^= 1u << b;
+        const uint32_t r0 = k * R, r1 = r0 + R < nrows ? r0 + R : nrows;
+        const uint32_t buf = buf0 + b * R * 512u + 16u * lane;
+        for (uint32_t i0 = r0; i0 < r1; i0 += 4u) {
+            float4 wb[4];
+            float p[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (i0 + q < r1) wb[q] = lds4(buf + (i0 + q - r0) * 512u);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                p[q] = 0.0f;
+                if (i0 + q >= r1) continue;
+                const uint32_t i = i0 + q;
+                const float2 rw = rowp[2u * i];
+                float4 w4 = wb[q];
+                if constexpr (SCALE) {
+                    w4.x *= rw.y;
+                    w4.y *= rw.y;
+                    w4.z *= rw.y;
+                    w4.w *= rw.y;
+                    if (live) __stcg(reinterpret_cast<float4*>(gbase + static_cast<size_t>(i) * ld), w4);
+                }
+                if constexpr (TRIP) p[q] = live ? unit_sum(w4) : 0.0f;
+                if (accumulate) {
+                    acc.x = fmaf(w4.x, rw.x, acc.x);
+                    acc.y = fmaf(w4.y, rw.x, acc.y);
+                    acc.z = fmaf(w4.z, rw.x, acc.z);
+                    acc.w = fmaf(w4.w, rw.x, acc.w);
+                }
+            }
+            if constexpr (TRIP) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) p[q] += __shfl_xor_sync(mask, p[q], o);
+                }
+                if (lane == 0) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        if (i0 + q < r1) sm.rsum[(B.trow + i0 + q) * n_chunks + chunk] = p[q];
+                }
+            }
+        }
+        // every lane is done with this buffer before lane 0 refills it
+        __syncwarp(mask);
+        if (k + 2u < nb) {
+            if (lane == 0) fence_proxy_async_shared();
+            issue(k + 2u);
+        }
+    }
+    if (lane == 0) sm.stage_phase[warp] = phase;
+    __syncwarp(mask);
+}
+
 // All blocks of segment SG for unit u; the partial sums go to the segment's slot.  `pending` = an
 // update of the previous step is to be applied (normalised triplet rows are rescaled and stored).
 // CARRY: the network has streamed triplet rows (a kernel instance of its own, so that networks
@@ -1038,6 +1182,10 @@ __device__ __forceinline__ void segment_unit(const Desc& D, const DSeg& SG, cons
                                              uint32_t npad, uint32_t n_chunks) {
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
     bool touched = false;
+    // the lanes of this warp that run this call: all of them in a segment with carried row sums,
+    // else those whose unit lies in the segment
+    const uint32_t left = SG.units - 32u * (u / 32u);
+    const unsigned wmask = (CARRY && SG.carried) || left >= 32u ? kFull : (1u << left) - 1u;
     for (uint32_t bk = SG.blk_begin; bk < SG.blk_end; ++bk) {
         const DBlk B = s_blk[bk];
         const DConn& C = D.conns[B.conn];
@@ -1045,6 +1193,17 @@ __device__ __forceinline__ void segment_unit(const Desc& D, const DSeg& SG, cons
         const bool scale = pending && trip;
         if (!scale && !accumulate) continue;
         touched = true;
+        if (CARRY && !B.resident && D.stage_rows) {
+            if (CARRY && trip && accumulate) {
+                if (scale) block_rows_staged<true, true>(D, B, C, u, live, wmask, sm, true, acc, n_chunks);
+                else block_rows_staged<false, true>(D, B, C, u, live, wmask, sm, true, acc, n_chunks);
+            } else if (scale) {
+                block_rows_staged<true, CARRY>(D, B, C, u, live, wmask, sm, accumulate, acc, n_chunks);
+            } else {
+                block_rows_staged<false, false>(D, B, C, u, live, wmask, sm, true, acc, n_chunks);
+            }
+            continue;
+        }
         if (CARRY && trip && accumulate && !B.resident) {
             if (scale) {
                 acc = B.resident ? block_rows<true, true, true>(B, C, u, live, sm, true, acc, n_chunks)
@@ -1075,6 +1234,9 @@ __device__ __forceinline__ void weight_pass(const Desc& D, const DCta& cta, bool
     float* part_out = D.partials + static_cast<size_t>(par) * D.n_slots * D.N_pad;
     const uint32_t npad = D.N_pad;
     for (uint32_t it0 = 0; it0 < cta.n_items; it0 += blockDim.x) {
+        // the staged loads keep per-warp buffer state in shared memory: the warp enters each
+        // item converged, after its lane 0 has recorded that state
+        if (CARRY && D.stage_rows) __syncwarp();
         const uint32_t it = it0 + threadIdx.x;
         const int s = seg_of_item(s_seg, n_seg, it);
         if (s < 0) continue;  // the whole warp
@@ -1134,7 +1296,7 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : kMaxThreadsPlain, 1)
     const NsLayout L0 = ns_layout(S->ns_ts, S->ns_pre, S->ns_post, S->ns_mon);
     const SmemSizes z = smem_sizes(S->resident_floats, max_rows, max_own, S->spk_words, n_spike_mons, S->n_groups,
                                    S->n_ts, S->n_conns, S->n_plast, S->n_mons, S->n_red, L0.fields,
-                                   S->max_trows * S->n_chunks);
+                                   S->max_trows * S->n_chunks, kMaxWarps, S->stage_rows);
     if (threadIdx.x == 0) {
         s_L = L0;
         unsigned char* p = smem_raw;
@@ -1162,6 +1324,15 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : kMaxThreadsPlain, 1)
         p += z.rsum;
         sm.red = reinterpret_cast<float*>(p);
         p += z.redscr;
+        {
+            const size_t buf = S->stage_rows ? (static_cast<size_t>(kMaxWarps) * 2u * S->stage_rows * 512u + 127u) &
+                                                   ~size_t(127)
+                                             : 0;
+            sm.stage = p;
+            sm.stage_bar = reinterpret_cast<uint64_t*>(p + buf);
+            sm.stage_phase = reinterpret_cast<uint32_t*>(p + buf + static_cast<size_t>(kMaxWarps) * 2u * sizeof(uint64_t));
+        }
+        p += z.stage;
         sm.bits = reinterpret_cast<uint32_t*>(p);
         p += z.bits;
         sm.desc = p;
@@ -1217,6 +1388,7 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : kMaxThreadsPlain, 1)
         s_d.replay = S->replay;
         s_d.barrier = S->barrier;
         s_d.error = S->error;
+        s_d.stage_rows = S->stage_rows;
         uint32_t base = 0;
         for (uint32_t m = 0; m < S->n_mons; ++m) {
             s_d.bitbase[m] = base;
@@ -1272,6 +1444,13 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : kMaxThreadsPlain, 1)
     }
     const uint32_t n_bits_words = n_spike_mons * (max_own / 32u + 2u);
     const uint32_t n_gbits = max_own / 32u + 2u;
+    if (D.stage_rows && (threadIdx.x & 31u) == 0u) {
+        const uint32_t w = threadIdx.x >> 5;
+        mbar_init(saddr(sm.stage_bar + 2u * w), 1u);
+        mbar_init(saddr(sm.stage_bar + 2u * w + 1u), 1u);
+        sm.stage_phase[w] = 0u;
+        fence_mbar_init();
+    }
     __syncthreads();
     move_resident(D, s_blk, s_nblk, sm, true);
     move_neuron_state(S, D, cta, sm, max_own, L, true, 0u, false);

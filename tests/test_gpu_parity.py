@@ -96,6 +96,27 @@ def test_resync_parity_with_rows_streamed_from_global_memory(monkeypatch, plasti
         compare_state(g, o, spec, RTOL, tag=f"streamed rows, resync block {block}")
 
 
+@pytest.mark.parametrize("stage_rows", ["0", "5", "16"])
+def test_streamed_rows_staged_through_shared_memory(monkeypatch, stage_rows):
+    """Streamed rows read directly (0) or staged through per-warp shared-memory buffers of 5 rows
+    (batches that do not divide the blocks' row counts) and 16 rows, on a network with about 14
+    rows per CTA, so that a block spans several batches."""
+    monkeypatch.setenv("BSNN_RESIDENT", "0")
+    monkeypatch.setenv("BSNN_STAGE", stage_rows)
+    spec = bsnn.random_network(1600, 400, steps=200, seed=13, plasticity=("triplet", "istdp", "stdp"))
+    g, o = make_pair(spec)
+    done = 0
+    for block in range(2):
+        g.run(done, 41)
+        o.run(done, 41)
+        done += 41
+        copy_state(g, o, spec)
+        g.step(done)
+        o.step(done)
+        done += 1
+        compare_state(g, o, spec, RTOL, tag=f"staged rows ({stage_rows}), resync block {block}")
+
+
 def test_launch_split_is_bit_exact():
     spec = bsnn.random_network(100, 25, steps=500, seed=3)
     sims = []
