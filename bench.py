@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="bsnn", choices=["bsnn", "reference"])
     ap.add_argument("--workload", default="example_plastic_3125")
+    ap.add_argument("--weight-format", default="f32", choices=["f32", "f32_rowscaled", "bf16", "fp8_e4m3"],
+                    help="weight storage form: f32 = the reference's arithmetic; the others keep FP32 masters with "
+                         "a per-row normalisation scale and propagate from a copy in that type")
     ap.add_argument("--sim-steps", type=int, default=10000)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bounded CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -119,9 +122,21 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def algorithmic_bytes_per_step(spec) -> float:
-    """Weight read of every connection once (FP32), read+write of the plastic matrices (the
-    update and the row normalisation, counted once at 4 B), and ~100 B/neuron of state."""
+COPY_BYTES = {"f32_rowscaled": 4, "bf16": 2, "fp8_e4m3": 1}
+FORM_NAMES = {"f32": "plain FP32 (reference arithmetic)",
+              "f32_rowscaled": "FP32 masters, per-row normalisation scale, GEMV from an FP32 copy",
+              "bf16": "FP32 masters, per-row normalisation scale, GEMV from a BF16 copy (FP32 accumulate)",
+              "fp8_e4m3": "FP32 masters, per-row normalisation scale, GEMV from an FP8 E4M3 copy with per-row "
+                          "scales (FP32 accumulate)"}
+
+
+def algorithmic_bytes_per_step(spec, form="f32") -> float:
+    """f32: weight read of every connection once (FP32), read+write of the plastic matrices (the
+    update and the row normalisation, counted once at 4 B), and ~100 B/neuron of state.
+    Row-scaled forms: one read of every connection's GEMV copy (4, 2 or 1 B per entry) and the
+    same state; the updates touch only the rows and columns of spiking neurons (not counted)."""
+    if form != "f32":
+        return float(sum(c.weights.size * COPY_BYTES[form] for c in spec.conns) + 100 * spec.num_neurons)
     b = sum(c.weights.size * 4 for c in spec.conns)
     plastic = {p.conn for p in spec.plasts}
     b += sum(2 * spec.conns[c].weights.size * 4 for c in plastic)
@@ -186,6 +201,8 @@ def run_bsnn(args, rank, world):
                                   seed=bsnn.network.WORKLOADS[args.workload]["seed"] + rank)
     sim = bsnn.Simulation(spec.num_excitatory, spec.num_inhibitory, device=dev, **spec.sim_kwargs())
     spec.build(sim)
+    if args.weight_format != "f32":
+        sim.set_weight_format(args.weight_format)
     sim.set_steps_per_launch(STEPS_PER_LAUNCH)
     stream = torch.cuda.ExternalStream(sim.stream())
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
@@ -231,12 +248,13 @@ def run_bsnn(args, rank, world):
     steps_per_s = K * S * world / (t_ms / 1e3)
     per_launch_ms = t_ms / max(1, launches)
     clock_steps_per_launch = K * S / max(1, launches)
-    bytes_step = algorithmic_bytes_per_step(spec)
+    bytes_step = algorithmic_bytes_per_step(spec, args.weight_format)
     achieved = bytes_step * clock_steps_per_launch / (per_launch_ms / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
     traffic = None
     if PROFILE_TRAFFIC.exists():
-        tr = json.loads(PROFILE_TRAFFIC.read_text()).get(args.workload)
+        key = args.workload if args.weight_format == "f32" else f"{args.workload}/{args.weight_format}"
+        tr = json.loads(PROFILE_TRAFFIC.read_text()).get(key)
         if tr:
             traffic = tr["dram_bytes_per_launch"]
     line = {
@@ -250,11 +268,12 @@ def run_bsnn(args, rank, world):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32",
+        "dtype": {"f32": "f32", "f32_rowscaled": "f32", "bf16": "bf16 weights, f32 accumulate",
+                  "fp8_e4m3": "fp8 e4m3 weights, f32 accumulate"}[args.weight_format],
         "data": "synthetic (seeded; reference example shapes, uniform[0, max_weight] weights)",
         "config": {"workload": args.workload, "neurons": spec.num_neurons, "synapse_entries": spec.synapse_entries(),
                    "clock_steps_per_bench_step": S, "dt_s": DT, "plasticity": "triplet(E->E)+iSTDP(I->E)",
-                   "form": "plain FP32 (reference arithmetic)", "parallelism": f"replicas x{world}",
+                   "form": FORM_NAMES[args.weight_format], "parallelism": f"replicas x{world}",
                    "l2": "flushed (256 MB write) between timed steps"},
         "dense_synaptic_updates_per_s": spec.synapse_entries() * steps_per_s,
         "spike_driven_events_per_s": events / (t_ms / 1e3),
@@ -265,7 +284,8 @@ def run_bsnn(args, rank, world):
                      "traffic": traffic, "peak_source": peak_kind,
                      "bytes_per_clock_step": bytes_step, "clock_steps_per_launch": clock_steps_per_launch,
                      "launch_ms": per_launch_ms,
-                     "note": "working set (~40 MB) is L2-resident, so frac of HBM peak can exceed 1"},
+                     "note": ("working set is L2-resident, so frac of HBM peak can exceed 1"
+                              if bytes_step < 100e6 else "working set exceeds L2: streamed from HBM")},
         "clocks": clocks.summary(),
     }
     sim.close()
@@ -285,6 +305,8 @@ def run_e2e(args, dev):
     t0 = time.perf_counter()
     sim = bsnn.Simulation(spec.num_excitatory, spec.num_inhibitory, device=dev, **spec.sim_kwargs())
     spec.build(sim)
+    if args.weight_format != "f32":
+        sim.set_weight_format(args.weight_format)
     sim.set_steps_per_launch(STEPS_PER_LAUNCH)
     d2h = 0
     for k in range(K):

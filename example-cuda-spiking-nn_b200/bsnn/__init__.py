@@ -6,13 +6,14 @@ The compute path is the CUDA library libbsnn.so; this package only wraps its C-A
 creating a Simulation does, and fails loudly if libbsnn.so is missing.
 """
 from ._ffi import (FIELD, NOISE_OFF, NOISE_PHILOX, NOISE_REPLAY, PLASTICITY_ISTDP, PLASTICITY_STDP, PLASTICITY_TRIPLET,
+                   WEIGHT_FORMATS,
                    BsnnError, ConnectionParams, ConnectionView, CudaError, DeviceTimeout, InvalidArgument, NeuronGroupParams,
                    OutOfRange, PlasticityParams, StateError, load_library)
 from .core import Simulation, connection_propagate
 from .network import NetworkSpec, random_network, synthetic_network
 
 __all__ = [
-    "FIELD", "NOISE_OFF", "NOISE_PHILOX", "NOISE_REPLAY", "PLASTICITY_ISTDP", "PLASTICITY_STDP", "PLASTICITY_TRIPLET",
+    "FIELD", "WEIGHT_FORMATS", "NOISE_OFF", "NOISE_PHILOX", "NOISE_REPLAY", "PLASTICITY_ISTDP", "PLASTICITY_STDP", "PLASTICITY_TRIPLET",
     "BsnnError", "ConnectionParams", "ConnectionView", "CudaError", "DeviceTimeout", "InvalidArgument", "NeuronGroupParams",
     "OutOfRange", "PlasticityParams", "StateError", "load_library", "Simulation", "connection_propagate", "NetworkSpec", "random_network",
     "synthetic_network",

@@ -32,6 +32,14 @@ NOISE_PHILOX = 0
 NOISE_OFF = 1
 NOISE_REPLAY = 2
 
+# Weight storage forms (bsnn_set_weight_format).
+WEIGHTS_F32 = 0
+WEIGHTS_F32_ROWSCALED = 1
+WEIGHTS_BF16 = 2
+WEIGHTS_FP8_E4M3 = 3
+WEIGHT_FORMATS = {"f32": WEIGHTS_F32, "f32_rowscaled": WEIGHTS_F32_ROWSCALED, "bf16": WEIGHTS_BF16,
+                  "fp8_e4m3": WEIGHTS_FP8_E4M3}
+
 FIELD = {
     "membrane_potentials": 1,
     "g_excitatory": 2,
@@ -53,6 +61,9 @@ FIELD = {
     "plasticity_triplet_pre_traces": 18,
     "plasticity_triplet_post_traces": 19,
     "plasticity_pre_weight_sums": 20,
+    "connection_row_scale": 21,
+    "connection_row_master_sum": 22,
+    "connection_row_quant_scale": 23,
 }
 UINT_FIELDS = {"refractory_counter", "spikes"}
 
@@ -263,6 +274,7 @@ SIGNATURES = {
     "bsnn_add_voltage_recorder": (_I32, [_P, _U32, _UP, _U32, _U32, _UP]),
     "bsnn_set_noise_mode": (_I32, [_P, _I32]),
     "bsnn_set_noise_replay": (_I32, [_P, ctypes.POINTER(ctypes.c_uint8), _U32]),
+    "bsnn_set_weight_format": (_I32, [_P, _I32]),
     "bsnn_step": (_I32, [_P, _U32]),
     "bsnn_run": (_I32, [_P, _U32, _U32]),
     "bsnn_synchronize": (_I32, [_P]),
@@ -271,6 +283,7 @@ SIGNATURES = {
     "bsnn_read_state": (_I32, [_P, _I32, _U32, _U32, _U32, _P]),
     "bsnn_write_state": (_I32, [_P, _I32, _U32, _U32, _U32, _P]),
     "bsnn_read_weights": (_I32, [_P, _U32, _FP]),
+    "bsnn_read_weight_copy": (_I32, [_P, _U32, _P]),
     "bsnn_read_spike_history": (_I32, [_P, _U32, _UP, _I32]),
     "bsnn_read_spike_bits": (_I32, [_P, _U32, _UP, _I32]),
     "bsnn_read_voltage_history": (_I32, [_P, _U32, _FP, _I32]),

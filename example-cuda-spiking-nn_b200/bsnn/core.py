@@ -131,6 +131,15 @@ class Simulation:
         n_steps = c.size // (2 * self.num_neurons)
         self._check(self._lib.bsnn_set_noise_replay(self._h, _ptr(c, ctypes.c_uint8), n_steps))
 
+    def set_weight_format(self, form):
+        """Weight storage form: "f32" (the reference's arithmetic), "f32_rowscaled", "bf16" or
+        "fp8_e4m3" (FP32 masters with a per-row normalisation scale; the propagation reads a copy
+        of the masters in that type).  Before the first step."""
+        from ._ffi import WEIGHT_FORMATS
+        code = WEIGHT_FORMATS[form] if isinstance(form, str) else int(form)
+        self._check(self._lib.bsnn_set_weight_format(self._h, code))
+        self._weight_format = code
+
     # -- hot path ---------------------------------------------------------------------------
     def step(self, clock_step: int):
         self._check(self._lib.bsnn_step(self._h, clock_step))
@@ -169,6 +178,17 @@ class Simulation:
         n_pre, n_post = self._conns[connection]
         out = np.empty((n_pre, n_post), dtype=np.float32)
         self._check(self._lib.bsnn_read_weights(self._h, connection, _ptr(out, ctypes.c_float)))
+        return out
+
+    def read_weight_copy(self, connection: int) -> np.ndarray:
+        """Row-scaled forms: the propagation's copy of the masters as stored -- float32, BF16 bit
+        patterns (uint16) or E4M3 bytes (uint8), [pre, post]."""
+        from ._ffi import WEIGHTS_BF16, WEIGHTS_FP8_E4M3
+        n_pre, n_post = self._conns[connection]
+        fmt = getattr(self, "_weight_format", 0)
+        dt = np.uint16 if fmt == WEIGHTS_BF16 else np.uint8 if fmt == WEIGHTS_FP8_E4M3 else np.float32
+        out = np.empty((n_pre, n_post), dtype=dt)
+        self._check(self._lib.bsnn_read_weight_copy(self._h, connection, out.ctypes.data_as(ctypes.c_void_p)))
         return out
 
     def read_spike_history(self, monitor: int, flush: bool = False) -> np.ndarray:

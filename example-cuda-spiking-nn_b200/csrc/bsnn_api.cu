@@ -103,6 +103,7 @@ struct bsnn_sim {
     std::unique_ptr<rec::Writer> writer;  // formats and writes recorded text off the stepping thread
     std::vector<HostStim> stims;
     int32_t noise_mode = BSNN_NOISE_PHILOX;
+    int32_t weight_format = BSNN_WEIGHTS_F32;
     std::vector<uint8_t> replay;
     uint32_t replay_steps = 0;
 
@@ -265,9 +266,9 @@ Plan build_plan(const bsnn_sim* s, uint32_t n_ctas, uint64_t cap_bytes, bool* re
         for (size_t c = 0; c < s->conns.size(); ++c) {
             const auto& C = s->conns[c];
             if (static_cast<int>(C.pre) != g) continue;
-            double w = 1.0;
+            double w = 1.0;  // (row-scaled forms only read their rows)
             for (const auto& pl : s->plasts)
-                if (pl.conn == c) w += pl.kind == BSNN_PLASTICITY_TRIPLET ? 2.0 : 1.0;
+                if (pl.conn == c && s->weight_format == BSNN_WEIGHTS_F32) w += pl.kind == BSNN_PLASTICITY_TRIPLET ? 2.0 : 1.0;
             cost[j] += w * round_up(s->groups[C.post].p.num_neurons, 4);
         }
     }
@@ -411,6 +412,13 @@ Plan build_plan(const bsnn_sim* s, uint32_t n_ctas, uint64_t cap_bytes, bool* re
     return P;
 }
 
+void launch_fill_copy(const DConn& C, int32_t fmt, cudaStream_t stream) {
+    const size_t n = static_cast<size_t>(C.qtiles) * C.n_pre * 128u;
+    const unsigned blocks = static_cast<unsigned>(std::min<size_t>((n + 255) / 256, 4096));
+    bsnn_fill_copy_kernel<<<blocks, 256, 0, stream>>>(C, fmt);
+    cuda_check(cudaGetLastError(), "fill weight copy");
+}
+
 void finalize(bsnn_sim* s) {
     if (s->finalized) return;
     require(!s->groups.empty(), BSNN_ERR_STATE, "no neuron groups were added");
@@ -499,7 +507,8 @@ void finalize(bsnn_sim* s) {
         o_ts[3 * t + 1] = A.take(n);
         o_ts[3 * t + 2] = A.take(n);
     }
-    std::vector<size_t> o_w(h.n_conns);
+    std::vector<size_t> o_w(h.n_conns), o_q(h.n_conns, 0), o_rowv(h.n_conns, 0);
+    const bool lazy = s->weight_format != BSNN_WEIGHTS_F32;
     s->conn_ld.assign(h.n_conns, 0);
     size_t wbytes = 0;
     for (uint32_t c = 0; c < h.n_conns; ++c) {
@@ -509,6 +518,13 @@ void finalize(bsnn_sim* s) {
         s->conn_ld[c] = ld;
         o_w[c] = A.take(sizeof(float) * static_cast<size_t>(n_pre) * ld);
         wbytes += sizeof(float) * static_cast<size_t>(n_pre) * ld;
+        if (lazy) {
+            const size_t eb = s->weight_format == BSNN_WEIGHTS_BF16 ? 2 : s->weight_format == BSNN_WEIGHTS_FP8_E4M3 ? 1 : 4;
+            const size_t tiles = (n_post + 127) / 128;
+            o_q[c] = A.take(eb * tiles * n_pre * 128);
+            wbytes += eb * tiles * n_pre * 128;
+            o_rowv[c] = A.take(sizeof(float) * 4 * static_cast<size_t>(n_pre));  // s, M, qs, 1/qs
+        }
     }
     struct PlOff { size_t pre, post, tpre, tpost, colA[2], colB[2], sums; };
     std::vector<PlOff> o_pl(h.n_plast);
@@ -543,10 +559,11 @@ void finalize(bsnn_sim* s) {
     // Shared memory: the largest opt-in dynamic allocation minus the kernel's static shared data.
     int optin = 0;
     cuda_check(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device), "smem attr");
-    cudaFuncAttributes fa{}, fa_carry{};
-    cuda_check(cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(&bsnn_step_kernel<false>)), "func attr");
-    cuda_check(cudaFuncGetAttributes(&fa_carry, reinterpret_cast<const void*>(&bsnn_step_kernel<true>)), "func attr");
-    fa.sharedSizeBytes = std::max(fa.sharedSizeBytes, fa_carry.sharedSizeBytes);
+    cudaFuncAttributes fa{}, fa_carry{}, fa_lazy{};
+    cuda_check(cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(&bsnn_step_kernel<false, false>)), "func attr");
+    cuda_check(cudaFuncGetAttributes(&fa_carry, reinterpret_cast<const void*>(&bsnn_step_kernel<true, false>)), "func attr");
+    cuda_check(cudaFuncGetAttributes(&fa_lazy, reinterpret_cast<const void*>(&bsnn_step_kernel<false, true>)), "func attr");
+    fa.sharedSizeBytes = std::max({fa.sharedSizeBytes, fa_carry.sharedSizeBytes, fa_lazy.sharedSizeBytes});
     uint32_t n_spike_mons = 0;
     for (const auto& M : s->mons) n_spike_mons += M.kind == kMonSpikes ? 1u : 0u;
     // Per-group role counts that size the shared-memory neuron state.
@@ -569,14 +586,15 @@ void finalize(bsnn_sim* s) {
     auto smem_of = [&](const Plan& pl, uint32_t resident_floats, uint32_t stage_rows) {
         return smem_sizes(resident_floats, pl.max_rows, pl.max_own, spk_words, n_spike_mons, h.n_groups, h.n_ts,
                           h.n_conns, h.n_plast, h.n_mons, static_cast<uint32_t>(pl.red_list.size()), ns_fields,
-                          pl.max_trows * pl.n_chunks, kMaxWarps, stage_rows)
+                          lazy ? 0u : pl.max_trows * pl.n_chunks, h.stage_warps, stage_rows, lazy ? pl.max_rows : 0u)
             .total;
     };
     const int64_t smem_limit = static_cast<int64_t>(optin) - static_cast<int64_t>(fa.sharedSizeBytes) - 128;
     // Plastic weight rows stay resident in shared memory for a whole launch when every CTA's
     // share fits; otherwise all rows stream from global memory (L2 / HBM).
-    bool use_resident = true;
-    if (const char* e = std::getenv("BSNN_RESIDENT")) use_resident = std::atoi(e) != 0;
+    // (The row-scaled forms always stream: their weight pass only reads.)
+    bool use_resident = !lazy;
+    if (const char* e = std::getenv("BSNN_RESIDENT"); e && !lazy) use_resident = std::atoi(e) != 0;
     Plan P;
     bool resident_ok = false;
     if (use_resident) {
@@ -595,29 +613,25 @@ void finalize(bsnn_sim* s) {
     h.n_ctas = n_ctas;
     h.n_slots = std::max(P.n_slots, 1u);
     h.max_rows = P.max_rows;
-    h.max_trows = P.max_trows;
+    h.max_trows = lazy ? 0u : P.max_trows;
     h.n_chunks = P.n_chunks;
     h.max_own = P.max_own;
-    // Networks with streamed triplet rows carry row sums between steps (a kernel instance of its
-    // own, with a lower thread limit: it needs more registers).
-    const bool carry = P.max_trows > 0;
-    // In that instance streamed rows go through per-warp double buffers in shared memory, filled
-    // by bulk asynchronous copies, when the room left after the plan holds them (the most rows
-    // per buffer that fit, up to 16).
-    {
-        uint32_t want = carry ? 16u : 0u;
-        if (const char* e = std::getenv("BSNN_STAGE"); e && carry)
-            want = std::min<uint32_t>(16u, static_cast<uint32_t>(std::max(0, std::atoi(e))));
-        h.stage_rows = 0;
-        for (uint32_t r = want; r >= 4u; r /= 2u)
-            if (static_cast<int64_t>(smem_of(P, h.resident_floats, r)) <= smem_limit) {
-                h.stage_rows = r;
-                break;
-            }
+    h.wfmt = s->weight_format;
+    h.q_nonneg = 0;
+    if (s->weight_format == BSNN_WEIGHTS_FP8_E4M3 && std::getenv("BSNN_FP8_CVT") == nullptr) {
+        bool nonneg = true;
+        for (const auto& C : s->conns)
+            for (float v : C.w) nonneg &= !(v < 0.0f);
+        for (const auto& PL : s->plasts) nonneg &= !(PL.p.weight_min < 0.0f);
+        h.q_nonneg = nonneg ? 1u : 0u;
     }
+    // Networks with streamed triplet rows carry row sums between steps (a kernel instance of its
+    // own, with a lower thread limit: it needs more registers); the row-scaled forms have an
+    // instance of their own.
+    const bool carry = !lazy && P.max_trows > 0;
     std::memcpy(h.red_begin, P.red_begin, sizeof(P.red_begin));
     std::memcpy(h.red_end, P.red_end, sizeof(P.red_end));
-    const uint32_t max_threads = static_cast<uint32_t>(carry ? kMaxThreads : kMaxThreadsPlain);
+    const uint32_t max_threads = static_cast<uint32_t>(carry ? kMaxThreads : lazy ? kMaxThreadsRows : kMaxThreadsPlain);
     require(P.max_own <= max_threads, BSNN_ERR_INVALID_ARGUMENT,
             "network too large for one persistent grid (more neurons per CTA than threads)");
     // Threads per CTA: the work items (32-aligned 4-column units of each segment) spread evenly
@@ -630,8 +644,26 @@ void finalize(bsnn_sim* s) {
     block = std::max(block, round_up(P.max_own, 32));
     s->grid = n_ctas;
     s->block = block;
-    s->kernel = carry ? reinterpret_cast<const void*>(&bsnn_step_kernel<true>)
-                      : reinterpret_cast<const void*>(&bsnn_step_kernel<false>);
+    s->kernel = lazy    ? reinterpret_cast<const void*>(&bsnn_step_kernel<false, true>)
+                : carry ? reinterpret_cast<const void*>(&bsnn_step_kernel<true, false>)
+                        : reinterpret_cast<const void*>(&bsnn_step_kernel<false, false>);
+    // In those two instances streamed rows go through per-warp double buffers in shared memory,
+    // filled by bulk asynchronous copies, when the room left after the plan holds them (the most
+    // rows per buffer that fit, up to 16).
+    h.stage_warps = block / 32;
+    {
+        uint32_t want = carry || lazy ? 16u : 0u;
+        if (const char* e = std::getenv("BSNN_STAGE"); e && (carry || lazy))
+            want = std::min<uint32_t>(16u, static_cast<uint32_t>(std::max(0, std::atoi(e))));
+        h.stage_rows = 0;
+        for (uint32_t r = want; r >= 4u; r /= 2u)
+            if (static_cast<int64_t>(smem_of(P, h.resident_floats, r)) <= smem_limit) {
+                h.stage_rows = r;
+                break;
+            }
+    }
+    require(!lazy || h.stage_rows > 0, BSNN_ERR_INVALID_ARGUMENT,
+            "row-scaled weight form: no shared memory left for the staging buffers");
 
     size_t o_part = A.take(sizeof(float) * 2 * static_cast<size_t>(h.n_slots) * h.N_pad);
     size_t o_red = A.take(sizeof(uint32_t) * P.red_list.size());
@@ -728,6 +760,44 @@ void finalize(bsnn_sim* s) {
             std::memcpy(&padded[static_cast<size_t>(i) * D.ld], &C.w[static_cast<size_t>(i) * D.n_post],
                         sizeof(float) * D.n_post);
         cuda_check(cudaMemcpy(D.w, padded.data(), sizeof(float) * padded.size(), cudaMemcpyHostToDevice), "H2D w");
+        if (lazy) {
+            const bool fp8 = s->weight_format == BSNN_WEIGHTS_FP8_E4M3;
+            D.q = base + o_q[c];
+            D.qtiles = (D.n_post + 127) / 128;
+            float* rv = F(o_rowv[c]);
+            D.lz_s = rv;
+            D.lz_m = rv + D.n_pre;
+            D.qscale = fp8 ? rv + 2 * static_cast<size_t>(D.n_pre) : nullptr;
+            D.qinv = fp8 ? rv + 3 * static_cast<size_t>(D.n_pre) : nullptr;
+            // s = 1, M = the row sum, and (FP8) qs = the larger of the row's largest magnitude and
+            // the plastic bound weight_max (doubled for a normalised row, whose masters may reach
+            // twice the bound before the normalisation folds s back into them), over 448 (the
+            // largest finite E4M3 value).
+            float wmax = 0.0f;
+            bool normalised = false;
+            for (const auto& PL : s->plasts)
+                if (PL.conn == c) {
+                    wmax = std::max(wmax, std::fabs(PL.p.weight_max));
+                    normalised |= PL.kind == BSNN_PLASTICITY_TRIPLET;
+                }
+            std::vector<float> rows(4 * static_cast<size_t>(D.n_pre), 1.0f);
+            for (uint32_t i = 0; i < D.n_pre; ++i) {
+                double sum = 0.0;
+                float big = 0.0f;
+                for (uint32_t q = 0; q < D.n_post; ++q) {
+                    const float v = C.w[static_cast<size_t>(i) * D.n_post + q];
+                    sum += v;
+                    big = std::max(big, std::fabs(v));
+                }
+                rows[D.n_pre + i] = static_cast<float>(sum);
+                float qs = std::max(big, wmax) * (normalised ? 2.0f : 1.0f) / 448.0f;
+                if (!(qs > 0.0f) || !std::isfinite(qs)) qs = 1.0f;
+                rows[2 * static_cast<size_t>(D.n_pre) + i] = qs;
+                rows[3 * static_cast<size_t>(D.n_pre) + i] = 1.0f / qs;
+            }
+            cuda_check(cudaMemcpy(rv, rows.data(), sizeof(float) * rows.size(), cudaMemcpyHostToDevice), "H2D rows");
+            launch_fill_copy(D, s->weight_format, s->stream);
+        }
     }
     for (uint32_t k = 0; k < h.n_plast; ++k) {
         const auto& PL = s->plasts[k];
@@ -960,6 +1030,15 @@ FieldRef field_ref(bsnn_sim* s, int32_t field, uint32_t index) {
         const uint32_t n = h.conns[index].n_pre;
         return {field == BSNN_FIELD_CONN_R_TRACES ? T.r : field == BSNN_FIELD_CONN_D_TRACES ? T.d : T.x, n};
     }
+    if (field >= BSNN_FIELD_CONN_ROW_SCALE && field <= BSNN_FIELD_CONN_ROW_QUANT_SCALE) {
+        require(index < h.n_conns, BSNN_ERR_OUT_OF_RANGE, "connection index out of range");
+        require(h.wfmt != kFmtF32, BSNN_ERR_INVALID_ARGUMENT, "no row scales in the BSNN_WEIGHTS_F32 form");
+        const DConn& C = h.conns[index];
+        if (field == BSNN_FIELD_CONN_ROW_SCALE) return {C.lz_s, C.n_pre};
+        if (field == BSNN_FIELD_CONN_ROW_MASTER_SUM) return {C.lz_m, C.n_pre};
+        require(C.qscale != nullptr, BSNN_ERR_INVALID_ARGUMENT, "no quantisation scales outside the FP8 form");
+        return {C.qscale, C.n_pre};
+    }
     if (field >= BSNN_FIELD_PLAST_PRE_TRACES && field <= BSNN_FIELD_PLAST_PRE_WEIGHT_SUMS) {
         require(index < h.n_plast, BSNN_ERR_OUT_OF_RANGE, "plasticity index out of range");
         const DPlast& P = h.plast[index];
@@ -982,6 +1061,18 @@ namespace {
 
 // Monitor::record(clock_step) for every recorder with an output (cpp_src/monitors/*.cpp): the
 // rings are copied to host memory and flushed here; the text is written by the writer thread.
+// A connection's weights as [n_pre][ld] floats: the stored matrix, or in a row-scaled form the
+// masters times their rows' normalisation scales.
+void download_weights(bsnn_sim* s, const DConn& C, float* out) {
+    const size_t n = static_cast<size_t>(C.n_pre) * C.ld;
+    cuda_check(cudaMemcpy(out, C.w, sizeof(float) * n, cudaMemcpyDeviceToHost), "D2H weights");
+    if (s->h.wfmt == kFmtF32) return;
+    std::vector<float> sc(C.n_pre);
+    cuda_check(cudaMemcpy(sc.data(), C.lz_s, sizeof(float) * C.n_pre, cudaMemcpyDeviceToHost), "D2H row scales");
+    for (uint32_t i = 0; i < C.n_pre; ++i)
+        for (uint32_t q = 0; q < C.ld; ++q) out[static_cast<size_t>(i) * C.ld + q] *= sc[i];
+}
+
 void record_all(bsnn_sim* s, uint32_t clock_step) {
     finalize(s);
     check_device_error(s);
@@ -1033,7 +1124,7 @@ void record_all(bsnn_sim* s, uint32_t clock_step) {
         const DConn& C = s->h.conns[wr.conn];
         const size_t n = static_cast<size_t>(C.n_pre) * C.ld;
         auto w = std::make_shared<std::vector<float>>(n);
-        cuda_check(cudaMemcpy(w->data(), C.w, sizeof(float) * n, cudaMemcpyDeviceToHost), "D2H weights");
+        download_weights(s, C, w->data());
         const std::string path = wr.path;
         const uint32_t n_pre = C.n_pre, n_post = C.n_post, ld = C.ld;
         s->writer->push([w, path, n_pre, n_post, ld, clock_step] {
@@ -1284,6 +1375,16 @@ BSNN_API bsnn_status bsnn_set_noise_mode(bsnn_sim* sim, int32_t mode) {
     });
 }
 
+BSNN_API bsnn_status bsnn_set_weight_format(bsnn_sim* sim, int32_t format) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        require_building(sim);
+        require(format >= BSNN_WEIGHTS_F32 && format <= BSNN_WEIGHTS_FP8_E4M3, BSNN_ERR_INVALID_ARGUMENT,
+                "unknown weight format");
+        sim->weight_format = format;
+    });
+}
+
 BSNN_API bsnn_status bsnn_set_noise_replay(bsnn_sim* sim, const uint8_t* counts, uint32_t n_steps) {
     if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
     return guarded(sim, [&] {
@@ -1348,8 +1449,9 @@ BSNN_API bsnn_status bsnn_write_state(bsnn_sim* sim, int32_t field, uint32_t ind
     return guarded(sim, [&] {
         finalize(sim);
         check_device_error(sim);
-        require(field != BSNN_FIELD_SPIKES && field != BSNN_FIELD_PLAST_PRE_WEIGHT_SUMS, BSNN_ERR_INVALID_ARGUMENT,
-                "field is not writable");
+        require(field != BSNN_FIELD_SPIKES && field != BSNN_FIELD_PLAST_PRE_WEIGHT_SUMS &&
+                    !(field >= BSNN_FIELD_CONN_ROW_SCALE && field <= BSNN_FIELD_CONN_ROW_QUANT_SCALE),
+                BSNN_ERR_INVALID_ARGUMENT, "field is not writable");
         const FieldRef f = field_ref(sim, field, index);
         require(offset <= f.len && count <= f.len - offset, BSNN_ERR_OUT_OF_RANGE, "write out of range");
         require(host_in != nullptr || count == 0, BSNN_ERR_INVALID_ARGUMENT, "null input");
@@ -1367,9 +1469,37 @@ BSNN_API bsnn_status bsnn_read_weights(bsnn_sim* sim, uint32_t connection, float
         require(connection < sim->h.n_conns, BSNN_ERR_OUT_OF_RANGE, "connection index out of range");
         require(host_out != nullptr, BSNN_ERR_INVALID_ARGUMENT, "null output");
         const DConn& C = sim->h.conns[connection];
-        cuda_check(cudaMemcpy2D(host_out, sizeof(float) * C.n_post, C.w, sizeof(float) * C.ld, sizeof(float) * C.n_post,
-                                C.n_pre, cudaMemcpyDeviceToHost),
-                   "D2H weights");
+        if (sim->h.wfmt == kFmtF32) {
+            cuda_check(cudaMemcpy2D(host_out, sizeof(float) * C.n_post, C.w, sizeof(float) * C.ld,
+                                    sizeof(float) * C.n_post, C.n_pre, cudaMemcpyDeviceToHost),
+                       "D2H weights");
+            return;
+        }
+        std::vector<float> w(static_cast<size_t>(C.n_pre) * C.ld);
+        download_weights(sim, C, w.data());
+        for (uint32_t i = 0; i < C.n_pre; ++i)
+            std::memcpy(host_out + static_cast<size_t>(i) * C.n_post, &w[static_cast<size_t>(i) * C.ld],
+                        sizeof(float) * C.n_post);
+    });
+}
+
+BSNN_API bsnn_status bsnn_read_weight_copy(bsnn_sim* sim, uint32_t connection, void* host_out) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        finalize(sim);
+        check_device_error(sim);
+        require(connection < sim->h.n_conns, BSNN_ERR_OUT_OF_RANGE, "connection index out of range");
+        require(host_out != nullptr, BSNN_ERR_INVALID_ARGUMENT, "null output");
+        require(sim->h.wfmt != kFmtF32, BSNN_ERR_INVALID_ARGUMENT, "no weight copy in the BSNN_WEIGHTS_F32 form");
+        const DConn& C = sim->h.conns[connection];
+        const size_t eb = sim->h.wfmt == kFmtBf16 ? 2 : sim->h.wfmt == kFmtFp8 ? 1 : 4;
+        std::vector<unsigned char> tiles(eb * C.qtiles * C.n_pre * 128);
+        cuda_check(cudaMemcpy(tiles.data(), C.q, tiles.size(), cudaMemcpyDeviceToHost), "D2H weight copy");
+        unsigned char* out = static_cast<unsigned char*>(host_out);
+        for (uint32_t i = 0; i < C.n_pre; ++i)
+            for (uint32_t q0 = 0; q0 < C.n_post; q0 += 128)
+                std::memcpy(out + eb * (static_cast<size_t>(i) * C.n_post + q0), &tiles[eb * copy_index(C.n_pre, i, q0)],
+                            eb * std::min<uint32_t>(128, C.n_post - q0));
     });
 }
 

@@ -26,16 +26,23 @@ constexpr int kMaxGroupRoles = 4;  // trace sets / plasticities / monitors per g
 constexpr int kMaxSegsPerCta = 2 * kMaxGroups;
 constexpr int kMaxBlksPerCta = kMaxConns;
 // Threads per CTA: the step-kernel instance that carries row sums needs up to 255 registers per
-// thread (256 threads); the other fits in 227 registers (288 threads, 9 warps).
+// thread (256 threads); the others fit in 168 registers (three warps share one scheduler's
+// quarter of the register file): 288 threads for the reference form, 384 for the row-scaled
+// forms.
 constexpr int kMaxThreads = 256;
 constexpr int kMaxThreadsPlain = 288;
-constexpr int kMaxWarps = kMaxThreadsPlain / 32;
+constexpr int kMaxThreadsRows = 384;
 
 enum : int32_t { kTargetExc = 0, kTargetInh = 1 };
 enum : int32_t { kKindTriplet = 1, kKindIstdp = 2, kKindStdp = 3 };
 enum : int32_t { kMonSpikes = 0, kMonVoltage = 1 };
 enum : int32_t { kNoisePhilox = 0, kNoiseOff = 1, kNoiseReplay = 2 };
 enum : int32_t { kErrNone = 0, kErrBarrierTimeout = 1, kErrStageTimeout = 2 };
+// Weight storage forms.  kFmtF32: the reference's arithmetic (every normalised row rescaled and
+// stored each step).  The others keep an FP32 master m per weight and a per-row normalisation
+// scale s (the weight is s m), so the normalisation touches one number per row; the GEMV reads a
+// copy of m in FP32, BF16, or FP8 E4M3 with a per-row quantisation scale.
+enum : int32_t { kFmtF32 = 0, kFmtF32Rows = 1, kFmtBf16 = 2, kFmtFp8 = 3 };
 
 // NeuronGroupView scalars (cpp_src/neuron_groups/neuron_group_view.h:8-49) plus derived values.
 struct DGroup {
@@ -76,6 +83,16 @@ struct DConn {
     int32_t ts;       // trace set
     int32_t plast;    // plasticity acting on this connection or -1
     float* w;         // [n_pre][ld]
+    // Row-scaled forms (kFmtF32Rows, kFmtBf16, kFmtFp8): the GEMV copy of the masters in
+    // 128-column tiles, element (row i, column q) at ((q / 128) * n_pre + i) * 128 + q % 128, so
+    // the rows of one tile are contiguous and a run of rows of one 32-unit chunk is one block of
+    // memory; columns past n_post are 0.
+    void* q;
+    uint32_t qtiles;  // ceil(n_post / 128)
+    float* qscale;    // [n_pre] FP8: per-row quantisation scale (value = e4m3 * qscale), else null
+    float* qinv;      // [n_pre] its reciprocal
+    float* lz_s;      // [n_pre] normalisation scale s of each row
+    float* lz_m;      // [n_pre] sum of the row's masters
 };
 
 // PlasticityView (cpp_src/plasticities/plasticity_view.h:8-38) plus per-step factor buffers.
@@ -149,6 +166,11 @@ struct DSim {
     // Streamed rows staged through shared memory by bulk asynchronous copies: rows per buffer
     // (two buffers per warp), 0 = off (no shared memory left over).
     uint32_t stage_rows;
+    uint32_t stage_warps;  // warps per CTA (the staging buffers are per warp)
+    int32_t wfmt;          // weight storage form (kFmt*)
+    // FP8 form with no negative weight possible (every weight and every plastic weight_min >= 0):
+    // the copy is decoded by bit placement, exact up to a factor 2^-120 that the row weights carry.
+    uint32_t q_nonneg;
     DGroup groups[kMaxGroups];
     DTraceSet ts[kMaxTraceSets];
     DConn conns[kMaxConns];

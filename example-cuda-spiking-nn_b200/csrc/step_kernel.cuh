@@ -32,6 +32,9 @@
 // launches the device state is the reference's state after step_the_clock.
 #pragma once
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_fp8.h>
 #include <cuda_runtime.h>
 
 #include "bsnn_device.cuh"
@@ -205,6 +208,8 @@ struct Desc {
     unsigned long long* barrier;
     int32_t* error;
     uint32_t stage_rows;  // rows per staging buffer (0 = streamed rows are loaded directly)
+    int32_t wfmt;         // weight storage form (kFmt*)
+    uint32_t q_nonneg;    // FP8 copy decoded by bit placement (non-negative weights)
 };
 
 // Values produced and consumed by the same CTA stay in shared memory: x of the own neurons, the
@@ -226,6 +231,11 @@ struct SmemLayout {
     unsigned char* stage;  // [warps][2][stage_rows][512 B] staging buffers for streamed rows
     uint64_t* stage_bar;   // [warps][2] their mbarriers
     uint32_t* stage_phase; // [warps] parity of each buffer's next completion (bit b: buffer b)
+    float* lzs;         // [max_rows] row-scaled forms: normalisation scale s of each row
+    float* lzm;         // [max_rows] sum of the row's masters
+    float* lzq;         // [max_rows] quantisation scale of the row's GEMV copy
+    float* lzqi;        // [max_rows] its reciprocal
+    float* lzf;         // [max_rows] this step's GEMV weight of the row, x s qs
     uint32_t* bits;     // [n_spike_monitors][max_own/32 + 2]
     unsigned char* desc;  // descriptor copies (DGroup, DTraceSet, DConn, DPlast, DMon, slot lists)
 };
@@ -254,7 +264,7 @@ __host__ __device__ __forceinline__ size_t align16(size_t x) { return (x + 15) &
 
 // Byte layout of the dynamic shared memory; the host sizes the launch with the same function.
 struct SmemSizes {
-    size_t wres, row, meta, rowflag, rowtgt, sbits, gbits, xown, rowfac, ns, rsum, redscr, stage, bits, groups, ts,
+    size_t wres, row, meta, rowflag, rowtgt, sbits, gbits, xown, rowfac, ns, rsum, redscr, stage, lz, bits, groups, ts,
         conns, plast, mons, red, total;
 };
 __host__ __device__ __forceinline__ SmemSizes smem_sizes(uint32_t resident_floats, uint32_t max_rows, uint32_t max_own,
@@ -262,7 +272,7 @@ __host__ __device__ __forceinline__ SmemSizes smem_sizes(uint32_t resident_float
                                                          uint32_t n_ts, uint32_t n_conns, uint32_t n_plast,
                                                          uint32_t n_mons, uint32_t n_red, uint32_t ns_fields,
                                                          uint32_t rsum_floats, uint32_t stage_warps,
-                                                         uint32_t stage_rows) {
+                                                         uint32_t stage_rows, uint32_t lazy_rows) {
     SmemSizes z;
     z.wres = align16(sizeof(float) * static_cast<size_t>(resident_floats));
     z.row = align16(sizeof(float4) * max_rows);
@@ -279,6 +289,7 @@ __host__ __device__ __forceinline__ SmemSizes smem_sizes(uint32_t resident_float
     z.stage = stage_rows ? ((static_cast<size_t>(stage_warps) * 2u * stage_rows * 512u + 127u) & ~size_t(127)) +
                                align16(static_cast<size_t>(stage_warps) * (2u * sizeof(uint64_t) + sizeof(uint32_t)))
                          : 0;
+    z.lz = align16(sizeof(float) * 5u * static_cast<size_t>(lazy_rows));
     z.bits = align16(sizeof(uint32_t) * n_spike_mons * (max_own / 32 + 2));
     z.groups = align16(sizeof(DGroup) * n_groups);
     z.ts = align16(sizeof(DTraceSet) * n_ts);
@@ -286,7 +297,7 @@ __host__ __device__ __forceinline__ SmemSizes smem_sizes(uint32_t resident_float
     z.plast = align16(sizeof(DPlast) * n_plast);
     z.mons = align16(sizeof(DMon) * n_mons);
     z.red = align16(sizeof(uint32_t) * n_red);
-    z.total = z.wres + z.row + z.meta + z.rowflag + z.rowtgt + z.sbits + z.gbits + z.xown + z.rowfac + z.ns + z.rsum + z.redscr + z.stage +
+    z.total = z.wres + z.row + z.meta + z.rowflag + z.rowtgt + z.sbits + z.gbits + z.xown + z.rowfac + z.ns + z.rsum + z.redscr + z.stage + z.lz +
               z.bits + z.groups + z.ts + z.conns + z.plast + z.mons + z.red;
     return z;
 }
@@ -706,7 +717,7 @@ __device__ __forceinline__ void rows_pending(const Desc& D, const DCta& cta, boo
         const DRowMeta meta = sm.meta[r];
         const DConn& C = D.conns[meta.conn];
         const uint32_t i = meta.j - cta.n0;  // rows belong to this CTA's own neurons
-        float4 row = make_float4(0.0f, 1.0f, 0.0f, 0.0f);
+        float4 row = make_float4(0.0f, D.wfmt != kFmtF32 ? sm.lzs[r] * sm.lzq[r] : 1.0f, 0.0f, 0.0f);
         uint32_t flag = 0;
         if (pending && C.plast >= 0) {
             const float2 f = sm.rowfac[(ppar * D.n_plast + static_cast<uint32_t>(C.plast)) * max_own + i];
@@ -720,11 +731,14 @@ __device__ __forceinline__ void rows_pending(const Desc& D, const DCta& cta, boo
 }
 
 // x = d - r of this step into the row table (after the neuron phase).
+// (Row-scaled forms: also the row's GEMV weight x s qs, with s qs from the row table.)
 __device__ __forceinline__ void rows_x(const Desc& D, const DCta& cta, const SmemLayout& sm, uint32_t max_own) {
     for (uint32_t r = threadIdx.x; r < cta.n_rows; r += blockDim.x) {
         const DRowMeta meta = sm.meta[r];
         const DConn& C = D.conns[meta.conn];
-        sm.row[r].x = sm.xown[static_cast<uint32_t>(C.ts) * max_own + (meta.j - cta.n0)];
+        const float x = sm.xown[static_cast<uint32_t>(C.ts) * max_own + (meta.j - cta.n0)];
+        sm.row[r].x = x;
+        if (D.wfmt != kFmtF32) sm.lzf[r] = x * sm.row[r].y;
     }
 }
 
@@ -1075,9 +1089,9 @@ __device__ __forceinline__ float4 block_rows(const DBlk& B, const DConn& C, uint
 // block_rows for a streamed block whose rows are staged through shared memory: the warp's 32
 // units of a row (one contiguous run of up to 512 bytes) arrive by bulk asynchronous copies,
 // `stage_rows` rows per buffer, two buffers per warp, so the next batch streams in while the
-// current one is used.  Lane 0 (always a live lane) issues the copies; every lane waits on the
-// buffer's mbarrier (bounded: on timeout the error word is set and the pass gives up).  Returns
-// A timeout sets the error word and turns staging off for the warp.
+// current one is used.  The lanes issue the copies (lane 0, always a live lane, sets the expected
+// byte count first); every lane waits on the buffer's mbarrier, with a bound: a timeout sets the
+// error word and turns staging off for the warp.
 template <bool SCALE, bool TRIP>
 __device__ __forceinline__ void block_rows_staged(const Desc& D, const DBlk& B, const DConn& C, uint32_t u, bool live,
                                                   unsigned mask, const SmemLayout& sm, bool accumulate, float4& acc,
@@ -1094,14 +1108,14 @@ __device__ __forceinline__ void block_rows_staged(const Desc& D, const DBlk& B, 
     const float2* rowp = reinterpret_cast<const float2*>(sm.row + B.srow);
     float* gbase = C.w + static_cast<size_t>(B.row_begin) * ld + 4u * u;
     const uint32_t nb = (nrows + R - 1u) / R;
+    const uint32_t rank = __popc(mask & ((1u << lane) - 1u)), nlanes = __popc(mask);
     auto issue = [&](uint32_t k) {
-        if (lane == 0) {
-            const uint32_t r0 = k * R, r1 = r0 + R < nrows ? r0 + R : nrows;
-            const uint32_t bar = bar0 + 8u * (k & 1u), dst = buf0 + (k & 1u) * R * 512u;
-            mbar_expect_tx(bar, (r1 - r0) * row_bytes);
-            for (uint32_t r = r0; r < r1; ++r)
-                bulk_load(dst + (r - r0) * 512u, src0 + static_cast<size_t>(r) * ld, row_bytes, bar);
-        }
+        const uint32_t r0 = k * R, r1 = r0 + R < nrows ? r0 + R : nrows;
+        const uint32_t bar = bar0 + 8u * (k & 1u), dst = buf0 + (k & 1u) * R * 512u;
+        if (lane == 0) mbar_expect_tx(bar, (r1 - r0) * row_bytes);
+        __syncwarp(mask);
+        for (uint32_t r = r0 + rank; r < r1; r += nlanes)
+            bulk_load(dst + (r - r0) * 512u, src0 + static_cast<size_t>(r) * ld, row_bytes, bar);
     };
     issue(0);
     if (nb > 1u) issue(1);
@@ -1161,15 +1175,192 @@ __device__ __forceinline__ void block_rows_staged(const Desc& D, const DBlk& B, 
                 }
             }
         }
-        // every lane is done with this buffer before lane 0 refills it
+        // every lane is done with this buffer before it is refilled
         __syncwarp(mask);
         if (k + 2u < nb) {
-            if (lane == 0) fence_proxy_async_shared();
+            fence_proxy_async_shared();
             issue(k + 2u);
         }
     }
     if (lane == 0) sm.stage_phase[warp] = phase;
     __syncwarp(mask);
+}
+
+// ---- Row-scaled weight forms (kFmtF32Rows, kFmtBf16, kFmtFp8) ----------------------------------
+// A weight is kept as an FP32 master m and the normalisation scale s of its row: the weight is
+// w = s m.  The update rules act on w exactly as in the reference form (LTP clamp, then LTD clamp)
+// and store m = w / s.  The triplet normalisation (the reference scales the row by target / sum of
+// its weights) becomes s = target / M, M being the sum of the row's masters: a row whose
+// presynaptic neuron spiked has all its entries updated, and M is summed again from the whole
+// row; otherwise M changes by the changes of the entries in the columns of spiking postsynaptic
+// neurons.  So the normalisation costs one number per row instead of a read and a write of the
+// whole matrix.  The GEMV reads a copy of the masters -- FP32, BF16, or FP8 E4M3 with a per-row
+// quantisation scale qs -- and weighs row i by x_i s_i qs_i.  Updates refresh the copy's entries
+// they change.
+
+__device__ __forceinline__ float4 bf16x4_to_float4(uint2 v) {
+    return make_float4(__uint_as_float(v.x << 16), __uint_as_float(v.x & 0xffff0000u), __uint_as_float(v.y << 16),
+                       __uint_as_float(v.y & 0xffff0000u));
+}
+__device__ __forceinline__ float2 e4m3x2_to_float2(uint32_t v16) {
+    const __half2_raw h = __nv_cvt_fp8x2_to_halfraw2(static_cast<__nv_fp8x2_storage_t>(v16), __NV_E4M3);
+    return __half22float2(__half2(h));
+}
+__device__ __forceinline__ float4 e4m3x4_to_float4(uint32_t v) {
+    const float2 a = e4m3x2_to_float2(v & 0xffffu), b = e4m3x2_to_float2(v >> 16);
+    return make_float4(a.x, a.y, b.x, b.y);
+}
+// Four non-negative E4M3 codes times 2^-120, by placing each code's 7 magnitude bits at bits 26:20
+// of an FP32 word: the E4M3 exponent field becomes the low 4 bits of the FP32 exponent field and
+// the 3 mantissa bits its top mantissa bits, so normals map to 2^(e-127) (1 + m/8) and subnormals
+// to FP32 denormals 2^-126 (m/8) -- the E4M3 values 2^(e-7) (1 + m/8) and 2^-6 (m/8) times 2^-120,
+// exactly.  (Two integer operations per value instead of two conversions.)
+__device__ __forceinline__ float4 e4m3x4_nonneg_scaled(uint32_t v) {
+    return make_float4(__uint_as_float((v << 20) & 0x07f00000u), __uint_as_float((v << 12) & 0x07f00000u),
+                       __uint_as_float((v << 4) & 0x07f00000u), __uint_as_float((v >> 4) & 0x07f00000u));
+}
+// One 4-column unit of the GEMV copy (EB bytes per element) from shared memory.
+template <int EB, bool NN = false>
+__device__ __forceinline__ float4 copy_unit_s(uint32_t a) {
+    if constexpr (EB == 4) {
+        return lds4(a);
+    } else if constexpr (EB == 2) {
+        uint2 v;
+        asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(a));
+        return bf16x4_to_float4(v);
+    } else {
+        uint32_t v;
+        asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(a));
+        if constexpr (NN) return e4m3x4_nonneg_scaled(v);
+        else return e4m3x4_to_float4(v);
+    }
+}
+// Element index of (row, column q) in a connection's tiled GEMV copy.
+__host__ __device__ __forceinline__ size_t copy_index(uint32_t n_pre, uint32_t row, uint32_t q) {
+    return ((static_cast<size_t>(q >> 7) * n_pre + row) << 7) + (q & 127u);
+}
+// Writes master m of (row, q) into the GEMV copy.
+__device__ __forceinline__ void store_copy(int32_t fmt, const DConn& C, uint32_t row, uint32_t q, float m, float qinv) {
+    const size_t e = copy_index(C.n_pre, row, q);
+    if (fmt == kFmtBf16) reinterpret_cast<__nv_bfloat16*>(C.q)[e] = __float2bfloat16_rn(m);
+    else if (fmt == kFmtFp8) reinterpret_cast<__nv_fp8_storage_t*>(C.q)[e] = __nv_cvt_float_to_fp8(m * qinv, __NV_SATFINITE, __NV_E4M3);
+    else reinterpret_cast<float*>(C.q)[e] = m;
+}
+
+// The pending plasticity update in a row-scaled form, on warps [w_first, w_first + nwarps): one
+// warp per row.  A row whose presynaptic neuron spiked gets LTP (where the postsynaptic neuron
+// spiked) then LTD on every entry, and M is summed from the new masters (lanes in column order,
+// then an xor-butterfly); another row gets LTP in the columns of the spiking postsynaptic
+// neurons and M grows by the sum of the changes (same fixed order).
+__device__ __forceinline__ void apply_updates_rows(const Desc& D, const DBlk* s_blk, uint32_t nblk, uint32_t ppar,
+                                                const SmemLayout& sm, uint32_t w_first, uint32_t nwarps) {
+    const uint32_t warp = (threadIdx.x >> 5) - w_first, lane = threadIdx.x & 31u;
+    const int32_t fmt = D.wfmt;
+    for (uint32_t bk = 0; bk < nblk; ++bk) {
+        const DBlk B = s_blk[bk];
+        const DConn& C = D.conns[B.conn];
+        if (C.plast < 0) continue;
+        const DPlast& P = D.plast[C.plast];
+        const uint32_t nrows = B.row_end - B.row_begin, n_post = C.n_post, post_off = C.post_off;
+        const float* colA = P.colA[ppar];
+        const float* colB = P.colB[ppar];
+        const uint32_t w0 = post_off >> 5, w1 = (post_off + n_post - 1u) >> 5;
+        bool any_post = false;
+        for (uint32_t w = w0 + lane; w <= w1; w += 32u) {
+            uint32_t bits = sm.sbits[w];
+            if (w == w0) bits &= 0xffffffffu << (post_off & 31u);
+            if (w == w1) bits &= 0xffffffffu >> (31u - ((post_off + n_post - 1u) & 31u));
+            any_post |= bits != 0u;
+        }
+        any_post = __any_sync(kFull, any_post);
+        for (uint32_t i = warp; i < nrows; i += nwarps) {
+            const uint32_t r = B.srow + i, pl = B.row_begin + i;
+            const bool pre_spk = sm.rowflag[r] != 0u;
+            if (!pre_spk && !any_post) continue;
+            const float4 rw = sm.row[r];
+            const float sc = sm.lzs[r], qinv = sm.lzqi[r];
+            float* mrow = C.w + static_cast<size_t>(pl) * C.ld;
+            float acc = 0.0f;
+            if (pre_spk) {
+                for (uint32_t q = lane; q < n_post; q += 32u) {
+                    const float m0 = __ldcg(mrow + q);
+                    float m = m0;
+                    if (q != pl) {
+                        const uint32_t g = post_off + q;
+                        const uint32_t post_spk = (sm.sbits[g >> 5] >> (g & 31u)) & 1u;
+                        const float w = plastic_update(sc * m0, q, pl, n_post, post_spk, 1u, rw.z, __ldcg(colA + q),
+                                                       __ldcg(colB + q), rw.w, P.wmin, P.wmax);
+                        m = __fdiv_rn(w, sc);
+                        __stcg(mrow + q, m);
+                        store_copy(fmt, C, pl, q, m, qinv);
+                    }
+                    acc += m;
+                }
+            } else {
+                for (uint32_t w = w0 + lane; w <= w1; w += 32u) {
+                    uint32_t bits = sm.sbits[w];
+                    if (w == w0) bits &= 0xffffffffu << (post_off & 31u);
+                    if (w == w1) bits &= 0xffffffffu >> (31u - ((post_off + n_post - 1u) & 31u));
+                    while (bits) {
+                        const uint32_t b = __ffs(bits) - 1u;
+                        bits &= bits - 1u;
+                        const uint32_t q = 32u * w + b - post_off;
+                        if (q == pl) continue;
+                        const float m0 = __ldcg(mrow + q);
+                        const float wv = clamp_w(fmaf(rw.z, __ldcg(colA + q), sc * m0), P.wmin, P.wmax);
+                        const float m = __fdiv_rn(wv, sc);
+                        __stcg(mrow + q, m);
+                        store_copy(fmt, C, pl, q, m, qinv);
+                        acc += m - m0;
+                    }
+                }
+            }
+            acc = warp_sum(acc);
+            if (lane == 0) sm.lzm[r] = pre_spk ? acc : sm.lzm[r] + acc;
+        }
+    }
+}
+
+// The triplet normalisation in a row-scaled form: s = target / M for every normalised row (the
+// reference leaves a row whose sum is not positive as it is), one warp per row on warps
+// [w_first, w_first + nwarps).  A scale outside [1/2, 2] is folded into the row instead: the
+// masters become the weights (m = s m, copy refreshed, M summed again) and s = 1, so a master
+// never exceeds twice the plastic bound (the FP8 copy's range) and a zero target zeroes the row.
+// The row's s qs goes to the row table.
+__device__ __forceinline__ void norm_rows_lazy(const Desc& D, const SmemLayout& sm, const DBlk* s_blk, uint32_t nblk,
+                                            uint32_t w_first, uint32_t nwarps) {
+    const uint32_t warp = (threadIdx.x >> 5) - w_first, lane = threadIdx.x & 31u;
+    for (uint32_t bk = 0; bk < nblk; ++bk) {
+        const DBlk B = s_blk[bk];
+        const DConn& C = D.conns[B.conn];
+        if (C.plast < 0 || D.plast[C.plast].kind != kKindTriplet) continue;
+        const uint32_t nrows = B.row_end - B.row_begin;
+        for (uint32_t i = warp; i < nrows; i += nwarps) {
+            const uint32_t r = B.srow + i;
+            const float M = sm.lzm[r];
+            if (!(M > 0.0f)) continue;
+            float sc = __fdiv_rn(sm.rowtgt[r], M);
+            if (!(sc >= 0.5f && sc <= 2.0f)) {
+                const uint32_t pl = B.row_begin + i;
+                const float qinv = sm.lzqi[r];
+                float* mrow = C.w + static_cast<size_t>(pl) * C.ld;
+                float acc = 0.0f;
+                for (uint32_t q = lane; q < C.n_post; q += 32u) {
+                    const float m = sc * __ldcg(mrow + q);
+                    __stcg(mrow + q, m);
+                    store_copy(D.wfmt, C, pl, q, m, qinv);
+                    acc += m;
+                }
+                acc = warp_sum(acc);
+                if (lane == 0) sm.lzm[r] = acc;
+                sc = 1.0f;
+            }
+            if (lane == 0) {
+                sm.lzs[r] = sc;
+                sm.row[r].y = sc * sm.lzq[r];
+            }
+        }
+    }
 }
 
 // All blocks of segment SG for unit u; the partial sums go to the segment's slot.  `pending` = an
@@ -1227,10 +1418,180 @@ __device__ __forceinline__ void segment_unit(const Desc& D, const DSeg& SG, cons
 // Pass 2: each thread owns work items (one 4-column unit of one segment) and walks all of the
 // segment's rows; per item the partial sums go to the parity-`par` slot of this CTA.  A warp's
 // 32 items always lie in one segment (segments start at multiples of 32 items).
-template <bool CARRY>
+// The row-scaled weight pass as one stream of batches per warp: the warp's tasks are its items
+// (it0 + 32 w + lane for it0 = 0, blockDim, ...; one 32-unit chunk of one segment), each item's
+// blocks with rows, and each block's batches of R rows.  In the tiled copy a batch is one
+// contiguous run of memory, so it arrives by ONE bulk asynchronous copy into one of the warp's two
+// shared-memory buffers.  A producer cursor runs up to two batches ahead of the consumer, across
+// block and item boundaries, so the next item's rows are in flight while the current one finishes.
+struct RowCursor {
+    uint32_t it0, seg, bk, k;
+    bool valid;
+};
+
+__device__ __forceinline__ bool nonempty_block(const DSeg& SG, const DBlk* s_blk, uint32_t from, uint32_t& bk) {
+    for (bk = from; bk < SG.blk_end; ++bk)
+        if (s_blk[bk].row_end > s_blk[bk].row_begin) return true;
+    return false;
+}
+
+// Moves c to the first batch of the warp's first item at or after c.it0 that has rows.  With
+// `zeros`, the items passed over (segments whose blocks have no rows) get zero partial sums.
+__device__ __forceinline__ void seek_item(RowCursor& c, uint32_t n_items, const DSeg* s_seg, uint32_t n_seg,
+                                          const DBlk* s_blk, bool zeros, float* part_out, uint32_t npad) {
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    for (; c.it0 < n_items; c.it0 += blockDim.x) {
+        const int s = seg_of_item(s_seg, n_seg, c.it0 + 32u * warp);
+        if (s < 0) continue;
+        const DSeg& SG = s_seg[s];
+        c.seg = static_cast<uint32_t>(s);
+        c.k = 0;
+        if (nonempty_block(SG, s_blk, SG.blk_begin, c.bk)) {
+            c.valid = true;
+            return;
+        }
+        const uint32_t u = c.it0 + 32u * warp + lane - SG.item_begin;
+        if (zeros && u < SG.units && SG.blk_end > SG.blk_begin)
+            *reinterpret_cast<float4*>(part_out + static_cast<size_t>(SG.slot) * npad + SG.pcol + 4u * u) =
+                make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    c.valid = false;
+}
+
+__device__ __forceinline__ void advance(RowCursor& c, uint32_t R, uint32_t n_items, const DSeg* s_seg, uint32_t n_seg,
+                                        const DBlk* s_blk, bool zeros, float* part_out, uint32_t npad) {
+    const DSeg& SG = s_seg[c.seg];
+    const DBlk& B = s_blk[c.bk];
+    if ((c.k + 1u) * R < B.row_end - B.row_begin) {
+        ++c.k;
+        return;
+    }
+    c.k = 0;
+    if (nonempty_block(SG, s_blk, c.bk + 1u, c.bk)) return;
+    c.it0 += blockDim.x;
+    seek_item(c, n_items, s_seg, n_seg, s_blk, zeros, part_out, npad);
+}
+
+template <int EB, bool NN>
+__device__ __forceinline__ void weight_pass_rows_stream(const Desc& D, const DCta& cta, uint32_t par, const SmemLayout& sm,
+                                                        const DSeg* s_seg, const DBlk* s_blk, uint32_t n_seg) {
+    constexpr uint32_t UB = 4u * EB, SB = 32u * UB;  // bytes per unit, per row of a tile
+    float* part_out = D.partials + static_cast<size_t>(par) * D.n_slots * D.N_pad;
+    const uint32_t npad = D.N_pad, n_items = cta.n_items, R = D.stage_rows * (512u / SB);
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t phase = sm.stage_phase[warp];
+    if (phase & kStageDead) return;
+    const uint32_t buf0 = saddr(sm.stage) + warp * 2u * D.stage_rows * 512u;
+    const uint32_t bar0 = saddr(sm.stage_bar + 2u * warp);
+    auto issue = [&](const RowCursor& c, uint32_t slot) {
+        if (lane == 0) {
+            const DSeg& SG = s_seg[c.seg];
+            const DBlk& B = s_blk[c.bk];
+            const DConn& C = D.conns[B.conn];
+            const uint32_t nrows = B.row_end - B.row_begin, r0 = c.k * R, n = nrows - r0 < R ? nrows - r0 : R;
+            const uint32_t chunk = (c.it0 + 32u * warp - SG.item_begin) / 32u;
+            const unsigned char* src =
+                static_cast<const unsigned char*>(C.q) + copy_index(C.n_pre, B.row_begin + r0, 128u * chunk) * EB;
+            const uint32_t bar = bar0 + 8u * slot;
+            mbar_expect_tx(bar, n * SB);
+            bulk_load(buf0 + slot * R * SB, src, n * SB, bar);
+        }
+    };
+    RowCursor cc{0u, 0u, 0u, 0u, false};
+    seek_item(cc, n_items, s_seg, n_seg, s_blk, true, part_out, npad);
+    RowCursor pc = cc;
+    uint32_t g_issue = 0, g_use = 0;
+    for (int f = 0; f < 2 && pc.valid; ++f) {
+        issue(pc, g_issue & 1u);
+        ++g_issue;
+        advance(pc, R, n_items, s_seg, n_seg, s_blk, false, part_out, npad);
+    }
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    while (cc.valid) {
+        const uint32_t b = g_use & 1u;
+        const bool got = mbar_wait(bar0 + 8u * b, (phase >> b) & 1u);
+        if (!__all_sync(kFull, got)) {
+            // give up for the launch: the batches in flight land (bounded) and the host sees the error
+            if (lane == 0) atomicExch(D.error, kErrStageTimeout);
+            if (!got) mbar_wait(bar0 + 8u * b, (phase >> b) & 1u);
+            if (g_issue > g_use + 1u) mbar_wait(bar0 + 8u * (b ^ 1u), (phase >> (b ^ 1u)) & 1u);
+            phase |= kStageDead;
+            break;
+        }
+        phase ^= 1u << b;
+        ++g_use;
+        const DSeg& SG = s_seg[cc.seg];
+        const DBlk B = s_blk[cc.bk];
+        const uint32_t nrows = B.row_end - B.row_begin, r0 = cc.k * R, r1 = r0 + R < nrows ? r0 + R : nrows;
+        const uint32_t buf = buf0 + b * R * SB + UB * lane - r0 * SB;
+        const float* rowf = sm.lzf + B.srow;
+        // whole groups of 8 rows (two accumulators for independent FMA chains), then the rest
+        float4 acc2 = make_float4(0.f, 0.f, 0.f, 0.f);
+        uint32_t i0 = r0;
+        for (; i0 + 8u <= r1; i0 += 8u) {
+            float4 wb[8];
+            float f[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                wb[q] = copy_unit_s<EB, NN>(buf + (i0 + q) * SB);
+                f[q] = rowf[i0 + q];
+            }
+#pragma unroll
+            for (int q = 0; q < 8; q += 2) {
+                acc.x = fmaf(wb[q].x, f[q], acc.x);
+                acc.y = fmaf(wb[q].y, f[q], acc.y);
+                acc.z = fmaf(wb[q].z, f[q], acc.z);
+                acc.w = fmaf(wb[q].w, f[q], acc.w);
+                acc2.x = fmaf(wb[q + 1].x, f[q + 1], acc2.x);
+                acc2.y = fmaf(wb[q + 1].y, f[q + 1], acc2.y);
+                acc2.z = fmaf(wb[q + 1].z, f[q + 1], acc2.z);
+                acc2.w = fmaf(wb[q + 1].w, f[q + 1], acc2.w);
+            }
+        }
+        for (; i0 < r1; ++i0) {
+            const float4 w = copy_unit_s<EB, NN>(buf + i0 * SB);
+            const float f = rowf[i0];
+            acc.x = fmaf(w.x, f, acc.x);
+            acc.y = fmaf(w.y, f, acc.y);
+            acc.z = fmaf(w.z, f, acc.z);
+            acc.w = fmaf(w.w, f, acc.w);
+        }
+        acc.x += acc2.x;
+        acc.y += acc2.y;
+        acc.z += acc2.z;
+        acc.w += acc2.w;
+        __syncwarp();
+        const RowCursor done = cc;
+        advance(cc, R, n_items, s_seg, n_seg, s_blk, true, part_out, npad);
+        if (!cc.valid || cc.it0 != done.it0) {  // the item is complete
+            const uint32_t u = done.it0 + 32u * warp + lane - SG.item_begin;
+            if (u < SG.units)
+                *reinterpret_cast<float4*>(part_out + static_cast<size_t>(SG.slot) * npad + SG.pcol + 4u * u) = acc;
+            acc = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        if (pc.valid) {  // refill the buffer just used
+            fence_proxy_async_shared();
+            issue(pc, g_issue & 1u);
+            ++g_issue;
+            advance(pc, R, n_items, s_seg, n_seg, s_blk, false, part_out, npad);
+        }
+    }
+    if (lane == 0) sm.stage_phase[warp] = phase;
+    __syncwarp();
+}
+
+template <bool CARRY, bool LAZY>
 __device__ __forceinline__ void weight_pass(const Desc& D, const DCta& cta, bool pending, bool accumulate, uint32_t par,
                                          const SmemLayout& sm, const DSeg* s_seg, const DBlk* s_blk, uint32_t n_seg,
                                          uint32_t n_chunks) {
+    if constexpr (LAZY) {  // (the host guarantees staging buffers in the row-scaled forms)
+        if (!accumulate) return;
+        if (D.wfmt == kFmtBf16) weight_pass_rows_stream<2, false>(D, cta, par, sm, s_seg, s_blk, n_seg);
+        else if (D.wfmt == kFmtFp8 && D.q_nonneg) weight_pass_rows_stream<1, true>(D, cta, par, sm, s_seg, s_blk, n_seg);
+        else if (D.wfmt == kFmtFp8) weight_pass_rows_stream<1, false>(D, cta, par, sm, s_seg, s_blk, n_seg);
+        else weight_pass_rows_stream<4, false>(D, cta, par, sm, s_seg, s_blk, n_seg);
+        return;
+    }
     float* part_out = D.partials + static_cast<size_t>(par) * D.n_slots * D.N_pad;
     const uint32_t npad = D.N_pad;
     for (uint32_t it0 = 0; it0 < cta.n_items; it0 += blockDim.x) {
@@ -1271,8 +1632,8 @@ __device__ __forceinline__ void copy_words(void* dst, const void* src, size_t by
     for (size_t k = threadIdx.x; k < bytes / 4; k += blockDim.x) d[k] = s[k];
 }
 
-template <bool CARRY>
-__global__ void __launch_bounds__(CARRY ? kMaxThreads : kMaxThreadsPlain, 1)
+template <bool CARRY, bool LAZY>
+__global__ void __launch_bounds__(CARRY ? kMaxThreads : LAZY ? kMaxThreadsRows : kMaxThreadsPlain, 1)
     bsnn_step_kernel(const DSim* __restrict__ S, uint32_t n_steps) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ Desc s_d;
@@ -1296,7 +1657,8 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : kMaxThreadsPlain, 1)
     const NsLayout L0 = ns_layout(S->ns_ts, S->ns_pre, S->ns_post, S->ns_mon);
     const SmemSizes z = smem_sizes(S->resident_floats, max_rows, max_own, S->spk_words, n_spike_mons, S->n_groups,
                                    S->n_ts, S->n_conns, S->n_plast, S->n_mons, S->n_red, L0.fields,
-                                   S->max_trows * S->n_chunks, kMaxWarps, S->stage_rows);
+                                   S->max_trows * S->n_chunks, S->stage_warps, S->stage_rows,
+                                   LAZY ? max_rows : 0u);
     if (threadIdx.x == 0) {
         s_L = L0;
         unsigned char* p = smem_raw;
@@ -1325,14 +1687,20 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : kMaxThreadsPlain, 1)
         sm.red = reinterpret_cast<float*>(p);
         p += z.redscr;
         {
-            const size_t buf = S->stage_rows ? (static_cast<size_t>(kMaxWarps) * 2u * S->stage_rows * 512u + 127u) &
+            const size_t buf = S->stage_rows ? (static_cast<size_t>(S->stage_warps) * 2u * S->stage_rows * 512u + 127u) &
                                                    ~size_t(127)
                                              : 0;
             sm.stage = p;
             sm.stage_bar = reinterpret_cast<uint64_t*>(p + buf);
-            sm.stage_phase = reinterpret_cast<uint32_t*>(p + buf + static_cast<size_t>(kMaxWarps) * 2u * sizeof(uint64_t));
+            sm.stage_phase = reinterpret_cast<uint32_t*>(p + buf + static_cast<size_t>(S->stage_warps) * 2u * sizeof(uint64_t));
         }
         p += z.stage;
+        sm.lzs = reinterpret_cast<float*>(p);
+        sm.lzm = sm.lzs + max_rows;
+        sm.lzq = sm.lzm + max_rows;
+        sm.lzqi = sm.lzq + max_rows;
+        sm.lzf = sm.lzqi + max_rows;
+        p += z.lz;
         sm.bits = reinterpret_cast<uint32_t*>(p);
         p += z.bits;
         sm.desc = p;
@@ -1389,6 +1757,8 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : kMaxThreadsPlain, 1)
         s_d.barrier = S->barrier;
         s_d.error = S->error;
         s_d.stage_rows = S->stage_rows;
+        s_d.wfmt = S->wfmt;
+        s_d.q_nonneg = S->q_nonneg;
         uint32_t base = 0;
         for (uint32_t m = 0; m < S->n_mons; ++m) {
             s_d.bitbase[m] = base;
@@ -1460,6 +1830,13 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : kMaxThreadsPlain, 1)
         const DConn& C = D.conns[meta.conn];
         sm.rowtgt[r] = C.plast >= 0 && D.plast[C.plast].kind == kKindTriplet ? __ldcg(D.plast[C.plast].sums + meta.pl)
                                                                               : 0.0f;
+        if constexpr (LAZY) {
+            sm.lzs[r] = __ldcg(C.lz_s + meta.pl);
+            sm.lzm[r] = __ldcg(C.lz_m + meta.pl);
+            // (the bit-placement decoding of non-negative FP8 codes yields values times 2^-120)
+            sm.lzq[r] = (C.qscale ? __ldcg(C.qscale + meta.pl) : 1.0f) * (D.q_nonneg ? 0x1p120f : 1.0f);
+            sm.lzqi[r] = C.qinv ? __ldcg(C.qinv + meta.pl) : 1.0f;
+        }
     }
     __syncthreads();
 
@@ -1514,22 +1891,26 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : kMaxThreadsPlain, 1)
                 neuron_phase(S, D, cta, t, clock, par, pending, sm, max_own, L, s_ev[0], s_ev[1]);
             } else if (pending) {
                 const uint32_t nw = nwarps - neuron_warps;
-                apply_updates(D, s_blk, s_nblk, ppar, sm, neuron_warps, nw);
+                if constexpr (LAZY) apply_updates_rows(D, s_blk, s_nblk, ppar, sm, neuron_warps, nw);
+                else apply_updates(D, s_blk, s_nblk, ppar, sm, neuron_warps, nw);
                 if (norm_now) {
                     named_barrier_sync(1u, 32u * nw);
-                    norm_rows<CARRY>(D, sm, s_blk, s_nblk, neuron_warps, nw, n_chunks);
+                    if constexpr (LAZY) norm_rows_lazy(D, sm, s_blk, s_nblk, neuron_warps, nw);
+                    else norm_rows<CARRY>(D, sm, s_blk, s_nblk, neuron_warps, nw, n_chunks);
                 }
             }
             __syncthreads();
         } else {
             if (pending) {
-                apply_updates(D, s_blk, s_nblk, ppar, sm, 0u, nwarps);
+                if constexpr (LAZY) apply_updates_rows(D, s_blk, s_nblk, ppar, sm, 0u, nwarps);
+                else apply_updates(D, s_blk, s_nblk, ppar, sm, 0u, nwarps);
                 __syncthreads();
             }
             neuron_phase(S, D, cta, t, clock, par, pending, sm, max_own, L, s_ev[0], s_ev[1]);
             __syncthreads();
             if (norm_now) {
-                norm_rows<CARRY>(D, sm, s_blk, s_nblk, 0u, nwarps, n_chunks);
+                if constexpr (LAZY) norm_rows_lazy(D, sm, s_blk, s_nblk, 0u, nwarps);
+                else norm_rows<CARRY>(D, sm, s_blk, s_nblk, 0u, nwarps, n_chunks);
                 __syncthreads();
             }
         }
@@ -1538,7 +1919,7 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : kMaxThreadsPlain, 1)
         rows_x(D, cta, sm, max_own);
         __syncthreads();
         BSNN_TMARK(2);
-        weight_pass<CARRY>(D, cta, pending, true, par, sm, s_seg, s_blk, n_seg, n_chunks);
+        weight_pass<CARRY, LAZY>(D, cta, pending, true, par, sm, s_seg, s_blk, n_seg, n_chunks);
         __syncthreads();
         BSNN_TMARK(4);
         if (!grid_barrier(D.barrier, D.error, bar0 + (k + 1ull) * gridDim.x, &s_ok)) {
@@ -1560,13 +1941,28 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : kMaxThreadsPlain, 1)
     stage_spike_bits(D, lpar, sm);
     rows_pending(D, cta, true, lpar, sm, max_own);
     __syncthreads();
-    apply_updates(D, s_blk, s_nblk, lpar, sm, 0u, nwarps);
-    __syncthreads();
-    if (s_has_norm) {
-        norm_rows<CARRY>(D, sm, s_blk, s_nblk, 0u, nwarps, n_chunks);
+    if constexpr (LAZY) {
+        apply_updates_rows(D, s_blk, s_nblk, lpar, sm, 0u, nwarps);
         __syncthreads();
+        if (s_has_norm) {
+            norm_rows_lazy(D, sm, s_blk, s_nblk, 0u, nwarps);
+            __syncthreads();
+        }
+        for (uint32_t r = threadIdx.x; r < cta.n_rows; r += blockDim.x) {
+            const DRowMeta meta = sm.meta[r];
+            const DConn& C = D.conns[meta.conn];
+            C.lz_s[meta.pl] = sm.lzs[r];
+            C.lz_m[meta.pl] = sm.lzm[r];
+        }
+    } else {
+        apply_updates(D, s_blk, s_nblk, lpar, sm, 0u, nwarps);
+        __syncthreads();
+        if (s_has_norm) {
+            norm_rows<CARRY>(D, sm, s_blk, s_nblk, 0u, nwarps, n_chunks);
+            __syncthreads();
+        }
+        weight_pass<CARRY, LAZY>(D, cta, true, false, lpar, sm, s_seg, s_blk, n_seg, n_chunks);
     }
-    weight_pass<CARRY>(D, cta, true, false, lpar, sm, s_seg, s_blk, n_seg, n_chunks);
     __syncthreads();
     move_resident(D, s_blk, s_nblk, sm, false);
     load_partials(S, D, cta, lpar, sm, max_own);
@@ -1575,6 +1971,20 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : kMaxThreadsPlain, 1)
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         *S->steps_done = t0 + n_steps;
         *S->clock = clock0 + n_steps;
+    }
+}
+
+// Fills the tiled GEMV copy of a connection (row-scaled forms) from its FP32 masters, with the
+// conversion the weight updates use; padding columns become 0.
+__global__ void bsnn_fill_copy_kernel(DConn C, int32_t fmt) {
+    const size_t n = static_cast<size_t>(C.qtiles) * C.n_pre * 128u;
+    for (size_t e = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < n;
+         e += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const uint32_t k = static_cast<uint32_t>(e & 127u);
+        const size_t tr = e >> 7;
+        const uint32_t i = static_cast<uint32_t>(tr % C.n_pre), q = static_cast<uint32_t>(tr / C.n_pre) * 128u + k;
+        const float m = q < C.n_post ? C.w[static_cast<size_t>(i) * C.ld + q] : 0.0f;
+        store_copy(fmt, C, i, q, m, C.qinv ? C.qinv[i] : 1.0f);
     }
 }
 

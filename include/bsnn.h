@@ -80,6 +80,21 @@ typedef int32_t bsnn_status;
 #define BSNN_FIELD_PLAST_TRIPLET_PRE 18      /* float [N_pre] of plasticity `index`                    */
 #define BSNN_FIELD_PLAST_TRIPLET_POST 19     /* float [N_post] of plasticity `index`                   */
 #define BSNN_FIELD_PLAST_PRE_WEIGHT_SUMS 20  /* float [N_pre] normalisation targets of plasticity     */
+/* Row-scaled weight forms only (read-only; `index` = connection): */
+#define BSNN_FIELD_CONN_ROW_SCALE 21         /* float [N_pre] normalisation scale s (weight = s * master) */
+#define BSNN_FIELD_CONN_ROW_MASTER_SUM 22    /* float [N_pre] sum of the row's FP32 masters              */
+#define BSNN_FIELD_CONN_ROW_QUANT_SCALE 23   /* float [N_pre] FP8 copy: value = e4m3 * scale             */
+
+/* Weight storage forms (bsnn_set_weight_format).  No reference counterpart: the reference stores
+ * FP32 weights and rescales every normalised row each step (BSNN_WEIGHTS_F32 keeps exactly that).
+ * The other forms keep an FP32 master m per weight of every connection and a per-row
+ * normalisation scale s (weight = s * m), so the triplet normalisation rewrites one number per
+ * row; the propagation reads a copy of the masters in the given type (FP8: E4M3 times a per-row
+ * scale fixed at upload), and weight updates refresh the entries they change. */
+#define BSNN_WEIGHTS_F32 0           /* the reference's arithmetic                              */
+#define BSNN_WEIGHTS_F32_ROWSCALED 1 /* FP32 masters, lazy row scale, FP32 GEMV copy            */
+#define BSNN_WEIGHTS_BF16 2          /* GEMV copy in BF16 (round to nearest even)               */
+#define BSNN_WEIGHTS_FP8_E4M3 3      /* GEMV copy in FP8 E4M3 (satfinite) with per-row scales   */
 
 /*
  * Parameter PODs.  Field names, order and types are those of the reference structs, so a
@@ -226,6 +241,8 @@ BSNN_API bsnn_status bsnn_set_noise_mode(bsnn_sim* sim, int32_t mode);
 /* counts[(s * N_total + neuron) * 2 + channel] for steps s = 0 .. num_steps-1 counted from the
  * sim's first step; channel 0 = excitatory, 1 = inhibitory.  Steps past num_steps draw 0. */
 BSNN_API bsnn_status bsnn_set_noise_replay(bsnn_sim* sim, const uint8_t* counts, uint32_t num_steps);
+/* Weight storage form (BSNN_WEIGHTS_*), before the first step.  No reference counterpart. */
+BSNN_API bsnn_status bsnn_set_weight_format(bsnn_sim* sim, int32_t format);
 
 /* ---- the hot path --------------------------------------------------------------------------- */
 
@@ -256,6 +273,9 @@ BSNN_API bsnn_status bsnn_write_state(bsnn_sim* sim, int32_t field, uint32_t ind
 /* GpuSimulationState::download_weight_matrix (cpp_src/gpu_core/gpu_simulation_state.cu:287-306):
  * row-major pre x post matrix of a connection. */
 BSNN_API bsnn_status bsnn_read_weights(bsnn_sim* sim, uint32_t connection, float* host_out);
+/* Row-scaled forms: the propagation's copy of the masters, row-major pre x post, as stored
+ * (4-byte floats, 2-byte BF16 or 1-byte E4M3 elements).  No reference counterpart. */
+BSNN_API bsnn_status bsnn_read_weight_copy(bsnn_sim* sim, uint32_t connection, void* host_out);
 /* GpuSimulationState::download_and_flush_spike_history (gpu_simulation_state.cu:239-261):
  * writes the spike ring of a spike recorder in the reference layout
  * host_out[neuron * interval + slot] (0/1) and, when `flush` is non-zero, zeroes the ring. */
