@@ -30,8 +30,9 @@ REF_MAIN = ROOT / "oracle" / "_ref" / "main_buryn"
 
 
 def spike_rows(path):
+    """{label: sorted neuron ids} of a spike recording (its first line is the header)."""
     rows = {}
-    for line in Path(path).read_text().splitlines():
+    for line in Path(path).read_text().splitlines()[1:]:
         label, _, ids = line.partition(",")
         rows[int(label)] = sorted(int(x) for x in ids.split())
     return rows
