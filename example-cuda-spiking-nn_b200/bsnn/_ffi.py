@@ -255,6 +255,22 @@ class ConnectionView(ctypes.Structure):
 
 
 # Exported symbols and their signatures (every entry point declared in include/bsnn.h).
+class BatchInfo(ctypes.Structure):
+    _fields_ = [
+        ("num_classes", ctypes.c_uint32),
+        ("num_instances", ctypes.c_uint32),
+        ("num_neurons", ctypes.c_uint32),
+        ("num_units", ctypes.c_uint32),
+        ("grid_ctas", ctypes.c_uint32),
+        ("block_threads", ctypes.c_uint32),
+        ("steps_done", ctypes.c_uint64),
+        ("device_bytes", ctypes.c_uint64),
+        ("weight_bytes", ctypes.c_uint64),
+        ("kernel_launches", ctypes.c_uint64),
+        ("smem_bytes", ctypes.c_uint64),
+    ]
+
+
 _P = ctypes.c_void_p
 _U32 = ctypes.c_uint32
 _I32 = ctypes.c_int32
@@ -265,6 +281,20 @@ SIGNATURES = {
     "bsnn_create": (_I32, [ctypes.POINTER(StateDesc), ctypes.POINTER(_P)]),
     "bsnn_destroy": (_I32, [_P]),
     "bsnn_last_error": (ctypes.c_char_p, [_P]),
+    "bsnn_batch_create": (_I32, [_I32, ctypes.POINTER(_P)]),
+    "bsnn_batch_destroy": (_I32, [_P]),
+    "bsnn_batch_last_error": (ctypes.c_char_p, [_P]),
+    "bsnn_batch_add_class": (_I32, [_P, _U32, _U32, _FP, _FP, _FP, _FP, _P, _P, ctypes.POINTER(_U32)]),
+    "bsnn_batch_add_instance": (_I32, [_P, _U32, _P, _P, _I32, ctypes.POINTER(_U32), _U32, ctypes.POINTER(_U32), _FP,
+                                       _U32, ctypes.POINTER(_U32)]),
+    "bsnn_batch_set_noise": (_I32, [_P, _I32]),
+    "bsnn_batch_set_steps_per_launch": (_I32, [_P, _U32]),
+    "bsnn_batch_run": (_I32, [_P, _U32]),
+    "bsnn_batch_synchronize": (_I32, [_P]),
+    "bsnn_batch_get_stream": (_I32, [_P, ctypes.POINTER(_P)]),
+    "bsnn_batch_read_state": (_I32, [_P, _U32, _I32, _P]),
+    "bsnn_batch_read_spike_counts": (_I32, [_P, ctypes.POINTER(ctypes.c_uint64)]),
+    "bsnn_batch_get_info": (_I32, [_P, ctypes.POINTER(BatchInfo)]),
     "bsnn_get_info": (_I32, [_P, ctypes.POINTER(Info)]),
     "bsnn_add_neuron_group": (_I32, [_P, ctypes.POINTER(NeuronGroupParams), _UP]),
     "bsnn_add_connection": (_I32, [_P, _U32, _U32, _FP, ctypes.POINTER(ConnectionParams), _UP]),

@@ -1,0 +1,616 @@
+// batch_api.cuh -- host side of the batched form (bsnn_batch_* in include/bsnn.h); included at
+// the end of bsnn_api.cu, whose helpers (cuda_check, require, ApiError, Arena) it uses.
+//
+// A batch is built from size classes (one shared weight set each, stored as BF16 W^T tiles in
+// the tensor cores' canonical layout) and instances (per-instance neuron-group parameters,
+// seed and stimulus).  The first call that needs the device plans the GEMM work units (a K chunk
+// of one 128-post tile of one class and presynaptic side), spreads them over the persistent CTAs
+// (longest first, onto the least loaded CTA), allocates one arena and uploads.  bsnn_batch_run
+// replays a captured CUDA graph of the cooperative launch per chunk of steps.
+#pragma once
+
+#include "batch_kernel.cuh"
+
+struct bsnn_batch {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+
+    struct HClass {
+        uint32_t E, I;
+        std::vector<uint16_t> A[2];  // tiled W^T, BF16 bits
+        float r_decay[2], d_decay[2], norm[2];
+        std::vector<uint32_t> instances;
+    };
+    struct HInst {
+        uint32_t cls;
+        bsnn_neuron_group_params g[2];
+        uint32_t seed;
+        std::vector<uint32_t> counts;
+        std::vector<uint32_t> neurons;
+        std::vector<float> deltas;
+    };
+    std::vector<HClass> classes;
+    std::vector<HInst> insts;
+    bool noise_on = true;
+
+    bool finalized = false, failed = false;
+    unsigned char* arena = nullptr;
+    size_t arena_bytes = 0;
+    BSim h{};
+    BSim* d_sim = nullptr;
+    std::vector<uint32_t> inst_order;  // instance id -> position in the class-sorted order
+    std::vector<uint32_t> nbase;       // per instance id: first neuron
+    uint32_t grid = 0;
+    size_t smem = 0;
+    uint64_t steps_done = 0, launches = 0;
+    uint32_t steps_per_launch = 1000;
+    std::map<uint32_t, cudaGraphExec_t> graphs;
+    float* scratch = nullptr;  // [2][max N] for reads of g with the pending propagation
+
+    ~bsnn_batch() {
+        for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+        if (arena) cudaFree(arena);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+template <class F>
+bsnn_status guarded_batch(bsnn_batch* b, F&& f) {
+    try {
+        int prev = -1;
+        if (b) {
+            cudaGetDevice(&prev);
+            cuda_check(cudaSetDevice(b->device), "cudaSetDevice");
+        }
+        f();
+        if (b && prev >= 0) cudaSetDevice(prev);
+        return BSNN_OK;
+    } catch (const ApiError& e) {
+        if (b) b->err = e.what();
+        g_thread_error = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        if (b) b->err = e.what();
+        g_thread_error = e.what();
+        return BSNN_ERR_RUNTIME;
+    }
+}
+
+uint16_t host_bf16(float v) {  // round to nearest even (finite values)
+    uint32_t u;
+    std::memcpy(&u, &v, 4);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return static_cast<uint16_t>(u >> 16);
+}
+
+DGroup batch_group(const bsnn_neuron_group_params& p, uint32_t off) {
+    DGroup G{};
+    G.off = off;
+    G.n = p.num_neurons;
+    G.inhib = p.is_inhibitory ? 1u : 0u;
+    G.refractory_steps = p.refractory_steps;
+    G.has_bg_e = p.mean_background_excitatory_spikes > 0.0f;
+    G.has_bg_i = p.mean_background_inhibitory_spikes > 0.0f;
+    G.timestep = p.timestep;
+    G.g_leak = p.g_leak;
+    G.cap = p.membrane_capacitance;
+    G.delta_t = p.depolarization_slope_factor;
+    G.v_eff = p.v_effective_spike_threshold;
+    G.e_exc = p.v_excitatory_reversal;
+    G.e_inh = p.v_inhibitory_reversal;
+    G.v_th = p.v_threshold;
+    G.v_reset = p.v_reset;
+    G.v_rest = p.v_rest;
+    G.exp_neg_mean_e = exp_neg_mean_of(p.mean_background_excitatory_spikes);
+    G.exp_neg_mean_i = exp_neg_mean_of(p.mean_background_inhibitory_spikes);
+    G.bg_er_decay = p.background_excitatory_postsynaptic_r_trace_decay;
+    G.bg_ed_decay = p.background_excitatory_postsynaptic_d_trace_decay;
+    G.bg_ir_decay = p.background_inhibitory_postsynaptic_r_trace_decay;
+    G.bg_id_decay = p.background_inhibitory_postsynaptic_d_trace_decay;
+    G.bg_scale_e = p.background_excitatory_scaling_factor;
+    G.bg_scale_i = p.background_inhibitory_scaling_factor;
+    return G;
+}
+
+void batch_finalize(bsnn_batch* b) {
+    if (b->finalized) return;
+    require(!b->classes.empty() && !b->insts.empty(), BSNN_ERR_STATE, "a batch needs at least one class and one instance");
+    BSim& h = b->h;
+    h = BSim{};
+    h.n_classes = static_cast<uint32_t>(b->classes.size());
+    h.n_inst = static_cast<uint32_t>(b->insts.size());
+    h.noise_on = b->noise_on ? 1 : 0;
+
+    // Instances in class order: the instance's row in its class's B operand is its rank there.
+    std::vector<uint32_t> row(h.n_inst);
+    b->nbase.assign(h.n_inst, 0);
+    uint32_t n_neurons = 0;
+    for (uint32_t c = 0; c < h.n_classes; ++c) {
+        const auto& HC = b->classes[c];
+        for (uint32_t r = 0; r < HC.instances.size(); ++r) row[HC.instances[r]] = r;
+    }
+    for (uint32_t i = 0; i < h.n_inst; ++i) {
+        const auto& HC = b->classes[b->insts[i].cls];
+        b->nbase[i] = n_neurons;
+        n_neurons += HC.E + HC.I;
+    }
+    h.n_neurons = n_neurons;
+
+    // Work units: K chunks of at most kc tiles, kc chosen so the largest unit is about the
+    // average work per CTA.
+    const uint32_t n_ctas = static_cast<uint32_t>(b->sm_count);
+    uint64_t total_tiles = 0;
+    for (const auto& HC : b->classes) {
+        const uint32_t MT = (HC.E + HC.I + 127) / 128;
+        total_tiles += static_cast<uint64_t>(MT) * ((HC.E + 63) / 64 + (HC.I + 63) / 64);
+    }
+    const uint32_t kc = std::max<uint32_t>(4u, static_cast<uint32_t>((total_tiles + n_ctas - 1) / n_ctas));
+    std::vector<BUnit> units;
+    size_t part_floats = 0;
+    for (uint32_t c = 0; c < h.n_classes; ++c) {
+        const auto& HC = b->classes[c];
+        BClass& C = h.cls[c];
+        C.E = HC.E;
+        C.I = HC.I;
+        C.N = HC.E + HC.I;
+        C.n_inst = static_cast<uint32_t>(HC.instances.size());
+        C.NP = std::max<uint32_t>(8u, round_up(C.n_inst, 8));
+        require(C.NP <= 128, BSNN_ERR_INVALID_ARGUMENT, "at most 128 instances per size class");
+        C.inst0 = HC.instances.empty() ? 0u : HC.instances[0];
+        C.MT = (C.N + 127) / 128;
+        for (int sd = 0; sd < 2; ++sd) {
+            const uint32_t K = sd == 0 ? C.E : C.I;
+            C.KT[sd] = (K + 63) / 64;
+            C.nkc[sd] = (C.KT[sd] + kc - 1) / kc;
+            C.pbase[sd] = part_floats;
+            C.r_decay[sd] = HC.r_decay[sd];
+            C.d_decay[sd] = HC.d_decay[sd];
+            C.norm[sd] = HC.norm[sd];
+            for (uint32_t mt = 0; mt < C.MT; ++mt)
+                for (uint32_t q = 0; q < C.nkc[sd]; ++q) {
+                    BUnit U{};
+                    U.cls = c;
+                    U.side = static_cast<uint32_t>(sd);
+                    U.mt = mt;
+                    U.k0 = q * kc;
+                    U.k1 = std::min(C.KT[sd], (q + 1) * kc);
+                    U.part = part_floats;
+                    part_floats += static_cast<size_t>(C.NP) * 128u;
+                    units.push_back(U);
+                }
+        }
+    }
+    h.n_units = static_cast<uint32_t>(units.size());
+    // longest first onto the least loaded CTA (cost: K tiles plus the epilogue)
+    std::vector<uint32_t> order(units.size());
+    std::iota(order.begin(), order.end(), 0u);
+    auto cost = [&](uint32_t u) { return static_cast<double>(units[u].k1 - units[u].k0) + 2.0; };
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t c) { return cost(a) > cost(c); });
+    std::vector<double> load(n_ctas, 0.0);
+    std::vector<std::vector<uint32_t>> per_cta(n_ctas);
+    for (uint32_t u : order) {
+        const uint32_t k = static_cast<uint32_t>(std::min_element(load.begin(), load.end()) - load.begin());
+        load[k] += cost(u);
+        per_cta[k].push_back(u);
+    }
+    std::vector<BUnit> units_cta;  // in CTA order
+    std::vector<uint32_t> cta_units(n_ctas + 1, 0);
+    for (uint32_t k = 0; k < n_ctas; ++k) {
+        cta_units[k] = static_cast<uint32_t>(units_cta.size());
+        for (uint32_t u : per_cta[k]) units_cta.push_back(units[u]);
+    }
+    cta_units[n_ctas] = static_cast<uint32_t>(units_cta.size());
+
+    // Stimulus: one CSR over all instances, events of a step sorted by neuron.
+    uint32_t stim_len = 0;
+    for (const auto& I : b->insts) stim_len = std::max<uint32_t>(stim_len, static_cast<uint32_t>(I.counts.size()));
+    std::vector<std::vector<std::pair<uint32_t, float>>> per_step(stim_len);
+    for (uint32_t i = 0; i < h.n_inst; ++i) {
+        const auto& I = b->insts[i];
+        size_t e = 0;
+        for (uint32_t t = 0; t < I.counts.size(); ++t)
+            for (uint32_t k = 0; k < I.counts[t]; ++k, ++e) per_step[t].emplace_back(b->nbase[i] + I.neurons[e], I.deltas[e]);
+    }
+    std::vector<uint32_t> stim_off(stim_len + 1, 0), ev_neuron;
+    std::vector<float> ev_delta;
+    for (uint32_t t = 0; t < stim_len; ++t) {
+        std::stable_sort(per_step[t].begin(), per_step[t].end(),
+                         [](const auto& a, const auto& c) { return a.first < c.first; });
+        for (const auto& ev : per_step[t]) {
+            ev_neuron.push_back(ev.first);
+            ev_delta.push_back(ev.second);
+        }
+        stim_off[t + 1] = static_cast<uint32_t>(ev_neuron.size());
+    }
+
+    // Arena.
+    Arena A;
+    const size_t fN = sizeof(float) * n_neurons;
+    size_t o_state[10];
+    for (auto& o : o_state) o = A.take(fN);
+    const size_t o_ref = A.take(sizeof(uint32_t) * n_neurons), o_spk = A.take(sizeof(uint32_t) * n_neurons);
+    const size_t o_cnt = A.take(sizeof(unsigned long long) * 2 * h.n_inst);
+    const size_t o_ninst = A.take(sizeof(uint32_t) * n_neurons);
+    const size_t o_inst = A.take(sizeof(BInst) * h.n_inst);
+    const size_t o_units = A.take(sizeof(BUnit) * units_cta.size());
+    const size_t o_cta = A.take(sizeof(uint32_t) * cta_units.size());
+    const size_t o_part = A.take(sizeof(float) * std::max<size_t>(part_floats, 1));
+    size_t o_a[kBatchMaxClasses][2], o_x[kBatchMaxClasses][2];
+    for (uint32_t c = 0; c < h.n_classes; ++c)
+        for (int sd = 0; sd < 2; ++sd) {
+            const BClass& C = h.cls[c];
+            o_a[c][sd] = A.take(static_cast<size_t>(C.MT) * C.KT[sd] * kATileBytes);
+            o_x[c][sd] = A.take(static_cast<size_t>(C.KT[sd]) * 2u * C.NP * 64u * 2u);
+        }
+    const size_t o_soff = A.take(sizeof(uint32_t) * stim_off.size());
+    const size_t o_evn = A.take(sizeof(uint32_t) * std::max<size_t>(ev_neuron.size(), 1));
+    const size_t o_evd = A.take(sizeof(float) * std::max<size_t>(ev_delta.size(), 1));
+    const size_t o_bar = A.take(sizeof(unsigned long long)), o_err = A.take(sizeof(int32_t));
+    const size_t o_sd = A.take(sizeof(unsigned long long));
+    uint32_t max_n = 0;
+    for (const auto& HC : b->classes) max_n = std::max(max_n, HC.E + HC.I);
+    const size_t o_scr = A.take(sizeof(float) * 2 * max_n);
+    const size_t o_sim = A.take(sizeof(BSim));
+    cuda_check(cudaMalloc(&b->arena, A.size), "cudaMalloc batch arena");
+    b->arena_bytes = A.size;
+    unsigned char* base = b->arena;
+    cuda_check(cudaMemset(base, 0, A.size), "cudaMemset batch arena");
+    auto F = [&](size_t o) { return reinterpret_cast<float*>(base + o); };
+    float** fields[10] = {&h.v, &h.ge, &h.gi, &h.istim, &h.er, &h.ed, &h.ir, &h.id, &h.tr, &h.td};
+    for (int k = 0; k < 10; ++k) *fields[k] = F(o_state[k]);
+    h.refrac = reinterpret_cast<uint32_t*>(base + o_ref);
+    h.spikes = reinterpret_cast<uint32_t*>(base + o_spk);
+    h.spike_counts = reinterpret_cast<unsigned long long*>(base + o_cnt);
+    h.partials = F(o_part);
+    h.barrier = reinterpret_cast<unsigned long long*>(base + o_bar);
+    h.error = reinterpret_cast<int32_t*>(base + o_err);
+    h.steps_done = reinterpret_cast<unsigned long long*>(base + o_sd);
+    b->scratch = F(o_scr);
+
+    // neuron -> instance, instance table, initial voltages and refractory counters
+    std::vector<uint32_t> ninst(n_neurons);
+    std::vector<BInst> inst(h.n_inst);
+    std::vector<float> v0(n_neurons);
+    for (uint32_t i = 0; i < h.n_inst; ++i) {
+        const auto& I = b->insts[i];
+        const auto& HC = b->classes[I.cls];
+        BInst& BI = inst[i];
+        BI.cls = I.cls;
+        BI.row = row[i];
+        BI.nbase = b->nbase[i];
+        BI.seed = I.seed;
+        BI.g[0] = batch_group(I.g[0], 0);
+        BI.g[1] = batch_group(I.g[1], HC.E);
+        for (uint32_t j = 0; j < HC.E + HC.I; ++j) {
+            ninst[b->nbase[i] + j] = i;
+            v0[b->nbase[i] + j] = I.g[j < HC.E ? 0 : 1].v_rest;  // NeuronGroup::initialize_data
+        }
+    }
+    h.neuron_inst = reinterpret_cast<const uint32_t*>(base + o_ninst);
+    h.inst = reinterpret_cast<const BInst*>(base + o_inst);
+    h.units = reinterpret_cast<const BUnit*>(base + o_units);
+    h.cta_units = reinterpret_cast<const uint32_t*>(base + o_cta);
+    cuda_check(cudaMemcpy(base + o_ninst, ninst.data(), sizeof(uint32_t) * n_neurons, cudaMemcpyHostToDevice), "H2D");
+    cuda_check(cudaMemcpy(base + o_inst, inst.data(), sizeof(BInst) * inst.size(), cudaMemcpyHostToDevice), "H2D");
+    cuda_check(cudaMemcpy(h.v, v0.data(), fN, cudaMemcpyHostToDevice), "H2D v");
+    cuda_check(cudaMemcpy(base + o_units, units_cta.data(), sizeof(BUnit) * units_cta.size(), cudaMemcpyHostToDevice),
+               "H2D units");
+    cuda_check(cudaMemcpy(base + o_cta, cta_units.data(), sizeof(uint32_t) * cta_units.size(), cudaMemcpyHostToDevice),
+               "H2D unit ranges");
+    for (uint32_t c = 0; c < h.n_classes; ++c)
+        for (int sd = 0; sd < 2; ++sd) {
+            h.cls[c].A[sd] = reinterpret_cast<const uint16_t*>(base + o_a[c][sd]);
+            h.cls[c].X[sd] = reinterpret_cast<uint16_t*>(base + o_x[c][sd]);
+            const auto& tiles = b->classes[c].A[sd];
+            cuda_check(cudaMemcpy(base + o_a[c][sd], tiles.data(), sizeof(uint16_t) * tiles.size(), cudaMemcpyHostToDevice),
+                       "H2D weight tiles");
+        }
+    h.stim_len = stim_len;
+    h.stim_off = reinterpret_cast<const uint32_t*>(base + o_soff);
+    h.ev_neuron = reinterpret_cast<const uint32_t*>(base + o_evn);
+    h.ev_delta = reinterpret_cast<const float*>(base + o_evd);
+    cuda_check(cudaMemcpy(base + o_soff, stim_off.data(), sizeof(uint32_t) * stim_off.size(), cudaMemcpyHostToDevice), "H2D");
+    if (!ev_neuron.empty()) {
+        cuda_check(cudaMemcpy(base + o_evn, ev_neuron.data(), sizeof(uint32_t) * ev_neuron.size(), cudaMemcpyHostToDevice), "H2D");
+        cuda_check(cudaMemcpy(base + o_evd, ev_delta.data(), sizeof(float) * ev_delta.size(), cudaMemcpyHostToDevice), "H2D");
+    }
+    b->d_sim = reinterpret_cast<BSim*>(base + o_sim);
+    cuda_check(cudaMemcpy(b->d_sim, &h, sizeof(BSim), cudaMemcpyHostToDevice), "H2D batch sim");
+    b->grid = n_ctas;
+    b->smem = kBatchStages * (kATileBytes + 2u * 128u * 64u * 2u);
+    cuda_check(cudaFuncSetAttribute(reinterpret_cast<const void*>(&bsnn_batch_kernel),
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(b->smem)),
+               "batch smem");
+    int per_sm = 0;
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, reinterpret_cast<const void*>(&bsnn_batch_kernel),
+                                                             kBatchThreads, b->smem),
+               "batch occupancy");
+    require(per_sm >= 1, BSNN_ERR_RUNTIME, "batch kernel does not fit on an SM");
+    b->finalized = true;
+}
+
+}  // namespace
+
+namespace {
+
+void batch_check_error(bsnn_batch* b) {
+    cuda_check(cudaStreamSynchronize(b->stream), "batch stream synchronize");
+    int32_t e = 0;
+    cuda_check(cudaMemcpy(&e, b->h.error, sizeof(e), cudaMemcpyDeviceToHost), "D2H batch error flag");
+    if (e != kErrNone) {
+        b->failed = true;
+        throw ApiError(BSNN_ERR_DEVICE_TIMEOUT, "batch kernel: a device-side wait timed out; the batch state is invalid");
+    }
+}
+
+void batch_launch(bsnn_batch* b, uint32_t n_steps) {
+    auto it = b->graphs.find(n_steps);
+    if (it == b->graphs.end()) {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        cuda_check(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "batch capture");
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(b->grid);
+        cfg.blockDim = dim3(kBatchThreads);
+        cfg.dynamicSmemBytes = b->smem;
+        cfg.stream = b->stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        const BSim* arg0 = b->d_sim;
+        void* args[2] = {&arg0, &n_steps};
+        const cudaError_t le = cudaLaunchKernelExC(&cfg, reinterpret_cast<const void*>(&bsnn_batch_kernel), args);
+        const cudaError_t ce = cudaStreamEndCapture(b->stream, &graph);
+        cuda_check(le, "batch launch (capture)");
+        cuda_check(ce, "batch end capture");
+        cuda_check(cudaGraphInstantiate(&exec, graph, 0), "batch graph instantiate");
+        cudaGraphDestroy(graph);
+        it = b->graphs.emplace(n_steps, exec).first;
+    }
+    cuda_check(cudaGraphLaunch(it->second, b->stream), "batch graph launch");
+    ++b->launches;
+}
+
+}  // namespace
+
+extern "C" {
+
+BSNN_API bsnn_status bsnn_batch_create(int32_t device, bsnn_batch** out) {
+    if (!out) return BSNN_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    return guarded_batch(nullptr, [&] {
+        int n = 0;
+        cuda_check(cudaGetDeviceCount(&n), "cudaGetDeviceCount");
+        require(device >= 0 && device < n, BSNN_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+        cuda_check(cudaSetDevice(device), "cudaSetDevice");
+        auto b = std::make_unique<bsnn_batch>();
+        b->device = device;
+        cuda_check(cudaDeviceGetAttribute(&b->sm_count, cudaDevAttrMultiProcessorCount, device), "SM count");
+        int major = 0;
+        cuda_check(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device), "compute capability");
+        require(major == 10, BSNN_ERR_RUNTIME, "the batched form needs an sm_100 GPU (tcgen05 tensor cores)");
+        cuda_check(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        *out = b.release();
+    });
+}
+
+BSNN_API bsnn_status bsnn_batch_destroy(bsnn_batch* b) {
+    if (!b) return BSNN_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    delete b;
+    return BSNN_OK;
+}
+
+BSNN_API const char* bsnn_batch_last_error(const bsnn_batch* b) { return b ? b->err.c_str() : g_thread_error.c_str(); }
+
+BSNN_API bsnn_status bsnn_batch_add_class(bsnn_batch* b, uint32_t num_e, uint32_t num_i, const float* w_ee,
+                                          const float* w_ei, const float* w_ie, const float* w_ii,
+                                          const bsnn_connection_params* excitatory_pre,
+                                          const bsnn_connection_params* inhibitory_pre, uint32_t* out_class) {
+    if (!b) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded_batch(b, [&] {
+        require(!b->finalized, BSNN_ERR_STATE, "classes cannot be added after the batch has started");
+        require(b->classes.size() < kBatchMaxClasses, BSNN_ERR_INVALID_ARGUMENT, "too many size classes");
+        require(num_e > 0 && num_i > 0, BSNN_ERR_INVALID_ARGUMENT, "a class needs excitatory and inhibitory neurons");
+        require(w_ee && w_ei && w_ie && w_ii && excitatory_pre && inhibitory_pre, BSNN_ERR_INVALID_ARGUMENT, "null argument");
+        bsnn_batch::HClass C;
+        C.E = num_e;
+        C.I = num_i;
+        const uint32_t N = num_e + num_i, MT = (N + 127) / 128;
+        const bsnn_connection_params* cp[2] = {excitatory_pre, inhibitory_pre};
+        for (int sd = 0; sd < 2; ++sd) {
+            const uint32_t K = sd == 0 ? num_e : num_i, KT = (K + 63) / 64;
+            // W_side[pre][post] = [W_x->E | W_x->I]; A = W_side^T, tiled (mt, kt), core-matrix layout
+            const float* wl = sd == 0 ? w_ee : w_ie;  // posts 0 .. E-1
+            const float* wr = sd == 0 ? w_ei : w_ii;  // posts E .. N-1
+            std::vector<uint16_t>& A = C.A[sd];
+            A.assign(static_cast<size_t>(MT) * KT * 128u * 64u, 0);
+            for (uint32_t pre = 0; pre < K; ++pre)
+                for (uint32_t post = 0; post < N; ++post) {
+                    const float w = post < num_e ? wl[static_cast<size_t>(pre) * num_e + post]
+                                                 : wr[static_cast<size_t>(pre) * num_i + (post - num_e)];
+                    require(!(w < 0.0f), BSNN_ERR_INVALID_ARGUMENT, "weights must be non-negative");
+                    const size_t tile = static_cast<size_t>(post >> 7) * KT + (pre >> 6);
+                    A[tile * 128u * 64u + core_offset(128u, post & 127u, pre & 63u)] = host_bf16(w);
+                }
+            C.r_decay[sd] = std::exp(-1.0f * cp[sd]->timestep / cp[sd]->rise_time);
+            C.d_decay[sd] = std::exp(-1.0f * cp[sd]->timestep / cp[sd]->decay_time);
+            C.norm[sd] = cp[sd]->postsynaptic_kernel_normalization_value;
+        }
+        b->classes.push_back(std::move(C));
+        if (out_class) *out_class = static_cast<uint32_t>(b->classes.size() - 1);
+    });
+}
+
+BSNN_API bsnn_status bsnn_batch_add_instance(bsnn_batch* b, uint32_t class_index, const bsnn_neuron_group_params* e_group,
+                                             const bsnn_neuron_group_params* i_group, int32_t rng_seed,
+                                             const uint32_t* stim_counts, uint32_t stim_steps, const uint32_t* stim_neurons,
+                                             const float* stim_deltas, uint32_t num_events, uint32_t* out_instance) {
+    if (!b) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded_batch(b, [&] {
+        require(!b->finalized, BSNN_ERR_STATE, "instances cannot be added after the batch has started");
+        require(class_index < b->classes.size(), BSNN_ERR_OUT_OF_RANGE, "class index out of range");
+        require(e_group && i_group, BSNN_ERR_INVALID_ARGUMENT, "null group parameters");
+        auto& HC = b->classes[class_index];
+        require(e_group->num_neurons == HC.E && i_group->num_neurons == HC.I, BSNN_ERR_INVALID_ARGUMENT,
+                "group sizes must match the class");
+        require((stim_counts || stim_steps == 0) && ((stim_neurons && stim_deltas) || num_events == 0),
+                BSNN_ERR_INVALID_ARGUMENT, "null stimulus arrays");
+        bsnn_batch::HInst I;
+        I.cls = class_index;
+        I.g[0] = *e_group;
+        I.g[1] = *i_group;
+        I.seed = static_cast<uint32_t>(rng_seed);
+        I.counts.assign(stim_counts, stim_counts + stim_steps);
+        uint64_t total = 0;
+        for (uint32_t c : I.counts) total += c;
+        require(total == num_events, BSNN_ERR_INVALID_ARGUMENT, "stimulus counts must add up to num_events");
+        I.neurons.assign(stim_neurons, stim_neurons + num_events);
+        I.deltas.assign(stim_deltas, stim_deltas + num_events);
+        for (uint32_t nrn : I.neurons) require(nrn < HC.E + HC.I, BSNN_ERR_OUT_OF_RANGE, "stimulus neuron out of range");
+        b->insts.push_back(std::move(I));
+        const uint32_t id = static_cast<uint32_t>(b->insts.size() - 1);
+        HC.instances.push_back(id);
+        if (out_instance) *out_instance = id;
+    });
+}
+
+BSNN_API bsnn_status bsnn_batch_set_noise(bsnn_batch* b, int32_t on) {
+    if (!b) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded_batch(b, [&] {
+        require(!b->finalized, BSNN_ERR_STATE, "set the noise before the first step");
+        b->noise_on = on != 0;
+    });
+}
+
+BSNN_API bsnn_status bsnn_batch_set_steps_per_launch(bsnn_batch* b, uint32_t steps) {
+    if (!b) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded_batch(b, [&] {
+        require(steps > 0, BSNN_ERR_INVALID_ARGUMENT, "steps per launch must be > 0");
+        b->steps_per_launch = steps;
+    });
+}
+
+BSNN_API bsnn_status bsnn_batch_run(bsnn_batch* b, uint32_t num_steps) {
+    if (!b) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded_batch(b, [&] {
+        batch_finalize(b);
+        require(!b->failed, BSNN_ERR_STATE, "the batch failed earlier (device timeout)");
+        uint32_t left = num_steps;
+        while (left > 0) {
+            const uint32_t n = std::min(left, b->steps_per_launch);
+            batch_launch(b, n);
+            left -= n;
+        }
+        b->steps_done += num_steps;
+    });
+}
+
+BSNN_API bsnn_status bsnn_batch_synchronize(bsnn_batch* b) {
+    if (!b) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded_batch(b, [&] {
+        if (b->finalized) batch_check_error(b);
+    });
+}
+
+BSNN_API bsnn_status bsnn_batch_get_stream(const bsnn_batch* b, void** out) {
+    if (!b || !out) return BSNN_ERR_INVALID_ARGUMENT;
+    *out = b->stream;
+    return BSNN_OK;
+}
+
+// Fields as in bsnn_read_state: membrane potentials, g (with the pending propagation), I_stim,
+// refractory counters, spikes, background conductances and traces, and the neuron's connection
+// traces r, d and x = d - r.  `host_out` holds the instance's E + I neurons.
+BSNN_API bsnn_status bsnn_batch_read_state(bsnn_batch* b, uint32_t instance, int32_t field, void* host_out) {
+    if (!b) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded_batch(b, [&] {
+        batch_finalize(b);
+        batch_check_error(b);
+        require(instance < b->insts.size(), BSNN_ERR_OUT_OF_RANGE, "instance index out of range");
+        require(host_out != nullptr, BSNN_ERR_INVALID_ARGUMENT, "null output");
+        const auto& HC = b->classes[b->insts[instance].cls];
+        const uint32_t n = HC.E + HC.I;
+        const size_t off = b->nbase[instance];
+        const BSim& h = b->h;
+        auto copy = [&](const void* src) {
+            cuda_check(cudaMemcpy(host_out, static_cast<const char*>(src) + 4 * off, 4ull * n, cudaMemcpyDeviceToHost), "D2H");
+        };
+        switch (field) {
+            case BSNN_FIELD_MEMBRANE_POTENTIALS: copy(h.v); return;
+            case BSNN_FIELD_I_STIMULUS: copy(h.istim); return;
+            case BSNN_FIELD_REFRACTORY_COUNTER: copy(h.refrac); return;
+            case BSNN_FIELD_SPIKES: copy(h.spikes); return;
+            case BSNN_FIELD_BG_G_EXCITATORY: copy(h.ge); return;
+            case BSNN_FIELD_BG_G_INHIBITORY: copy(h.gi); return;
+            case BSNN_FIELD_BG_E_R_TRACES: copy(h.er); return;
+            case BSNN_FIELD_BG_E_D_TRACES: copy(h.ed); return;
+            case BSNN_FIELD_BG_I_R_TRACES: copy(h.ir); return;
+            case BSNN_FIELD_BG_I_D_TRACES: copy(h.id); return;
+            case BSNN_FIELD_CONN_R_TRACES: copy(h.tr); return;
+            case BSNN_FIELD_CONN_D_TRACES: copy(h.td); return;
+            case BSNN_FIELD_CONN_SUMMED: {
+                std::vector<float> r(n), d(n);
+                cuda_check(cudaMemcpy(r.data(), h.tr + off, 4ull * n, cudaMemcpyDeviceToHost), "D2H");
+                cuda_check(cudaMemcpy(d.data(), h.td + off, 4ull * n, cudaMemcpyDeviceToHost), "D2H");
+                float* o = static_cast<float*>(host_out);
+                for (uint32_t k = 0; k < n; ++k) o[k] = d[k] - r[k];
+                return;
+            }
+            case BSNN_FIELD_G_EXCITATORY:
+            case BSNN_FIELD_G_INHIBITORY: {
+                bsnn_batch_gsum_kernel<<<(n + 255) / 256, 256, 0, b->stream>>>(b->d_sim, instance, b->scratch,
+                                                                               b->scratch + n);
+                cuda_check(cudaGetLastError(), "batch g read");
+                cuda_check(cudaMemcpyAsync(host_out, b->scratch + (field == BSNN_FIELD_G_EXCITATORY ? 0 : n), 4ull * n,
+                                           cudaMemcpyDeviceToHost, b->stream),
+                           "D2H g");
+                cuda_check(cudaStreamSynchronize(b->stream), "sync");
+                return;
+            }
+            default: throw ApiError(BSNN_ERR_INVALID_ARGUMENT, "unknown field " + std::to_string(field));
+        }
+    });
+}
+
+// Spike counts since creation, [instance][0 = E, 1 = I].
+BSNN_API bsnn_status bsnn_batch_read_spike_counts(bsnn_batch* b, uint64_t* host_out) {
+    if (!b || !host_out) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded_batch(b, [&] {
+        batch_finalize(b);
+        batch_check_error(b);
+        cuda_check(cudaMemcpy(host_out, b->h.spike_counts, sizeof(uint64_t) * 2 * b->insts.size(), cudaMemcpyDeviceToHost),
+                   "D2H spike counts");
+    });
+}
+
+BSNN_API bsnn_status bsnn_batch_get_info(bsnn_batch* b, bsnn_batch_info* out) {
+    if (!b || !out) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded_batch(b, [&] {
+        batch_finalize(b);
+        bsnn_batch_info i{};
+        i.num_classes = b->h.n_classes;
+        i.num_instances = b->h.n_inst;
+        i.num_neurons = b->h.n_neurons;
+        i.num_units = b->h.n_units;
+        i.grid_ctas = b->grid;
+        i.block_threads = kBatchThreads;
+        i.steps_done = b->steps_done;
+        i.device_bytes = b->arena_bytes;
+        uint64_t wb = 0;
+        for (const auto& C : b->classes) wb += 2ull * (C.A[0].size() + C.A[1].size());
+        i.weight_bytes = wb;
+        i.kernel_launches = b->launches;
+        i.smem_bytes = b->smem;
+        *out = i;
+    });
+}
+
+}  // extern "C"

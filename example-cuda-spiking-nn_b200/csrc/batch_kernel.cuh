@@ -1,0 +1,448 @@
+// batch_kernel.cuh -- the batched form: many independent networks ("instances") of uneven size,
+// without plasticity, stepped together by one persistent cooperative kernel.
+//
+// Instances of one size class share one weight set, stored once in BF16, so the class's
+// propagation for all its instances is a GEMM: for the excitatory presynaptic side
+//     G_E[post, instance] = sum_pre W_E[pre, post] x_E[instance, pre]
+// with W_E = [W_EE | W_EI] (E posts, then I posts), and likewise for the inhibitory side with
+// W_I = [W_IE | W_II].  It runs on the 5th-generation tensor cores: D[128 posts x N] in tensor
+// memory += A[128 posts x 64 pre] (W^T tile) * B[64 pre x N] (x tile), kind::f16 with BF16
+// operands and FP32 accumulation.  x is split into a BF16 high part and a BF16 low part
+// (x = hi + lo to about 2^-17), the two parts being the first and second halves of B's N
+// columns, so the GEMM keeps x at nearly FP32 precision; the epilogue adds the two halves.
+//
+// Per clock step:
+//   phase A (all neurons of all instances, grid-strided threads): g = g_base + the previous
+//     step's GEMM partial sums (fixed order over K chunks), background Poisson shot noise
+//     (the same counter-based Philox draw as the single-network kernel, keyed by the instance's
+//     seed and the neuron's index in its instance), the conductance-EIF Euler step, the stimulus
+//     events of the step, the connection traces, and x = d - r written as BF16 hi / lo into the
+//     B operand tiles; spike counts per instance and group.
+//   grid barrier
+//   phase B (work units, a fixed list per CTA): one unit = (class, presynaptic side, 128-post
+//     tile, a chunk of 64-pre K tiles).  One thread streams the unit's A and B tiles into a ring
+//     of shared-memory stages by bulk asynchronous copies (one copy per operand tile; the
+//     operands are stored pre-tiled in the canonical no-swizzle K-major core-matrix layout)
+//     and issues the MMAs; tcgen05.commit releases each stage and finally signals the
+//     accumulator; four warps read the 128 x N accumulator from tensor memory and write the
+//     unit's partial sums.
+//   grid barrier
+//
+// Every wait is bounded (2 s): a timeout sets the error word and the kernel stops stepping,
+// still releasing its tensor memory.
+#pragma once
+
+#include "step_kernel.cuh"
+
+namespace bsnn {
+
+constexpr uint32_t kBatchMaxClasses = 8;
+constexpr uint32_t kBatchStages = 4;        // shared-memory ring of operand stages
+constexpr uint32_t kBatchTmemCols = 256;    // accumulator columns (N <= 256)
+constexpr uint32_t kBatchThreads = 384;
+constexpr uint32_t kATileBytes = 128u * 64u * 2u;  // one 128 x 64 BF16 A tile
+
+// A size class: instances with the same numbers of neurons share its weights.
+struct BClass {
+    uint32_t E, I, N;        // neurons per instance (N = E + I)
+    uint32_t n_inst, NP;     // instances; NP = n_inst rounded up to 8 (B has 2 NP rows: hi, lo)
+    uint32_t inst0;          // first instance id of the class
+    uint32_t MT;             // 128-post tiles
+    uint32_t KT[2];          // 64-pre K tiles of the E and I sides
+    uint32_t nkc[2];         // K chunks per post tile (one unit each)
+    size_t pbase[2];         // float offset of the partial sums of (side, post tile 0, chunk 0);
+                             // unit (mt, kc) of a side holds NP x 128 floats at
+                             // pbase + (mt * nkc + kc) * NP * 128
+    const uint16_t* A[2];    // [MT][KT] tiles of W^T (BF16 bits), core-matrix layout
+    uint16_t* X[2];          // [KT] tiles of x (2 NP rows), core-matrix layout
+    float r_decay[2], d_decay[2], norm[2];  // connection traces of the E- and I-side connections
+};
+
+// One instance: its class, its row in the class's B operand, its neurons, seed and groups.
+struct BInst {
+    uint32_t cls, row, nbase, seed;
+    DGroup g[2];  // E, I (off / n are instance-local)
+};
+
+struct BUnit {
+    uint32_t cls, side, mt, k0, k1;
+    size_t part;  // float offset of the unit's partial sums [NP][128]
+};
+
+struct BSim {
+    uint32_t n_classes, n_inst, n_neurons, n_units;
+    BClass cls[kBatchMaxClasses];
+    const BInst* inst;
+    const uint32_t* neuron_inst;  // [n_neurons] instance of each neuron
+    const BUnit* units;           // in CTA order
+    const uint32_t* cta_units;    // [n_ctas + 1] unit ranges per CTA
+    float* partials;
+    // neuron state [n_neurons]
+    float *v, *ge, *gi, *istim, *er, *ed, *ir, *id, *tr, *td;
+    uint32_t* refrac;
+    uint32_t* spikes;
+    unsigned long long* spike_counts;  // [n_inst][2]
+    // stimulus: events of step t are ev_*[stim_off[t] .. stim_off[t+1]), sorted by neuron
+    uint32_t stim_len;
+    const uint32_t* stim_off;
+    const uint32_t* ev_neuron;
+    const float* ev_delta;
+    int32_t noise_on;
+    unsigned long long* barrier;
+    int32_t* error;
+    unsigned long long* steps_done;
+};
+
+// ---- tcgen05 / tensor-memory wrappers ---------------------------------------------------------
+__device__ __forceinline__ void tmem_alloc(uint32_t dst_smem, uint32_t cols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst_smem), "r"(cols) : "memory");
+}
+__device__ __forceinline__ void tmem_relinquish() {
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t cols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(cols) : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+// D[tmem] (+)= A[smem] * B[smem], BF16 x BF16 -> FP32, M = 128.
+__device__ __forceinline__ void tc_mma_bf16(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                            uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+// 16 consecutive 32-bit accumulator columns of this thread's lane.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* out) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int k = 0; k < 16; ++k) out[k] = __uint_as_float(r[k]);
+}
+__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+
+// Shared-memory matrix descriptor, canonical K-major layout without swizzle: 8-row x 16-byte
+// core matrices; `lbo` = bytes between the two core matrices of one K=16 step, `sbo` = bytes
+// between consecutive 8-row groups; descriptor version 1 (bits 46-47).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return static_cast<uint64_t>((addr >> 4) & 0x3FFFu) | (static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16) |
+           (static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+// Instruction descriptor: FP32 accumulator, BF16 A and B, both K-major, M = 128, N = n.
+__device__ __forceinline__ uint32_t idesc_bf16_m128(uint32_t n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((128u >> 4) << 24);
+}
+// Element offset of (row, k) in a [rows x 64] operand tile in core-matrix layout.
+__host__ __device__ __forceinline__ uint32_t core_offset(uint32_t rows, uint32_t row, uint32_t k) {
+    return ((((k >> 3) * (rows >> 3) + (row >> 3)) << 3) + (row & 7u)) * 8u + (k & 7u);
+}
+
+__device__ __forceinline__ uint16_t bf16_bits_rn(float v) { return __bfloat16_as_ushort(__float2bfloat16_rn(v)); }
+
+// ---- phase A ------------------------------------------------------------------------------------
+__device__ __forceinline__ void batch_neurons(const BSim* S, unsigned long long t) {
+    const uint32_t total = gridDim.x * blockDim.x;
+    for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < S->n_neurons; n += total) {
+        const BInst& B = S->inst[__ldg(S->neuron_inst + n)];
+        const BClass& C = S->cls[B.cls];
+        const uint32_t j = n - B.nbase;  // index in the instance
+        const uint32_t side = j < C.E ? 0u : 1u;
+        const DGroup& G = B.g[side];
+        const uint32_t loc = j - (side ? C.E : 0u);
+
+        float ge_used = __ldcg(S->ge + n), gi_used = __ldcg(S->gi + n);
+        if (t > 0) {  // the previous step's propagation, K chunks in order
+            const uint32_t mt = j >> 7, row = j & 127u;
+            for (uint32_t sd = 0; sd < 2; ++sd) {
+                float dot = 0.0f;
+                const float* p = S->partials + C.pbase[sd] + static_cast<size_t>(mt) * C.nkc[sd] * C.NP * 128u +
+                                 static_cast<size_t>(B.row) * 128u + row;
+                for (uint32_t kc = 0; kc < C.nkc[sd]; ++kc) dot += __ldcg(p + static_cast<size_t>(kc) * C.NP * 128u);
+                if (sd == 0) ge_used = ge_used + dot;
+                else gi_used = gi_used + dot;
+            }
+        }
+        float er = flush_tiny(__ldcg(S->er + n) * G.bg_er_decay);
+        float ir = flush_tiny(__ldcg(S->ir + n) * G.bg_ir_decay);
+        float ed = flush_tiny(__ldcg(S->ed + n) * G.bg_ed_decay);
+        float id = flush_tiny(__ldcg(S->id + n) * G.bg_id_decay);
+        uint32_t ne = 0, ni = 0;
+        if (S->noise_on) {
+            if (G.has_bg_e) ne = poisson_knuth(G.exp_neg_mean_e, B.seed, j, t, 0u);
+            if (G.has_bg_i) ni = poisson_knuth(G.exp_neg_mean_i, B.seed, j, t, 1u);
+        }
+        if (ne > 0u) {
+            const float inc = static_cast<float>(ne);
+            er += inc;
+            ed += inc;
+        }
+        const float bg_ge = (ed - er) * G.bg_scale_e;
+        if (ni > 0u) {
+            const float inc = static_cast<float>(ni);
+            ir += inc;
+            id += inc;
+        }
+        const float bg_gi = (id - ir) * G.bg_scale_i;
+
+        float v = __ldcg(S->v + n);
+        float istim = __ldcg(S->istim + n);
+        uint32_t refrac = __ldcg(S->refrac + n), spike = 0;
+        if (refrac > 0) {
+            --refrac;
+            v = G.v_reset;
+        } else {
+            const float linear_leak_term = -1.0f * G.g_leak * (v - G.v_rest);
+            const float exponential_depolarization_term = G.g_leak * G.delta_t * expf((v - G.v_eff) / G.delta_t);
+            const float excitatory_synaptic_term = -1.0f * ge_used * (v - G.e_exc);
+            const float inhibitory_synaptic_term = -1.0f * gi_used * (v - G.e_inh);
+            const float dv = (G.timestep / G.cap) * (linear_leak_term + exponential_depolarization_term +
+                                                     excitatory_synaptic_term + inhibitory_synaptic_term + istim);
+            const float v_next = v + dv;
+            if (v_next >= G.v_th) {
+                refrac = G.refractory_steps;
+                spike = 1;
+                v = G.v_th;
+            } else {
+                v = v_next;
+            }
+        }
+        S->er[n] = er;
+        S->ed[n] = ed;
+        S->ir[n] = ir;
+        S->id[n] = id;
+        S->v[n] = v;
+        S->refrac[n] = refrac;
+        S->ge[n] = bg_ge;  // reset for the next propagation
+        S->gi[n] = bg_gi;
+        S->spikes[n] = spike;
+        if (spike) atomicAdd(S->spike_counts + 2u * (S->neuron_inst[n]) + side, 1ull);
+
+        // stimulus events of this step act from the next step
+        if (t < S->stim_len) {
+            uint32_t lo = __ldg(S->stim_off + t), hi = __ldg(S->stim_off + t + 1);
+            const uint32_t end = hi;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (__ldg(S->ev_neuron + mid) < n) lo = mid + 1;
+                else hi = mid;
+            }
+            bool any = false;
+            for (uint32_t k = lo; k < end && __ldg(S->ev_neuron + k) == n; ++k) {
+                istim = istim + __ldg(S->ev_delta + k);
+                any = true;
+            }
+            if (any) S->istim[n] = istim;
+        }
+
+        // connection traces of the neuron's presynaptic side, and x as BF16 hi / lo in B
+        float d = flush_tiny(__ldcg(S->td + n) * C.d_decay[side]);
+        float r = flush_tiny(__ldcg(S->tr + n) * C.r_decay[side]);
+        if (spike == 1) {
+            r += C.norm[side];
+            d += C.norm[side];
+        }
+        S->tr[n] = r;
+        S->td[n] = d;
+        const float x = d - r;
+        const uint16_t hi = bf16_bits_rn(x);
+        const float lo_f = x - __uint_as_float(static_cast<uint32_t>(hi) << 16);
+        const uint16_t lo = bf16_bits_rn(lo_f);
+        uint16_t* X = C.X[side] + static_cast<size_t>(loc >> 6) * (2u * C.NP * 64u);
+        X[core_offset(2u * C.NP, B.row, loc & 63u)] = hi;
+        X[core_offset(2u * C.NP, C.NP + B.row, loc & 63u)] = lo;
+    }
+}
+
+// ---- phase B ------------------------------------------------------------------------------------
+struct BatchSmem {
+    uint32_t tmem;          // tensor-memory base address
+    uint32_t ok;
+    uint64_t full[kBatchStages];
+    uint64_t empty[kBatchStages];
+    uint64_t accum;
+};
+
+__global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim* __restrict__ S, uint32_t n_steps) {
+    extern __shared__ __align__(1024) unsigned char bsm_raw[];
+    __shared__ BatchSmem bs;
+    __shared__ int s_ok;
+    __shared__ unsigned long long s_bar0, s_t0;
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+    // stage s: A tile at s * stage_bytes, B tile after it
+    const uint32_t max_b = 2u * 128u * 64u * 2u;  // B tile of N = 256 rows
+    const uint32_t stage_bytes = kATileBytes + max_b;
+    const uint32_t smem_base = saddr(bsm_raw);
+
+    if (tid == 0) {
+        bs.ok = 1u;
+        for (uint32_t s = 0; s < kBatchStages; ++s) {
+            mbar_init(saddr(&bs.full[s]), 1u);
+            mbar_init(saddr(&bs.empty[s]), 1u);
+        }
+        mbar_init(saddr(&bs.accum), 1u);
+        fence_mbar_init();
+        s_bar0 = ld_acquire_u64(S->barrier) / gridDim.x * gridDim.x;
+        s_t0 = *S->steps_done;
+    }
+    if (warp == 0) {
+        tmem_alloc(saddr(&bs.tmem), kBatchTmemCols);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = bs.tmem;
+    const unsigned long long bar0 = s_bar0, t0 = s_t0;
+    const uint32_t u_begin = S->cta_units[blockIdx.x], u_end = S->cta_units[blockIdx.x + 1];
+    // producer / MMA state (thread 0 only)
+    uint32_t full_ph = 0, empty_ph = 0, accum_ph = 0;
+    uint32_t empty_pend[kBatchStages] = {0, 0, 0, 0};
+    uint32_t g_load = 0, g_use = 0;
+    bool ok = true;
+
+    for (uint32_t k = 0; k < n_steps && ok; ++k) {
+        const unsigned long long t = t0 + k;
+        batch_neurons(S, t);
+        fence_proxy_async_global();
+        if (!grid_barrier(S->barrier, S->error, bar0 + (2ull * k + 1ull) * gridDim.x, &s_ok)) {
+            ok = false;
+            break;
+        }
+        if (tid == 0) fence_proxy_async_global();
+
+        for (uint32_t ui = u_begin; ui < u_end && ok; ++ui) {
+            const BUnit U = S->units[ui];
+            const BClass& C = S->cls[U.cls];
+            const uint32_t N = 2u * C.NP, b_bytes = N * 128u, nk = U.k1 - U.k0;
+            if (tid == 0) {
+                const unsigned char* a_src =
+                    reinterpret_cast<const unsigned char*>(C.A[U.side]) +
+                    (static_cast<size_t>(U.mt) * C.KT[U.side] + U.k0) * kATileBytes;
+                const unsigned char* b_src =
+                    reinterpret_cast<const unsigned char*>(C.X[U.side]) + static_cast<size_t>(U.k0) * b_bytes;
+                auto load = [&](uint32_t i) {  // K tile i of the unit into stage g_load % S
+                    const uint32_t s = g_load % kBatchStages;
+                    const uint32_t bar = saddr(&bs.full[s]);
+                    const uint32_t dst = smem_base + s * stage_bytes;
+                    mbar_expect_tx(bar, kATileBytes + b_bytes);
+                    bulk_load(dst, a_src + static_cast<size_t>(i) * kATileBytes, kATileBytes, bar);
+                    bulk_load(dst + kATileBytes, b_src + static_cast<size_t>(i) * b_bytes, b_bytes, bar);
+                    ++g_load;
+                };
+                const uint32_t idesc = idesc_bf16_m128(N);
+                uint32_t next = 0;
+                for (; next < nk && next < kBatchStages; ++next) load(next);
+                for (uint32_t i = 0; i < nk; ++i) {
+                    const uint32_t s = g_use % kBatchStages;
+                    if (!mbar_wait(saddr(&bs.full[s]), (full_ph >> s) & 1u)) {
+                        atomicExch(S->error, kErrStageTimeout);
+                        bs.ok = 0u;
+                        break;
+                    }
+                    full_ph ^= 1u << s;
+                    tc_fence_after();
+                    const uint32_t a = smem_base + s * stage_bytes, b = a + kATileBytes;
+#pragma unroll
+                    for (uint32_t ks = 0; ks < 4; ++ks)
+                        tc_mma_bf16(tmem, smem_desc(a + ks * 2u * 2048u, 2048u, 128u),
+                                    smem_desc(b + ks * 2u * (N * 16u), N * 16u, 128u), idesc, (i | ks) != 0u);
+                    tc_commit(saddr(&bs.empty[s]));
+                    ++empty_pend[s];
+                    ++g_use;
+                    // refill the stage the previous MMAs read, once they are done
+                    if (i > 0 && next < nk) {
+                        const uint32_t sp = (g_use - 2u) % kBatchStages;
+                        if (!mbar_wait(saddr(&bs.empty[sp]), (empty_ph >> sp) & 1u)) {
+                            atomicExch(S->error, kErrStageTimeout);
+                            bs.ok = 0u;
+                            break;
+                        }
+                        empty_ph ^= 1u << sp;
+                        --empty_pend[sp];
+                        load(next++);
+                    }
+                }
+                tc_commit(saddr(&bs.accum));
+                // the stage releases not yet waited for (at most one per stage) complete too
+                for (uint32_t s = 0; s < kBatchStages; ++s) {
+                    if (empty_pend[s] == 0u) continue;
+                    if (!mbar_wait(saddr(&bs.empty[s]), (empty_ph >> s) & 1u)) {
+                        atomicExch(S->error, kErrStageTimeout);
+                        bs.ok = 0u;
+                    }
+                    empty_ph ^= 1u << s;
+                    empty_pend[s] = 0;
+                }
+            }
+            // the accumulator is complete once every MMA of the unit has finished
+            if (!mbar_wait(saddr(&bs.accum), accum_ph & 1u)) {
+                atomicExch(S->error, kErrStageTimeout);
+                bs.ok = 0u;
+            }
+            accum_ph ^= 1u;
+            __syncthreads();
+            ok = bs.ok != 0u;  // the same for every thread of the CTA
+            tc_fence_after();
+            if (warp < 4 && ok) {
+                const uint32_t row = 32u * warp + lane;
+                float* part = S->partials + U.part;
+                for (uint32_t c0 = 0; c0 < C.NP; c0 += 16u) {
+                    float hi[16], lo[16];
+                    tmem_ld16(tmem + ((32u * warp) << 16) + c0, hi);
+                    tmem_ld16(tmem + ((32u * warp) << 16) + C.NP + c0, lo);
+#pragma unroll
+                    for (uint32_t q = 0; q < 16; ++q)
+                        if (c0 + q < C.n_inst) part[static_cast<size_t>(c0 + q) * 128u + row] = hi[q] + lo[q];
+                }
+            }
+            tc_fence_before();
+            __syncthreads();
+            tc_fence_after();
+        }
+        if (!ok) break;
+        if (!grid_barrier(S->barrier, S->error, bar0 + (2ull * k + 2ull) * gridDim.x, &s_ok)) {
+            ok = false;
+            break;
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, kBatchTmemCols);
+    if (blockIdx.x == 0 && tid == 0 && ok) *S->steps_done = t0 + n_steps;
+}
+
+// g of one instance's neurons including the propagation still pending in the partial sums (the
+// value the reference holds after step_the_clock): reads only.
+__global__ void bsnn_batch_gsum_kernel(const BSim* __restrict__ S, uint32_t instance, float* out_ge, float* out_gi) {
+    const BInst& B = S->inst[instance];
+    const BClass& C = S->cls[B.cls];
+    const bool pending = *S->steps_done > 0;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < C.N; j += gridDim.x * blockDim.x) {
+        const uint32_t n = B.nbase + j, mt = j >> 7, row = j & 127u;
+        float g[2] = {S->ge[n], S->gi[n]};
+        if (pending)
+            for (uint32_t sd = 0; sd < 2; ++sd) {
+                const float* p = S->partials + C.pbase[sd] + static_cast<size_t>(mt) * C.nkc[sd] * C.NP * 128u +
+                                 static_cast<size_t>(B.row) * 128u + row;
+                float dot = 0.0f;
+                for (uint32_t kc = 0; kc < C.nkc[sd]; ++kc) dot += p[static_cast<size_t>(kc) * C.NP * 128u];
+                g[sd] = g[sd] + dot;
+            }
+        out_ge[j] = g[0];
+        out_gi[j] = g[1];
+    }
+}
+
+}  // namespace bsnn

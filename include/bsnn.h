@@ -369,6 +369,60 @@ BSNN_API bsnn_status bsnn_connection_propagate(const bsnn_connection_view* view,
  *    from different host threads) race and give wrong results.  Order them (one stream, or events). */
 BSNN_API bsnn_status bsnn_connection_propagate_noalloc(const bsnn_connection_view* view, void* stream);
 
+/* ---- the batched form (no reference counterpart) ---------------------------------------------
+ * Many independent networks ("instances") of uneven size, without plasticity, stepped together by
+ * one persistent launch.  Each instance is the reference's two-group network (E group, I group,
+ * connections E->E, E->I, I->E, I->I, one stimulus, background noise) with its own neuron-group
+ * parameters, seed and stimulus; instances of one size class share one weight set, stored once in
+ * BF16, so the class's propagation is a GEMM on the tensor cores (BF16 weights, traces split into
+ * BF16 high and low parts, FP32 accumulation).  Needs an sm_100 GPU. */
+typedef struct bsnn_batch bsnn_batch;
+
+typedef struct bsnn_batch_info {
+    uint32_t num_classes;
+    uint32_t num_instances;
+    uint32_t num_neurons;      /* over all instances                                      */
+    uint32_t num_units;        /* GEMM work units per step                                */
+    uint32_t grid_ctas;
+    uint32_t block_threads;
+    uint64_t steps_done;
+    uint64_t device_bytes;
+    uint64_t weight_bytes;     /* BF16 weight tiles, padding included                     */
+    uint64_t kernel_launches;
+    uint64_t smem_bytes;
+} bsnn_batch_info;
+
+BSNN_API bsnn_status bsnn_batch_create(int32_t device, bsnn_batch** out_batch);
+BSNN_API bsnn_status bsnn_batch_destroy(bsnn_batch* batch);
+BSNN_API const char* bsnn_batch_last_error(const bsnn_batch* batch);
+/* A size class: weight matrices row-major [pre][post] (non-negative FP32, stored as BF16) and the
+ * connection parameters of its excitatory-presynaptic (E->E, E->I) and inhibitory-presynaptic
+ * (I->E, I->I) connections.  At most 8 classes. */
+BSNN_API bsnn_status bsnn_batch_add_class(bsnn_batch* batch, uint32_t num_excitatory, uint32_t num_inhibitory,
+                                          const float* w_ee, const float* w_ei, const float* w_ie, const float* w_ii,
+                                          const bsnn_connection_params* excitatory_pre,
+                                          const bsnn_connection_params* inhibitory_pre, uint32_t* out_class);
+/* An instance of a class (at most 128 per class): its two groups' parameters (num_neurons must
+ * match the class; offset is ignored), its noise seed (rng_seed of the single-network form) and
+ * its stimulus as per-step event counts, each event an (instance-local neuron, amplitude change). */
+BSNN_API bsnn_status bsnn_batch_add_instance(bsnn_batch* batch, uint32_t class_index,
+                                             const bsnn_neuron_group_params* excitatory_group,
+                                             const bsnn_neuron_group_params* inhibitory_group, int32_t rng_seed,
+                                             const uint32_t* stimulus_counts, uint32_t stimulus_steps,
+                                             const uint32_t* stimulus_neurons, const float* stimulus_deltas,
+                                             uint32_t num_events, uint32_t* out_instance);
+BSNN_API bsnn_status bsnn_batch_set_noise(bsnn_batch* batch, int32_t on);
+BSNN_API bsnn_status bsnn_batch_set_steps_per_launch(bsnn_batch* batch, uint32_t steps);
+BSNN_API bsnn_status bsnn_batch_run(bsnn_batch* batch, uint32_t num_steps);
+BSNN_API bsnn_status bsnn_batch_synchronize(bsnn_batch* batch);
+BSNN_API bsnn_status bsnn_batch_get_stream(const bsnn_batch* batch, void** out_stream);
+/* One instance's per-neuron field (BSNN_FIELD_* per-neuron fields; CONN_* = the neuron's own
+ * presynaptic traces), E neurons then I neurons. */
+BSNN_API bsnn_status bsnn_batch_read_state(bsnn_batch* batch, uint32_t instance, int32_t field, void* host_out);
+/* Spikes since creation, host_out[2 * instance + 0 / 1] for the E / I group. */
+BSNN_API bsnn_status bsnn_batch_read_spike_counts(bsnn_batch* batch, uint64_t* host_out);
+BSNN_API bsnn_status bsnn_batch_get_info(bsnn_batch* batch, bsnn_batch_info* out);
+
 #ifdef __cplusplus
 }
 #endif

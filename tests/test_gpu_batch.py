@@ -1,0 +1,119 @@
+"""GPU: the batched form (bsnn_batch_*) against the CPU oracle, instance by instance.
+
+Each instance of a batch is an ordinary network whose weights are its class's weights rounded to
+BF16 (`BatchSpec.instance_network`).  The batch computes the propagation on the tensor cores from
+the BF16 weights and the traces split into BF16 high and low parts (x = hi + lo to about 2^-17)
+with FP32 accumulation, so against the FP32 oracle run on the same BF16-valued weights it agrees
+to within 2e-5 relative (to the field's largest magnitude) in g, v and the traces over the first
+steps, with identical spikes and refractory counters.  Over longer runs (chaotic divergence), the
+population spike counts are compared instead.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import bsnn
+import oracle
+from conftest import assert_close
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 2e-5
+FIELDS = ["membrane_potentials", "g_excitatory", "g_inhibitory", "i_stimulus", "background_g_excitatory",
+          "background_excitatory_r_traces", "background_excitatory_d_traces", "connection_summed"]
+
+
+def oracle_for(spec, b, precision=oracle.PREC_F32):
+    net = spec.instance_network(b)
+    o = oracle.OracleSimulation(net.num_excitatory, net.num_inhibitory, precision=precision, **net.sim_kwargs())
+    net.build(o)
+    return o, net
+
+
+def oracle_field(o, net, name):
+    if name == "connection_summed":  # the neuron's own presynaptic trace: E from conn 0, I from conn 2
+        return np.concatenate([o.read(name, 0), o.read(name, 2)])
+    return o.read(name)
+
+
+def compare_instance(g, b, o, net, tag):
+    np.testing.assert_array_equal(g.read(b, "spikes"), o.read("spikes"), err_msg=f"{tag} spikes")
+    np.testing.assert_array_equal(g.read(b, "refractory_counter"), o.read("refractory_counter"), err_msg=f"{tag} refrac")
+    for f in FIELDS:
+        assert_close(g.read(b, f), oracle_field(o, net, f), RTOL, f"{tag} {f}")
+
+
+@pytest.mark.parametrize("noise", [True, False])
+def test_batch_matches_the_oracle_over_the_first_steps(noise):
+    spec = bsnn.config4_batch(n_instances=5, steps=400, seed=3, sizes=(400, 900), stim_window=(5, 300))
+    g = bsnn.BatchSimulation(spec, noise=noise)
+    info = g.info()
+    assert info.num_instances == 5 and info.num_classes == len(spec.classes)
+    oracles = []
+    for b in range(len(spec.instances)):
+        o, net = oracle_for(spec, b)
+        if not noise:
+            o.set_noise_mode(bsnn.NOISE_OFF)
+        oracles.append((o, net))
+    done = 0
+    for block in (1, 9, 30):
+        g.run(block)
+        for o, _ in oracles:
+            o.run(done, block)
+        done += block
+        for b, (o, net) in enumerate(oracles):
+            compare_instance(g, b, o, net, f"instance {b} after {done} steps")
+    g.close()
+
+
+def test_batch_launch_split_and_spike_counts():
+    """The same batch in one launch and in launches of 7 steps gives the same state bit for bit;
+    the spike counter agrees with the oracle's spike history."""
+    spec = bsnn.config4_batch(n_instances=4, steps=300, seed=5, sizes=(400, 900), stim_window=(10, 200))
+    a = bsnn.BatchSimulation(spec)
+    a.run(120)
+    b = bsnn.BatchSimulation(spec)
+    b.set_steps_per_launch(7)
+    b.run(120)
+    for k in range(4):
+        for f in ("membrane_potentials", "g_excitatory", "connection_summed"):
+            np.testing.assert_array_equal(a.read(k, f), b.read(k, f), err_msg=f)
+    np.testing.assert_array_equal(a.spike_counts(), b.spike_counts())
+    counts = a.spike_counts()
+    for k in range(2):
+        o, net = oracle_for(spec, k)
+        total = np.zeros(2, np.int64)
+        for t in range(60):  # spike counts over the first 60 steps, step by step
+            o.step(t)
+            s = o.read("spikes")
+            total += [int(s[: net.num_excitatory].sum()), int(s[net.num_excitatory:].sum())]
+        c = bsnn.BatchSimulation(spec)
+        c.run(60)
+        np.testing.assert_array_equal(c.spike_counts()[k], total)
+        c.close()
+    assert counts.sum() > 0
+    a.close()
+    b.close()
+
+
+def test_batch_rates_against_fp64():
+    """Population rates over 2,000 steps against the FP64 oracle for a few instances; the bound is
+    stated per instance and population (relative, or 2 spikes for near-silent populations)."""
+    spec = bsnn.config4_batch(n_instances=6, steps=2000, seed=7, sizes=(400, 900, 1600), stim_window=(200, 1500))
+    g = bsnn.BatchSimulation(spec)
+    g.run(2000)
+    counts = g.spike_counts().astype(np.int64)
+    worst = 0.0
+    for b in range(3):
+        o, net = oracle_for(spec, b, precision=oracle.PREC_F64)
+        o.run(0, 2000)
+        ref = np.array([int(o.read_spike_history(0).sum()), int(o.read_spike_history(1).sum())])
+        for p in range(2):
+            err = abs(counts[b, p] - ref[p]) / max(ref[p], 1)
+            print(f"instance {b} pop {p}: {counts[b, p]} spikes vs FP64 {ref[p]}")
+            assert abs(counts[b, p] - ref[p]) <= max(2, 0.05 * ref[p]), (b, p, counts[b, p], ref[p])
+            if ref[p] > 100:
+                worst = max(worst, err)
+    print(f"largest relative rate error (populations with > 100 spikes): {worst:.2e}")
+    g.close()
