@@ -122,6 +122,131 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def measured_tensor_peak():
+    """Dense BF16 TFLOP/s: the burst figure (a kernel timed alone)."""
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        if "bf16_tflops" in d:
+            return float(d["bf16_tflops"]), "measured"
+    return 1590.0, "fallback"
+
+
+BATCH_WORKLOADS = {"config4_batch_192": 192}
+
+
+def run_batch(args, rank, world):
+    """The batched form: 192 independent networks (E from {400, 900, 1600, 2500, 3600}, I = E/4,
+    own seed, g_leak and stimulus amplitude, plasticity off) in one persistent launch per bench
+    step (a captured CUDA graph of --sim-steps clock steps).  Beside it, the plain form: the
+    single-network engine stepping one instance at a time, timed per size class."""
+    import torch
+
+    import bsnn
+    torch.cuda.set_device(rank % max(1, torch.cuda.device_count()))
+    dev = torch.cuda.current_device()
+    S, K, W = args.sim_steps, args.steps, args.warmup
+    n_inst = BATCH_WORKLOADS[args.workload]
+    spec = bsnn.config4_batch(n_inst, steps=(W + K) * S + 1, seed=rank)
+    sim = bsnn.BatchSimulation(spec, device=dev)
+    sim.set_steps_per_launch(S)
+    stream = torch.cuda.ExternalStream(sim.stream())
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
+    for _ in range(W):
+        sim.run(S)
+    sim.synchronize()
+    info0 = sim.info()
+    c0 = sim.spike_counts().astype(np.int64)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    times_ms = []
+    with ClockSampler(dev) as clocks:
+        for _ in range(K):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            sim.run(S)
+            e1.record(stream)
+            e1.synchronize()
+            times_ms.append(e0.elapsed_time(e1))
+        sim.synchronize()
+    info1 = sim.info()
+    spikes = int((sim.spike_counts().astype(np.int64) - c0).sum())
+    t_ms = float(sum(times_ms))
+    if world > 1:
+        t_ms, _, spikes = reduce_over_ranks(t_ms, 0, spikes, dev)
+    launches = int(info1.kernel_launches - info0.kernel_launches)
+    sim_seconds = n_inst * K * S * DT * world
+    value = sim_seconds / (t_ms / 1e3)
+    # algorithmic work per clock step: the propagation 2 * sum N_pre * N_post over instances
+    sizes = [spec.classes[i.cls].num_e + spec.classes[i.cls].num_i for i in spec.instances]
+    flops_step = 2.0 * sum(n * n for n in sizes)
+    synapses = sum(n * n for n in sizes)
+    step_s = t_ms / 1e3 / (K * S)
+    achieved = flops_step / step_s / 1e12
+    peak, peak_kind = measured_tensor_peak()
+    weight_bytes = float(info1.weight_bytes)
+    line = {
+        "metric": "simulated-s per wall-s (and synaptic events/s) at 1 B200", "value": value,
+        "unit": "simulated-s/wall-s", "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": t_ms / K,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16 weights and traces (hi + lo), f32 accumulate",
+        "data": "synthetic (seeded; reference example shapes, uniform[0, max_weight] weights)",
+        "config": {"workload": args.workload, "instances": n_inst, "neurons": int(sum(sizes)),
+                   "synapse_entries": int(synapses), "size_classes": len(spec.classes),
+                   "clock_steps_per_bench_step": S, "dt_s": DT, "plasticity": "off",
+                   "form": "batched: one persistent launch per bench step, shared-weight propagation as a "
+                           "tcgen05 BF16 GEMM per size class", "parallelism": f"replicas x{world}",
+                   "l2": "flushed (256 MB write) between timed steps"},
+        "dense_synaptic_updates_per_s": synapses / step_s * world,
+        "spikes_per_s_simulated": spikes / max(sim_seconds, 1e-12),
+        "clock_steps_per_s": 1.0 / step_s,
+        "gpu_launches": launches,
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "traffic": None, "peak_source": peak_kind, "flops_per_clock_step": flops_step,
+                     "bf16_weight_bytes_per_clock_step": weight_bytes,
+                     "weight_read_gbs": weight_bytes / step_s / 1e9,
+                     "note": "a GEMV-shaped GEMM (N = instances of a class x 2): bound by the weight stream "
+                             "from L2 and the step's two grid barriers, not by the tensor pipe"},
+        "clocks": clocks.summary(),
+    }
+    sim.close()
+    return line, spec
+
+
+def plain_form_baseline(spec, steps=2000):
+    """The plain form of the same batch: the single-network engine (FP32, the reference's
+    arithmetic) stepping one instance at a time; the time per clock step of one instance of each
+    size class, weighted by the class's instances."""
+    import torch
+
+    import bsnn
+    per_class = {}
+    for b, inst in enumerate(spec.instances):
+        if inst.cls in per_class:
+            continue
+        net = spec.instance_network(b)
+        sim = bsnn.Simulation(net.num_excitatory, net.num_inhibitory, **net.sim_kwargs())
+        net.build(sim)
+        sim.run(0, 200)
+        sim.synchronize()
+        stream = torch.cuda.ExternalStream(sim.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sim.run(200, steps)
+        e1.record(stream)
+        e1.synchronize()
+        per_class[inst.cls] = e0.elapsed_time(e1) / 1e3 / steps
+        sim.close()
+    wall = sum(per_class[i.cls] for i in spec.instances)  # seconds per clock step of all instances
+    return {"value": len(spec.instances) * DT / wall, "unit": "simulated-s/wall-s",
+            "seconds_per_clock_step_by_class": {str(k): v for k, v in sorted(per_class.items())},
+            "sample": f"{steps} clock steps of one instance per size class through the single-network engine, "
+                      f"weighted by the class's instance count"}
+
+
 COPY_BYTES = {"f32_rowscaled": 4, "bf16": 2, "fp8_e4m3": 1}
 FORM_NAMES = {"f32": "plain FP32 (reference arithmetic)",
               "f32_rowscaled": "FP32 masters, per-row normalisation scale, GEMV from an FP32 copy",
@@ -292,6 +417,30 @@ def run_bsnn(args, rank, world):
     return line, spec
 
 
+def run_batch_e2e(args, spec):
+    """The batch through its public API with host buffers: build (weights and stimulus uploaded from
+    host memory), run K bench steps, read the spike counts back each step."""
+    import torch
+
+    import bsnn
+    S, K = args.sim_steps, args.steps
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sim = bsnn.BatchSimulation(spec)
+    sim.set_steps_per_launch(S)
+    d2h = 0
+    for _ in range(K):
+        sim.run(S)
+        d2h += sim.spike_counts().nbytes
+    sim.synchronize()
+    el = time.perf_counter() - t0
+    h2d = sum(sum(w.nbytes for w in c.weights) for c in spec.classes)
+    h2d += sum(sum(np.asarray(a).nbytes for a in i.stimulus) for i in spec.instances)
+    sim.close()
+    return {"value": len(spec.instances) * K * S * DT / el, "unit": "simulated-s/wall-s", "h2d_bytes_per_step": h2d // K,
+            "d2h_bytes_per_step": d2h // K, "includes": "create + upload, run, per-step spike-count reads"}
+
+
 def run_e2e(args, dev):
     """Same metric through the public API with host buffers: build from host arrays (H2D of
     weights, parameters, stimulus), run, drain the spike and voltage rings to host memory every
@@ -329,6 +478,9 @@ def run_reference(args, rank, world):
     timed over a bounded sample; falls back to the CPU oracle when the build is absent."""
     import bsnn
     sys.path.insert(0, str(ROOT / "oracle"))
+    if args.workload in BATCH_WORKLOADS:
+        return {"impl": "reference", "unavailable": "the reference has no batched form (it steps one network per "
+                "process); its per-network speed is its line on the default workload"}
     spec_steps = 3000
     spec = bsnn.synthetic_network(args.workload, steps=spec_steps + 1, weight_values="uniform",
                                   recording_interval_steps=args.sim_steps)
@@ -376,13 +528,28 @@ def main():
         import datetime
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    line, spec = run_bsnn(args, int(os.environ.get("LOCAL_RANK", "0")), world)
-    if rank == 0:
-        if not args.no_e2e:
-            line["e2e"] = run_e2e(args, torch.cuda.current_device())
-        if not args.no_cpu_baseline and world == 1:
-            line["cpu_baseline"] = cpu_baseline(spec, args.cpu_seconds)
-        print(json.dumps(line), flush=True)
+    if args.workload in BATCH_WORKLOADS:
+        line, spec = run_batch(args, int(os.environ.get("LOCAL_RANK", "0")), world)
+        if rank == 0:
+            if not args.no_e2e:
+                line["e2e"] = run_batch_e2e(args, spec)
+            if world == 1:
+                pf = plain_form_baseline(spec)
+                line["plain_form"] = pf
+                line["batched_over_plain"] = line["value"] / pf["value"]
+            if not args.no_cpu_baseline and world == 1:
+                cb = cpu_baseline(spec.instance_network(0), args.cpu_seconds / 2)
+                line["cpu_baseline"] = dict(cb, value=cb["value"], sample=cb["sample"] + " (one instance; the "
+                                            "batch's aggregate is the instance count times slower per instance)")
+            print(json.dumps(line), flush=True)
+    else:
+        line, spec = run_bsnn(args, int(os.environ.get("LOCAL_RANK", "0")), world)
+        if rank == 0:
+            if not args.no_e2e:
+                line["e2e"] = run_e2e(args, torch.cuda.current_device())
+            if not args.no_cpu_baseline and world == 1:
+                line["cpu_baseline"] = cpu_baseline(spec, args.cpu_seconds)
+            print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()

@@ -87,11 +87,8 @@ uint16_t host_bf16(float v) {  // round to nearest even (finite values)
     return static_cast<uint16_t>(u >> 16);
 }
 
-DGroup batch_group(const bsnn_neuron_group_params& p, uint32_t off) {
-    DGroup G{};
-    G.off = off;
-    G.n = p.num_neurons;
-    G.inhib = p.is_inhibitory ? 1u : 0u;
+BGroupP batch_group(const bsnn_neuron_group_params& p) {
+    BGroupP G{};
     G.refractory_steps = p.refractory_steps;
     G.has_bg_e = p.mean_background_excitatory_spikes > 0.0f;
     G.has_bg_i = p.mean_background_inhibitory_spikes > 0.0f;
@@ -234,7 +231,7 @@ void batch_finalize(bsnn_batch* b) {
     for (auto& o : o_state) o = A.take(fN);
     const size_t o_ref = A.take(sizeof(uint32_t) * n_neurons), o_spk = A.take(sizeof(uint32_t) * n_neurons);
     const size_t o_cnt = A.take(sizeof(unsigned long long) * 2 * h.n_inst);
-    const size_t o_ninst = A.take(sizeof(uint32_t) * n_neurons);
+    const size_t o_pns = A.take(sizeof(unsigned long long) * 8 * n_ctas);
     const size_t o_inst = A.take(sizeof(BInst) * h.n_inst);
     const size_t o_units = A.take(sizeof(BUnit) * units_cta.size());
     const size_t o_cta = A.take(sizeof(uint32_t) * cta_units.size());
@@ -272,7 +269,7 @@ void batch_finalize(bsnn_batch* b) {
     b->scratch = F(o_scr);
 
     // neuron -> instance, instance table, initial voltages and refractory counters
-    std::vector<uint32_t> ninst(n_neurons);
+
     std::vector<BInst> inst(h.n_inst);
     std::vector<float> v0(n_neurons);
     for (uint32_t i = 0; i < h.n_inst; ++i) {
@@ -283,18 +280,15 @@ void batch_finalize(bsnn_batch* b) {
         BI.row = row[i];
         BI.nbase = b->nbase[i];
         BI.seed = I.seed;
-        BI.g[0] = batch_group(I.g[0], 0);
-        BI.g[1] = batch_group(I.g[1], HC.E);
-        for (uint32_t j = 0; j < HC.E + HC.I; ++j) {
-            ninst[b->nbase[i] + j] = i;
+        BI.g[0] = batch_group(I.g[0]);
+        BI.g[1] = batch_group(I.g[1]);
+        for (uint32_t j = 0; j < HC.E + HC.I; ++j)
             v0[b->nbase[i] + j] = I.g[j < HC.E ? 0 : 1].v_rest;  // NeuronGroup::initialize_data
-        }
     }
-    h.neuron_inst = reinterpret_cast<const uint32_t*>(base + o_ninst);
+    h.phase_ns = reinterpret_cast<unsigned long long*>(base + o_pns);
     h.inst = reinterpret_cast<const BInst*>(base + o_inst);
     h.units = reinterpret_cast<const BUnit*>(base + o_units);
     h.cta_units = reinterpret_cast<const uint32_t*>(base + o_cta);
-    cuda_check(cudaMemcpy(base + o_ninst, ninst.data(), sizeof(uint32_t) * n_neurons, cudaMemcpyHostToDevice), "H2D");
     cuda_check(cudaMemcpy(base + o_inst, inst.data(), sizeof(BInst) * inst.size(), cudaMemcpyHostToDevice), "H2D");
     cuda_check(cudaMemcpy(h.v, v0.data(), fN, cudaMemcpyHostToDevice), "H2D v");
     cuda_check(cudaMemcpy(base + o_units, units_cta.data(), sizeof(BUnit) * units_cta.size(), cudaMemcpyHostToDevice),
@@ -321,7 +315,15 @@ void batch_finalize(bsnn_batch* b) {
     b->d_sim = reinterpret_cast<BSim*>(base + o_sim);
     cuda_check(cudaMemcpy(b->d_sim, &h, sizeof(BSim), cudaMemcpyHostToDevice), "H2D batch sim");
     b->grid = n_ctas;
-    b->smem = kBatchStages * (kATileBytes + 2u * 128u * 64u * 2u);
+    uint32_t max_b = 0;
+    for (uint32_t c = 0; c < h.n_classes; ++c) max_b = std::max(max_b, 2u * h.cls[c].NP * 128u);
+    h.stage_bytes = (kATileBytes + max_b + 1023u) & ~1023u;
+    b->smem = kBatchStages * h.stage_bytes + sizeof(BInst) * h.n_inst;
+    int optin = 0;
+    cuda_check(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device), "smem attr");
+    require(b->smem + 4096 <= static_cast<size_t>(optin), BSNN_ERR_INVALID_ARGUMENT,
+            "batch too large: the instance table and the operand stages do not fit in shared memory");
+    cuda_check(cudaMemcpy(b->d_sim, &h, sizeof(BSim), cudaMemcpyHostToDevice), "H2D batch sim");
     cuda_check(cudaFuncSetAttribute(reinterpret_cast<const void*>(&bsnn_batch_kernel),
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(b->smem)),
                "batch smem");
@@ -612,5 +614,16 @@ BSNN_API bsnn_status bsnn_batch_get_info(bsnn_batch* b, bsnn_batch_info* out) {
         *out = i;
     });
 }
+
+#ifdef BSNN_PHASE_TIMING
+// Profiling builds: per-CTA clock tallies of the batch kernel's phases [grid][8].
+BSNN_API bsnn_status bsnn_batch_debug_phase_ns(bsnn_batch* b, unsigned long long* out) {
+    if (!b || !out) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded_batch(b, [&] {
+        batch_finalize(b);
+        cuda_check(cudaMemcpy(out, b->h.phase_ns, 8 * sizeof(unsigned long long) * b->grid, cudaMemcpyDeviceToHost), "D2H");
+    });
+}
+#endif
 
 }  // extern "C"

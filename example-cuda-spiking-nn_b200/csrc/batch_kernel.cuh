@@ -39,7 +39,7 @@ namespace bsnn {
 constexpr uint32_t kBatchMaxClasses = 8;
 constexpr uint32_t kBatchStages = 4;        // shared-memory ring of operand stages
 constexpr uint32_t kBatchTmemCols = 256;    // accumulator columns (N <= 256)
-constexpr uint32_t kBatchThreads = 384;
+constexpr uint32_t kBatchThreads = 512;
 constexpr uint32_t kATileBytes = 128u * 64u * 2u;  // one 128 x 64 BF16 A tile
 
 // A size class: instances with the same numbers of neurons share its weights.
@@ -58,10 +58,18 @@ struct BClass {
     float r_decay[2], d_decay[2], norm[2];  // connection traces of the E- and I-side connections
 };
 
-// One instance: its class, its row in the class's B operand, its neurons, seed and groups.
+// The neuron-group parameters the neuron phase uses (NeuronGroupView, plus the Poisson means'
+// exp(-mean)).
+struct BGroupP {
+    float timestep, g_leak, cap, delta_t, v_eff, e_exc, e_inh, v_th, v_reset, v_rest;
+    float exp_neg_mean_e, exp_neg_mean_i, bg_er_decay, bg_ed_decay, bg_ir_decay, bg_id_decay, bg_scale_e, bg_scale_i;
+    uint32_t refractory_steps, has_bg_e, has_bg_i;
+};
+
+// One instance: its class, its row in the class's B operand, its first neuron, seed and groups.
 struct BInst {
     uint32_t cls, row, nbase, seed;
-    DGroup g[2];  // E, I (off / n are instance-local)
+    BGroupP g[2];  // E, I
 };
 
 struct BUnit {
@@ -73,7 +81,7 @@ struct BSim {
     uint32_t n_classes, n_inst, n_neurons, n_units;
     BClass cls[kBatchMaxClasses];
     const BInst* inst;
-    const uint32_t* neuron_inst;  // [n_neurons] instance of each neuron
+    uint32_t stage_bytes;         // one shared-memory operand stage (A tile + the largest B tile)
     const BUnit* units;           // in CTA order
     const uint32_t* cta_units;    // [n_ctas + 1] unit ranges per CTA
     float* partials;
@@ -88,6 +96,7 @@ struct BSim {
     const uint32_t* ev_neuron;
     const float* ev_delta;
     int32_t noise_on;
+    unsigned long long* phase_ns;  // [n_ctas][8] phase clock tallies (profiling builds)
     unsigned long long* barrier;
     int32_t* error;
     unsigned long long* steps_done;
@@ -152,116 +161,174 @@ __host__ __device__ __forceinline__ uint32_t core_offset(uint32_t rows, uint32_t
 __device__ __forceinline__ uint16_t bf16_bits_rn(float v) { return __bfloat16_as_ushort(__float2bfloat16_rn(v)); }
 
 // ---- phase A ------------------------------------------------------------------------------------
-__device__ __forceinline__ void batch_neurons(const BSim* S, unsigned long long t) {
-    const uint32_t total = gridDim.x * blockDim.x;
-    for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < S->n_neurons; n += total) {
-        const BInst& B = S->inst[__ldg(S->neuron_inst + n)];
-        const BClass& C = S->cls[B.cls];
-        const uint32_t j = n - B.nbase;  // index in the instance
-        const uint32_t side = j < C.E ? 0u : 1u;
-        const DGroup& G = B.g[side];
-        const uint32_t loc = j - (side ? C.E : 0u);
+// Each CTA takes a contiguous range of neurons, four per thread at a time: all loads of the four
+// are issued before any is computed, to keep more memory requests in flight.  The instance and
+// class tables live in shared memory (an instance is found by binary search on its first neuron),
+// so a neuron's only global reads are its own state and its partial sums.
+struct NeuronIn {
+    uint32_t n, inst;
+    bool valid;
+    float v, ge, gi, istim, er, ed, ir, id, tr, td;
+    uint32_t refrac;
+};
 
-        float ge_used = __ldcg(S->ge + n), gi_used = __ldcg(S->gi + n);
-        if (t > 0) {  // the previous step's propagation, K chunks in order
-            const uint32_t mt = j >> 7, row = j & 127u;
-            for (uint32_t sd = 0; sd < 2; ++sd) {
-                float dot = 0.0f;
-                const float* p = S->partials + C.pbase[sd] + static_cast<size_t>(mt) * C.nkc[sd] * C.NP * 128u +
-                                 static_cast<size_t>(B.row) * 128u + row;
-                for (uint32_t kc = 0; kc < C.nkc[sd]; ++kc) dot += __ldcg(p + static_cast<size_t>(kc) * C.NP * 128u);
-                if (sd == 0) ge_used = ge_used + dot;
-                else gi_used = gi_used + dot;
-            }
-        }
-        float er = flush_tiny(__ldcg(S->er + n) * G.bg_er_decay);
-        float ir = flush_tiny(__ldcg(S->ir + n) * G.bg_ir_decay);
-        float ed = flush_tiny(__ldcg(S->ed + n) * G.bg_ed_decay);
-        float id = flush_tiny(__ldcg(S->id + n) * G.bg_id_decay);
-        uint32_t ne = 0, ni = 0;
-        if (S->noise_on) {
-            if (G.has_bg_e) ne = poisson_knuth(G.exp_neg_mean_e, B.seed, j, t, 0u);
-            if (G.has_bg_i) ni = poisson_knuth(G.exp_neg_mean_i, B.seed, j, t, 1u);
-        }
-        if (ne > 0u) {
-            const float inc = static_cast<float>(ne);
-            er += inc;
-            ed += inc;
-        }
-        const float bg_ge = (ed - er) * G.bg_scale_e;
-        if (ni > 0u) {
-            const float inc = static_cast<float>(ni);
-            ir += inc;
-            id += inc;
-        }
-        const float bg_gi = (id - ir) * G.bg_scale_i;
+__device__ __forceinline__ uint32_t instance_of(const BInst* s_inst, uint32_t n_inst, uint32_t n) {
+    uint32_t lo = 0, hi = n_inst;  // last instance whose first neuron is <= n
+    while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (s_inst[mid].nbase <= n) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
 
-        float v = __ldcg(S->v + n);
-        float istim = __ldcg(S->istim + n);
-        uint32_t refrac = __ldcg(S->refrac + n), spike = 0;
-        if (refrac > 0) {
-            --refrac;
-            v = G.v_reset;
+__device__ __forceinline__ void neuron_load(const BSim* S, const BInst* s_inst, const BClass* s_cls, uint32_t n,
+                                            bool valid, unsigned long long t, NeuronIn& a) {
+    a.n = n;
+    a.valid = valid;
+    if (!valid) return;
+    a.v = __ldcg(S->v + n);
+    a.ge = __ldcg(S->ge + n);
+    a.gi = __ldcg(S->gi + n);
+    a.istim = __ldcg(S->istim + n);
+    a.er = __ldcg(S->er + n);
+    a.ed = __ldcg(S->ed + n);
+    a.ir = __ldcg(S->ir + n);
+    a.id = __ldcg(S->id + n);
+    a.tr = __ldcg(S->tr + n);
+    a.td = __ldcg(S->td + n);
+    a.refrac = __ldcg(S->refrac + n);
+    a.inst = instance_of(s_inst, S->n_inst, n);
+    if (t > 0) {  // the previous step's propagation, K chunks in order
+        const BInst& B = s_inst[a.inst];
+        const BClass& C = s_cls[B.cls];
+        const uint32_t j = n - B.nbase, stride = C.NP * 128u;
+        const size_t tile = static_cast<size_t>(j >> 7), r = static_cast<size_t>(B.row) * 128u + (j & 127u);
+        const float* pe = S->partials + C.pbase[0] + tile * C.nkc[0] * stride + r;
+        const float* pi = S->partials + C.pbase[1] + tile * C.nkc[1] * stride + r;
+        float de = 0.0f, di = 0.0f;
+        for (uint32_t kc = 0; kc < C.nkc[0]; ++kc) de += __ldcg(pe + kc * stride);
+        for (uint32_t kc = 0; kc < C.nkc[1]; ++kc) di += __ldcg(pi + kc * stride);
+        a.ge = a.ge + de;
+        a.gi = a.gi + di;
+    }
+}
+
+__device__ __forceinline__ void neuron_step(const BSim* S, const BInst* s_inst, const BClass* s_cls,
+                                            unsigned long long t, const NeuronIn& a) {
+    if (!a.valid) return;
+    const uint32_t n = a.n;
+    const BInst& B = s_inst[a.inst];
+    const BClass& C = s_cls[B.cls];
+    const uint32_t j = n - B.nbase;  // index in the instance
+    const uint32_t side = j < C.E ? 0u : 1u;
+    const BGroupP& G = B.g[side];
+    const uint32_t loc = j - (side ? C.E : 0u);
+    const float ge_used = a.ge, gi_used = a.gi;
+
+    float er = flush_tiny(a.er * G.bg_er_decay);
+    float ir = flush_tiny(a.ir * G.bg_ir_decay);
+    float ed = flush_tiny(a.ed * G.bg_ed_decay);
+    float id = flush_tiny(a.id * G.bg_id_decay);
+    uint32_t ne = 0, ni = 0;
+    if (S->noise_on) {
+        if (G.has_bg_e) ne = poisson_knuth(G.exp_neg_mean_e, B.seed, j, t, 0u);
+        if (G.has_bg_i) ni = poisson_knuth(G.exp_neg_mean_i, B.seed, j, t, 1u);
+    }
+    if (ne > 0u) {
+        const float inc = static_cast<float>(ne);
+        er += inc;
+        ed += inc;
+    }
+    const float bg_ge = (ed - er) * G.bg_scale_e;
+    if (ni > 0u) {
+        const float inc = static_cast<float>(ni);
+        ir += inc;
+        id += inc;
+    }
+    const float bg_gi = (id - ir) * G.bg_scale_i;
+
+    float v = a.v, istim = a.istim;
+    uint32_t refrac = a.refrac, spike = 0;
+    if (refrac > 0) {
+        --refrac;
+        v = G.v_reset;
+    } else {
+        const float linear_leak_term = -1.0f * G.g_leak * (v - G.v_rest);
+        const float exponential_depolarization_term = G.g_leak * G.delta_t * expf((v - G.v_eff) / G.delta_t);
+        const float excitatory_synaptic_term = -1.0f * ge_used * (v - G.e_exc);
+        const float inhibitory_synaptic_term = -1.0f * gi_used * (v - G.e_inh);
+        const float dv = (G.timestep / G.cap) * (linear_leak_term + exponential_depolarization_term +
+                                                 excitatory_synaptic_term + inhibitory_synaptic_term + istim);
+        const float v_next = v + dv;
+        if (v_next >= G.v_th) {
+            refrac = G.refractory_steps;
+            spike = 1;
+            v = G.v_th;
         } else {
-            const float linear_leak_term = -1.0f * G.g_leak * (v - G.v_rest);
-            const float exponential_depolarization_term = G.g_leak * G.delta_t * expf((v - G.v_eff) / G.delta_t);
-            const float excitatory_synaptic_term = -1.0f * ge_used * (v - G.e_exc);
-            const float inhibitory_synaptic_term = -1.0f * gi_used * (v - G.e_inh);
-            const float dv = (G.timestep / G.cap) * (linear_leak_term + exponential_depolarization_term +
-                                                     excitatory_synaptic_term + inhibitory_synaptic_term + istim);
-            const float v_next = v + dv;
-            if (v_next >= G.v_th) {
-                refrac = G.refractory_steps;
-                spike = 1;
-                v = G.v_th;
-            } else {
-                v = v_next;
-            }
+            v = v_next;
         }
-        S->er[n] = er;
-        S->ed[n] = ed;
-        S->ir[n] = ir;
-        S->id[n] = id;
-        S->v[n] = v;
-        S->refrac[n] = refrac;
-        S->ge[n] = bg_ge;  // reset for the next propagation
-        S->gi[n] = bg_gi;
-        S->spikes[n] = spike;
-        if (spike) atomicAdd(S->spike_counts + 2u * (S->neuron_inst[n]) + side, 1ull);
+    }
+    S->er[n] = er;
+    S->ed[n] = ed;
+    S->ir[n] = ir;
+    S->id[n] = id;
+    S->v[n] = v;
+    S->refrac[n] = refrac;
+    S->ge[n] = bg_ge;  // reset for the next propagation
+    S->gi[n] = bg_gi;
+    S->spikes[n] = spike;
+    if (spike) atomicAdd(S->spike_counts + 2u * a.inst + side, 1ull);
 
-        // stimulus events of this step act from the next step
-        if (t < S->stim_len) {
-            uint32_t lo = __ldg(S->stim_off + t), hi = __ldg(S->stim_off + t + 1);
-            const uint32_t end = hi;
-            while (lo < hi) {
-                const uint32_t mid = (lo + hi) >> 1;
-                if (__ldg(S->ev_neuron + mid) < n) lo = mid + 1;
-                else hi = mid;
-            }
-            bool any = false;
-            for (uint32_t k = lo; k < end && __ldg(S->ev_neuron + k) == n; ++k) {
-                istim = istim + __ldg(S->ev_delta + k);
-                any = true;
-            }
-            if (any) S->istim[n] = istim;
+    // stimulus events of this step act from the next step
+    if (t < S->stim_len) {
+        uint32_t lo = __ldg(S->stim_off + t), hi = __ldg(S->stim_off + t + 1);
+        const uint32_t end = hi;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (__ldg(S->ev_neuron + mid) < n) lo = mid + 1;
+            else hi = mid;
         }
+        bool any = false;
+        for (uint32_t k = lo; k < end && __ldg(S->ev_neuron + k) == n; ++k) {
+            istim = istim + __ldg(S->ev_delta + k);
+            any = true;
+        }
+        if (any) S->istim[n] = istim;
+    }
 
-        // connection traces of the neuron's presynaptic side, and x as BF16 hi / lo in B
-        float d = flush_tiny(__ldcg(S->td + n) * C.d_decay[side]);
-        float r = flush_tiny(__ldcg(S->tr + n) * C.r_decay[side]);
-        if (spike == 1) {
-            r += C.norm[side];
-            d += C.norm[side];
-        }
-        S->tr[n] = r;
-        S->td[n] = d;
-        const float x = d - r;
-        const uint16_t hi = bf16_bits_rn(x);
-        const float lo_f = x - __uint_as_float(static_cast<uint32_t>(hi) << 16);
-        const uint16_t lo = bf16_bits_rn(lo_f);
-        uint16_t* X = C.X[side] + static_cast<size_t>(loc >> 6) * (2u * C.NP * 64u);
-        X[core_offset(2u * C.NP, B.row, loc & 63u)] = hi;
-        X[core_offset(2u * C.NP, C.NP + B.row, loc & 63u)] = lo;
+    // connection traces of the neuron's presynaptic side, and x as BF16 hi / lo in B
+    float d = flush_tiny(a.td * C.d_decay[side]);
+    float r = flush_tiny(a.tr * C.r_decay[side]);
+    if (spike == 1) {
+        r += C.norm[side];
+        d += C.norm[side];
+    }
+    S->tr[n] = r;
+    S->td[n] = d;
+    const float x = d - r;
+    const uint16_t hi = bf16_bits_rn(x);
+    const float lo_f = x - __uint_as_float(static_cast<uint32_t>(hi) << 16);
+    const uint16_t lo = bf16_bits_rn(lo_f);
+    uint16_t* X = C.X[side] + static_cast<size_t>(loc >> 6) * (2u * C.NP * 64u);
+    X[core_offset(2u * C.NP, B.row, loc & 63u)] = hi;
+    X[core_offset(2u * C.NP, C.NP + B.row, loc & 63u)] = lo;
+}
+
+constexpr uint32_t kNeuronsInFlight = 4;
+
+__device__ __forceinline__ void batch_neurons(const BSim* S, const BInst* s_inst, const BClass* s_cls,
+                                              unsigned long long t) {
+    const uint32_t per = (S->n_neurons + gridDim.x - 1) / gridDim.x;
+    const uint32_t n0 = blockIdx.x * per;
+    const uint32_t n1 = n0 + per < S->n_neurons ? n0 + per : S->n_neurons;
+    for (uint32_t n = n0 + threadIdx.x; n < n1; n += kNeuronsInFlight * blockDim.x) {
+        NeuronIn a[kNeuronsInFlight];
+#pragma unroll
+        for (uint32_t q = 0; q < kNeuronsInFlight; ++q)
+            neuron_load(S, s_inst, s_cls, n + q * blockDim.x, n + q * blockDim.x < n1, t, a[q]);
+#pragma unroll
+        for (uint32_t q = 0; q < kNeuronsInFlight; ++q) neuron_step(S, s_inst, s_cls, t, a[q]);
     }
 }
 
@@ -277,13 +344,18 @@ struct BatchSmem {
 __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim* __restrict__ S, uint32_t n_steps) {
     extern __shared__ __align__(1024) unsigned char bsm_raw[];
     __shared__ BatchSmem bs;
+    __shared__ BClass s_cls[kBatchMaxClasses];
     __shared__ int s_ok;
     __shared__ unsigned long long s_bar0, s_t0;
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
-    // stage s: A tile at s * stage_bytes, B tile after it
-    const uint32_t max_b = 2u * 128u * 64u * 2u;  // B tile of N = 256 rows
-    const uint32_t stage_bytes = kATileBytes + max_b;
+    // stage s: A tile at s * stage_bytes, B tile after it; then the instance table
+    const uint32_t stage_bytes = S->stage_bytes;
     const uint32_t smem_base = saddr(bsm_raw);
+    BInst* s_inst = reinterpret_cast<BInst*>(bsm_raw + kBatchStages * stage_bytes);
+    for (uint32_t i = tid; i < S->n_inst * (sizeof(BInst) / 4u); i += blockDim.x)
+        reinterpret_cast<uint32_t*>(s_inst)[i] = reinterpret_cast<const uint32_t*>(S->inst)[i];
+    for (uint32_t i = tid; i < S->n_classes * (sizeof(BClass) / 4u); i += blockDim.x)
+        reinterpret_cast<uint32_t*>(s_cls)[i] = reinterpret_cast<const uint32_t*>(S->cls)[i];
 
     if (tid == 0) {
         bs.ok = 1u;
@@ -311,20 +383,29 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
     uint32_t empty_pend[kBatchStages] = {0, 0, 0, 0};
     uint32_t g_load = 0, g_use = 0;
     bool ok = true;
+#ifdef BSNN_PHASE_TIMING
+    __shared__ unsigned long long s_tally_[8];
+    if (tid == 0)
+        for (int i = 0; i < 8; ++i) s_tally_[i] = 0;
+    unsigned long long t_mark_ = static_cast<unsigned long long>(clock64());
+#endif
 
     for (uint32_t k = 0; k < n_steps && ok; ++k) {
         const unsigned long long t = t0 + k;
-        batch_neurons(S, t);
+        batch_neurons(S, s_inst, s_cls, t);
         fence_proxy_async_global();
+        __syncthreads();
+        BSNN_TMARK(0);
         if (!grid_barrier(S->barrier, S->error, bar0 + (2ull * k + 1ull) * gridDim.x, &s_ok)) {
             ok = false;
             break;
         }
+        BSNN_TMARK(1);
         if (tid == 0) fence_proxy_async_global();
 
         for (uint32_t ui = u_begin; ui < u_end && ok; ++ui) {
             const BUnit U = S->units[ui];
-            const BClass& C = S->cls[U.cls];
+            const BClass& C = s_cls[U.cls];
             const uint32_t N = 2u * C.NP, b_bytes = N * 128u, nk = U.k1 - U.k0;
             if (tid == 0) {
                 const unsigned char* a_src =
@@ -412,11 +493,17 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
             tc_fence_after();
         }
         if (!ok) break;
+        BSNN_TMARK(2);
         if (!grid_barrier(S->barrier, S->error, bar0 + (2ull * k + 2ull) * gridDim.x, &s_ok)) {
             ok = false;
             break;
         }
+        BSNN_TMARK(3);
     }
+#ifdef BSNN_PHASE_TIMING
+    if (tid == 0)
+        for (int i = 0; i < 8; ++i) S->phase_ns[blockIdx.x * 8u + i] += s_tally_[i];
+#endif
     tc_fence_before();
     __syncthreads();
     if (warp == 0) tmem_dealloc(tmem, kBatchTmemCols);
