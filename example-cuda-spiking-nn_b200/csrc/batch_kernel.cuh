@@ -141,6 +141,22 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* out) {
     for (int k = 0; k < 16; ++k) out[k] = __uint_as_float(r[k]);
 }
 __device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+// An L2 policy that keeps the lines it touches (the weight tiles: every step reads all of them,
+// and with the neuron state and the partial sums they fit in L2 together).
+__device__ __forceinline__ uint64_t l2_evict_last_policy() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ void bulk_load_keep(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar, uint64_t pol) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(dst),
+        "l"(src), "r"(bytes), "r"(bar), "l"(pol)
+        : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
 
 // Shared-memory matrix descriptor, canonical K-major layout without swizzle: 8-row x 16-byte
 // core matrices; `lbo` = bytes between the two core matrices of one K=16 step, `sbo` = bytes
@@ -182,11 +198,14 @@ __device__ __forceinline__ uint32_t instance_of(const BInst* s_inst, uint32_t n_
     return lo;
 }
 
+// `cur`: the instance of this thread's previous neuron (neurons only move forward).
 __device__ __forceinline__ void neuron_load(const BSim* S, const BInst* s_inst, const BClass* s_cls, uint32_t n,
-                                            bool valid, unsigned long long t, NeuronIn& a) {
+                                            bool valid, unsigned long long t, uint32_t& cur, NeuronIn& a) {
     a.n = n;
     a.valid = valid;
     if (!valid) return;
+    while (cur + 1u < S->n_inst && s_inst[cur + 1u].nbase <= n) ++cur;
+    a.inst = cur;
     a.v = __ldcg(S->v + n);
     a.ge = __ldcg(S->ge + n);
     a.gi = __ldcg(S->gi + n);
@@ -198,7 +217,6 @@ __device__ __forceinline__ void neuron_load(const BSim* S, const BInst* s_inst, 
     a.tr = __ldcg(S->tr + n);
     a.td = __ldcg(S->td + n);
     a.refrac = __ldcg(S->refrac + n);
-    a.inst = instance_of(s_inst, S->n_inst, n);
     if (t > 0) {  // the previous step's propagation, K chunks in order
         const BInst& B = s_inst[a.inst];
         const BClass& C = s_cls[B.cls];
@@ -322,11 +340,12 @@ __device__ __forceinline__ void batch_neurons(const BSim* S, const BInst* s_inst
     const uint32_t per = (S->n_neurons + gridDim.x - 1) / gridDim.x;
     const uint32_t n0 = blockIdx.x * per;
     const uint32_t n1 = n0 + per < S->n_neurons ? n0 + per : S->n_neurons;
+    uint32_t cur = instance_of(s_inst, S->n_inst, n0 + threadIdx.x < n1 ? n0 + threadIdx.x : n0);
     for (uint32_t n = n0 + threadIdx.x; n < n1; n += kNeuronsInFlight * blockDim.x) {
         NeuronIn a[kNeuronsInFlight];
 #pragma unroll
         for (uint32_t q = 0; q < kNeuronsInFlight; ++q)
-            neuron_load(S, s_inst, s_cls, n + q * blockDim.x, n + q * blockDim.x < n1, t, a[q]);
+            neuron_load(S, s_inst, s_cls, n + q * blockDim.x, n + q * blockDim.x < n1, t, cur, a[q]);
 #pragma unroll
         for (uint32_t q = 0; q < kNeuronsInFlight; ++q) neuron_step(S, s_inst, s_cls, t, a[q]);
     }
@@ -338,7 +357,8 @@ struct BatchSmem {
     uint32_t ok;
     uint64_t full[kBatchStages];
     uint64_t empty[kBatchStages];
-    uint64_t accum;
+    uint64_t accum;   // the MMA thread's commit: the unit's accumulator is complete
+    uint64_t tfree;   // the 4 epilogue warps: the accumulator has been read
 };
 
 __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim* __restrict__ S, uint32_t n_steps) {
@@ -364,6 +384,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
             mbar_init(saddr(&bs.empty[s]), 1u);
         }
         mbar_init(saddr(&bs.accum), 1u);
+        mbar_init(saddr(&bs.tfree), 4u);
         fence_mbar_init();
         s_bar0 = ld_acquire_u64(S->barrier) / gridDim.x * gridDim.x;
         s_t0 = *S->steps_done;
@@ -379,9 +400,10 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
     const unsigned long long bar0 = s_bar0, t0 = s_t0;
     const uint32_t u_begin = S->cta_units[blockIdx.x], u_end = S->cta_units[blockIdx.x + 1];
     // producer / MMA state (thread 0 only)
-    uint32_t full_ph = 0, empty_ph = 0, accum_ph = 0;
+    uint32_t full_ph = 0, empty_ph = 0, accum_ph = 0, tfree_ph = 0;
     uint32_t empty_pend[kBatchStages] = {0, 0, 0, 0};
-    uint32_t g_load = 0, g_use = 0;
+    uint32_t g_load = 0, g_use = 0, units_issued = 0;
+    const bool producer = tid == 128u;  // warp 4: loads and MMAs; warps 0-3: the epilogue
     bool ok = true;
 #ifdef BSNN_PHASE_TIMING
     __shared__ unsigned long long s_tally_[8];
@@ -401,35 +423,50 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
             break;
         }
         BSNN_TMARK(1);
-        if (tid == 0) fence_proxy_async_global();
-
-        for (uint32_t ui = u_begin; ui < u_end && ok; ++ui) {
-            const BUnit U = S->units[ui];
-            const BClass& C = s_cls[U.cls];
-            const uint32_t N = 2u * C.NP, b_bytes = N * 128u, nk = U.k1 - U.k0;
-            if (tid == 0) {
-                const unsigned char* a_src =
-                    reinterpret_cast<const unsigned char*>(C.A[U.side]) +
-                    (static_cast<size_t>(U.mt) * C.KT[U.side] + U.k0) * kATileBytes;
+        if (producer) {
+            fence_proxy_async_global();
+            const uint64_t keep = l2_evict_last_policy();
+            for (uint32_t ui = u_begin; ui < u_end; ++ui) {
+                const BUnit U = S->units[ui];
+                const BClass& C = s_cls[U.cls];
+                const uint32_t N = 2u * C.NP, b_bytes = N * 128u, nk = U.k1 - U.k0;
+                if (bs.ok == 0u) {  // after a timeout: only release the epilogue
+                    tc_commit(saddr(&bs.accum));
+                    continue;
+                }
+                const unsigned char* a_src = reinterpret_cast<const unsigned char*>(C.A[U.side]) +
+                                             (static_cast<size_t>(U.mt) * C.KT[U.side] + U.k0) * kATileBytes;
                 const unsigned char* b_src =
                     reinterpret_cast<const unsigned char*>(C.X[U.side]) + static_cast<size_t>(U.k0) * b_bytes;
-                auto load = [&](uint32_t i) {  // K tile i of the unit into stage g_load % S
+                bool good = true;
+                // K tile i of the unit into stage g_load % S, once the MMAs that read the stage last
+                // are done
+                auto load = [&](uint32_t i) {
                     const uint32_t s = g_load % kBatchStages;
+                    if (empty_pend[s]) {
+                        if (!mbar_wait(saddr(&bs.empty[s]), (empty_ph >> s) & 1u)) good = false;
+                        empty_ph ^= 1u << s;
+                        empty_pend[s] = 0;
+                    }
                     const uint32_t bar = saddr(&bs.full[s]);
                     const uint32_t dst = smem_base + s * stage_bytes;
                     mbar_expect_tx(bar, kATileBytes + b_bytes);
-                    bulk_load(dst, a_src + static_cast<size_t>(i) * kATileBytes, kATileBytes, bar);
+                    bulk_load_keep(dst, a_src + static_cast<size_t>(i) * kATileBytes, kATileBytes, bar, keep);
                     bulk_load(dst + kATileBytes, b_src + static_cast<size_t>(i) * b_bytes, b_bytes, bar);
                     ++g_load;
                 };
                 const uint32_t idesc = idesc_bf16_m128(N);
                 uint32_t next = 0;
                 for (; next < nk && next < kBatchStages; ++next) load(next);
-                for (uint32_t i = 0; i < nk; ++i) {
+                // the epilogue of the previous unit has read the accumulator
+                if (units_issued > 0u) {
+                    if (!mbar_wait(saddr(&bs.tfree), tfree_ph & 1u)) good = false;
+                    tfree_ph ^= 1u;
+                }
+                for (uint32_t i = 0; i < nk && good; ++i) {
                     const uint32_t s = g_use % kBatchStages;
                     if (!mbar_wait(saddr(&bs.full[s]), (full_ph >> s) & 1u)) {
-                        atomicExch(S->error, kErrStageTimeout);
-                        bs.ok = 0u;
+                        good = false;
                         break;
                     }
                     full_ph ^= 1u << s;
@@ -440,44 +477,31 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
                         tc_mma_bf16(tmem, smem_desc(a + ks * 2u * 2048u, 2048u, 128u),
                                     smem_desc(b + ks * 2u * (N * 16u), N * 16u, 128u), idesc, (i | ks) != 0u);
                     tc_commit(saddr(&bs.empty[s]));
-                    ++empty_pend[s];
+                    empty_pend[s] = 1u;
                     ++g_use;
-                    // refill the stage the previous MMAs read, once they are done
-                    if (i > 0 && next < nk) {
-                        const uint32_t sp = (g_use - 2u) % kBatchStages;
-                        if (!mbar_wait(saddr(&bs.empty[sp]), (empty_ph >> sp) & 1u)) {
-                            atomicExch(S->error, kErrStageTimeout);
-                            bs.ok = 0u;
-                            break;
-                        }
-                        empty_ph ^= 1u << sp;
-                        --empty_pend[sp];
-                        load(next++);
-                    }
+                    // refill the stage of the previous iteration (its MMAs have had an MMA's time to
+                    // finish; load() waits for them)
+                    if (i > 0u && next < nk) load(next++);
                 }
                 tc_commit(saddr(&bs.accum));
-                // the stage releases not yet waited for (at most one per stage) complete too
-                for (uint32_t s = 0; s < kBatchStages; ++s) {
-                    if (empty_pend[s] == 0u) continue;
-                    if (!mbar_wait(saddr(&bs.empty[s]), (empty_ph >> s) & 1u)) {
-                        atomicExch(S->error, kErrStageTimeout);
-                        bs.ok = 0u;
-                    }
-                    empty_ph ^= 1u << s;
-                    empty_pend[s] = 0;
+                ++units_issued;
+                if (!good) {
+                    atomicExch(S->error, kErrStageTimeout);
+                    bs.ok = 0u;
                 }
             }
-            // the accumulator is complete once every MMA of the unit has finished
-            if (!mbar_wait(saddr(&bs.accum), accum_ph & 1u)) {
-                atomicExch(S->error, kErrStageTimeout);
-                bs.ok = 0u;
-            }
-            accum_ph ^= 1u;
-            __syncthreads();
-            ok = bs.ok != 0u;  // the same for every thread of the CTA
-            tc_fence_after();
-            if (warp < 4 && ok) {
-                const uint32_t row = 32u * warp + lane;
+        } else if (warp < 4) {
+            const uint32_t row = 32u * warp + lane;
+            for (uint32_t ui = u_begin; ui < u_end; ++ui) {
+                const BUnit U = S->units[ui];
+                const BClass& C = s_cls[U.cls];
+                const bool got = mbar_wait(saddr(&bs.accum), accum_ph & 1u);
+                accum_ph ^= 1u;
+                if (!got) {
+                    atomicExch(S->error, kErrStageTimeout);
+                    bs.ok = 0u;
+                }
+                tc_fence_after();
                 float* part = S->partials + U.part;
                 for (uint32_t c0 = 0; c0 < C.NP; c0 += 16u) {
                     float hi[16], lo[16];
@@ -487,11 +511,13 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
                     for (uint32_t q = 0; q < 16; ++q)
                         if (c0 + q < C.n_inst) part[static_cast<size_t>(c0 + q) * 128u + row] = hi[q] + lo[q];
                 }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(saddr(&bs.tfree));
             }
-            tc_fence_before();
-            __syncthreads();
-            tc_fence_after();
         }
+        __syncthreads();
+        ok = bs.ok != 0u;  // the same for every thread of the CTA
         if (!ok) break;
         BSNN_TMARK(2);
         if (!grid_barrier(S->barrier, S->error, bar0 + (2ull * k + 2ull) * gridDim.x, &s_ok)) {
