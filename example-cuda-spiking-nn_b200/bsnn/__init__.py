@@ -9,6 +9,7 @@ from ._ffi import (FIELD, NOISE_OFF, NOISE_PHILOX, NOISE_REPLAY, PLASTICITY_ISTD
                    WEIGHT_FORMATS,
                    BsnnError, ConnectionParams, ConnectionView, CudaError, DeviceTimeout, InvalidArgument, NeuronGroupParams,
                    OutOfRange, PlasticityParams, StateError, load_library)
+from .adjoint import AdjointNetwork, config5_network, spiking_loss_function
 from .batch import BatchSimulation, BatchSpec, config4_batch
 from .core import Simulation, connection_propagate
 from .network import NetworkSpec, random_network, synthetic_network
@@ -17,6 +18,6 @@ __all__ = [
     "FIELD", "WEIGHT_FORMATS", "NOISE_OFF", "NOISE_PHILOX", "NOISE_REPLAY", "PLASTICITY_ISTDP", "PLASTICITY_STDP", "PLASTICITY_TRIPLET",
     "BsnnError", "ConnectionParams", "ConnectionView", "CudaError", "DeviceTimeout", "InvalidArgument", "NeuronGroupParams",
     "OutOfRange", "PlasticityParams", "StateError", "load_library", "Simulation", "BatchSimulation", "BatchSpec",
-    "config4_batch", "connection_propagate", "NetworkSpec", "random_network",
+    "config4_batch", "AdjointNetwork", "config5_network", "spiking_loss_function", "connection_propagate", "NetworkSpec", "random_network",
     "synthetic_network",
 ]

@@ -271,6 +271,14 @@ class BatchInfo(ctypes.Structure):
     ]
 
 
+class AdjointDesc(ctypes.Structure):
+    """bsnn_adjoint_desc."""
+    _fields_ = [("num_excitatory", ctypes.c_uint32), ("num_inhibitory", ctypes.c_uint32),
+                ("num_steps", ctypes.c_uint32), ("checkpoint_interval", ctypes.c_uint32),
+                ("rng_seed", ctypes.c_int32), ("noise_on", ctypes.c_int32), ("rate_tau", ctypes.c_float),
+                ("surrogate_beta", ctypes.c_float), ("rate_weight", ctypes.c_float), ("voltage_weight", ctypes.c_float)]
+
+
 _P = ctypes.c_void_p
 _U32 = ctypes.c_uint32
 _I32 = ctypes.c_int32
@@ -295,6 +303,13 @@ SIGNATURES = {
     "bsnn_batch_read_state": (_I32, [_P, _U32, _I32, _P]),
     "bsnn_batch_read_spike_counts": (_I32, [_P, ctypes.POINTER(ctypes.c_uint64)]),
     "bsnn_batch_get_info": (_I32, [_P, ctypes.POINTER(BatchInfo)]),
+    "bsnn_adjoint_create": (_I32, [ctypes.POINTER(AdjointDesc), _P, _P, _P, _P, _FP, _FP, _FP, _FP, _UP, _U32, _UP, _FP,
+                                   _U32, _I32, ctypes.POINTER(_P)]),
+    "bsnn_adjoint_destroy": (_I32, [_P]),
+    "bsnn_adjoint_last_error": (ctypes.c_char_p, [_P]),
+    "bsnn_adjoint_set_params": (_I32, [_P, _FP, ctypes.c_float]),
+    "bsnn_adjoint_forward": (_I32, [_P, _FP, _FP, _FP, _FP, _FP]),
+    "bsnn_adjoint_backward": (_I32, [_P, _FP, ctypes.POINTER(ctypes.c_double)]),
     "bsnn_get_info": (_I32, [_P, ctypes.POINTER(Info)]),
     "bsnn_add_neuron_group": (_I32, [_P, ctypes.POINTER(NeuronGroupParams), _UP]),
     "bsnn_add_connection": (_I32, [_P, _U32, _U32, _FP, ctypes.POINTER(ConnectionParams), _UP]),

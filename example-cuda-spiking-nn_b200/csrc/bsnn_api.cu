@@ -1684,3 +1684,4 @@ extern "C" BSNN_API bsnn_status bsnn_debug_phase_ns(bsnn_sim* sim, unsigned long
 }
 #endif
 #include "batch_api.cuh"
+#include "adjoint_api.cuh"

@@ -423,6 +423,50 @@ BSNN_API bsnn_status bsnn_batch_read_state(bsnn_batch* batch, uint32_t instance,
 BSNN_API bsnn_status bsnn_batch_read_spike_counts(bsnn_batch* batch, uint64_t* host_out);
 BSNN_API bsnn_status bsnn_batch_get_info(bsnn_batch* batch, bsnn_batch_info* out);
 
+/* ---- the differentiation form (no reference counterpart) -------------------------------------
+ * A surrogate-gradient adjoint of the two-group network with frozen weights: the forward pass is
+ * the reference's step without plasticity (FP32), checkpointed every checkpoint_interval steps;
+ * the backward pass replays each segment and propagates adjoints back through time, with the
+ * spike's derivative replaced by the fast sigmoid 1 / (1 + |u - v_th| / surrogate_beta)^2 (0 turns
+ * it off) and the reset not differentiated.  The loss is
+ *   rate_weight / T * sum_t (rho_t - rho*_t)^2 + voltage_weight / T * sum_t (vbar_{t+1} - v*_t)^2,
+ * rho the excitatory population rate (Hz) smoothed with time constant rate_tau, vbar the mean
+ * excitatory membrane potential; the gradients are dL/dW_EE and dL/dg_leak (g_leak shared by the
+ * two groups).  Needs only plain CUDA. */
+typedef struct bsnn_adjoint bsnn_adjoint;
+
+typedef struct bsnn_adjoint_desc {
+    uint32_t num_excitatory;
+    uint32_t num_inhibitory;
+    uint32_t num_steps;
+    uint32_t checkpoint_interval;
+    int32_t rng_seed;
+    int32_t noise_on;
+    float rate_tau;        /* s  */
+    float surrogate_beta;  /* V  */
+    float rate_weight;
+    float voltage_weight;
+} bsnn_adjoint_desc;
+
+BSNN_API bsnn_status bsnn_adjoint_create(const bsnn_adjoint_desc* desc, const bsnn_neuron_group_params* excitatory_group,
+                                         const bsnn_neuron_group_params* inhibitory_group,
+                                         const bsnn_connection_params* excitatory_pre,
+                                         const bsnn_connection_params* inhibitory_pre, const float* w_ee,
+                                         const float* w_ei, const float* w_ie, const float* w_ii,
+                                         const uint32_t* stimulus_counts, uint32_t stimulus_steps,
+                                         const uint32_t* stimulus_neurons, const float* stimulus_deltas,
+                                         uint32_t num_events, int32_t device, bsnn_adjoint** out_adjoint);
+BSNN_API bsnn_status bsnn_adjoint_destroy(bsnn_adjoint* adjoint);
+BSNN_API const char* bsnn_adjoint_last_error(const bsnn_adjoint* adjoint);
+/* New E->E weights (row-major [E][E]; null keeps them) and g_leak (NaN keeps it). */
+BSNN_API bsnn_status bsnn_adjoint_set_params(bsnn_adjoint* adjoint, const float* w_ee, float g_leak);
+/* Forward pass over num_steps: targets of num_steps values (voltage_target may be null when
+ * voltage_weight is 0); optional outputs: the loss, rho_t and vbar_{t+1}. */
+BSNN_API bsnn_status bsnn_adjoint_forward(bsnn_adjoint* adjoint, const float* rate_target, const float* voltage_target,
+                                          float* loss_out, float* rate_out, float* mean_voltage_out);
+/* Gradients of the last forward pass's loss: dL/dW_EE (row-major [E][E]) and dL/dg_leak. */
+BSNN_API bsnn_status bsnn_adjoint_backward(bsnn_adjoint* adjoint, float* grad_w_ee, double* grad_g_leak);
+
 #ifdef __cplusplus
 }
 #endif
