@@ -216,6 +216,122 @@ def run_batch(args, rank, world):
     return line, spec
 
 
+ADJOINT_WORKLOADS = {"config5_adjoint_3125": 2000}
+
+
+def run_adjoint(args, rank, world):
+    """The differentiation form: one bench step is one gradient of the rate loss with respect to
+    W_EE and g_leak (forward pass over 2,000 clock steps with checkpoints every 100, then the
+    checkpointed backward pass) on the example network (2,500 E + 625 I, plasticity off), the
+    target rate trace made by the same network with perturbed W_EE."""
+    import torch
+
+    import bsnn
+    torch.cuda.set_device(rank % max(1, torch.cuda.device_count()))
+    dev = torch.cuda.current_device()
+    T, K, W = ADJOINT_WORKLOADS[args.workload], args.steps, args.warmup
+    spec, w_target = bsnn.config5_network(steps=T, seed=11 + rank)
+    net = bsnn.AdjointNetwork(spec, T, checkpoint=100, noise=True, beta=0.5e-3, rate_weight=1.0, device=dev)
+    net.set_params(w_target, None)
+    _, target, _ = net.forward(np.zeros(T, np.float32))
+    net.set_params(spec.conns[0].weights, None)
+    stream = torch.cuda.ExternalStream(net.stream())
+    for _ in range(W):
+        net.forward(target)
+        net.backward()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    fwd_ms, tot_ms = [], []
+    launches0 = net.launches()
+    with ClockSampler(dev) as clocks:
+        for _ in range(K):
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record(stream)
+            loss, rho, _ = net.forward(target)
+            e1.record(stream)
+            dW, dgl = net.backward()
+            e2.record(stream)
+            e2.synchronize()
+            fwd_ms.append(e0.elapsed_time(e1))
+            tot_ms.append(e0.elapsed_time(e2))
+    t_ms = float(sum(tot_ms))
+    if world > 1:
+        t_ms, _, _ = reduce_over_ranks(t_ms, 0, 0, dev)
+    launches = net.launches() - launches0
+    sim_s = T * DT
+    value = K * world * sim_s / (t_ms / 1e3)
+    N, E, I = spec.num_neurons, spec.num_excitatory, spec.num_inhibitory
+    w_bytes = 4.0 * (E + I) * N
+    # per gradient: the forward pass and the replay each stream the rows of spiking neurons (x != 0),
+    # the backward pass streams all of W once per clock step (the pull-back GEMV)
+    grad_bytes = T * w_bytes
+    achieved = grad_bytes / (t_ms / K / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    line = {
+        "metric": "simulated-s per wall-s (and synaptic events/s) at 1 B200", "value": value,
+        "unit": "simulated-s/wall-s (forward + backward)", "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": t_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded; reference example shapes, uniform[0, max_weight] weights)",
+        "config": {"workload": args.workload, "neurons": N, "clock_steps": T, "checkpoint_interval": 100,
+                   "dt_s": DT, "plasticity": "off", "loss": "MSE of the 5 ms-smoothed E rate vs a target trace",
+                   "surrogate": "fast sigmoid, beta 0.5 mV", "parallelism": f"replicas x{world}",
+                   "l2": "W (39 MB) is L2-resident by design; no flush"},
+        "gradients_per_s": K * world / (t_ms / 1e3),
+        "forward_ms": float(np.mean(fwd_ms)), "backward_ms": float(np.mean(tot_ms) - np.mean(fwd_ms)),
+        "forward_simulated_s_per_wall_s": sim_s / (float(np.mean(fwd_ms)) / 1e3),
+        "loss": loss, "mean_rate_hz": float(rho.mean()), "target_mean_rate_hz": float(target.mean()),
+        "grad_norm_w_ee": float(np.linalg.norm(dW)), "grad_g_leak": dgl,
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_source": peak_kind, "bytes_per_gradient": grad_bytes,
+                     "note": "algorithmic bytes: the pull-back GEMV's dense W stream, once per clock step; "
+                             "W is L2-resident, so this is an L2-served stream measured against the HBM peak"},
+        "clocks": clocks.summary(),
+    }
+    return line, (spec, w_target, target, net)
+
+
+def run_adjoint_e2e(args, state):
+    """The gradient through the public API with host buffers, as torch.autograd sees it: W_EE and
+    g_leak uploaded (set_params), forward, backward, dW_EE read back, every bench step."""
+    import bsnn
+    spec, w_target, target, net = state
+    SpikingLoss = bsnn.spiking_loss_function()
+    import torch
+    w = torch.tensor(spec.conns[0].weights, requires_grad=True)
+    gl = torch.tensor(float(np.float32(spec.groups[0]["g_leak"])), requires_grad=True)
+    K = args.steps
+    t0 = time.perf_counter()
+    for _ in range(K):
+        w.grad = None
+        loss = SpikingLoss.apply(w, gl, net, target)
+        loss.backward()
+    el = time.perf_counter() - t0
+    T = ADJOINT_WORKLOADS[args.workload]
+    return {"value": K * T * DT / el, "unit": "simulated-s/wall-s (forward + backward)",
+            "h2d_bytes_per_step": w.numel() * 4 + target.nbytes, "d2h_bytes_per_step": w.numel() * 4 + 8 + 4 * 2 * T,
+            "includes": "torch.autograd.Function: W_EE upload, forward, backward, dW_EE download"}
+
+
+def adjoint_cpu_baseline(spec, seconds: float):
+    """The FP64 restatement of the same gradient (numpy, noise off) on the host cores, over a
+    bounded number of clock steps."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import adjoint_ref
+    steps = 20
+    while True:
+        t0 = time.perf_counter()
+        adjoint_ref.reference_gradient(spec, steps, np.zeros(steps), beta=0.5e-3)
+        el = time.perf_counter() - t0
+        if el > seconds / 4 or steps >= 2000:
+            break
+        steps *= 2
+    return {"value": steps * DT / el, "unit": "simulated-s/wall-s (forward + backward)", "cores": os.cpu_count(),
+            "kind": "port", "sample": f"the FP64 numpy restatement of the gradient over {steps} clock steps "
+                                      f"(noise off), BLAS threads as numpy sets them"}
+
+
 def plain_form_baseline(spec, steps=2000):
     """The plain form of the same batch: the single-network engine (FP32, the reference's
     arithmetic) stepping one instance at a time; the time per clock step of one instance of each
@@ -481,6 +597,9 @@ def run_reference(args, rank, world):
     if args.workload in BATCH_WORKLOADS:
         return {"impl": "reference", "unavailable": "the reference has no batched form (it steps one network per "
                 "process); its per-network speed is its line on the default workload"}
+    if args.workload in ADJOINT_WORKLOADS:
+        return {"impl": "reference", "unavailable": "the reference has no gradient of the simulation (forward only); "
+                "its forward speed is its line on the default workload"}
     spec_steps = 3000
     spec = bsnn.synthetic_network(args.workload, steps=spec_steps + 1, weight_values="uniform",
                                   recording_interval_steps=args.sim_steps)
@@ -528,7 +647,16 @@ def main():
         import datetime
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    if args.workload in BATCH_WORKLOADS:
+    if args.workload in ADJOINT_WORKLOADS:
+        line, state = run_adjoint(args, int(os.environ.get("LOCAL_RANK", "0")), world)
+        if rank == 0:
+            if not args.no_e2e:
+                line["e2e"] = run_adjoint_e2e(args, state)
+            if not args.no_cpu_baseline and world == 1:
+                line["cpu_baseline"] = adjoint_cpu_baseline(state[0], args.cpu_seconds)
+            print(json.dumps(line), flush=True)
+        state[3].close()
+    elif args.workload in BATCH_WORKLOADS:
         line, spec = run_batch(args, int(os.environ.get("LOCAL_RANK", "0")), world)
         if rank == 0:
             if not args.no_e2e:

@@ -308,6 +308,8 @@ SIGNATURES = {
     "bsnn_adjoint_destroy": (_I32, [_P]),
     "bsnn_adjoint_last_error": (ctypes.c_char_p, [_P]),
     "bsnn_adjoint_set_params": (_I32, [_P, _FP, ctypes.c_float]),
+    "bsnn_adjoint_get_stream": (_I32, [_P, ctypes.POINTER(_P)]),
+    "bsnn_adjoint_kernel_launches": (_I32, [_P, ctypes.POINTER(ctypes.c_uint64)]),
     "bsnn_adjoint_forward": (_I32, [_P, _FP, _FP, _FP, _FP, _FP]),
     "bsnn_adjoint_backward": (_I32, [_P, _FP, ctypes.POINTER(ctypes.c_double)]),
     "bsnn_get_info": (_I32, [_P, ctypes.POINTER(Info)]),

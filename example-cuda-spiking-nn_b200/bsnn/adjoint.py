@@ -90,6 +90,17 @@ class AdjointNetwork:
                                                     ctypes.byref(gl)))
         return g, float(gl.value)
 
+    def stream(self) -> int:
+        p = ctypes.c_void_p()
+        self._check(self._lib.bsnn_adjoint_get_stream(self._h, ctypes.byref(p)))
+        return p.value or 0
+
+    def launches(self) -> int:
+        """Kernels run so far (those of the captured graphs included)."""
+        n = ctypes.c_uint64()
+        self._check(self._lib.bsnn_adjoint_kernel_launches(self._h, ctypes.byref(n)))
+        return int(n.value)
+
     def close(self):
         if self._h:
             self._lib.bsnn_adjoint_destroy(self._h)

@@ -24,18 +24,35 @@ struct bsnn_adjoint {
     float *tv = nullptr, *tu = nullptr, *tge = nullptr, *tgi = nullptr, *tx = nullptr, *lge_all = nullptr;
     uint8_t *ts = nullptr, *tref = nullptr;
     float *lam_v = nullptr, *lam_d = nullptr, *lam_r = nullptr, *lam_x = nullptr, *lam_gi = nullptr;
+    float *c_s = nullptr, *c_v = nullptr;  // [T] loss sensitivities, uploaded before the backward pass
     float* dW = nullptr;
     double* gl_acc = nullptr;
-    double* vsum = nullptr;       // [T][vblocks] partial sums of the E voltages after each step
+    double* vsum = nullptr;       // [T][nb] per-block sums of the E voltages after each step
     uint32_t* counts = nullptr;   // [T] E spikes per step
-    float* ckpt = nullptr;        // [n_ckpt][12][N]: 11 state arrays + x
-    uint32_t n_ckpt = 0, vblocks = 0;
-    std::vector<float> v0;        // initial voltages
+    float* ckpt = nullptr;        // [n_ckpt][kAdjCkptArrays][N]
+    uint32_t n_ckpt = 0, nb = 0;
+    uint32_t ld = 0;              // row length of W_E, W_I and the lambda_g rows: N rounded up to 4
+    // one captured graph per checkpoint segment for each pass (captured on first use, dropped when
+    // g_leak changes, since the group parameters are kernel arguments)
+    std::vector<cudaGraphExec_t> fwd_graphs, bwd_graphs;
+    std::vector<size_t> fwd_nodes, bwd_nodes;  // kernels per graph
+    uint64_t launches = 0;                     // kernels run (graph nodes included)
     // forward results
     std::vector<double> rho, vbar;
     std::vector<float> rate_target, v_target;
     bool have_forward = false;
+    void drop_graphs() {
+        fwd_nodes.clear();
+        bwd_nodes.clear();
+        for (auto g : fwd_graphs)
+            if (g) cudaGraphExecDestroy(g);
+        for (auto g : bwd_graphs)
+            if (g) cudaGraphExecDestroy(g);
+        fwd_graphs.clear();
+        bwd_graphs.clear();
+    }
     ~bsnn_adjoint() {
+        drop_graphs();
         if (arena) cudaFree(arena);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -86,55 +103,80 @@ AdjGroupP adj_group(const bsnn_neuron_group_params& p) {
     return G;
 }
 
-// Partial sums of the E voltages (after a forward step) per block of 256 neurons, fixed order.
-__global__ void bsnn_adj_vsum(const float* v, uint32_t E, double* out) {
-    __shared__ double red[256];
-    const uint32_t n = blockIdx.x * 256u + threadIdx.x;
-    red[threadIdx.x] = n < E ? static_cast<double>(v[n]) : 0.0;
-    __syncthreads();
-    for (uint32_t o = 128; o > 0; o >>= 1) {
-        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
-        __syncthreads();
+// One forward step t: the neuron update (tape rows where the pointers are set; the step's E spike
+// count and voltage sums in the forward pass), then the propagation of x_{t+1}.
+void adj_step(bsnn_adjoint* a, uint32_t t, size_t tape_row, bool tape, float* x_next, bool forward) {
+    const uint32_t N = a->h.N;
+    const dim3 pg((N + kAdjBlock - 1) / kAdjBlock, 2 * kAdjChunks);
+    bsnn_adj_neuron_fwd<<<a->nb, kAdjBlock, 0, a->stream>>>(
+        a->h, t, a->part, tape ? a->tv + tape_row : nullptr, tape ? a->tu + tape_row : nullptr,
+        tape ? a->tge + tape_row : nullptr, tape ? a->tgi + tape_row : nullptr, tape ? a->ts + tape_row : nullptr,
+        tape ? a->tref + tape_row : nullptr, x_next, forward ? a->counts + t : nullptr,
+        forward ? a->vsum + static_cast<size_t>(t) * a->nb : nullptr);
+    bsnn_adj_propagate<<<pg, kAdjBlock, 0, a->stream>>>(a->WE, a->WI, a->h.E, a->h.I, N, a->ld, x_next, a->part);
+}
+
+// Forward segment c: save the checkpoint, then run its steps.
+void adj_forward_segment(bsnn_adjoint* a, uint32_t c) {
+    const uint32_t T = a->d.num_steps, C = a->d.checkpoint_interval;
+    const uint32_t t0 = c * C, t1 = std::min(T, t0 + C);
+    float* slot = a->ckpt + static_cast<size_t>(c) * kAdjCkptArrays * a->h.N;
+    bsnn_adj_save<<<a->nb, kAdjBlock, 0, a->stream>>>(a->h, a->part, a->x_cur, slot);
+    for (uint32_t t = t0; t < t1; ++t) adj_step(a, t, 0, false, a->x_cur, true);
+}
+
+// Backward segment c: restore its checkpoint, replay its steps keeping the tape, then walk them
+// backwards (neuron adjoints, pull-back of the g adjoints through the weights), then add the
+// segment's x_t lambda_ge(t)^T to dW_EE.
+void adj_backward_segment(bsnn_adjoint* a, uint32_t c) {
+    const uint32_t T = a->d.num_steps, C = a->d.checkpoint_interval, N = a->h.N, E = a->h.E;
+    const uint32_t t0 = c * C, t1 = std::min(T, t0 + C), steps = t1 - t0;
+    const float* slot = a->ckpt + static_cast<size_t>(c) * kAdjCkptArrays * N;
+    bsnn_adj_restore<<<a->nb, kAdjBlock, 0, a->stream>>>(a->h, a->part, a->tx, slot);
+    for (uint32_t k = 0; k < steps; ++k) {
+        const size_t o = static_cast<size_t>(k) * N;
+        adj_step(a, t0 + k, o, true, a->tx + o + N, false);
     }
-    if (threadIdx.x == 0) out[blockIdx.x] = red[0];
-}
-
-float** adj_state(bsnn_adjoint* a, int k) {
-    float** f[11] = {&a->h.v, &a->h.ge, &a->h.gi, &a->h.istim, &a->h.er, &a->h.ed, &a->h.ir, &a->h.id, &a->h.tr, &a->h.td,
-                     reinterpret_cast<float**>(&a->h.refrac)};
-    return f[k];
-}
-
-void adj_reset(bsnn_adjoint* a) {
-    const size_t bytes = 4ull * a->h.N;
-    for (int k = 0; k < 11; ++k) cuda_check(cudaMemsetAsync(*adj_state(a, k), 0, bytes, a->stream), "memset state");
-    cuda_check(cudaMemcpyAsync(a->h.v, a->v0.data(), bytes, cudaMemcpyHostToDevice, a->stream), "H2D v0");
-    cuda_check(cudaMemsetAsync(a->x_cur, 0, bytes, a->stream), "memset x");
-}
-
-void adj_checkpoint(bsnn_adjoint* a, uint32_t c, bool save) {
-    const size_t bytes = 4ull * a->h.N;
-    float* base = a->ckpt + static_cast<size_t>(c) * 12u * a->h.N;
-    for (int k = 0; k < 12; ++k) {
-        float* dev = k < 11 ? *adj_state(a, k) : a->x_cur;
-        float* slot = base + static_cast<size_t>(k) * a->h.N;
-        cuda_check(cudaMemcpyAsync(save ? slot : dev, save ? dev : slot, bytes, cudaMemcpyDeviceToDevice, a->stream),
-                   "checkpoint copy");
+    const float beta = a->d.surrogate_beta;
+    for (uint32_t k = steps; k-- > 0;) {
+        const size_t o = static_cast<size_t>(k) * N;
+        float* lge = a->lge_all + static_cast<size_t>(k) * a->ld;
+        bsnn_adj_neuron_bwd<<<a->nb, kAdjBlock, 0, a->stream>>>(
+            a->h, a->tv + o, a->tu + o, a->tge + o, a->tgi + o, a->ts + o, a->tref + o, a->lam_v, a->lam_d, a->lam_r,
+            a->lam_x, a->c_s + t0 + k, a->c_v + t0 + k, beta, lge, a->lam_gi, a->gl_acc);
+        // lambda_x(t) = W lambda_g(t), used by step t - 1
+        bsnn_adj_pullback<<<(N * 32 + 255) / 256, 256, 0, a->stream>>>(a->WE, a->WI, E, N, a->ld, lge, a->lam_gi,
+                                                                       a->lam_x);
     }
+    const dim3 og((E + 31) / 32, (E + 31) / 32);
+    bsnn_adj_outer<<<og, 256, 0, a->stream>>>(a->tx, N, a->lge_all, a->ld, steps, E, a->dW);
 }
 
-// One forward step t: neuron update (tape rows at the given pointers), then g += W^T x_{t+1}.
-void adj_step(bsnn_adjoint* a, uint32_t t, float* tv, float* tu, float* tge, float* tgi, uint8_t* ts, uint8_t* tref,
-              float* x_next) {
-    const uint32_t N = a->h.N, E = a->h.E, I = a->h.I;
-    const uint32_t nb = (N + 255) / 256;
-    bsnn_adj_neuron_fwd<<<nb, 256, 0, a->stream>>>(a->h, t, tv, tu, tge, tgi, ts, tref, x_next, a->counts + t);
-    const dim3 pg((N + 255) / 256, kAdjChunks);
-    bsnn_adj_propagate<<<pg, 256, 0, a->stream>>>(a->WE, E, N, x_next, a->part);
-    bsnn_adj_reduce<<<nb, 256, 0, a->stream>>>(a->part, kAdjChunks, N, a->h.ge);
-    bsnn_adj_propagate<<<pg, 256, 0, a->stream>>>(a->WI, I, N, x_next + E, a->part);
-    bsnn_adj_reduce<<<nb, 256, 0, a->stream>>>(a->part, kAdjChunks, N, a->h.gi);
-    cuda_check(cudaGetLastError(), "adjoint forward step");
+// Captures fn(c) for every segment c into one graph each (once), then launches them in `order`.
+template <class F>
+void adj_run_graphs(bsnn_adjoint* a, std::vector<cudaGraphExec_t>& graphs, std::vector<size_t>& nodes, bool reverse,
+                    F&& fn, const char* what) {
+    if (graphs.empty()) {
+        graphs.assign(a->n_ckpt, nullptr);
+        nodes.assign(a->n_ckpt, 0);
+        for (uint32_t c = 0; c < a->n_ckpt; ++c) {
+            cudaGraph_t g = nullptr;
+            cuda_check(cudaStreamBeginCapture(a->stream, cudaStreamCaptureModeThreadLocal), what);
+            fn(c);
+            const cudaError_t launch_err = cudaGetLastError();
+            cuda_check(cudaStreamEndCapture(a->stream, &g), what);
+            cuda_check(launch_err, what);
+            cudaGraphGetNodes(g, nullptr, &nodes[c]);
+            const cudaError_t ie = cudaGraphInstantiate(&graphs[c], g, 0);
+            cudaGraphDestroy(g);
+            cuda_check(ie, what);
+        }
+    }
+    for (uint32_t k = 0; k < a->n_ckpt; ++k) {
+        const uint32_t c = reverse ? a->n_ckpt - 1 - k : k;
+        cuda_check(cudaGraphLaunch(graphs[c], a->stream), what);
+        a->launches += nodes[c];
+    }
 }
 
 }  // namespace
@@ -184,7 +226,9 @@ BSNN_API bsnn_status bsnn_adjoint_create(const bsnn_adjoint_desc* desc, const bs
             h.norm[sd] = cp[sd]->postsynaptic_kernel_normalization_value;
         }
         a->n_ckpt = (T + C - 1) / C;
-        a->vblocks = (E + 255) / 256;
+        a->nb = (N + kAdjBlock - 1) / kAdjBlock;
+        a->ld = (N + 3u) & ~3u;
+        const uint32_t ld = a->ld;
         // stimulus CSR
         std::vector<std::vector<std::pair<uint32_t, float>>> per(stimulus_steps);
         size_t e = 0;
@@ -209,25 +253,29 @@ BSNN_API bsnn_status bsnn_adjoint_create(const bsnn_adjoint_desc* desc, const bs
         const size_t fN = 4ull * N;
         size_t o_state[11];
         for (auto& o : o_state) o = A.take(fN);
-        const size_t o_we = A.take(4ull * E * N), o_wi = A.take(4ull * I * N);
-        const size_t o_part = A.take(4ull * kAdjChunks * N), o_x = A.take(fN);
+        const size_t o_cs = A.take(4ull * T), o_cv = A.take(4ull * T);
+        const size_t o_we = A.take(4ull * E * ld), o_wi = A.take(4ull * I * ld);
+        const size_t o_part = A.take(4ull * 2 * kAdjChunks * N), o_x = A.take(fN);
         const size_t o_tv = A.take(fN * C), o_tu = A.take(fN * C), o_tge = A.take(fN * C), o_tgi = A.take(fN * C);
-        const size_t o_tx = A.take(fN * (C + 1)), o_lge = A.take(fN * C);
+        const size_t o_tx = A.take(fN * (C + 1)), o_lge = A.take(4ull * ld * C);
         const size_t o_ts = A.take(static_cast<size_t>(N) * C), o_tref = A.take(static_cast<size_t>(N) * C);
-        const size_t o_lv = A.take(fN), o_ld = A.take(fN), o_lr = A.take(fN), o_lx = A.take(fN), o_lgi = A.take(fN);
+        const size_t o_lv = A.take(fN), o_ld = A.take(fN), o_lr = A.take(fN), o_lx = A.take(fN), o_lgi = A.take(4ull * ld);
         const size_t o_dw = A.take(4ull * E * E);
-        const uint32_t nb = (N + 255) / 256;
-        const size_t o_gl = A.take(8ull * nb);
-        const size_t o_vs = A.take(8ull * a->vblocks * T);
+        const size_t o_gl = A.take(8ull * a->nb);
+        const size_t o_vs = A.take(8ull * a->nb * T);
         const size_t o_cnt = A.take(4ull * T);
-        const size_t o_ck = A.take(fN * 12u * a->n_ckpt);
+        const size_t o_ck = A.take(fN * kAdjCkptArrays * a->n_ckpt);
         const size_t o_soff = A.take(4ull * soff.size()), o_evn = A.take(4ull * std::max<size_t>(evn.size(), 1)),
                      o_evd = A.take(4ull * std::max<size_t>(evd.size(), 1));
         cuda_check(cudaMalloc(&a->arena, A.size), "cudaMalloc adjoint arena");
         unsigned char* base = a->arena;
         cuda_check(cudaMemset(base, 0, A.size), "cudaMemset adjoint arena");
         auto F = [&](size_t o) { return reinterpret_cast<float*>(base + o); };
-        for (int k = 0; k < 11; ++k) *adj_state(a.get(), k) = F(o_state[k]);
+        float** state[10] = {&h.v, &h.ge, &h.gi, &h.istim, &h.er, &h.ed, &h.ir, &h.id, &h.tr, &h.td};
+        for (int k = 0; k < 10; ++k) *state[k] = F(o_state[k]);
+        h.refrac = reinterpret_cast<uint32_t*>(base + o_state[10]);
+        a->c_s = F(o_cs);
+        a->c_v = F(o_cv);
         a->WE = F(o_we);
         a->WI = F(o_wi);
         h.WE = a->WE;
@@ -261,20 +309,20 @@ BSNN_API bsnn_status bsnn_adjoint_create(const bsnn_adjoint_desc* desc, const bs
             cuda_check(cudaMemcpy(base + o_evn, evn.data(), 4ull * evn.size(), cudaMemcpyHostToDevice), "H2D");
             cuda_check(cudaMemcpy(base + o_evd, evd.data(), 4ull * evd.size(), cudaMemcpyHostToDevice), "H2D");
         }
-        // W_E = [W_EE | W_EI], W_I = [W_IE | W_II], row-major [pre][N]
-        std::vector<float> row(N);
+        // W_E = [W_EE | W_EI], W_I = [W_IE | W_II], row-major [pre][ld], zero beyond N
+        std::vector<float> row(ld, 0.0f);
         for (uint32_t i = 0; i < E; ++i) {
             std::memcpy(row.data(), w_ee + static_cast<size_t>(i) * E, 4ull * E);
             std::memcpy(row.data() + E, w_ei + static_cast<size_t>(i) * I, 4ull * I);
-            cuda_check(cudaMemcpy(a->WE + static_cast<size_t>(i) * N, row.data(), fN, cudaMemcpyHostToDevice), "H2D W");
+            cuda_check(cudaMemcpy(a->WE + static_cast<size_t>(i) * ld, row.data(), 4ull * ld, cudaMemcpyHostToDevice),
+                       "H2D W");
         }
         for (uint32_t i = 0; i < I; ++i) {
             std::memcpy(row.data(), w_ie + static_cast<size_t>(i) * E, 4ull * E);
             std::memcpy(row.data() + E, w_ii + static_cast<size_t>(i) * I, 4ull * I);
-            cuda_check(cudaMemcpy(a->WI + static_cast<size_t>(i) * N, row.data(), fN, cudaMemcpyHostToDevice), "H2D W");
+            cuda_check(cudaMemcpy(a->WI + static_cast<size_t>(i) * ld, row.data(), 4ull * ld, cudaMemcpyHostToDevice),
+                       "H2D W");
         }
-        a->v0.resize(N);
-        for (uint32_t n = 0; n < N; ++n) a->v0[n] = n < E ? e_group->v_rest : i_group->v_rest;
         *out = a.release();
     });
 }
@@ -289,17 +337,34 @@ BSNN_API bsnn_status bsnn_adjoint_destroy(bsnn_adjoint* a) {
 
 BSNN_API const char* bsnn_adjoint_last_error(const bsnn_adjoint* a) { return a ? a->err.c_str() : g_thread_error.c_str(); }
 
+BSNN_API bsnn_status bsnn_adjoint_get_stream(bsnn_adjoint* a, void** out_stream) {
+    if (!a || !out_stream) return BSNN_ERR_INVALID_ARGUMENT;
+    *out_stream = a->stream;
+    return BSNN_OK;
+}
+
+BSNN_API bsnn_status bsnn_adjoint_kernel_launches(bsnn_adjoint* a, uint64_t* out) {
+    if (!a || !out) return BSNN_ERR_INVALID_ARGUMENT;
+    *out = a->launches;
+    return BSNN_OK;
+}
+
 // New parameter values: the E->E weights (row-major [E][E]; null keeps them) and g_leak of both
 // groups (a NaN keeps it).
 BSNN_API bsnn_status bsnn_adjoint_set_params(bsnn_adjoint* a, const float* w_ee, float g_leak) {
     if (!a) return BSNN_ERR_INVALID_ARGUMENT;
     return guarded_adj(a, [&] {
-        const uint32_t E = a->h.E, N = a->h.N;
-        if (w_ee)
-            cuda_check(cudaMemcpy2D(a->WE, 4ull * N, w_ee, 4ull * E, 4ull * E, E, cudaMemcpyHostToDevice), "H2D W_EE");
-        if (!std::isnan(g_leak)) {
+        const uint32_t E = a->h.E;
+        if (w_ee) {
+            cuda_check(cudaStreamSynchronize(a->stream), "adjoint sync");
+            cuda_check(cudaMemcpy2D(a->WE, 4ull * a->ld, w_ee, 4ull * E, 4ull * E, E, cudaMemcpyHostToDevice),
+                       "H2D W_EE");
+        }
+        if (!std::isnan(g_leak) && (g_leak != a->h.g[0].g_leak || g_leak != a->h.g[1].g_leak)) {
+            cuda_check(cudaStreamSynchronize(a->stream), "adjoint sync");
             a->h.g[0].g_leak = g_leak;
             a->h.g[1].g_leak = g_leak;
+            a->drop_graphs();
         }
         a->have_forward = false;
     });
@@ -311,20 +376,17 @@ BSNN_API bsnn_status bsnn_adjoint_forward(bsnn_adjoint* a, const float* rate_tar
                                           float* loss_out, float* rate_out, float* mean_voltage_out) {
     if (!a) return BSNN_ERR_INVALID_ARGUMENT;
     return guarded_adj(a, [&] {
-        const uint32_t T = a->d.num_steps, C = a->d.checkpoint_interval, N = a->h.N, E = a->h.E;
+        const uint32_t T = a->d.num_steps, E = a->h.E;
         require(rate_target != nullptr, BSNN_ERR_INVALID_ARGUMENT, "null rate target");
         require(voltage_target != nullptr || !(a->d.voltage_weight != 0.0f), BSNN_ERR_INVALID_ARGUMENT,
                 "null voltage target with a voltage weight");
-        adj_reset(a);
+        bsnn_adj_restore<<<a->nb, kAdjBlock, 0, a->stream>>>(a->h, a->part, a->x_cur, nullptr);
         cuda_check(cudaMemsetAsync(a->counts, 0, 4ull * T, a->stream), "memset counts");
-        for (uint32_t t = 0; t < T; ++t) {
-            if (t % C == 0) adj_checkpoint(a, t / C, true);
-            // tape rows go to slot 0 (not kept in the forward pass); x_{t+1} into x_cur
-            adj_step(a, t, a->tv, a->tu, a->tge, a->tgi, a->ts, a->tref, a->x_cur);
-            bsnn_adj_vsum<<<a->vblocks, 256, 0, a->stream>>>(a->h.v, E, a->vsum + static_cast<size_t>(t) * a->vblocks);
-        }
+        a->launches += 1;
+        adj_run_graphs(a, a->fwd_graphs, a->fwd_nodes, false, [&](uint32_t c) { adj_forward_segment(a, c); },
+                       "adjoint forward");
         std::vector<uint32_t> cnt(T);
-        std::vector<double> vs(static_cast<size_t>(T) * a->vblocks);
+        std::vector<double> vs(static_cast<size_t>(T) * a->nb);
         cuda_check(cudaMemcpyAsync(cnt.data(), a->counts, 4ull * T, cudaMemcpyDeviceToHost, a->stream), "D2H counts");
         cuda_check(cudaMemcpyAsync(vs.data(), a->vsum, 8ull * vs.size(), cudaMemcpyDeviceToHost, a->stream), "D2H vsum");
         cuda_check(cudaStreamSynchronize(a->stream), "adjoint forward");
@@ -339,7 +401,7 @@ BSNN_API bsnn_status bsnn_adjoint_forward(bsnn_adjoint* a, const float* rate_tar
             rho = ka * rho + (1.0 - ka) * static_cast<double>(cnt[t]) / (static_cast<double>(E) * dt);
             a->rho[t] = rho;
             double s = 0.0;
-            for (uint32_t b = 0; b < a->vblocks; ++b) s += vs[static_cast<size_t>(t) * a->vblocks + b];
+            for (uint32_t b = 0; b < a->nb; ++b) s += vs[static_cast<size_t>(t) * a->nb + b];
             a->vbar[t] = s / E;
             const double er = rho - rate_target[t], ev = a->vbar[t] - a->v_target[t];
             loss += a->d.rate_weight * er * er + a->d.voltage_weight * ev * ev;
@@ -348,7 +410,6 @@ BSNN_API bsnn_status bsnn_adjoint_forward(bsnn_adjoint* a, const float* rate_tar
         }
         if (loss_out) *loss_out = static_cast<float>(loss / T);
         a->have_forward = true;
-        (void)N;
     });
 }
 
@@ -357,9 +418,8 @@ BSNN_API bsnn_status bsnn_adjoint_backward(bsnn_adjoint* a, float* grad_w_ee, do
     if (!a) return BSNN_ERR_INVALID_ARGUMENT;
     return guarded_adj(a, [&] {
         require(a->have_forward, BSNN_ERR_STATE, "run bsnn_adjoint_forward first");
-        const uint32_t T = a->d.num_steps, C = a->d.checkpoint_interval, N = a->h.N, E = a->h.E, I = a->h.I;
+        const uint32_t T = a->d.num_steps, N = a->h.N, E = a->h.E;
         const size_t fN = 4ull * N;
-        const uint32_t nb = (N + 255) / 256;
         const double dt = a->h.g[0].timestep, ka = std::exp(-dt / static_cast<double>(a->d.rate_tau));
         // the loss's sensitivities to the step's E spikes (through rho) and to vbar_{t+1}
         std::vector<float> c_s(T), c_v(T);
@@ -369,40 +429,16 @@ BSNN_API bsnn_status bsnn_adjoint_backward(bsnn_adjoint* a, float* grad_w_ee, do
             c_s[t] = static_cast<float>(lrho * (1.0 - ka) / (static_cast<double>(E) * dt));
             c_v[t] = static_cast<float>(a->d.voltage_weight * 2.0 / T * (a->vbar[t] - a->v_target[t]) / E);
         }
+        cuda_check(cudaMemcpyAsync(a->c_s, c_s.data(), 4ull * T, cudaMemcpyHostToDevice, a->stream), "H2D c_s");
+        cuda_check(cudaMemcpyAsync(a->c_v, c_v.data(), 4ull * T, cudaMemcpyHostToDevice, a->stream), "H2D c_v");
         for (float* p : {a->lam_v, a->lam_d, a->lam_r, a->lam_x})
             cuda_check(cudaMemsetAsync(p, 0, fN, a->stream), "memset adjoints");
         cuda_check(cudaMemsetAsync(a->dW, 0, 4ull * E * E, a->stream), "memset dW");
-        cuda_check(cudaMemsetAsync(a->gl_acc, 0, 8ull * nb, a->stream), "memset g_leak");
-        const float beta = a->d.surrogate_beta;
-        for (uint32_t c = a->n_ckpt; c-- > 0;) {
-            const uint32_t t0 = c * C, t1 = std::min(T, t0 + C), steps = t1 - t0;
-            // replay the segment, keeping every step's tape row
-            adj_checkpoint(a, c, false);
-            cuda_check(cudaMemcpyAsync(a->tx, a->x_cur, fN, cudaMemcpyDeviceToDevice, a->stream), "x_t0");
-            for (uint32_t k = 0; k < steps; ++k) {
-                const size_t o = static_cast<size_t>(k) * N;
-                adj_step(a, t0 + k, a->tv + o, a->tu + o, a->tge + o, a->tgi + o, a->ts + o, a->tref + o,
-                         a->tx + o + N);
-            }
-            // backwards through the segment
-            for (uint32_t k = steps; k-- > 0;) {
-                const size_t o = static_cast<size_t>(k) * N;
-                float* lge = a->lge_all + o;
-                bsnn_adj_neuron_bwd<<<nb, 256, 0, a->stream>>>(a->h, a->tv + o, a->tu + o, a->tge + o, a->tgi + o,
-                                                               a->ts + o, a->tref + o, a->lam_v, a->lam_d, a->lam_r,
-                                                               a->lam_x, c_s[t0 + k], c_v[t0 + k], beta, lge, a->lam_gi,
-                                                               a->gl_acc);
-                // lambda_x(t) = W lambda_g(t), for step t - 1
-                bsnn_adj_pullback<<<(E * 32 + 255) / 256, 256, 0, a->stream>>>(a->WE, E, N, lge, a->lam_x);
-                bsnn_adj_pullback<<<(I * 32 + 255) / 256, 256, 0, a->stream>>>(a->WI, I, N, a->lam_gi, a->lam_x + E);
-            }
-            // dW_EE += sum over the segment of x_t lambda_ge(t)^T
-            const dim3 og((E + 31) / 32, (E + 31) / 32);
-            bsnn_adj_outer<<<og, 256, 0, a->stream>>>(a->tx, a->lge_all, steps, N, E, a->dW);
-            cuda_check(cudaGetLastError(), "adjoint backward segment");
-        }
-        std::vector<double> gl(nb);
-        cuda_check(cudaMemcpyAsync(gl.data(), a->gl_acc, 8ull * nb, cudaMemcpyDeviceToHost, a->stream), "D2H g_leak");
+        cuda_check(cudaMemsetAsync(a->gl_acc, 0, 8ull * a->nb, a->stream), "memset g_leak");
+        adj_run_graphs(a, a->bwd_graphs, a->bwd_nodes, true, [&](uint32_t c) { adj_backward_segment(a, c); },
+                       "adjoint backward");
+        std::vector<double> gl(a->nb);
+        cuda_check(cudaMemcpyAsync(gl.data(), a->gl_acc, 8ull * a->nb, cudaMemcpyDeviceToHost, a->stream), "D2H g_leak");
         if (grad_w_ee)
             cuda_check(cudaMemcpyAsync(grad_w_ee, a->dW, 4ull * E * E, cudaMemcpyDeviceToHost, a->stream), "D2H dW");
         cuda_check(cudaStreamSynchronize(a->stream), "adjoint backward");

@@ -458,6 +458,10 @@ BSNN_API bsnn_status bsnn_adjoint_create(const bsnn_adjoint_desc* desc, const bs
                                          uint32_t num_events, int32_t device, bsnn_adjoint** out_adjoint);
 BSNN_API bsnn_status bsnn_adjoint_destroy(bsnn_adjoint* adjoint);
 BSNN_API const char* bsnn_adjoint_last_error(const bsnn_adjoint* adjoint);
+/* The stream the passes run on (cudaStream_t), and the number of kernels run so far (the kernels
+ * of the captured per-segment graphs included). */
+BSNN_API bsnn_status bsnn_adjoint_get_stream(bsnn_adjoint* adjoint, void** out_stream);
+BSNN_API bsnn_status bsnn_adjoint_kernel_launches(bsnn_adjoint* adjoint, uint64_t* out);
 /* New E->E weights (row-major [E][E]; null keeps them) and g_leak (NaN keeps it). */
 BSNN_API bsnn_status bsnn_adjoint_set_params(bsnn_adjoint* adjoint, const float* w_ee, float g_leak);
 /* Forward pass over num_steps: targets of num_steps values (voltage_target may be null when
