@@ -268,6 +268,8 @@ class BatchInfo(ctypes.Structure):
         ("weight_bytes", ctypes.c_uint64),
         ("kernel_launches", ctypes.c_uint64),
         ("smem_bytes", ctypes.c_uint64),
+        ("state_in_smem", ctypes.c_uint32),
+        ("operand_stages", ctypes.c_uint32),
     ]
 
 

@@ -48,6 +48,7 @@ struct bsnn_batch {
     uint32_t steps_per_launch = 1000;
     std::map<uint32_t, cudaGraphExec_t> graphs;
     float* scratch = nullptr;  // [2][max N] for reads of g with the pending propagation
+    const void* kernel = nullptr;  // bsnn_batch_kernel<state in shared memory or not>
 
     ~bsnn_batch() {
         for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
@@ -92,9 +93,8 @@ BGroupP batch_group(const bsnn_neuron_group_params& p) {
     G.refractory_steps = p.refractory_steps;
     G.has_bg_e = p.mean_background_excitatory_spikes > 0.0f;
     G.has_bg_i = p.mean_background_inhibitory_spikes > 0.0f;
-    G.timestep = p.timestep;
+    G.dt_c = p.timestep / p.membrane_capacitance;  // the quotient the reference forms every step
     G.g_leak = p.g_leak;
-    G.cap = p.membrane_capacitance;
     G.delta_t = p.depolarization_slope_factor;
     G.v_eff = p.v_effective_spike_threshold;
     G.e_exc = p.v_excitatory_reversal;
@@ -182,25 +182,14 @@ void batch_finalize(bsnn_batch* b) {
         }
     }
     h.n_units = static_cast<uint32_t>(units.size());
-    // longest first onto the least loaded CTA (cost: K tiles plus the epilogue)
+    // longest first: CTAs take units from a shared dispenser in this order
     std::vector<uint32_t> order(units.size());
     std::iota(order.begin(), order.end(), 0u);
     auto cost = [&](uint32_t u) { return static_cast<double>(units[u].k1 - units[u].k0) + 2.0; };
     std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t c) { return cost(a) > cost(c); });
-    std::vector<double> load(n_ctas, 0.0);
-    std::vector<std::vector<uint32_t>> per_cta(n_ctas);
-    for (uint32_t u : order) {
-        const uint32_t k = static_cast<uint32_t>(std::min_element(load.begin(), load.end()) - load.begin());
-        load[k] += cost(u);
-        per_cta[k].push_back(u);
-    }
-    std::vector<BUnit> units_cta;  // in CTA order
-    std::vector<uint32_t> cta_units(n_ctas + 1, 0);
-    for (uint32_t k = 0; k < n_ctas; ++k) {
-        cta_units[k] = static_cast<uint32_t>(units_cta.size());
-        for (uint32_t u : per_cta[k]) units_cta.push_back(units[u]);
-    }
-    cta_units[n_ctas] = static_cast<uint32_t>(units_cta.size());
+    std::vector<BUnit> units_sorted;
+    units_sorted.reserve(units.size());
+    for (uint32_t u : order) units_sorted.push_back(units[u]);
 
     // Stimulus: one CSR over all instances, events of a step sorted by neuron.
     uint32_t stim_len = 0;
@@ -227,14 +216,14 @@ void batch_finalize(bsnn_batch* b) {
     // Arena.
     Arena A;
     const size_t fN = sizeof(float) * n_neurons;
-    size_t o_state[10];
+    size_t o_state[8];
     for (auto& o : o_state) o = A.take(fN);
     const size_t o_ref = A.take(sizeof(uint32_t) * n_neurons), o_spk = A.take(sizeof(uint32_t) * n_neurons);
     const size_t o_cnt = A.take(sizeof(unsigned long long) * 2 * h.n_inst);
     const size_t o_pns = A.take(sizeof(unsigned long long) * 8 * n_ctas);
     const size_t o_inst = A.take(sizeof(BInst) * h.n_inst);
-    const size_t o_units = A.take(sizeof(BUnit) * units_cta.size());
-    const size_t o_cta = A.take(sizeof(uint32_t) * cta_units.size());
+    const size_t o_units = A.take(sizeof(BUnit) * units_sorted.size());
+    const size_t o_ctr = A.take(sizeof(unsigned long long));
     const size_t o_part = A.take(sizeof(float) * std::max<size_t>(part_floats, 1));
     size_t o_a[kBatchMaxClasses][2], o_x[kBatchMaxClasses][2];
     for (uint32_t c = 0; c < h.n_classes; ++c)
@@ -257,8 +246,8 @@ void batch_finalize(bsnn_batch* b) {
     unsigned char* base = b->arena;
     cuda_check(cudaMemset(base, 0, A.size), "cudaMemset batch arena");
     auto F = [&](size_t o) { return reinterpret_cast<float*>(base + o); };
-    float** fields[10] = {&h.v, &h.ge, &h.gi, &h.istim, &h.er, &h.ed, &h.ir, &h.id, &h.tr, &h.td};
-    for (int k = 0; k < 10; ++k) *fields[k] = F(o_state[k]);
+    float** fields[8] = {&h.v, &h.istim, &h.er, &h.ed, &h.ir, &h.id, &h.tr, &h.td};
+    for (int k = 0; k < 8; ++k) *fields[k] = F(o_state[k]);
     h.refrac = reinterpret_cast<uint32_t*>(base + o_ref);
     h.spikes = reinterpret_cast<uint32_t*>(base + o_spk);
     h.spike_counts = reinterpret_cast<unsigned long long*>(base + o_cnt);
@@ -288,13 +277,12 @@ void batch_finalize(bsnn_batch* b) {
     h.phase_ns = reinterpret_cast<unsigned long long*>(base + o_pns);
     h.inst = reinterpret_cast<const BInst*>(base + o_inst);
     h.units = reinterpret_cast<const BUnit*>(base + o_units);
-    h.cta_units = reinterpret_cast<const uint32_t*>(base + o_cta);
+    h.unit_ctr = reinterpret_cast<unsigned long long*>(base + o_ctr);
     cuda_check(cudaMemcpy(base + o_inst, inst.data(), sizeof(BInst) * inst.size(), cudaMemcpyHostToDevice), "H2D");
     cuda_check(cudaMemcpy(h.v, v0.data(), fN, cudaMemcpyHostToDevice), "H2D v");
-    cuda_check(cudaMemcpy(base + o_units, units_cta.data(), sizeof(BUnit) * units_cta.size(), cudaMemcpyHostToDevice),
+    cuda_check(cudaMemcpy(base + o_units, units_sorted.data(), sizeof(BUnit) * units_sorted.size(),
+                          cudaMemcpyHostToDevice),
                "H2D units");
-    cuda_check(cudaMemcpy(base + o_cta, cta_units.data(), sizeof(uint32_t) * cta_units.size(), cudaMemcpyHostToDevice),
-               "H2D unit ranges");
     for (uint32_t c = 0; c < h.n_classes; ++c)
         for (int sd = 0; sd < 2; ++sd) {
             h.cls[c].A[sd] = reinterpret_cast<const uint16_t*>(base + o_a[c][sd]);
@@ -313,22 +301,55 @@ void batch_finalize(bsnn_batch* b) {
         cuda_check(cudaMemcpy(base + o_evd, ev_delta.data(), sizeof(float) * ev_delta.size(), cudaMemcpyHostToDevice), "H2D");
     }
     b->d_sim = reinterpret_cast<BSim*>(base + o_sim);
-    cuda_check(cudaMemcpy(b->d_sim, &h, sizeof(BSim), cudaMemcpyHostToDevice), "H2D batch sim");
     b->grid = n_ctas;
+    // Shared memory: the operand ring, then optionally the instance table and the CTA's neuron
+    // state.  Keeping the state resident matters most (phase A then touches global memory only
+    // for the partial sums and x), then at least three stages, then the table.
     uint32_t max_b = 0;
     for (uint32_t c = 0; c < h.n_classes; ++c) max_b = std::max(max_b, 2u * h.cls[c].NP * 128u);
     h.stage_bytes = (kATileBytes + max_b + 1023u) & ~1023u;
-    b->smem = kBatchStages * h.stage_bytes + sizeof(BInst) * h.n_inst;
+    h.per_cta = (n_neurons + n_ctas - 1) / n_ctas;
     int optin = 0;
     cuda_check(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device), "smem attr");
-    require(b->smem + 4096 <= static_cast<size_t>(optin), BSNN_ERR_INVALID_ARGUMENT,
-            "batch too large: the instance table and the operand stages do not fit in shared memory");
+    const size_t avail = static_cast<size_t>(optin) - 4096;  // the kernel's static shared memory
+    const size_t table_bytes = sizeof(BInst) * h.n_inst;
+    const size_t state_bytes = (static_cast<size_t>(h.per_cta) * (9u * 4u + 1u) + 15u) & ~size_t(15);
+    const size_t noise_bytes = sizeof(uint16_t) * h.per_cta;  // the next step's Poisson counts
+    const char* env_state = std::getenv("BSNN_BATCH_STATE");    // "global": keep the state in global memory
+    const char* env_stages = std::getenv("BSNN_BATCH_STAGES");  // 2 .. 4
+    const bool allow_smem_state = !(env_state && std::string(env_state) == "global");
+    const uint32_t forced_stages = env_stages ? static_cast<uint32_t>(std::atoi(env_stages)) : 0u;
+    struct Choice { uint32_t state, stages, table; };
+    const Choice choices[] = {{1, 4, 1}, {1, 3, 1}, {1, 4, 0}, {1, 3, 0}, {1, 2, 1}, {1, 2, 0},
+                              {0, 4, 1}, {0, 3, 1}, {0, 4, 0}, {0, 3, 0}, {0, 2, 1}, {0, 2, 0}};
+    bool placed = false;
+    for (const Choice& ch : choices) {
+        if (ch.state && !allow_smem_state) continue;
+        if (forced_stages && ch.stages != forced_stages) continue;
+        const size_t ring = static_cast<size_t>(ch.stages) * h.stage_bytes;
+        const size_t noise_off = (ring + (ch.table ? table_bytes : 0) + 15u) & ~size_t(15);
+        const size_t state_off = (noise_off + noise_bytes + 15u) & ~size_t(15);
+        const size_t need = state_off + (ch.state ? state_bytes : 0);
+        if (need > avail) continue;
+        h.n_stages = ch.stages;
+        h.inst_in_smem = ch.table;
+        h.state_in_smem = ch.state;
+        h.state_off = static_cast<uint32_t>(state_off);
+        h.noise_off = static_cast<uint32_t>(noise_off);
+        b->smem = need;
+        placed = true;
+        break;
+    }
+    require(placed, BSNN_ERR_INVALID_ARGUMENT, "batch too large: the operand stages do not fit in shared memory");
     cuda_check(cudaMemcpy(b->d_sim, &h, sizeof(BSim), cudaMemcpyHostToDevice), "H2D batch sim");
-    cuda_check(cudaFuncSetAttribute(reinterpret_cast<const void*>(&bsnn_batch_kernel),
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(b->smem)),
+    b->kernel = h.state_in_smem ? reinterpret_cast<const void*>(&bsnn_batch_kernel<true>)
+                                : reinterpret_cast<const void*>(&bsnn_batch_kernel<false>);
+    // the limit is per function and shared by every batch in the process: allow the most any
+    // batch may use, so one batch's smaller setting never invalidates another's launches
+    cuda_check(cudaFuncSetAttribute(b->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(avail)),
                "batch smem");
     int per_sm = 0;
-    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, reinterpret_cast<const void*>(&bsnn_batch_kernel),
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, b->kernel,
                                                              kBatchThreads, b->smem),
                "batch occupancy");
     require(per_sm >= 1, BSNN_ERR_RUNTIME, "batch kernel does not fit on an SM");
@@ -367,7 +388,7 @@ void batch_launch(bsnn_batch* b, uint32_t n_steps) {
         cfg.numAttrs = 1;
         const BSim* arg0 = b->d_sim;
         void* args[2] = {&arg0, &n_steps};
-        const cudaError_t le = cudaLaunchKernelExC(&cfg, reinterpret_cast<const void*>(&bsnn_batch_kernel), args);
+        const cudaError_t le = cudaLaunchKernelExC(&cfg, b->kernel, args);
         const cudaError_t ce = cudaStreamEndCapture(b->stream, &graph);
         cuda_check(le, "batch launch (capture)");
         cuda_check(ce, "batch end capture");
@@ -550,8 +571,7 @@ BSNN_API bsnn_status bsnn_batch_read_state(bsnn_batch* b, uint32_t instance, int
             case BSNN_FIELD_I_STIMULUS: copy(h.istim); return;
             case BSNN_FIELD_REFRACTORY_COUNTER: copy(h.refrac); return;
             case BSNN_FIELD_SPIKES: copy(h.spikes); return;
-            case BSNN_FIELD_BG_G_EXCITATORY: copy(h.ge); return;
-            case BSNN_FIELD_BG_G_INHIBITORY: copy(h.gi); return;
+
             case BSNN_FIELD_BG_E_R_TRACES: copy(h.er); return;
             case BSNN_FIELD_BG_E_D_TRACES: copy(h.ed); return;
             case BSNN_FIELD_BG_I_R_TRACES: copy(h.ir); return;
@@ -567,12 +587,16 @@ BSNN_API bsnn_status bsnn_batch_read_state(bsnn_batch* b, uint32_t instance, int
                 return;
             }
             case BSNN_FIELD_G_EXCITATORY:
-            case BSNN_FIELD_G_INHIBITORY: {
-                bsnn_batch_gsum_kernel<<<(n + 255) / 256, 256, 0, b->stream>>>(b->d_sim, instance, b->scratch,
-                                                                               b->scratch + n);
+            case BSNN_FIELD_G_INHIBITORY:
+            case BSNN_FIELD_BG_G_EXCITATORY:
+            case BSNN_FIELD_BG_G_INHIBITORY: {
+                const bool with_pending = field == BSNN_FIELD_G_EXCITATORY || field == BSNN_FIELD_G_INHIBITORY;
+                const bool exc = field == BSNN_FIELD_G_EXCITATORY || field == BSNN_FIELD_BG_G_EXCITATORY;
+                bsnn_batch_g_kernel<<<(n + 255) / 256, 256, 0, b->stream>>>(b->d_sim, instance, with_pending ? 1 : 0,
+                                                                            b->scratch, b->scratch + n);
                 cuda_check(cudaGetLastError(), "batch g read");
-                cuda_check(cudaMemcpyAsync(host_out, b->scratch + (field == BSNN_FIELD_G_EXCITATORY ? 0 : n), 4ull * n,
-                                           cudaMemcpyDeviceToHost, b->stream),
+                cuda_check(cudaMemcpyAsync(host_out, b->scratch + (exc ? 0 : n), 4ull * n, cudaMemcpyDeviceToHost,
+                                           b->stream),
                            "D2H g");
                 cuda_check(cudaStreamSynchronize(b->stream), "sync");
                 return;
@@ -611,6 +635,8 @@ BSNN_API bsnn_status bsnn_batch_get_info(bsnn_batch* b, bsnn_batch_info* out) {
         i.weight_bytes = wb;
         i.kernel_launches = b->launches;
         i.smem_bytes = b->smem;
+        i.state_in_smem = b->h.state_in_smem;
+        i.operand_stages = b->h.n_stages;
         *out = i;
     });
 }

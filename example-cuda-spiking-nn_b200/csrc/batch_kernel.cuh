@@ -28,6 +28,17 @@
 //     unit's partial sums.
 //   grid barrier
 //
+// Each CTA steps a fixed contiguous range of neurons.  When the range's state fits beside the
+// operand stages, it stays in shared memory for the whole launch (loaded at the start, written
+// back at the end), so phase A's only global traffic is the partial sums in and x out, and the
+// weight tiles have L2 to themselves; otherwise phase A reads and writes the state in global
+// memory.  The stored background conductance is not kept: it is recomputed as (d - r) * scale
+// from the background traces, the same expression that produced it.
+//
+// The background Poisson counts of a step depend only on (instance seed, neuron, step), so the
+// warps that phase B leaves idle (5-15) draw the next step's counts for the CTA's neurons into
+// shared memory while the GEMM runs, and phase A only reads them.
+//
 // Every wait is bounded (2 s): a timeout sets the error word and the kernel stops stepping,
 // still releasing its tensor memory.
 #pragma once
@@ -37,7 +48,7 @@
 namespace bsnn {
 
 constexpr uint32_t kBatchMaxClasses = 8;
-constexpr uint32_t kBatchStages = 4;        // shared-memory ring of operand stages
+constexpr uint32_t kBatchStages = 4;        // the largest shared-memory ring of operand stages
 constexpr uint32_t kBatchTmemCols = 256;    // accumulator columns (N <= 256)
 constexpr uint32_t kBatchThreads = 512;
 constexpr uint32_t kATileBytes = 128u * 64u * 2u;  // one 128 x 64 BF16 A tile
@@ -61,7 +72,8 @@ struct BClass {
 // The neuron-group parameters the neuron phase uses (NeuronGroupView, plus the Poisson means'
 // exp(-mean)).
 struct BGroupP {
-    float timestep, g_leak, cap, delta_t, v_eff, e_exc, e_inh, v_th, v_reset, v_rest;
+    float dt_c;  // timestep / membrane_capacitance, divided once on the host (the same IEEE quotient)
+    float g_leak, delta_t, v_eff, e_exc, e_inh, v_th, v_reset, v_rest;
     float exp_neg_mean_e, exp_neg_mean_i, bg_er_decay, bg_ed_decay, bg_ir_decay, bg_id_decay, bg_scale_e, bg_scale_i;
     uint32_t refractory_steps, has_bg_e, has_bg_i;
 };
@@ -82,11 +94,17 @@ struct BSim {
     BClass cls[kBatchMaxClasses];
     const BInst* inst;
     uint32_t stage_bytes;         // one shared-memory operand stage (A tile + the largest B tile)
-    const BUnit* units;           // in CTA order
-    const uint32_t* cta_units;    // [n_ctas + 1] unit ranges per CTA
+    uint32_t n_stages;            // operand stages in the ring (2 .. kBatchStages)
+    uint32_t inst_in_smem;        // the instance table is copied into shared memory
+    uint32_t state_in_smem;       // the CTA's neuron state lives in shared memory
+    uint32_t per_cta;             // neurons per CTA (the last CTA may have fewer)
+    uint32_t state_off;           // byte offset of the shared-memory state
+    uint32_t noise_off;           // byte offset of the shared-memory noise counts [per_cta] (u16)
+    const BUnit* units;           // longest first; CTAs take them in this order
+    unsigned long long* unit_ctr; // unit dispenser: n_units takes per clock step
     float* partials;
     // neuron state [n_neurons]
-    float *v, *ge, *gi, *istim, *er, *ed, *ir, *id, *tr, *td;
+    float *v, *istim, *er, *ed, *ir, *id, *tr, *td;
     uint32_t* refrac;
     uint32_t* spikes;
     unsigned long long* spike_counts;  // [n_inst][2]
@@ -178,71 +196,98 @@ __device__ __forceinline__ uint16_t bf16_bits_rn(float v) { return __bfloat16_as
 
 // ---- phase A ------------------------------------------------------------------------------------
 // Each CTA takes a contiguous range of neurons, four per thread at a time: all loads of the four
-// are issued before any is computed, to keep more memory requests in flight.  The instance and
-// class tables live in shared memory (an instance is found by binary search on its first neuron),
-// so a neuron's only global reads are its own state and its partial sums.
+// are issued before any is computed, to keep more memory requests in flight.  An instance is
+// found by walking the instance table from the thread's previous neuron (neurons only move
+// forward).
+
+// The state a CTA steps: shared-memory arrays indexed by n - base (base = the CTA's first
+// neuron), or the global arrays (base = 0).  Spikes are bytes in shared memory, words in global.
+struct BState {
+    float *v, *istim, *er, *ed, *ir, *id, *tr, *td;
+    uint32_t* refrac;
+    uint8_t* spike8;
+    uint32_t* spike32;
+    uint32_t base;
+};
+
 struct NeuronIn {
     uint32_t n, inst;
     bool valid;
-    float v, ge, gi, istim, er, ed, ir, id, tr, td;
+    float v, dge, dgi, istim, er, ed, ir, id, tr, td;
     uint32_t refrac;
 };
 
-__device__ __forceinline__ uint32_t instance_of(const BInst* s_inst, uint32_t n_inst, uint32_t n) {
+template <bool SMEM>
+__device__ __forceinline__ float st_ld(const float* p) {
+    if constexpr (SMEM) return *p;
+    else return __ldcg(p);
+}
+template <bool SMEM>
+__device__ __forceinline__ uint32_t st_ld(const uint32_t* p) {
+    if constexpr (SMEM) return *p;
+    else return __ldcg(p);
+}
+
+__device__ __forceinline__ uint32_t instance_of(const BInst* P, uint32_t n_inst, uint32_t n) {
     uint32_t lo = 0, hi = n_inst;  // last instance whose first neuron is <= n
     while (hi - lo > 1u) {
         const uint32_t mid = (lo + hi) >> 1;
-        if (s_inst[mid].nbase <= n) lo = mid;
+        if (P[mid].nbase <= n) lo = mid;
         else hi = mid;
     }
     return lo;
 }
 
-// `cur`: the instance of this thread's previous neuron (neurons only move forward).
-__device__ __forceinline__ void neuron_load(const BSim* S, const BInst* s_inst, const BClass* s_cls, uint32_t n,
-                                            bool valid, unsigned long long t, uint32_t& cur, NeuronIn& a) {
+// `cur`: the instance of this thread's previous neuron.
+template <bool SMEM>
+__device__ __forceinline__ void neuron_load(const BSim* S, const BInst* P, const BClass* s_cls, const BState& X,
+                                            uint32_t n, bool valid, unsigned long long t, uint32_t& cur, NeuronIn& a) {
     a.n = n;
     a.valid = valid;
     if (!valid) return;
-    while (cur + 1u < S->n_inst && s_inst[cur + 1u].nbase <= n) ++cur;
+    while (cur + 1u < S->n_inst && P[cur + 1u].nbase <= n) ++cur;
     a.inst = cur;
-    a.v = __ldcg(S->v + n);
-    a.ge = __ldcg(S->ge + n);
-    a.gi = __ldcg(S->gi + n);
-    a.istim = __ldcg(S->istim + n);
-    a.er = __ldcg(S->er + n);
-    a.ed = __ldcg(S->ed + n);
-    a.ir = __ldcg(S->ir + n);
-    a.id = __ldcg(S->id + n);
-    a.tr = __ldcg(S->tr + n);
-    a.td = __ldcg(S->td + n);
-    a.refrac = __ldcg(S->refrac + n);
+    const uint32_t i = n - X.base;
+    a.v = st_ld<SMEM>(X.v + i);
+    a.istim = st_ld<SMEM>(X.istim + i);
+    a.er = st_ld<SMEM>(X.er + i);
+    a.ed = st_ld<SMEM>(X.ed + i);
+    a.ir = st_ld<SMEM>(X.ir + i);
+    a.id = st_ld<SMEM>(X.id + i);
+    a.tr = st_ld<SMEM>(X.tr + i);
+    a.td = st_ld<SMEM>(X.td + i);
+    a.refrac = st_ld<SMEM>(X.refrac + i);
+    a.dge = 0.0f;
+    a.dgi = 0.0f;
     if (t > 0) {  // the previous step's propagation, K chunks in order
-        const BInst& B = s_inst[a.inst];
+        const BInst& B = P[a.inst];
         const BClass& C = s_cls[B.cls];
         const uint32_t j = n - B.nbase, stride = C.NP * 128u;
         const size_t tile = static_cast<size_t>(j >> 7), r = static_cast<size_t>(B.row) * 128u + (j & 127u);
         const float* pe = S->partials + C.pbase[0] + tile * C.nkc[0] * stride + r;
         const float* pi = S->partials + C.pbase[1] + tile * C.nkc[1] * stride + r;
-        float de = 0.0f, di = 0.0f;
-        for (uint32_t kc = 0; kc < C.nkc[0]; ++kc) de += __ldcg(pe + kc * stride);
-        for (uint32_t kc = 0; kc < C.nkc[1]; ++kc) di += __ldcg(pi + kc * stride);
-        a.ge = a.ge + de;
-        a.gi = a.gi + di;
+        for (uint32_t kc = 0; kc < C.nkc[0]; ++kc) a.dge += __ldcg(pe + kc * stride);
+        for (uint32_t kc = 0; kc < C.nkc[1]; ++kc) a.dgi += __ldcg(pi + kc * stride);
     }
 }
 
-__device__ __forceinline__ void neuron_step(const BSim* S, const BInst* s_inst, const BClass* s_cls,
-                                            unsigned long long t, const NeuronIn& a) {
+template <bool SMEM>
+__device__ __forceinline__ void neuron_step(const BSim* S, const BInst* P, const BClass* s_cls, const BState& X,
+                                            const uint16_t* nz, uint32_t n0, unsigned long long t, const NeuronIn& a) {
     if (!a.valid) return;
-    const uint32_t n = a.n;
-    const BInst& B = s_inst[a.inst];
+    const uint32_t n = a.n, i = n - X.base;
+    const BInst& B = P[a.inst];
     const BClass& C = s_cls[B.cls];
     const uint32_t j = n - B.nbase;  // index in the instance
     const uint32_t side = j < C.E ? 0u : 1u;
     const BGroupP& G = B.g[side];
     const uint32_t loc = j - (side ? C.E : 0u);
-    const float ge_used = a.ge, gi_used = a.gi;
+    // g = the background of the previous step (recomputed from its traces) + its propagation
+    float ge_used = (a.ed - a.er) * G.bg_scale_e, gi_used = (a.id - a.ir) * G.bg_scale_i;
+    if (t > 0) {
+        ge_used = ge_used + a.dge;
+        gi_used = gi_used + a.dgi;
+    }
 
     float er = flush_tiny(a.er * G.bg_er_decay);
     float ir = flush_tiny(a.ir * G.bg_ir_decay);
@@ -250,21 +295,20 @@ __device__ __forceinline__ void neuron_step(const BSim* S, const BInst* s_inst, 
     float id = flush_tiny(a.id * G.bg_id_decay);
     uint32_t ne = 0, ni = 0;
     if (S->noise_on) {
-        if (G.has_bg_e) ne = poisson_knuth(G.exp_neg_mean_e, B.seed, j, t, 0u);
-        if (G.has_bg_i) ni = poisson_knuth(G.exp_neg_mean_i, B.seed, j, t, 1u);
+        const uint32_t c = nz[n - n0];
+        ne = c & 0xFFu;
+        ni = c >> 8;
     }
     if (ne > 0u) {
         const float inc = static_cast<float>(ne);
         er += inc;
         ed += inc;
     }
-    const float bg_ge = (ed - er) * G.bg_scale_e;
     if (ni > 0u) {
         const float inc = static_cast<float>(ni);
         ir += inc;
         id += inc;
     }
-    const float bg_gi = (id - ir) * G.bg_scale_i;
 
     float v = a.v, istim = a.istim;
     uint32_t refrac = a.refrac, spike = 0;
@@ -276,8 +320,8 @@ __device__ __forceinline__ void neuron_step(const BSim* S, const BInst* s_inst, 
         const float exponential_depolarization_term = G.g_leak * G.delta_t * expf((v - G.v_eff) / G.delta_t);
         const float excitatory_synaptic_term = -1.0f * ge_used * (v - G.e_exc);
         const float inhibitory_synaptic_term = -1.0f * gi_used * (v - G.e_inh);
-        const float dv = (G.timestep / G.cap) * (linear_leak_term + exponential_depolarization_term +
-                                                 excitatory_synaptic_term + inhibitory_synaptic_term + istim);
+        const float dv = G.dt_c * (linear_leak_term + exponential_depolarization_term + excitatory_synaptic_term +
+                                   inhibitory_synaptic_term + istim);
         const float v_next = v + dv;
         if (v_next >= G.v_th) {
             refrac = G.refractory_steps;
@@ -287,15 +331,14 @@ __device__ __forceinline__ void neuron_step(const BSim* S, const BInst* s_inst, 
             v = v_next;
         }
     }
-    S->er[n] = er;
-    S->ed[n] = ed;
-    S->ir[n] = ir;
-    S->id[n] = id;
-    S->v[n] = v;
-    S->refrac[n] = refrac;
-    S->ge[n] = bg_ge;  // reset for the next propagation
-    S->gi[n] = bg_gi;
-    S->spikes[n] = spike;
+    X.er[i] = er;
+    X.ed[i] = ed;
+    X.ir[i] = ir;
+    X.id[i] = id;
+    X.v[i] = v;
+    X.refrac[i] = refrac;
+    if constexpr (SMEM) X.spike8[i] = static_cast<uint8_t>(spike);
+    else X.spike32[i] = spike;
     if (spike) atomicAdd(S->spike_counts + 2u * a.inst + side, 1ull);
 
     // stimulus events of this step act from the next step
@@ -312,7 +355,7 @@ __device__ __forceinline__ void neuron_step(const BSim* S, const BInst* s_inst, 
             istim = istim + __ldg(S->ev_delta + k);
             any = true;
         }
-        if (any) S->istim[n] = istim;
+        if (any) X.istim[i] = istim;
     }
 
     // connection traces of the neuron's presynaptic side, and x as BF16 hi / lo in B
@@ -322,32 +365,69 @@ __device__ __forceinline__ void neuron_step(const BSim* S, const BInst* s_inst, 
         r += C.norm[side];
         d += C.norm[side];
     }
-    S->tr[n] = r;
-    S->td[n] = d;
+    X.tr[i] = r;
+    X.td[i] = d;
     const float x = d - r;
     const uint16_t hi = bf16_bits_rn(x);
     const float lo_f = x - __uint_as_float(static_cast<uint32_t>(hi) << 16);
     const uint16_t lo = bf16_bits_rn(lo_f);
-    uint16_t* X = C.X[side] + static_cast<size_t>(loc >> 6) * (2u * C.NP * 64u);
-    X[core_offset(2u * C.NP, B.row, loc & 63u)] = hi;
-    X[core_offset(2u * C.NP, C.NP + B.row, loc & 63u)] = lo;
+    uint16_t* Xt = C.X[side] + static_cast<size_t>(loc >> 6) * (2u * C.NP * 64u);
+    Xt[core_offset(2u * C.NP, B.row, loc & 63u)] = hi;
+    Xt[core_offset(2u * C.NP, C.NP + B.row, loc & 63u)] = lo;
 }
 
 constexpr uint32_t kNeuronsInFlight = 4;
 
-__device__ __forceinline__ void batch_neurons(const BSim* S, const BInst* s_inst, const BClass* s_cls,
-                                              unsigned long long t) {
-    const uint32_t per = (S->n_neurons + gridDim.x - 1) / gridDim.x;
-    const uint32_t n0 = blockIdx.x * per;
-    const uint32_t n1 = n0 + per < S->n_neurons ? n0 + per : S->n_neurons;
-    uint32_t cur = instance_of(s_inst, S->n_inst, n0 + threadIdx.x < n1 ? n0 + threadIdx.x : n0);
+template <bool SMEM>
+__device__ __forceinline__ void batch_neurons(const BSim* S, const BInst* P, const BClass* s_cls, const BState& X,
+                                              const uint16_t* nz, uint32_t n0, uint32_t n1, unsigned long long t) {
+    uint32_t cur = instance_of(P, S->n_inst, n0 + threadIdx.x < n1 ? n0 + threadIdx.x : n0);
     for (uint32_t n = n0 + threadIdx.x; n < n1; n += kNeuronsInFlight * blockDim.x) {
         NeuronIn a[kNeuronsInFlight];
 #pragma unroll
         for (uint32_t q = 0; q < kNeuronsInFlight; ++q)
-            neuron_load(S, s_inst, s_cls, n + q * blockDim.x, n + q * blockDim.x < n1, t, cur, a[q]);
+            neuron_load<SMEM>(S, P, s_cls, X, n + q * blockDim.x, n + q * blockDim.x < n1, t, cur, a[q]);
 #pragma unroll
-        for (uint32_t q = 0; q < kNeuronsInFlight; ++q) neuron_step(S, s_inst, s_cls, t, a[q]);
+        for (uint32_t q = 0; q < kNeuronsInFlight; ++q) neuron_step<SMEM>(S, P, s_cls, X, nz, n0, t, a[q]);
+    }
+}
+
+// The background Poisson counts of step t for neurons [n0, n1), threads `first` .. `first +
+// count - 1` of the CTA: nz[n - n0] = n_e | n_i << 8 (each saturates at 255).
+__device__ __forceinline__ void noise_ahead(const BSim* S, const BInst* P, uint16_t* nz, uint32_t n0, uint32_t n1,
+                                            unsigned long long t, uint32_t first, uint32_t count) {
+    const uint32_t me = threadIdx.x - first;
+    uint32_t cur = instance_of(P, S->n_inst, n0 + me < n1 ? n0 + me : n0);
+    for (uint32_t n = n0 + me; n < n1; n += count) {
+        while (cur + 1u < S->n_inst && P[cur + 1u].nbase <= n) ++cur;
+        const BInst& B = P[cur];
+        const uint32_t j = n - B.nbase;
+        const BGroupP& G = B.g[j < S->cls[B.cls].E ? 0 : 1];
+        const uint32_t ne = G.has_bg_e ? poisson_knuth(G.exp_neg_mean_e, B.seed, j, t, 0u) : 0u;
+        const uint32_t ni = G.has_bg_i ? poisson_knuth(G.exp_neg_mean_i, B.seed, j, t, 1u) : 0u;
+        nz[n - n0] = static_cast<uint16_t>(ne | (ni << 8));
+    }
+}
+constexpr uint32_t kNoiseFirstThread = 160;  // warps 5-15: idle in phase B
+
+// Copies the CTA's state between global memory and its shared-memory arrays.
+__device__ __forceinline__ void state_copy(const BSim* S, const BState& X, uint32_t n0, uint32_t n1, bool to_smem) {
+    float* g[8] = {S->v, S->istim, S->er, S->ed, S->ir, S->id, S->tr, S->td};
+    float* sm[8] = {X.v, X.istim, X.er, X.ed, X.ir, X.id, X.tr, X.td};
+    for (uint32_t n = n0 + threadIdx.x; n < n1; n += blockDim.x) {
+        const uint32_t i = n - n0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (to_smem) sm[k][i] = g[k][n];
+            else g[k][n] = sm[k][i];
+        }
+        if (to_smem) {
+            X.refrac[i] = S->refrac[n];
+            X.spike8[i] = static_cast<uint8_t>(S->spikes[n]);
+        } else {
+            S->refrac[n] = X.refrac[i];
+            S->spikes[n] = X.spike8[i];
+        }
     }
 }
 
@@ -358,9 +438,12 @@ struct BatchSmem {
     uint64_t full[kBatchStages];
     uint64_t empty[kBatchStages];
     uint64_t accum;   // the MMA thread's commit: the unit's accumulator is complete
+    uint64_t ready[2];  // the producer has taken a unit (or found none left) and named it in unit[]
+    uint32_t unit[2];
     uint64_t tfree;   // the 4 epilogue warps: the accumulator has been read
 };
 
+template <bool SMEM_STATE>
 __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim* __restrict__ S, uint32_t n_steps) {
     extern __shared__ __align__(1024) unsigned char bsm_raw[];
     __shared__ BatchSmem bs;
@@ -368,22 +451,60 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
     __shared__ int s_ok;
     __shared__ unsigned long long s_bar0, s_t0;
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
-    // stage s: A tile at s * stage_bytes, B tile after it; then the instance table
-    const uint32_t stage_bytes = S->stage_bytes;
+    // stage s: A tile at s * stage_bytes, B tile after it; then the instance table (when it is
+    // kept in shared memory), then the neuron state (when it is kept in shared memory)
+    const uint32_t stage_bytes = S->stage_bytes, n_stages = S->n_stages;
     const uint32_t smem_base = saddr(bsm_raw);
-    BInst* s_inst = reinterpret_cast<BInst*>(bsm_raw + kBatchStages * stage_bytes);
-    for (uint32_t i = tid; i < S->n_inst * (sizeof(BInst) / 4u); i += blockDim.x)
-        reinterpret_cast<uint32_t*>(s_inst)[i] = reinterpret_cast<const uint32_t*>(S->inst)[i];
+    const BInst* P = S->inst;
+    if (S->inst_in_smem) {
+        BInst* s_inst = reinterpret_cast<BInst*>(bsm_raw + n_stages * stage_bytes);
+        for (uint32_t i = tid; i < S->n_inst * (sizeof(BInst) / 4u); i += blockDim.x)
+            reinterpret_cast<uint32_t*>(s_inst)[i] = reinterpret_cast<const uint32_t*>(S->inst)[i];
+        P = s_inst;
+    }
+    const uint32_t n0 = min(blockIdx.x * S->per_cta, S->n_neurons);
+    const uint32_t n1 = min(n0 + S->per_cta, S->n_neurons);
+    BState X{};
+    if constexpr (SMEM_STATE) {
+        const uint32_t per = S->per_cta;
+        float* f = reinterpret_cast<float*>(bsm_raw + S->state_off);
+        X.v = f;
+        X.istim = f + per;
+        X.er = f + 2 * per;
+        X.ed = f + 3 * per;
+        X.ir = f + 4 * per;
+        X.id = f + 5 * per;
+        X.tr = f + 6 * per;
+        X.td = f + 7 * per;
+        X.refrac = reinterpret_cast<uint32_t*>(f + 8 * per);
+        X.spike8 = reinterpret_cast<uint8_t*>(f + 9 * per);
+        X.base = n0;
+        state_copy(S, X, n0, n1, true);
+    } else {
+        X.v = S->v;
+        X.istim = S->istim;
+        X.er = S->er;
+        X.ed = S->ed;
+        X.ir = S->ir;
+        X.id = S->id;
+        X.tr = S->tr;
+        X.td = S->td;
+        X.refrac = S->refrac;
+        X.spike32 = S->spikes;
+        X.base = 0;
+    }
     for (uint32_t i = tid; i < S->n_classes * (sizeof(BClass) / 4u); i += blockDim.x)
         reinterpret_cast<uint32_t*>(s_cls)[i] = reinterpret_cast<const uint32_t*>(S->cls)[i];
 
     if (tid == 0) {
         bs.ok = 1u;
-        for (uint32_t s = 0; s < kBatchStages; ++s) {
+        for (uint32_t s = 0; s < n_stages; ++s) {
             mbar_init(saddr(&bs.full[s]), 1u);
             mbar_init(saddr(&bs.empty[s]), 1u);
         }
         mbar_init(saddr(&bs.accum), 1u);
+        mbar_init(saddr(&bs.ready[0]), 1u);
+        mbar_init(saddr(&bs.ready[1]), 1u);
         mbar_init(saddr(&bs.tfree), 4u);
         fence_mbar_init();
         s_bar0 = ld_acquire_u64(S->barrier) / gridDim.x * gridDim.x;
@@ -398,11 +519,12 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
     tc_fence_after();
     const uint32_t tmem = bs.tmem;
     const unsigned long long bar0 = s_bar0, t0 = s_t0;
-    const uint32_t u_begin = S->cta_units[blockIdx.x], u_end = S->cta_units[blockIdx.x + 1];
+    const uint32_t n_units = S->n_units;
     // producer / MMA state (thread 0 only)
     uint32_t full_ph = 0, empty_ph = 0, accum_ph = 0, tfree_ph = 0;
     uint32_t empty_pend[kBatchStages] = {0, 0, 0, 0};
-    uint32_t g_load = 0, g_use = 0, units_issued = 0;
+    uint32_t load_s = 0, use_s = 0, units_issued = 0;
+    uint32_t ready_slot = 0, ready_ph = 0;  // the unit ring (producer and epilogue alike)
     const bool producer = tid == 128u;  // warp 4: loads and MMAs; warps 0-3: the epilogue
     bool ok = true;
 #ifdef BSNN_PHASE_TIMING
@@ -412,9 +534,13 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
     unsigned long long t_mark_ = static_cast<unsigned long long>(clock64());
 #endif
 
+    uint16_t* s_nz = reinterpret_cast<uint16_t*>(bsm_raw + S->noise_off);
+    if (S->noise_on) noise_ahead(S, P, s_nz, n0, n1, t0, 0u, blockDim.x);
+    __syncthreads();
+
     for (uint32_t k = 0; k < n_steps && ok; ++k) {
         const unsigned long long t = t0 + k;
-        batch_neurons(S, s_inst, s_cls, t);
+        batch_neurons<SMEM_STATE>(S, P, s_cls, X, s_nz, n0, n1, t);
         fence_proxy_async_global();
         __syncthreads();
         BSNN_TMARK(0);
@@ -426,12 +552,25 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
         if (producer) {
             fence_proxy_async_global();
             const uint64_t keep = l2_evict_last_policy();
-            for (uint32_t ui = u_begin; ui < u_end; ++ui) {
+            // Units are sorted longest first.  CTA b starts with unit b; after issuing a unit's MMAs
+            // it takes the next from a dispenser shared by all CTAs (units grid, grid + 1, ...), so
+            // the CTAs that finish early do the rest.  Every processed unit is followed by exactly
+            // one take, so a clock step makes n_units takes, numbered from t * n_units.
+            const unsigned long long take0 = t * n_units;
+            auto take = [&]() { return gridDim.x + static_cast<uint32_t>(atomicAdd(S->unit_ctr, 1ull) - take0); };
+            uint32_t ui = blockIdx.x;
+            for (;;) {
+                const bool none = ui >= n_units;
+                bs.unit[ready_slot] = none ? 0xFFFFFFFFu : ui;
+                mbar_arrive(saddr(&bs.ready[ready_slot]));
+                ready_slot ^= 1u;
+                if (none) break;
                 const BUnit U = S->units[ui];
                 const BClass& C = s_cls[U.cls];
                 const uint32_t N = 2u * C.NP, b_bytes = N * 128u, nk = U.k1 - U.k0;
                 if (bs.ok == 0u) {  // after a timeout: only release the epilogue
                     tc_commit(saddr(&bs.accum));
+                    ui = take();
                     continue;
                 }
                 const unsigned char* a_src = reinterpret_cast<const unsigned char*>(C.A[U.side]) +
@@ -439,10 +578,10 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
                 const unsigned char* b_src =
                     reinterpret_cast<const unsigned char*>(C.X[U.side]) + static_cast<size_t>(U.k0) * b_bytes;
                 bool good = true;
-                // K tile i of the unit into stage g_load % S, once the MMAs that read the stage last
+                // K tile i of the unit into stage load_s, once the MMAs that read the stage last
                 // are done
                 auto load = [&](uint32_t i) {
-                    const uint32_t s = g_load % kBatchStages;
+                    const uint32_t s = load_s;
                     if (empty_pend[s]) {
                         if (!mbar_wait(saddr(&bs.empty[s]), (empty_ph >> s) & 1u)) good = false;
                         empty_ph ^= 1u << s;
@@ -453,18 +592,18 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
                     mbar_expect_tx(bar, kATileBytes + b_bytes);
                     bulk_load_keep(dst, a_src + static_cast<size_t>(i) * kATileBytes, kATileBytes, bar, keep);
                     bulk_load(dst + kATileBytes, b_src + static_cast<size_t>(i) * b_bytes, b_bytes, bar);
-                    ++g_load;
+                    load_s = load_s + 1u == n_stages ? 0u : load_s + 1u;
                 };
                 const uint32_t idesc = idesc_bf16_m128(N);
                 uint32_t next = 0;
-                for (; next < nk && next < kBatchStages; ++next) load(next);
+                for (; next < nk && next < n_stages; ++next) load(next);
                 // the epilogue of the previous unit has read the accumulator
                 if (units_issued > 0u) {
                     if (!mbar_wait(saddr(&bs.tfree), tfree_ph & 1u)) good = false;
                     tfree_ph ^= 1u;
                 }
                 for (uint32_t i = 0; i < nk && good; ++i) {
-                    const uint32_t s = g_use % kBatchStages;
+                    const uint32_t s = use_s;
                     if (!mbar_wait(saddr(&bs.full[s]), (full_ph >> s) & 1u)) {
                         good = false;
                         break;
@@ -478,7 +617,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
                                     smem_desc(b + ks * 2u * (N * 16u), N * 16u, 128u), idesc, (i | ks) != 0u);
                     tc_commit(saddr(&bs.empty[s]));
                     empty_pend[s] = 1u;
-                    ++g_use;
+                    use_s = use_s + 1u == n_stages ? 0u : use_s + 1u;
                     // refill the stage of the previous iteration (its MMAs have had an MMA's time to
                     // finish; load() waits for them)
                     if (i > 0u && next < nk) load(next++);
@@ -489,10 +628,21 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
                     atomicExch(S->error, kErrStageTimeout);
                     bs.ok = 0u;
                 }
+                ui = take();
             }
         } else if (warp < 4) {
             const uint32_t row = 32u * warp + lane;
-            for (uint32_t ui = u_begin; ui < u_end; ++ui) {
+            for (;;) {
+                // the unit the producer took (or the end of the step's units)
+                if (!mbar_wait(saddr(&bs.ready[ready_slot]), (ready_ph >> ready_slot) & 1u)) {
+                    atomicExch(S->error, kErrStageTimeout);
+                    bs.ok = 0u;
+                    break;
+                }
+                ready_ph ^= 1u << ready_slot;
+                const uint32_t ui = bs.unit[ready_slot];
+                ready_slot ^= 1u;
+                if (ui == 0xFFFFFFFFu) break;
                 const BUnit U = S->units[ui];
                 const BClass& C = s_cls[U.cls];
                 const bool got = mbar_wait(saddr(&bs.accum), accum_ph & 1u);
@@ -515,6 +665,8 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
                 __syncwarp();
                 if (lane == 0) mbar_arrive(saddr(&bs.tfree));
             }
+        } else if (tid >= kNoiseFirstThread && S->noise_on && k + 1u < n_steps) {
+            noise_ahead(S, P, s_nz, n0, n1, t + 1ull, kNoiseFirstThread, blockDim.x - kNoiseFirstThread);
         }
         __syncthreads();
         ok = bs.ok != 0u;  // the same for every thread of the CTA
@@ -532,19 +684,23 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
 #endif
     tc_fence_before();
     __syncthreads();
+    if constexpr (SMEM_STATE) state_copy(S, X, n0, n1, false);
     if (warp == 0) tmem_dealloc(tmem, kBatchTmemCols);
     if (blockIdx.x == 0 && tid == 0 && ok) *S->steps_done = t0 + n_steps;
 }
 
-// g of one instance's neurons including the propagation still pending in the partial sums (the
-// value the reference holds after step_the_clock): reads only.
-__global__ void bsnn_batch_gsum_kernel(const BSim* __restrict__ S, uint32_t instance, float* out_ge, float* out_gi) {
+// g of one instance's neurons: the background conductance (d - r) * scale of the background
+// traces, plus, with `pending`, the propagation still pending in the partial sums (the value the
+// reference holds after step_the_clock).  Reads only.
+__global__ void bsnn_batch_g_kernel(const BSim* __restrict__ S, uint32_t instance, int with_pending, float* out_ge,
+                                    float* out_gi) {
     const BInst& B = S->inst[instance];
     const BClass& C = S->cls[B.cls];
-    const bool pending = *S->steps_done > 0;
+    const bool pending = with_pending && *S->steps_done > 0;
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < C.N; j += gridDim.x * blockDim.x) {
         const uint32_t n = B.nbase + j, mt = j >> 7, row = j & 127u;
-        float g[2] = {S->ge[n], S->gi[n]};
+        const BGroupP& G = B.g[j < C.E ? 0 : 1];
+        float g[2] = {(S->ed[n] - S->er[n]) * G.bg_scale_e, (S->id[n] - S->ir[n]) * G.bg_scale_i};
         if (pending)
             for (uint32_t sd = 0; sd < 2; ++sd) {
                 const float* p = S->partials + C.pbase[sd] + static_cast<size_t>(mt) * C.nkc[sd] * C.NP * 128u +

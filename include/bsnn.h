@@ -390,6 +390,8 @@ typedef struct bsnn_batch_info {
     uint64_t weight_bytes;     /* BF16 weight tiles, padding included                     */
     uint64_t kernel_launches;
     uint64_t smem_bytes;
+    uint32_t state_in_smem;    /* 1: each CTA's neuron state stays in shared memory      */
+    uint32_t operand_stages;   /* shared-memory operand stages of the GEMM ring           */
 } bsnn_batch_info;
 
 BSNN_API bsnn_status bsnn_batch_create(int32_t device, bsnn_batch** out_batch);

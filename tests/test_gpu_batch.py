@@ -10,6 +10,8 @@ population spike counts are compared instead.
 """
 from __future__ import annotations
 
+import os
+
 import numpy as np
 import pytest
 
@@ -21,6 +23,7 @@ pytestmark = pytest.mark.gpu
 
 RTOL = 2e-5
 FIELDS = ["membrane_potentials", "g_excitatory", "g_inhibitory", "i_stimulus", "background_g_excitatory",
+          "background_g_inhibitory",
           "background_excitatory_r_traces", "background_excitatory_d_traces", "connection_summed"]
 
 
@@ -117,3 +120,37 @@ def test_batch_rates_against_fp64():
                 worst = max(worst, err)
     print(f"largest relative rate error (populations with > 100 spikes): {worst:.2e}")
     g.close()
+
+
+@pytest.mark.parametrize("env", [{"BSNN_BATCH_STATE": "global"}, {"BSNN_BATCH_STAGES": "2"},
+                                 {"BSNN_BATCH_STATE": "global", "BSNN_BATCH_STAGES": "4"}])
+def test_batch_placements_are_bit_exact(env):
+    """Neuron state in shared memory (the default when it fits) or in global memory, and the
+    operand ring's depth, change where data lives, not the arithmetic: the states are identical."""
+    spec = bsnn.config4_batch(n_instances=6, steps=200, seed=9, sizes=(400, 900, 1600), stim_window=(10, 150))
+    a = bsnn.BatchSimulation(spec)
+    ia = a.info()
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
+    try:
+        b = bsnn.BatchSimulation(spec)
+        ib = b.info()
+    finally:
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    assert ia.state_in_smem == 1
+    assert ib.state_in_smem == (0 if env.get("BSNN_BATCH_STATE") == "global" else 1)
+    if "BSNN_BATCH_STAGES" in env:
+        assert ib.operand_stages == int(env["BSNN_BATCH_STAGES"])
+    for sim in (a, b):
+        sim.set_steps_per_launch(37)
+        sim.run(150)
+    for k in range(len(spec.instances)):
+        for f in FIELDS + ["spikes", "refractory_counter"]:
+            np.testing.assert_array_equal(a.read(k, f), b.read(k, f), err_msg=f"instance {k} {f}")
+    np.testing.assert_array_equal(a.spike_counts(), b.spike_counts())
+    a.close()
+    b.close()
