@@ -195,8 +195,11 @@ __host__ __device__ __forceinline__ uint32_t core_offset(uint32_t rows, uint32_t
 __device__ __forceinline__ uint16_t bf16_bits_rn(float v) { return __bfloat16_as_ushort(__float2bfloat16_rn(v)); }
 
 // ---- phase A ------------------------------------------------------------------------------------
-// Each CTA takes a contiguous range of neurons, four per thread at a time: all loads of the four
-// are issued before any is computed, to keep more memory requests in flight.  An instance is
+// Each CTA takes a contiguous range of neurons, BSNN_BATCH_NEURONS_IN_FLIGHT per thread at a time:
+// all loads of those are issued before any is computed.  With the state in shared memory only
+// the partial sums come from L2, and one at a time measured fastest on B200 (38.5 us per clock
+// step for 192 networks, against 40.0 with two, 44.8 with four and 53.3 with eight in flight:
+// the extra registers cost more than the latency they hide).  An instance is
 // found by walking the instance table from the thread's previous neuron (neurons only move
 // forward).
 
@@ -376,7 +379,10 @@ __device__ __forceinline__ void neuron_step(const BSim* S, const BInst* P, const
     Xt[core_offset(2u * C.NP, C.NP + B.row, loc & 63u)] = lo;
 }
 
-constexpr uint32_t kNeuronsInFlight = 4;
+#ifndef BSNN_BATCH_NEURONS_IN_FLIGHT
+#define BSNN_BATCH_NEURONS_IN_FLIGHT 1
+#endif
+constexpr uint32_t kNeuronsInFlight = BSNN_BATCH_NEURONS_IN_FLIGHT;
 
 template <bool SMEM>
 __device__ __forceinline__ void batch_neurons(const BSim* S, const BInst* P, const BClass* s_cls, const BState& X,
@@ -392,11 +398,10 @@ __device__ __forceinline__ void batch_neurons(const BSim* S, const BInst* P, con
     }
 }
 
-// The background Poisson counts of step t for neurons [n0, n1), threads `first` .. `first +
-// count - 1` of the CTA: nz[n - n0] = n_e | n_i << 8 (each saturates at 255).
+// The background Poisson counts of step t for neurons [n0, n1), drawn by `count` threads of the
+// CTA, this one being number `me`: nz[n - n0] = n_e | n_i << 8 (each saturates at 255).
 __device__ __forceinline__ void noise_ahead(const BSim* S, const BInst* P, uint16_t* nz, uint32_t n0, uint32_t n1,
-                                            unsigned long long t, uint32_t first, uint32_t count) {
-    const uint32_t me = threadIdx.x - first;
+                                            unsigned long long t, uint32_t me, uint32_t count) {
     uint32_t cur = instance_of(P, S->n_inst, n0 + me < n1 ? n0 + me : n0);
     for (uint32_t n = n0 + me; n < n1; n += count) {
         while (cur + 1u < S->n_inst && P[cur + 1u].nbase <= n) ++cur;
@@ -408,7 +413,22 @@ __device__ __forceinline__ void noise_ahead(const BSim* S, const BInst* P, uint1
         nz[n - n0] = static_cast<uint16_t>(ne | (ni << 8));
     }
 }
-constexpr uint32_t kNoiseFirstThread = 160;  // warps 5-15: idle in phase B
+// The warps idle in phase B that draw the noise: (BSNN_BATCH_NOISE_WARPS = 1, the default) warps
+// 5-15 except those on the producer's scheduler (warp 4 runs on sub-partition 0, so warps 8 and 12
+// are left out: the single producer thread's issue latency gates the whole GEMM), or (0) all of
+// warps 5-15.
+#ifndef BSNN_BATCH_NOISE_WARPS
+#define BSNN_BATCH_NOISE_WARPS 1
+#endif
+__device__ __forceinline__ bool noise_warp(uint32_t warp) {
+    if (BSNN_BATCH_NOISE_WARPS == 1) return warp >= 5u && (warp & 3u) != 0u;
+    return warp >= 5u;
+}
+__device__ __forceinline__ uint32_t noise_rank(uint32_t warp) {  // among the noise warps
+    if (BSNN_BATCH_NOISE_WARPS == 1) return (warp - 5u) - (warp >= 8u ? 1u : 0u) - (warp >= 12u ? 1u : 0u);
+    return warp - 5u;
+}
+constexpr uint32_t kNoiseWarps = BSNN_BATCH_NOISE_WARPS == 1 ? 9u : 11u;
 
 // Copies the CTA's state between global memory and its shared-memory arrays.
 __device__ __forceinline__ void state_copy(const BSim* S, const BState& X, uint32_t n0, uint32_t n1, bool to_smem) {
@@ -535,7 +555,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
 #endif
 
     uint16_t* s_nz = reinterpret_cast<uint16_t*>(bsm_raw + S->noise_off);
-    if (S->noise_on) noise_ahead(S, P, s_nz, n0, n1, t0, 0u, blockDim.x);
+    if (S->noise_on) noise_ahead(S, P, s_nz, n0, n1, t0, tid, blockDim.x);
     __syncthreads();
 
     for (uint32_t k = 0; k < n_steps && ok; ++k) {
@@ -665,8 +685,8 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
                 __syncwarp();
                 if (lane == 0) mbar_arrive(saddr(&bs.tfree));
             }
-        } else if (tid >= kNoiseFirstThread && S->noise_on && k + 1u < n_steps) {
-            noise_ahead(S, P, s_nz, n0, n1, t + 1ull, kNoiseFirstThread, blockDim.x - kNoiseFirstThread);
+        } else if (noise_warp(warp) && S->noise_on && k + 1u < n_steps) {
+            noise_ahead(S, P, s_nz, n0, n1, t + 1ull, 32u * noise_rank(warp) + lane, 32u * kNoiseWarps);
         }
         __syncthreads();
         ok = bs.ok != 0u;  // the same for every thread of the CTA
