@@ -149,6 +149,7 @@ def run_batch(args, rank, world):
     n_inst = BATCH_WORKLOADS[args.workload]
     spec = bsnn.config4_batch(n_inst, steps=(W + K) * S + 1, seed=rank)
     sim = bsnn.BatchSimulation(spec, device=dev)
+    tuning = sim.autotune(200)  # GEMM unit size and operand ring depth, timed on this GPU
     sim.set_steps_per_launch(S)
     stream = torch.cuda.ExternalStream(sim.stream())
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
@@ -199,7 +200,12 @@ def run_batch(args, rank, world):
                    "clock_steps_per_bench_step": S, "dt_s": DT, "plasticity": "off",
                    "form": "batched: one persistent launch per bench step, shared-weight propagation as a "
                            "tcgen05 BF16 GEMM per size class", "parallelism": f"replicas x{world}",
-                   "l2": "flushed (256 MB write) between timed steps"},
+                   "l2": "flushed (256 MB write) between timed steps",
+                   "autotuned": {"k_tiles_per_unit": tuning["k_tiles_per_unit"],
+                                 "operand_stages": tuning["operand_stages"],
+                                 "candidates": tuning["candidates"],
+                                 "default_us_per_step": tuning["default_us_per_step"],
+                                 "tuned_us_per_step": tuning["us_per_step"]}},
         "dense_synaptic_updates_per_s": synapses / step_s * world,
         "spikes_per_s_simulated": spikes / max(sim_seconds, 1e-12),
         "clock_steps_per_s": 1.0 / step_s,
@@ -213,7 +219,7 @@ def run_batch(args, rank, world):
         "clocks": clocks.summary(),
     }
     sim.close()
-    return line, spec
+    return line, (spec, tuning)
 
 
 ADJOINT_WORKLOADS = {"config5_adjoint_3125": 2000}
@@ -530,12 +536,13 @@ def run_bsnn(args, rank, world):
         "clocks": clocks.summary(),
     }
     sim.close()
-    return line, spec
+    return line, (spec, tuning)
 
 
-def run_batch_e2e(args, spec):
+def run_batch_e2e(args, spec, tuning):
     """The batch through its public API with host buffers: build (weights and stimulus uploaded from
-    host memory), run K bench steps, read the spike counts back each step."""
+    host memory) with the shapes the autotuner chose, run K bench steps, read the spike counts
+    back each step."""
     import torch
 
     import bsnn
@@ -543,6 +550,7 @@ def run_batch_e2e(args, spec):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     sim = bsnn.BatchSimulation(spec)
+    sim.set_tuning(tuning)
     sim.set_steps_per_launch(S)
     d2h = 0
     for _ in range(K):
@@ -657,10 +665,10 @@ def main():
             print(json.dumps(line), flush=True)
         state[3].close()
     elif args.workload in BATCH_WORKLOADS:
-        line, spec = run_batch(args, int(os.environ.get("LOCAL_RANK", "0")), world)
+        line, (spec, tuning) = run_batch(args, int(os.environ.get("LOCAL_RANK", "0")), world)
         if rank == 0:
             if not args.no_e2e:
-                line["e2e"] = run_batch_e2e(args, spec)
+                line["e2e"] = run_batch_e2e(args, spec, tuning)
             if world == 1:
                 pf = plain_form_baseline(spec)
                 line["plain_form"] = pf

@@ -281,6 +281,13 @@ class AdjointDesc(ctypes.Structure):
                 ("surrogate_beta", ctypes.c_float), ("rate_weight", ctypes.c_float), ("voltage_weight", ctypes.c_float)]
 
 
+class BatchTuning(ctypes.Structure):
+    """bsnn_batch_tuning."""
+    _fields_ = [("k_tiles_per_unit", ctypes.c_uint32), ("operand_stages", ctypes.c_uint32),
+                ("candidates", ctypes.c_uint32), ("us_per_step", ctypes.c_float),
+                ("default_us_per_step", ctypes.c_float)]
+
+
 _P = ctypes.c_void_p
 _U32 = ctypes.c_uint32
 _I32 = ctypes.c_int32
@@ -305,6 +312,8 @@ SIGNATURES = {
     "bsnn_batch_read_state": (_I32, [_P, _U32, _I32, _P]),
     "bsnn_batch_read_spike_counts": (_I32, [_P, ctypes.POINTER(ctypes.c_uint64)]),
     "bsnn_batch_get_info": (_I32, [_P, ctypes.POINTER(BatchInfo)]),
+    "bsnn_batch_autotune": (_I32, [_P, _U32, ctypes.POINTER(BatchTuning)]),
+    "bsnn_batch_set_tuning": (_I32, [_P, ctypes.POINTER(BatchTuning)]),
     "bsnn_adjoint_create": (_I32, [ctypes.POINTER(AdjointDesc), _P, _P, _P, _P, _FP, _FP, _FP, _FP, _UP, _U32, _UP, _FP,
                                    _U32, _I32, ctypes.POINTER(_P)]),
     "bsnn_adjoint_destroy": (_I32, [_P]),

@@ -184,6 +184,22 @@ class BatchSimulation:
         self._check(self._lib.bsnn_batch_read_spike_counts(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))))
         return out
 
+    def autotune(self, trial_steps: int = 200) -> dict:
+        """Times candidate GEMM unit sizes and ring depths (before the first step) and keeps the
+        fastest; returns the choice."""
+        from ._ffi import BatchTuning
+        r = BatchTuning()
+        self._check(self._lib.bsnn_batch_autotune(self._h, trial_steps, ctypes.byref(r)))
+        return {"k_tiles_per_unit": r.k_tiles_per_unit, "operand_stages": r.operand_stages,
+                "candidates": r.candidates, "us_per_step": r.us_per_step,
+                "default_us_per_step": r.default_us_per_step}
+
+    def set_tuning(self, tuning: dict):
+        """Applies shapes an earlier autotune() returned (before the first step)."""
+        from ._ffi import BatchTuning
+        r = BatchTuning(tuning.get("k_tiles_per_unit", 0), tuning.get("operand_stages", 0), 0, 0.0, 0.0)
+        self._check(self._lib.bsnn_batch_set_tuning(self._h, ctypes.byref(r)))
+
     def info(self):
         from ._ffi import BatchInfo
         i = BatchInfo()

@@ -4,9 +4,11 @@
 // A batch is built from size classes (one shared weight set each, stored as BF16 W^T tiles in
 // the tensor cores' canonical layout) and instances (per-instance neuron-group parameters,
 // seed and stimulus).  The first call that needs the device plans the GEMM work units (a K chunk
-// of one 128-post tile of one class and presynaptic side), spreads them over the persistent CTAs
-// (longest first, onto the least loaded CTA), allocates one arena and uploads.  bsnn_batch_run
-// replays a captured CUDA graph of the cooperative launch per chunk of steps.
+// of one 128-post tile of one class and presynaptic side, sorted longest first), places the
+// operand ring, instance table and neuron state in shared memory, allocates one arena and
+// uploads.  bsnn_batch_run replays a captured CUDA graph of the cooperative launch per chunk of
+// steps.  bsnn_batch_autotune times candidate unit sizes and ring depths on the device before
+// the first step and keeps the fastest.
 #pragma once
 
 #include "batch_kernel.cuh"
@@ -49,6 +51,9 @@ struct bsnn_batch {
     std::map<uint32_t, cudaGraphExec_t> graphs;
     float* scratch = nullptr;  // [2][max N] for reads of g with the pending propagation
     const void* kernel = nullptr;  // bsnn_batch_kernel<state in shared memory or not>
+    uint32_t tune_kc = 0;          // K tiles per GEMM unit (0: the default rule)
+    uint32_t tune_stages = 0;      // operand stages (0: the placement's choice)
+    uint32_t kc = 0;               // the unit size in use
 
     ~bsnn_batch() {
         for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
@@ -145,7 +150,9 @@ void batch_finalize(bsnn_batch* b) {
         const uint32_t MT = (HC.E + HC.I + 127) / 128;
         total_tiles += static_cast<uint64_t>(MT) * ((HC.E + 63) / 64 + (HC.I + 63) / 64);
     }
-    const uint32_t kc = std::max<uint32_t>(4u, static_cast<uint32_t>((total_tiles + n_ctas - 1) / n_ctas));
+    const uint32_t kc = b->tune_kc ? b->tune_kc
+                                   : std::max<uint32_t>(4u, static_cast<uint32_t>((total_tiles + n_ctas - 1) / n_ctas));
+    b->kc = kc;
     std::vector<BUnit> units;
     size_t part_floats = 0;
     for (uint32_t c = 0; c < h.n_classes; ++c) {
@@ -318,7 +325,8 @@ void batch_finalize(bsnn_batch* b) {
     const char* env_state = std::getenv("BSNN_BATCH_STATE");    // "global": keep the state in global memory
     const char* env_stages = std::getenv("BSNN_BATCH_STAGES");  // 2 .. 4
     const bool allow_smem_state = !(env_state && std::string(env_state) == "global");
-    const uint32_t forced_stages = env_stages ? static_cast<uint32_t>(std::atoi(env_stages)) : 0u;
+    const uint32_t forced_stages =
+        b->tune_stages ? b->tune_stages : env_stages ? static_cast<uint32_t>(std::atoi(env_stages)) : 0u;
     struct Choice { uint32_t state, stages, table; };
     const Choice choices[] = {{1, 4, 1}, {1, 3, 1}, {1, 4, 0}, {1, 3, 0}, {1, 2, 1}, {1, 2, 0},
                               {0, 4, 1}, {0, 3, 1}, {0, 4, 0}, {0, 3, 0}, {0, 2, 1}, {0, 2, 0}};
@@ -368,6 +376,20 @@ void batch_check_error(bsnn_batch* b) {
         b->failed = true;
         throw ApiError(BSNN_ERR_DEVICE_TIMEOUT, "batch kernel: a device-side wait timed out; the batch state is invalid");
     }
+}
+
+// Releases the device side (graphs, arena): the next call that needs it plans and uploads anew,
+// from step 0.
+void batch_teardown(bsnn_batch* b) {
+    cuda_check(cudaStreamSynchronize(b->stream), "batch stream synchronize");
+    for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+    b->graphs.clear();
+    if (b->arena) cudaFree(b->arena);
+    b->arena = nullptr;
+    b->arena_bytes = 0;
+    b->d_sim = nullptr;
+    b->finalized = false;
+    b->steps_done = 0;
 }
 
 void batch_launch(bsnn_batch* b, uint32_t n_steps) {
@@ -614,6 +636,103 @@ BSNN_API bsnn_status bsnn_batch_read_spike_counts(bsnn_batch* b, uint64_t* host_
         batch_check_error(b);
         cuda_check(cudaMemcpy(host_out, b->h.spike_counts, sizeof(uint64_t) * 2 * b->insts.size(), cudaMemcpyDeviceToHost),
                    "D2H spike counts");
+    });
+}
+
+// Times candidate GEMM unit sizes (K tiles per unit, around the default rule) with the placement's
+// ring depth, then ring depths of 2, 3 and 4 stages for the best unit size, each over
+// `trial_steps` clock steps after a warm-up, and keeps the fastest.  Only before the first step:
+// the batch is left at step 0 with the chosen shapes.  The unit size sets how many K chunks a
+// neuron's partial sums add up, so it is part of the batch's arithmetic (results stay
+// deterministic for a given choice); the ring depth is not.
+BSNN_API bsnn_status bsnn_batch_autotune(bsnn_batch* b, uint32_t trial_steps, bsnn_batch_tuning* out) {
+    if (!b) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded_batch(b, [&] {
+        require(b->steps_done == 0, BSNN_ERR_STATE, "autotune runs before the first step");
+        require(trial_steps > 0, BSNN_ERR_INVALID_ARGUMENT, "trial_steps must be > 0");
+        batch_teardown(b);
+        b->tune_kc = 0;
+        b->tune_stages = 0;
+        batch_finalize(b);
+        const uint32_t kc0 = b->kc;
+        uint32_t kt_max = 1;
+        for (uint32_t c = 0; c < b->h.n_classes; ++c) kt_max = std::max(kt_max, std::max(b->h.cls[c].KT[0], b->h.cls[c].KT[1]));
+        cudaEvent_t e0, e1;
+        cuda_check(cudaEventCreate(&e0), "event");
+        cuda_check(cudaEventCreate(&e1), "event");
+        uint32_t tried = 0;
+        // one trial: a fresh device side with (kc, stages), a warm-up launch, then a timed one
+        auto trial = [&](uint32_t kc, uint32_t stages) -> double {
+            batch_teardown(b);
+            b->tune_kc = kc;
+            b->tune_stages = stages;
+            try {
+                batch_finalize(b);
+            } catch (const ApiError&) {
+                return -1.0;  // this ring depth does not fit
+            }
+            const uint32_t warm = std::max<uint32_t>(8u, trial_steps / 4u);
+            batch_launch(b, warm);
+            cuda_check(cudaEventRecord(e0, b->stream), "event record");
+            batch_launch(b, trial_steps);
+            cuda_check(cudaEventRecord(e1, b->stream), "event record");
+            cuda_check(cudaEventSynchronize(e1), "event sync");
+            batch_check_error(b);
+            float ms = 0.0f;
+            cuda_check(cudaEventElapsedTime(&ms, e0, e1), "event time");
+            ++tried;
+            return 1e3 * ms / trial_steps;
+        };
+        std::vector<uint32_t> kcs = {kc0, std::max(1u, kc0 / 2), std::max(1u, (kc0 * 3) / 4), (kc0 * 3) / 2, kc0 * 2, kt_max};
+        std::sort(kcs.begin(), kcs.end());
+        kcs.erase(std::unique(kcs.begin(), kcs.end()), kcs.end());
+        const double t_default = trial(kc0, 0);
+        double best = t_default;
+        uint32_t best_kc = kc0, best_st = 0;
+        for (uint32_t kc : kcs) {
+            if (kc == kc0 || kc > kt_max) continue;
+            const double us = trial(kc, 0);
+            if (us > 0.0 && us < best) {
+                best = us;
+                best_kc = kc;
+            }
+        }
+        for (uint32_t st = 2; st <= kBatchStages; ++st) {
+            const double us = trial(best_kc, st);
+            if (us > 0.0 && us < best) {
+                best = us;
+                best_st = st;
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        batch_teardown(b);
+        b->tune_kc = best_kc;
+        b->tune_stages = best_st;
+        batch_finalize(b);
+        if (out) {
+            bsnn_batch_tuning r{};
+            r.k_tiles_per_unit = best_kc;
+            r.operand_stages = b->h.n_stages;
+            r.candidates = tried;
+            r.us_per_step = static_cast<float>(best);
+            r.default_us_per_step = static_cast<float>(t_default);
+            *out = r;
+        }
+    });
+}
+
+// Applies shapes found by an earlier autotune (k_tiles_per_unit and operand_stages; 0 keeps the
+// default rule), before the first step.
+BSNN_API bsnn_status bsnn_batch_set_tuning(bsnn_batch* b, const bsnn_batch_tuning* t) {
+    if (!b || !t) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded_batch(b, [&] {
+        require(b->steps_done == 0, BSNN_ERR_STATE, "shapes are set before the first step");
+        require(t->operand_stages == 0 || (t->operand_stages >= 2 && t->operand_stages <= kBatchStages),
+                BSNN_ERR_INVALID_ARGUMENT, "operand_stages must be 0 or 2..4");
+        batch_teardown(b);
+        b->tune_kc = t->k_tiles_per_unit;
+        b->tune_stages = t->operand_stages;
     });
 }
 

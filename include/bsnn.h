@@ -425,6 +425,23 @@ BSNN_API bsnn_status bsnn_batch_read_state(bsnn_batch* batch, uint32_t instance,
 BSNN_API bsnn_status bsnn_batch_read_spike_counts(bsnn_batch* batch, uint64_t* host_out);
 BSNN_API bsnn_status bsnn_batch_get_info(bsnn_batch* batch, bsnn_batch_info* out);
 
+/* The autotuner's choice: GEMM unit size (K tiles of 64 presynaptic neurons per unit), operand
+ * ring depth, how many candidates were timed, and the clock-step times of the choice and of the
+ * default shapes. */
+typedef struct bsnn_batch_tuning {
+    uint32_t k_tiles_per_unit;
+    uint32_t operand_stages;
+    uint32_t candidates;
+    float us_per_step;
+    float default_us_per_step;
+} bsnn_batch_tuning;
+
+/* Before the first step: times candidate unit sizes and ring depths over trial_steps clock steps
+ * each on the device and keeps the fastest (the batch stays at step 0).  out may be null. */
+BSNN_API bsnn_status bsnn_batch_autotune(bsnn_batch* batch, uint32_t trial_steps, bsnn_batch_tuning* out);
+/* Applies shapes an earlier autotune found (0 fields keep the defaults), before the first step. */
+BSNN_API bsnn_status bsnn_batch_set_tuning(bsnn_batch* batch, const bsnn_batch_tuning* tuning);
+
 /* ---- the differentiation form (no reference counterpart) -------------------------------------
  * A surrogate-gradient adjoint of the two-group network with frozen weights: the forward pass is
  * the reference's step without plasticity (FP32), checkpointed every checkpoint_interval steps;

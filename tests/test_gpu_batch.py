@@ -188,3 +188,30 @@ def test_batch_rate_error_over_a_simulated_second():
     agg = abs(tot_b - tot_r) / tot_r
     print(f"aggregate: {tot_b} vs FP64 {tot_r} (relative {agg:.1e})")
     assert agg <= 1e-3
+
+
+def test_autotune_keeps_a_valid_choice():
+    """The autotuner times its candidates, leaves the batch at step 0 with the fastest shapes, and
+    the tuned batch still matches the oracle; it refuses to run after the first step."""
+    spec = bsnn.config4_batch(n_instances=5, steps=400, seed=3, sizes=(400, 900), stim_window=(5, 300))
+    g = bsnn.BatchSimulation(spec)
+    r = g.autotune(40)
+    print(r)
+    assert r["candidates"] >= 3 and 0 < r["us_per_step"] <= r["default_us_per_step"]
+    assert 2 <= r["operand_stages"] <= 4 and r["k_tiles_per_unit"] >= 1
+    assert g.info().steps_done == 0
+    oracles = [oracle_for(spec, b) for b in range(len(spec.instances))]
+    g.run(30)
+    for o, _ in oracles:
+        o.run(0, 30)
+    for b, (o, net) in enumerate(oracles):
+        compare_instance(g, b, o, net, f"tuned instance {b}")
+    with pytest.raises(bsnn.StateError):
+        g.autotune(40)
+    h = bsnn.BatchSimulation(spec)
+    h.set_tuning(r)
+    h.run(30)
+    for b in range(len(spec.instances)):
+        np.testing.assert_array_equal(g.read(b, "membrane_potentials"), h.read(b, "membrane_potentials"))
+    g.close()
+    h.close()
