@@ -324,6 +324,8 @@ SIGNATURES = {
     "bsnn_adjoint_forward": (_I32, [_P, _FP, _FP, _FP, _FP, _FP]),
     "bsnn_adjoint_backward": (_I32, [_P, _FP, ctypes.POINTER(ctypes.c_double)]),
     "bsnn_get_info": (_I32, [_P, ctypes.POINTER(Info)]),
+    "bsnn_save_checkpoint": (_I32, [_P, ctypes.c_char_p]),
+    "bsnn_load_checkpoint": (_I32, [_P, ctypes.c_char_p]),
     "bsnn_add_neuron_group": (_I32, [_P, ctypes.POINTER(NeuronGroupParams), _UP]),
     "bsnn_add_connection": (_I32, [_P, _U32, _U32, _FP, ctypes.POINTER(ConnectionParams), _UP]),
     "bsnn_add_stimulus": (_I32, [_P, _UP, _U32, _UP, _UP, _FP, _U32]),

@@ -174,6 +174,14 @@ class Simulation:
         a = np.ascontiguousarray(values, dtype=np.uint32 if name in UINT_FIELDS else np.float32)
         self._check(self._lib.bsnn_write_state(self._h, FIELD[name], index, offset, a.size, a.ctypes.data_as(ctypes.c_void_p)))
 
+    def save_checkpoint(self, path):
+        """Writes the whole device state and the clock cursor to `path` (binary)."""
+        self._check(self._lib.bsnn_save_checkpoint(self._h, str(path).encode()))
+
+    def load_checkpoint(self, path):
+        """Restores a checkpoint written by a simulation built from the same components."""
+        self._check(self._lib.bsnn_load_checkpoint(self._h, str(path).encode()))
+
     def read_weights(self, connection: int) -> np.ndarray:
         n_pre, n_post = self._conns[connection]
         out = np.empty((n_pre, n_post), dtype=np.float32)

@@ -1428,6 +1428,117 @@ BSNN_API bsnn_status bsnn_set_steps_per_launch(bsnn_sim* sim, uint32_t steps) {
     });
 }
 
+// ---- checkpoint / resume ---------------------------------------------------------------------
+// A checkpoint is the simulation's whole device arena (neuron state, traces, weights and their
+// copies, plasticity traces, monitor rings, the step counters, the planned work lists) plus the
+// host's clock cursor.  The arena's layout is a function of the components and their order, the
+// weight form and the device's SM count, so a checkpoint loads into a simulation built the same
+// way on the same kind of GPU: the header carries a fingerprint of that layout.  The one region
+// holding device addresses, the kernel's descriptor, is rewritten from the loading simulation's
+// own copy.  Text recording (files written by monitors) is not part of it.
+namespace {
+
+constexpr char kCkptMagic[8] = {'B', 'S', 'N', 'N', 'C', 'K', 'P', 'T'};
+constexpr uint32_t kCkptVersion = 1;
+
+struct CkptHeader {
+    char magic[8];
+    uint32_t version;
+    uint32_t N;
+    uint64_t arena_bytes;
+    uint64_t fingerprint;
+    uint64_t steps_done;
+    uint32_t next_clock;
+    int32_t weight_format;
+};
+
+uint64_t fnv1a(uint64_t h, const void* p, size_t n) {
+    const unsigned char* c = static_cast<const unsigned char*>(p);
+    for (size_t i = 0; i < n; ++i) {
+        h ^= c[i];
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+// The layout: sizes and counts of every component and of the launch plan.
+uint64_t layout_fingerprint(const bsnn_sim* s) {
+    uint64_t h = 1469598103934665603ull;
+    const DSim& d = s->h;
+    const uint32_t head[] = {d.N, d.N_pad, d.n_groups, d.n_conns, d.n_ts, d.n_plast, d.n_mons, d.n_ctas, d.n_slots,
+                             d.max_rows, d.max_own, d.resident_floats, d.max_trows, d.n_chunks, d.stage_rows,
+                             d.stage_warps, static_cast<uint32_t>(d.wfmt), d.spk_words, d.n_red, d.stim_len,
+                             d.replay_steps, s->grid, s->block};
+    h = fnv1a(h, head, sizeof(head));
+    for (const auto& g : s->groups) h = fnv1a(h, &g.p.num_neurons, sizeof(g.p.num_neurons));
+    for (const auto& c : s->conns) {
+        const uint32_t cc[] = {c.pre, c.post};
+        h = fnv1a(h, cc, sizeof(cc));
+    }
+    for (const auto& p : s->plasts) h = fnv1a(h, &p.kind, sizeof(p.kind));
+    for (const auto& m : s->mons) {
+        const uint32_t mm[] = {static_cast<uint32_t>(m.kind), m.group, m.interval, static_cast<uint32_t>(m.sel.size())};
+        h = fnv1a(h, mm, sizeof(mm));
+    }
+    const uint64_t sizes[] = {s->arena_bytes, s->smem_bytes};
+    return fnv1a(h, sizes, sizeof(sizes));
+}
+
+}  // namespace
+
+BSNN_API bsnn_status bsnn_save_checkpoint(bsnn_sim* sim, const char* path) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        require(path != nullptr, BSNN_ERR_INVALID_ARGUMENT, "null path");
+        finalize(sim);
+        check_device_error(sim);
+        std::vector<unsigned char> blob(sim->arena_bytes);
+        cuda_check(cudaMemcpy(blob.data(), sim->arena, sim->arena_bytes, cudaMemcpyDeviceToHost), "D2H checkpoint");
+        CkptHeader hd{};
+        std::memcpy(hd.magic, kCkptMagic, sizeof(kCkptMagic));
+        hd.version = kCkptVersion;
+        hd.N = sim->N;
+        hd.arena_bytes = sim->arena_bytes;
+        hd.fingerprint = layout_fingerprint(sim);
+        hd.steps_done = sim->steps_done;
+        hd.next_clock = sim->next_clock;
+        hd.weight_format = sim->weight_format;
+        std::ofstream f(path, std::ios::binary | std::ios::trunc);
+        require(f.good(), BSNN_ERR_INVALID_ARGUMENT, std::string("cannot open ") + path + " for writing");
+        f.write(reinterpret_cast<const char*>(&hd), sizeof(hd));
+        f.write(reinterpret_cast<const char*>(blob.data()), static_cast<std::streamsize>(blob.size()));
+        require(f.good(), BSNN_ERR_RUNTIME, std::string("write to ") + path + " failed");
+    });
+}
+
+BSNN_API bsnn_status bsnn_load_checkpoint(bsnn_sim* sim, const char* path) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        require(path != nullptr, BSNN_ERR_INVALID_ARGUMENT, "null path");
+        finalize(sim);
+        require(!sim->failed, BSNN_ERR_STATE, "simulation failed earlier (device timeout)");
+        std::ifstream f(path, std::ios::binary);
+        require(f.good(), BSNN_ERR_INVALID_ARGUMENT, std::string("cannot open ") + path);
+        CkptHeader hd{};
+        f.read(reinterpret_cast<char*>(&hd), sizeof(hd));
+        require(f.good() && std::memcmp(hd.magic, kCkptMagic, sizeof(kCkptMagic)) == 0, BSNN_ERR_INVALID_ARGUMENT,
+                std::string(path) + " is not a bsnn checkpoint");
+        require(hd.version == kCkptVersion, BSNN_ERR_INVALID_ARGUMENT, "unsupported checkpoint version");
+        require(hd.N == sim->N && hd.arena_bytes == sim->arena_bytes && hd.weight_format == sim->weight_format &&
+                    hd.fingerprint == layout_fingerprint(sim),
+                BSNN_ERR_INVALID_ARGUMENT,
+                "checkpoint was written by a differently built simulation (components, weight form or GPU)");
+        std::vector<unsigned char> blob(hd.arena_bytes);
+        f.read(reinterpret_cast<char*>(blob.data()), static_cast<std::streamsize>(blob.size()));
+        require(f.good(), BSNN_ERR_INVALID_ARGUMENT, std::string(path) + " is truncated");
+        cuda_check(cudaStreamSynchronize(sim->stream), "stream synchronize");
+        cuda_check(cudaMemcpy(sim->arena, blob.data(), blob.size(), cudaMemcpyHostToDevice), "H2D checkpoint");
+        cuda_check(cudaMemcpy(sim->d_sim, &sim->h, sizeof(DSim), cudaMemcpyHostToDevice), "H2D descriptor");
+        sim->steps_done = hd.steps_done;
+        sim->next_clock = hd.next_clock;
+    });
+}
+
 BSNN_API bsnn_status bsnn_read_state(bsnn_sim* sim, int32_t field, uint32_t index, uint32_t offset, uint32_t count,
                                      void* host_out) {
     if (!sim) return BSNN_ERR_INVALID_ARGUMENT;

@@ -263,6 +263,13 @@ BSNN_API bsnn_status bsnn_set_steps_per_launch(bsnn_sim* sim, uint32_t steps);
 
 /* ---- state access (GpuSimulationState download helpers) ------------------------------------ */
 
+/* Checkpoint / resume (no reference counterpart): the whole device state and the clock cursor to
+ * a binary file, and back into a simulation built from the same components in the same order,
+ * with the same weight form, on the same kind of GPU (checked; BSNN_ERR_INVALID_ARGUMENT
+ * otherwise).  Files written by text monitors are not part of a checkpoint. */
+BSNN_API bsnn_status bsnn_save_checkpoint(bsnn_sim* sim, const char* path);
+BSNN_API bsnn_status bsnn_load_checkpoint(bsnn_sim* sim, const char* path);
+
 /* Copies `count` elements starting at `offset` of a field (BSNN_FIELD_*) to host memory.
  * `index` selects the connection / plasticity for the per-component fields. */
 BSNN_API bsnn_status bsnn_read_state(bsnn_sim* sim, int32_t field, uint32_t index, uint32_t offset,
