@@ -288,6 +288,15 @@ class BatchTuning(ctypes.Structure):
                 ("default_us_per_step", ctypes.c_float)]
 
 
+class WeightGenerationParams(ctypes.Structure):
+    """bsnn_weight_generation_params."""
+    _fields_ = [("max_weight_value", ctypes.c_float), ("max_distance", ctypes.c_float),
+                ("spread_scale", ctypes.c_float), ("probability_multiplier", ctypes.c_float),
+                ("x_location_length", ctypes.c_float), ("y_location_length", ctypes.c_float),
+                ("weight_value_normal_dropoff", ctypes.c_int32), ("probabilistic_normal_not_uniform", ctypes.c_int32),
+                ("no_diagonal_connections", ctypes.c_int32), ("uniform_values", ctypes.c_int32)]
+
+
 _P = ctypes.c_void_p
 _U32 = ctypes.c_uint32
 _I32 = ctypes.c_int32
@@ -324,6 +333,8 @@ SIGNATURES = {
     "bsnn_adjoint_forward": (_I32, [_P, _FP, _FP, _FP, _FP, _FP]),
     "bsnn_adjoint_backward": (_I32, [_P, _FP, ctypes.POINTER(ctypes.c_double)]),
     "bsnn_get_info": (_I32, [_P, ctypes.POINTER(Info)]),
+    "bsnn_generate_distance_weights": (_I32, [_FP, _U32, _FP, _U32, ctypes.POINTER(WeightGenerationParams),
+                                              ctypes.c_uint64, _I32, _FP]),
     "bsnn_save_checkpoint": (_I32, [_P, ctypes.c_char_p]),
     "bsnn_load_checkpoint": (_I32, [_P, ctypes.c_char_p]),
     "bsnn_add_neuron_group": (_I32, [_P, ctypes.POINTER(NeuronGroupParams), _UP]),

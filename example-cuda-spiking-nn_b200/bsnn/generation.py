@@ -134,3 +134,33 @@ def partial_group_multiple_square_waves(max_timestep: int, selected_input_ids, s
         counts[ev[0]] += 1
     return (counts, np.array([e[2] for e in events], np.uint32), np.array([e[1] for e in events], np.uint32),
             np.array([e[3] for e in events], np.float32))
+
+
+def distance_2d_weights_gpu(pre_loc: np.ndarray, post_loc: np.ndarray, *, max_weight_value: float, max_distance: float,
+                            spread_scale: float, weight_value_normal_dropoff: bool,
+                            probabilistic_normal_not_uniform: bool, probability_multiplier: float,
+                            no_diagonal_connections: bool, x_location_length: float, y_location_length: float,
+                            rng_seed: int, value_mode: str = "reference", device: int = 0, library=None) -> np.ndarray:
+    """The same rule as distance_2d_weights, generated on the GPU with counter-based draws per
+    (seed, pre, post) (bsnn_generate_distance_weights): identical candidate sets, equal in
+    distribution, not bit for bit."""
+    import ctypes
+
+    from ._ffi import WeightGenerationParams, error_for, load_library
+    lib = library if library is not None else load_library()
+    pre = np.ascontiguousarray(pre_loc, dtype=np.float32).reshape(-1, 2)
+    post = np.ascontiguousarray(post_loc, dtype=np.float32).reshape(-1, 2)
+    if value_mode not in ("reference", "uniform"):
+        raise ValueError(f"unknown value_mode {value_mode!r}")
+    p = WeightGenerationParams(max_weight_value, max_distance, spread_scale, probability_multiplier,
+                               x_location_length, y_location_length, int(weight_value_normal_dropoff),
+                               int(probabilistic_normal_not_uniform), int(no_diagonal_connections),
+                               int(value_mode == "uniform"))
+    w = np.empty((len(pre), len(post)), dtype=np.float32)
+    fp = ctypes.POINTER(ctypes.c_float)
+    st = lib.bsnn_generate_distance_weights(pre.ctypes.data_as(fp), len(pre), post.ctypes.data_as(fp), len(post),
+                                            ctypes.byref(p), int(rng_seed) & 0xFFFFFFFFFFFFFFFF, device,
+                                            w.ctypes.data_as(fp))
+    if st != 0:
+        raise error_for(st, lib.bsnn_last_error(None).decode())
+    return w

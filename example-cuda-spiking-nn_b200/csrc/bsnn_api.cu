@@ -1794,5 +1794,68 @@ extern "C" BSNN_API bsnn_status bsnn_debug_phase_ns(bsnn_sim* sim, unsigned long
     });
 }
 #endif
+#include "generate.cuh"
+
+extern "C" {
+
+// Distance-dependent weights generated on the GPU (see generate.cuh): pre_xy / post_xy hold
+// (x, y) per neuron; w_out (host memory, n_pre * n_post floats, row-major) receives the matrix.
+BSNN_API bsnn_status bsnn_generate_distance_weights(const float* pre_xy, uint32_t n_pre, const float* post_xy,
+                                                    uint32_t n_post, const bsnn_weight_generation_params* params,
+                                                    uint64_t seed, int32_t device, float* w_out) {
+    return guarded(nullptr, [&] {
+        require(pre_xy && post_xy && params && w_out, BSNN_ERR_INVALID_ARGUMENT, "null argument");
+        require(n_pre > 0 && n_post > 0, BSNN_ERR_INVALID_ARGUMENT, "neuron groups must not be empty");
+        require(params->spread_scale > 0.0f, BSNN_ERR_INVALID_ARGUMENT, "spread_scale must be > 0");
+        require(params->max_weight_value >= 0.0f, BSNN_ERR_INVALID_ARGUMENT,
+                "max_weight_value must be >= 0 (the reference rejects negative weights)");
+        int nd = 0;
+        cuda_check(cudaGetDeviceCount(&nd), "cudaGetDeviceCount");
+        require(device >= 0 && device < nd, BSNN_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+        DeviceGuard g(device);
+        const uint64_t n = static_cast<uint64_t>(n_pre) * n_post;
+        GenParams P{};
+        P.max_weight_value = params->max_weight_value;
+        P.max_distance = params->max_distance;
+        P.spread_scale = params->spread_scale;
+        P.probability_multiplier = params->probability_multiplier;
+        P.lx = params->x_location_length;
+        P.ly = params->y_location_length;
+        P.value_dropoff = params->weight_value_normal_dropoff ? 1u : 0u;
+        P.normal_probability = params->probabilistic_normal_not_uniform ? 1u : 0u;
+        P.no_diagonal = params->no_diagonal_connections ? 1u : 0u;
+        P.uniform_values = params->uniform_values ? 1u : 0u;
+        P.seed_lo = static_cast<uint32_t>(seed);
+        P.seed_hi = static_cast<uint32_t>(seed >> 32);
+        cudaStream_t st = nullptr;
+        cuda_check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
+        unsigned char* buf = nullptr;
+        const size_t xy = 8ull * (n_pre + n_post);
+        const cudaError_t me = cudaMallocAsync(reinterpret_cast<void**>(&buf), xy + 4ull * n + 256, st);
+        if (me != cudaSuccess) {
+            cudaStreamDestroy(st);
+            cuda_check(me, "cudaMallocAsync generation buffer");
+        }
+        float* dpre = reinterpret_cast<float*>(buf);
+        float* dpost = dpre + 2ull * n_pre;
+        float* dw = reinterpret_cast<float*>(buf + ((xy + 255) & ~size_t(255)));
+        cudaError_t e = cudaMemcpyAsync(dpre, pre_xy, 8ull * n_pre, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dpost, post_xy, 8ull * n_post, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) {
+            const uint64_t blocks = (n + 255) / 256;
+            bsnn_generate_weights_kernel<<<static_cast<uint32_t>(blocks), 256, 0, st>>>(dpre, n_pre, dpost, n_post, P, dw);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaMemcpyAsync(w_out, dw, 4ull * n, cudaMemcpyDeviceToHost, st);
+        cudaFreeAsync(buf, st);
+        const cudaError_t se = cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+        cuda_check(e, "weight generation");
+        cuda_check(se, "weight generation sync");
+    });
+}
+
+}  // extern "C"
+
 #include "batch_api.cuh"
 #include "adjoint_api.cuh"

@@ -376,6 +376,31 @@ BSNN_API bsnn_status bsnn_connection_propagate(const bsnn_connection_view* view,
  *    from different host threads) race and give wrong results.  Order them (one stream, or events). */
 BSNN_API bsnn_status bsnn_connection_propagate_noalloc(const bsnn_connection_view* view, void* stream);
 
+/* ---- network generation on the GPU (a flagged alternative to cpp_src/generation/generate_weights.cpp:10-103)
+ * The reference's rule (candidates off the diagonal when excluded and within max_distance on the
+ * periodic layout; existence with probability multiplier [x exp(-d^2/S)]; value max_weight [x the
+ * same Gaussian]) with counter-based Philox draws per (seed, pre, post) instead of one mt19937
+ * stream: the candidate sets equal the reference's, the matrix equals it in distribution, not bit
+ * for bit (the host generator in bsnn_generate.hpp is the byte-identical one).  uniform_values
+ * draws each existing weight from U[0, max_weight_value). */
+typedef struct bsnn_weight_generation_params {
+    float max_weight_value;
+    float max_distance;
+    float spread_scale;
+    float probability_multiplier;
+    float x_location_length;
+    float y_location_length;
+    int32_t weight_value_normal_dropoff;
+    int32_t probabilistic_normal_not_uniform;
+    int32_t no_diagonal_connections;
+    int32_t uniform_values;
+} bsnn_weight_generation_params;
+
+/* pre_xy / post_xy: (x, y) per neuron; w_out: host memory for n_pre * n_post floats, row-major. */
+BSNN_API bsnn_status bsnn_generate_distance_weights(const float* pre_xy, uint32_t n_pre, const float* post_xy,
+                                                    uint32_t n_post, const bsnn_weight_generation_params* params,
+                                                    uint64_t seed, int32_t device, float* w_out);
+
 /* ---- the batched form (no reference counterpart) ---------------------------------------------
  * Many independent networks ("instances") of uneven size, without plasticity, stepped together by
  * one persistent launch.  Each instance is the reference's two-group network (E group, I group,
