@@ -405,12 +405,12 @@ def spike_events_from_bits(bits, group_offset, n, nnz):
     return int(per_neuron.sum()), int((per_neuron * nnz[group_offset:group_offset + n]).sum())
 
 
-def cpu_baseline(spec, seconds: float):
-    """The CPU oracle (FP32 restatement of the reference step, all host threads) on a bounded
-    sample of the same workload."""
+def _oracle_rate(spec, seconds: float, precision: int):
+    """Simulated-s per wall-s of the CPU oracle stepping `spec` for about `seconds`."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle
-    o = oracle.OracleSimulation(spec.num_excitatory, spec.num_inhibitory, **spec.sim_kwargs())
+    o = oracle.OracleSimulation(spec.num_excitatory, spec.num_inhibitory, precision=precision,
+                                **spec.sim_kwargs())
     spec.build(o)
     o.run(0, 2)
     t0 = time.perf_counter()
@@ -419,9 +419,23 @@ def cpu_baseline(spec, seconds: float):
         o.run(2 + n, 10)
         n += 10
     el = time.perf_counter() - t0
+    o.close()
+    return n * DT / el, n, el
+
+
+def cpu_baseline(spec, seconds: float):
+    """The CPU oracle on a bounded sample of the same workload, on all host threads: the FP32
+    restatement of the reference step (the line's value: the reference's arithmetic) and, beside
+    it, the same step in FP64."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
     threads = int(os.environ.get("ORACLE_THREADS", os.cpu_count() or 1))
-    return {"value": n * DT / el, "unit": "simulated-s/wall-s", "cores": threads, "kind": "port",
-            "sample": f"{n} clock steps of {spec.name} (FP32 oracle, {threads} threads), {el:.1f} s"}
+    v32, n32, el32 = _oracle_rate(spec, seconds * 2 / 3, oracle.PREC_F32)
+    v64, n64, el64 = _oracle_rate(spec, seconds / 3, oracle.PREC_F64)
+    return {"value": v32, "unit": "simulated-s/wall-s", "cores": threads, "kind": "port",
+            "sample": f"{n32} clock steps of {spec.name} (FP32 oracle, {threads} threads), {el32:.1f} s",
+            "fp64": {"value": v64, "unit": "simulated-s/wall-s", "cores": threads,
+                     "sample": f"{n64} clock steps of {spec.name} (FP64 oracle, {threads} threads), {el64:.1f} s"}}
 
 
 def reduce_over_ranks(t_ms: float, events: int, spikes: int, device):
@@ -536,7 +550,7 @@ def run_bsnn(args, rank, world):
         "clocks": clocks.summary(),
     }
     sim.close()
-    return line, (spec, tuning)
+    return line, spec
 
 
 def run_batch_e2e(args, spec, tuning):

@@ -66,3 +66,37 @@ def test_reference_arm_prints_on_rank_zero_only(rank, expect_line):
         import json
         line = json.loads(res.stdout.strip().splitlines()[-1])
         assert line["impl"] == "reference" and line["value"] > 0 and line["cpu_baseline"]["kind"] == "port"
+
+
+def _undefined_names(path):
+    """Names that a function of `path` reads as globals but that neither the module nor the
+    builtins define (what a linter reports as an undefined name)."""
+    import builtins
+    import symtable
+    src = path.read_text()
+    top = symtable.symtable(src, str(path), "exec")
+    defined = {s.get_name() for s in top.get_symbols() if s.is_assigned() or s.is_imported()
+               or s.is_namespace()} | set(dir(builtins))
+    missing = []
+
+    def walk(table):
+        for child in table.get_children():
+            if child.get_type() == "function":
+                for s in child.get_symbols():
+                    if s.is_global() and s.is_referenced() and s.get_name() not in defined:
+                        missing.append(f"{child.get_name()}: {s.get_name()}")
+            walk(child)
+    walk(top)
+    return missing
+
+
+_PY_FILES = sorted(["bench.py", "__graft_entry__.py"]
+                   + [str(p.relative_to(ROOT)) for d in ("example-cuda-spiking-nn_b200/bsnn", "oracle", "tests",
+                                                         "tests/golden") for p in (ROOT / d).glob("*.py")])
+
+
+@pytest.mark.parametrize("name", _PY_FILES)
+def test_no_undefined_names(name):
+    """The bench and most of the package run only on a GPU, so a name left undefined by an edit
+    would first show there; catch it here."""
+    assert _undefined_names(ROOT / name) == []
