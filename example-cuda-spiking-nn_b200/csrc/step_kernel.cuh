@@ -236,6 +236,7 @@ struct SmemLayout {
     float* lzq;         // [max_rows] quantisation scale of the row's GEMV copy
     float* lzqi;        // [max_rows] its reciprocal
     float* lzf;         // [max_rows] this step's GEMV weight of the row, x s qs
+    float* lzw;         // [32] per-warp partial master sums of a spiking row (row-scaled forms)
     uint32_t* bits;     // [n_spike_monitors][max_own/32 + 2]
     unsigned char* desc;  // descriptor copies (DGroup, DTraceSet, DConn, DPlast, DMon, slot lists)
 };
@@ -289,7 +290,7 @@ __host__ __device__ __forceinline__ SmemSizes smem_sizes(uint32_t resident_float
     z.stage = stage_rows ? ((static_cast<size_t>(stage_warps) * 2u * stage_rows * 512u + 127u) & ~size_t(127)) +
                                align16(static_cast<size_t>(stage_warps) * (2u * sizeof(uint64_t) + sizeof(uint32_t)))
                          : 0;
-    z.lz = align16(sizeof(float) * 5u * static_cast<size_t>(lazy_rows));
+    z.lz = align16(sizeof(float) * (5u * static_cast<size_t>(lazy_rows) + (lazy_rows ? 32u : 0u)));
     z.bits = align16(sizeof(uint32_t) * n_spike_mons * (max_own / 32 + 2));
     z.groups = align16(sizeof(DGroup) * n_groups);
     z.ts = align16(sizeof(DTraceSet) * n_ts);
@@ -830,10 +831,17 @@ __device__ __forceinline__ float* weight_ptr(const DBlk& B, const DConn& C, cons
 // The two passes touch disjoint weights, so each weight gets the reference's LTP-then-LTD
 // sequence exactly once.  The column factors come from the owners' parity buffers in global
 // memory, the row factors from the row table.
+// Every warp enumerates the spiking neurons in the same order (lanes over the bitmask words or the
+// rows, then a ballot), and all the threads share out each one: the rows of a spiking column, or
+// the columns of a spiking row, kUpdUnroll columns per thread at a time with all their loads
+// issued before the first update.  A row streamed from global memory thus costs a few memory
+// round trips instead of one per 32 columns.  Each weight is still updated by exactly one thread.
 // Runs on warps [w_first, w_first + nwarps) of the CTA.
+constexpr uint32_t kUpdUnroll = 4;
+
 __device__ __forceinline__ void apply_updates(const Desc& D, const DBlk* s_blk, uint32_t nblk, uint32_t ppar,
                                            const SmemLayout& sm, uint32_t w_first, uint32_t nwarps) {
-    const uint32_t tid = threadIdx.x - 32u * w_first, nthr = 32u * nwarps, warp = tid >> 5, lane = tid & 31u;
+    const uint32_t tid = threadIdx.x - 32u * w_first, nthr = 32u * nwarps, lane = tid & 31u;
     for (uint32_t bk = 0; bk < nblk; ++bk) {
         const DBlk B = s_blk[bk];
         const DConn& C = D.conns[B.conn];
@@ -842,37 +850,67 @@ __device__ __forceinline__ void apply_updates(const Desc& D, const DBlk* s_blk, 
         const uint32_t nrows = B.row_end - B.row_begin, n_post = C.n_post, post_off = C.post_off;
         const float* colA = P.colA[ppar];
         const float* colB = P.colB[ppar];
-        // column pass: threads scan the bitmask words of the postsynaptic group
+        // column pass: lanes scan the bitmask words of the postsynaptic group
         const uint32_t w0 = post_off >> 5, w1 = (post_off + n_post - 1u) >> 5;
-        for (uint32_t w = w0 + tid; w <= w1; w += nthr) {
-            uint32_t bits = sm.sbits[w];
-            if (w == w0) bits &= 0xffffffffu << (post_off & 31u);
-            if (w == w1) bits &= 0xffffffffu >> (31u - ((post_off + n_post - 1u) & 31u));
-            while (bits) {
-                const uint32_t b = __ffs(bits) - 1u;
-                bits &= bits - 1u;
-                const uint32_t q = 32u * w + b - post_off;
-                const float cA = __ldcg(colA + q), cB = __ldcg(colB + q);
-                for (uint32_t i = 0; i < nrows; ++i) {
-                    const uint32_t r = B.srow + i;
-                    if (sm.rowflag[r]) continue;  // the row pass owns this weight
-                    float* wp = weight_ptr(B, C, sm, i, q);
-                    const float4 rw = sm.row[r];
-                    *wp = plastic_update(*wp, q, B.row_begin + i, n_post, 1u, 0u, rw.z, cA, cB, rw.w, P.wmin, P.wmax);
+        for (uint32_t wb = w0; wb <= w1; wb += 32u) {
+            const uint32_t w = wb + lane;
+            uint32_t bits = 0u;
+            if (w <= w1) {
+                bits = sm.sbits[w];
+                if (w == w0) bits &= 0xffffffffu << (post_off & 31u);
+                if (w == w1) bits &= 0xffffffffu >> (31u - ((post_off + n_post - 1u) & 31u));
+            }
+            uint32_t nz = __ballot_sync(kFull, bits != 0u);
+            while (nz) {
+                const uint32_t src = __ffs(nz) - 1u;
+                nz &= nz - 1u;
+                uint32_t wbits = __shfl_sync(kFull, bits, src);
+                while (wbits) {
+                    const uint32_t b = __ffs(wbits) - 1u;
+                    wbits &= wbits - 1u;
+                    const uint32_t q = 32u * (wb + src) + b - post_off;
+                    const float cA = __ldcg(colA + q), cB = __ldcg(colB + q);
+                    for (uint32_t i = tid; i < nrows; i += nthr) {
+                        const uint32_t r = B.srow + i;
+                        if (sm.rowflag[r]) continue;  // the row pass owns this weight
+                        float* wp = weight_ptr(B, C, sm, i, q);
+                        const float4 rw = sm.row[r];
+                        *wp = plastic_update(*wp, q, B.row_begin + i, n_post, 1u, 0u, rw.z, cA, cB, rw.w, P.wmin,
+                                             P.wmax);
+                    }
                 }
             }
         }
-        // row pass: one warp per spiking row, lanes over the columns
-        for (uint32_t i = warp; i < nrows; i += nwarps) {
-            const uint32_t r = B.srow + i;
-            if (!sm.rowflag[r]) continue;
-            const float4 rw = sm.row[r];
-            for (uint32_t q = lane; q < n_post; q += 32u) {
-                const uint32_t g = post_off + q;
-                const uint32_t post_spk = (sm.sbits[g >> 5] >> (g & 31u)) & 1u;
-                float* wp = weight_ptr(B, C, sm, i, q);
-                *wp = plastic_update(*wp, q, B.row_begin + i, n_post, post_spk, 1u, rw.z, __ldcg(colA + q),
-                                     __ldcg(colB + q), rw.w, P.wmin, P.wmax);
+        // row pass: lanes scan the rows
+        for (uint32_t i0 = 0; i0 < nrows; i0 += 32u) {
+            uint32_t spk = __ballot_sync(kFull, i0 + lane < nrows && sm.rowflag[B.srow + i0 + lane] != 0u);
+            while (spk) {
+                const uint32_t i = i0 + __ffs(spk) - 1u;
+                spk &= spk - 1u;
+                const float4 rw = sm.row[B.srow + i];
+                for (uint32_t qb = tid; qb < n_post; qb += kUpdUnroll * nthr) {
+                    float wv[kUpdUnroll], a[kUpdUnroll], b[kUpdUnroll];
+#pragma unroll
+                    for (uint32_t u = 0; u < kUpdUnroll; ++u) {
+                        const uint32_t q = qb + u * nthr;
+                        wv[u] = a[u] = b[u] = 0.0f;
+                        if (q < n_post) {
+                            wv[u] = *weight_ptr(B, C, sm, i, q);
+                            a[u] = __ldcg(colA + q);
+                            b[u] = __ldcg(colB + q);
+                        }
+                    }
+#pragma unroll
+                    for (uint32_t u = 0; u < kUpdUnroll; ++u) {
+                        const uint32_t q = qb + u * nthr;
+                        if (q < n_post) {
+                            const uint32_t g = post_off + q;
+                            const uint32_t post_spk = (sm.sbits[g >> 5] >> (g & 31u)) & 1u;
+                            *weight_ptr(B, C, sm, i, q) = plastic_update(wv[u], q, B.row_begin + i, n_post, post_spk,
+                                                                         1u, rw.z, a[u], b[u], rw.w, P.wmin, P.wmax);
+                        }
+                    }
+                }
             }
         }
     }
@@ -1247,14 +1285,17 @@ __device__ __forceinline__ void store_copy(int32_t fmt, const DConn& C, uint32_t
     else reinterpret_cast<float*>(C.q)[e] = m;
 }
 
-// The pending plasticity update in a row-scaled form, on warps [w_first, w_first + nwarps): one
-// warp per row.  A row whose presynaptic neuron spiked gets LTP (where the postsynaptic neuron
-// spiked) then LTD on every entry, and M is summed from the new masters (lanes in column order,
-// then an xor-butterfly); another row gets LTP in the columns of the spiking postsynaptic
-// neurons and M grows by the sum of the changes (same fixed order).
+// The pending plasticity update in a row-scaled form, on warps [w_first, w_first + nwarps).
+// A row whose presynaptic neuron did not spike gets LTP in the columns of the spiking postsynaptic
+// neurons, one warp per row, and M grows by the sum of the changes (lanes over the bitmask words
+// in order, then an xor-butterfly).  A row whose presynaptic neuron spiked gets LTP (where the
+// postsynaptic neuron spiked) then LTD on every entry, shared out over all the threads
+// (kUpdUnroll columns each at a time, loads issued first); M is summed from the new masters: each
+// thread its columns in order, an xor-butterfly per warp, then the warp sums in warp order.
+// Named barrier 2 (all the warps given) orders the per-warp sums.
 __device__ __forceinline__ void apply_updates_rows(const Desc& D, const DBlk* s_blk, uint32_t nblk, uint32_t ppar,
                                                 const SmemLayout& sm, uint32_t w_first, uint32_t nwarps) {
-    const uint32_t warp = (threadIdx.x >> 5) - w_first, lane = threadIdx.x & 31u;
+    const uint32_t tid = threadIdx.x - 32u * w_first, nthr = 32u * nwarps, warp = tid >> 5, lane = tid & 31u;
     const int32_t fmt = D.wfmt;
     for (uint32_t bk = 0; bk < nblk; ++bk) {
         const DBlk B = s_blk[bk];
@@ -1273,30 +1314,14 @@ __device__ __forceinline__ void apply_updates_rows(const Desc& D, const DBlk* s_
             any_post |= bits != 0u;
         }
         any_post = __any_sync(kFull, any_post);
-        for (uint32_t i = warp; i < nrows; i += nwarps) {
-            const uint32_t r = B.srow + i, pl = B.row_begin + i;
-            const bool pre_spk = sm.rowflag[r] != 0u;
-            if (!pre_spk && !any_post) continue;
-            const float4 rw = sm.row[r];
-            const float sc = sm.lzs[r], qinv = sm.lzqi[r];
-            float* mrow = C.w + static_cast<size_t>(pl) * C.ld;
-            float acc = 0.0f;
-            if (pre_spk) {
-                for (uint32_t q = lane; q < n_post; q += 32u) {
-                    const float m0 = __ldcg(mrow + q);
-                    float m = m0;
-                    if (q != pl) {
-                        const uint32_t g = post_off + q;
-                        const uint32_t post_spk = (sm.sbits[g >> 5] >> (g & 31u)) & 1u;
-                        const float w = plastic_update(sc * m0, q, pl, n_post, post_spk, 1u, rw.z, __ldcg(colA + q),
-                                                       __ldcg(colB + q), rw.w, P.wmin, P.wmax);
-                        m = __fdiv_rn(w, sc);
-                        __stcg(mrow + q, m);
-                        store_copy(fmt, C, pl, q, m, qinv);
-                    }
-                    acc += m;
-                }
-            } else {
+        if (any_post) {
+            for (uint32_t i = warp; i < nrows; i += nwarps) {
+                const uint32_t r = B.srow + i, pl = B.row_begin + i;
+                if (sm.rowflag[r] != 0u) continue;  // the row pass below owns this row
+                const float4 rw = sm.row[r];
+                const float sc = sm.lzs[r], qinv = sm.lzqi[r];
+                float* mrow = C.w + static_cast<size_t>(pl) * C.ld;
+                float acc = 0.0f;
                 for (uint32_t w = w0 + lane; w <= w1; w += 32u) {
                     uint32_t bits = sm.sbits[w];
                     if (w == w0) bits &= 0xffffffffu << (post_off & 31u);
@@ -1314,9 +1339,59 @@ __device__ __forceinline__ void apply_updates_rows(const Desc& D, const DBlk* s_
                         acc += m - m0;
                     }
                 }
+                acc = warp_sum(acc);
+                if (lane == 0) sm.lzm[r] = sm.lzm[r] + acc;
             }
-            acc = warp_sum(acc);
-            if (lane == 0) sm.lzm[r] = pre_spk ? acc : sm.lzm[r] + acc;
+        }
+        for (uint32_t i0 = 0; i0 < nrows; i0 += 32u) {
+            uint32_t spk = __ballot_sync(kFull, i0 + lane < nrows && sm.rowflag[B.srow + i0 + lane] != 0u);
+            while (spk) {
+                const uint32_t i = i0 + __ffs(spk) - 1u;
+                spk &= spk - 1u;
+                const uint32_t r = B.srow + i, pl = B.row_begin + i;
+                const float4 rw = sm.row[r];
+                const float sc = sm.lzs[r], qinv = sm.lzqi[r];
+                float* mrow = C.w + static_cast<size_t>(pl) * C.ld;
+                float acc = 0.0f;
+                for (uint32_t qb = tid; qb < n_post; qb += kUpdUnroll * nthr) {
+                    float m0[kUpdUnroll], a[kUpdUnroll], b[kUpdUnroll];
+#pragma unroll
+                    for (uint32_t u = 0; u < kUpdUnroll; ++u) {
+                        const uint32_t q = qb + u * nthr;
+                        m0[u] = a[u] = b[u] = 0.0f;
+                        if (q < n_post) {
+                            m0[u] = __ldcg(mrow + q);
+                            a[u] = __ldcg(colA + q);
+                            b[u] = __ldcg(colB + q);
+                        }
+                    }
+#pragma unroll
+                    for (uint32_t u = 0; u < kUpdUnroll; ++u) {
+                        const uint32_t q = qb + u * nthr;
+                        if (q >= n_post) continue;
+                        float m = m0[u];
+                        if (q != pl) {
+                            const uint32_t g = post_off + q;
+                            const uint32_t post_spk = (sm.sbits[g >> 5] >> (g & 31u)) & 1u;
+                            const float w = plastic_update(sc * m0[u], q, pl, n_post, post_spk, 1u, rw.z, a[u], b[u],
+                                                           rw.w, P.wmin, P.wmax);
+                            m = __fdiv_rn(w, sc);
+                            __stcg(mrow + q, m);
+                            store_copy(fmt, C, pl, q, m, qinv);
+                        }
+                        acc += m;
+                    }
+                }
+                acc = warp_sum(acc);
+                if (lane == 0) sm.lzw[warp] = acc;
+                named_barrier_sync(2u, nthr);
+                if (tid == 0) {
+                    float M = 0.0f;
+                    for (uint32_t w = 0; w < nwarps; ++w) M += sm.lzw[w];
+                    sm.lzm[r] = M;
+                }
+                named_barrier_sync(2u, nthr);  // the per-warp sums are rewritten for the next row
+            }
         }
     }
 }
@@ -1700,6 +1775,7 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : LAZY ? kMaxThreadsRows :
         sm.lzq = sm.lzm + max_rows;
         sm.lzqi = sm.lzq + max_rows;
         sm.lzf = sm.lzqi + max_rows;
+        sm.lzw = sm.lzf + max_rows;
         p += z.lz;
         sm.bits = reinterpret_cast<uint32_t*>(p);
         p += z.bits;
