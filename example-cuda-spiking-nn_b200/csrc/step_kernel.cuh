@@ -1287,8 +1287,8 @@ __device__ __forceinline__ void store_copy(int32_t fmt, const DConn& C, uint32_t
 
 // The pending plasticity update in a row-scaled form, on warps [w_first, w_first + nwarps).
 // A row whose presynaptic neuron did not spike gets LTP in the columns of the spiking postsynaptic
-// neurons, one warp per row, and M grows by the sum of the changes (lanes over the bitmask words
-// in order, then an xor-butterfly).  A row whose presynaptic neuron spiked gets LTP (where the
+// neurons: every warp enumerates those columns in the same order, the threads take the rows, and
+// M grows by each change in column order.  A row whose presynaptic neuron spiked gets LTP (where the
 // postsynaptic neuron spiked) then LTD on every entry, shared out over all the threads
 // (kUpdUnroll columns each at a time, loads issued first); M is summed from the new masters: each
 // thread its columns in order, an xor-butterfly per warp, then the warp sums in warp order.
@@ -1306,41 +1306,37 @@ __device__ __forceinline__ void apply_updates_rows(const Desc& D, const DBlk* s_
         const float* colA = P.colA[ppar];
         const float* colB = P.colB[ppar];
         const uint32_t w0 = post_off >> 5, w1 = (post_off + n_post - 1u) >> 5;
-        bool any_post = false;
-        for (uint32_t w = w0 + lane; w <= w1; w += 32u) {
-            uint32_t bits = sm.sbits[w];
-            if (w == w0) bits &= 0xffffffffu << (post_off & 31u);
-            if (w == w1) bits &= 0xffffffffu >> (31u - ((post_off + n_post - 1u) & 31u));
-            any_post |= bits != 0u;
-        }
-        any_post = __any_sync(kFull, any_post);
-        if (any_post) {
-            for (uint32_t i = warp; i < nrows; i += nwarps) {
-                const uint32_t r = B.srow + i, pl = B.row_begin + i;
-                if (sm.rowflag[r] != 0u) continue;  // the row pass below owns this row
-                const float4 rw = sm.row[r];
-                const float sc = sm.lzs[r], qinv = sm.lzqi[r];
-                float* mrow = C.w + static_cast<size_t>(pl) * C.ld;
-                float acc = 0.0f;
-                for (uint32_t w = w0 + lane; w <= w1; w += 32u) {
-                    uint32_t bits = sm.sbits[w];
-                    if (w == w0) bits &= 0xffffffffu << (post_off & 31u);
-                    if (w == w1) bits &= 0xffffffffu >> (31u - ((post_off + n_post - 1u) & 31u));
-                    while (bits) {
-                        const uint32_t b = __ffs(bits) - 1u;
-                        bits &= bits - 1u;
-                        const uint32_t q = 32u * w + b - post_off;
-                        if (q == pl) continue;
+        for (uint32_t wb = w0; wb <= w1; wb += 32u) {
+            const uint32_t w = wb + lane;
+            uint32_t bits = 0u;
+            if (w <= w1) {
+                bits = sm.sbits[w];
+                if (w == w0) bits &= 0xffffffffu << (post_off & 31u);
+                if (w == w1) bits &= 0xffffffffu >> (31u - ((post_off + n_post - 1u) & 31u));
+            }
+            uint32_t nz = __ballot_sync(kFull, bits != 0u);
+            while (nz) {
+                const uint32_t src = __ffs(nz) - 1u;
+                nz &= nz - 1u;
+                uint32_t wbits = __shfl_sync(kFull, bits, src);
+                while (wbits) {
+                    const uint32_t b = __ffs(wbits) - 1u;
+                    wbits &= wbits - 1u;
+                    const uint32_t q = 32u * (wb + src) + b - post_off;
+                    const float cA = __ldcg(colA + q);
+                    for (uint32_t i = tid; i < nrows; i += nthr) {
+                        const uint32_t r = B.srow + i, pl = B.row_begin + i;
+                        if (sm.rowflag[r] != 0u || q == pl) continue;  // the row pass below owns this row
+                        const float sc = sm.lzs[r];
+                        float* mrow = C.w + static_cast<size_t>(pl) * C.ld;
                         const float m0 = __ldcg(mrow + q);
-                        const float wv = clamp_w(fmaf(rw.z, __ldcg(colA + q), sc * m0), P.wmin, P.wmax);
+                        const float wv = clamp_w(fmaf(sm.row[r].z, cA, sc * m0), P.wmin, P.wmax);
                         const float m = __fdiv_rn(wv, sc);
                         __stcg(mrow + q, m);
-                        store_copy(fmt, C, pl, q, m, qinv);
-                        acc += m - m0;
+                        store_copy(fmt, C, pl, q, m, sm.lzqi[r]);
+                        sm.lzm[r] += m - m0;  // row i always belongs to this thread: a fixed order
                     }
                 }
-                acc = warp_sum(acc);
-                if (lane == 0) sm.lzm[r] = sm.lzm[r] + acc;
             }
         }
         for (uint32_t i0 = 0; i0 < nrows; i0 += 32u) {
