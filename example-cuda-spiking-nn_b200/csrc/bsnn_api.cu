@@ -174,6 +174,10 @@ bsnn_status guarded(bsnn_sim* sim, F&& f) {
 void require(bool cond, bsnn_status code, const std::string& msg) {
     if (!cond) throw ApiError(code, msg);
 }
+// A literal message builds its std::string only when the check fails (checks run once per weight).
+void require(bool cond, bsnn_status code, const char* msg) {
+    if (!cond) throw ApiError(code, std::string(msg));
+}
 
 void require_building(const bsnn_sim* s) {
     require(!s->finalized, BSNN_ERR_STATE, "components cannot be added after the simulation has started");
@@ -1249,9 +1253,8 @@ BSNN_API bsnn_status bsnn_add_connection(bsnn_sim* sim, uint32_t pre_group, uint
         const size_t n = static_cast<size_t>(n_pre) * n_post;
         c.w.assign(weights, weights + n);
         // GpuSimulationState::require_nonnegative_weights (gpu_simulation_state.cu:221-229)
-        for (size_t k = 0; k < n; ++k)
-            require(!(c.w[k] < 0.0f), BSNN_ERR_INVALID_ARGUMENT,
-                    "connection weight_matrix must be non-negative to preserve inhibitory routing contract");
+        require(std::none_of(c.w.begin(), c.w.end(), [](float x) { return x < 0.0f; }), BSNN_ERR_INVALID_ARGUMENT,
+                "connection weight_matrix must be non-negative to preserve inhibitory routing contract");
         // Connection::make_gpu_view (connection.cpp:46-47): decays in float on the host.
         c.r_decay = std::exp(-1.0f * p->timestep / p->rise_time);
         c.d_decay = std::exp(-1.0f * p->timestep / p->decay_time);

@@ -290,3 +290,12 @@ def test_errors_surface_as_reference_exceptions():
     g.step(0)
     with pytest.raises(bsnn.StateError):
         g.add_spike_recorder(0)
+    # one negative entry anywhere in the matrix (GpuSimulationState::require_nonnegative_weights)
+    h = bsnn.Simulation(10, 5, **spec.sim_kwargs())
+    h.add_neuron_group(bsnn.NeuronGroupParams.make(offset=0, num_neurons=10))
+    neg = np.zeros((10, 10), np.float32)
+    neg[9, 7] = -1e-12
+    with pytest.raises(bsnn.InvalidArgument, match="non-negative"):
+        h.add_connection(0, 0, neg, bsnn.ConnectionParams.make(timestep=1e-4, decay_time=2e-3, rise_time=3e-4,
+                                                                weight_matrix_idx=0))
+    h.close()
