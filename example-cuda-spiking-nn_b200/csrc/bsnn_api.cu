@@ -1785,9 +1785,11 @@ BSNN_API bsnn_status bsnn_connection_propagate_noalloc(const bsnn_connection_vie
 }  // extern "C"
 
 #ifdef BSNN_PHASE_TIMING
-// Profiling builds only: SM clock cycles each CTA spent per phase (0 partial reduction, 1 neuron
-// update, 2 row table, 3 normalisation pass, 4 weight pass, 5 grid barrier), accumulated since
-// creation; out[cta * 8 + phase] for the first grid_ctas CTAs.
+// Profiling builds only (-DBSNN_PHASE_TIMING, `make libbsnn_phase.so`): SM clock cycles thread 0
+// of each CTA spent per phase of the step kernel (0 step inputs other than the partial sums,
+// 1 neuron phase beside the plasticity update and normalisation, 2 spike bits and row table,
+// 3 partial-sum loads, 4 weight pass, 5 grid barrier; 6 and 7 unused), accumulated since
+// creation; out[cta * 8 + phase] for every CTA of the grid.
 extern "C" BSNN_API bsnn_status bsnn_debug_phase_ns(bsnn_sim* sim, unsigned long long* out) {
     if (!sim || !out) return BSNN_ERR_INVALID_ARGUMENT;
     return guarded(sim, [&] {
