@@ -828,13 +828,14 @@ void finalize(bsnn_sim* s) {
         Gq.plast_post[Gq.n_plast_post++] = static_cast<int32_t>(k);
         if (PL.kind == BSNN_PLASTICITY_TRIPLET) {
             // TripletPlasticity::initialize_data (cpp_src/plasticities/triplet_plasticity.cpp:21-31):
-            // initial column sums (float, ascending pre), applied as row targets.
+            // initial column sums (float, ascending pre), applied as row targets.  Rows in the outer
+            // loop: each column still adds its entries in ascending pre order, so the sums are the
+            // same floats, without a strided walk down the columns of a row-major matrix.
             const auto& W = s->conns[PL.conn].w;
             std::vector<float> sums(C.n_pre, 0.0f);
-            for (uint32_t q = 0; q < C.n_pre; ++q) {
-                float sum = 0.0f;
-                for (uint32_t i = 0; i < C.n_pre; ++i) sum += W[static_cast<size_t>(i) * C.n_post + q];
-                sums[q] = sum;
+            for (uint32_t i = 0; i < C.n_pre; ++i) {
+                const float* row = &W[static_cast<size_t>(i) * C.n_post];
+                for (uint32_t q = 0; q < C.n_pre; ++q) sums[q] += row[q];
             }
             cuda_check(cudaMemcpy(D.sums, sums.data(), sizeof(float) * sums.size(), cudaMemcpyHostToDevice), "H2D sums");
         }

@@ -582,13 +582,13 @@ BSNN_API int32_t or_add_plasticity(or_sim* s, int32_t kind, uint32_t conn, const
                 throw Err(BSNN_ERR_INVALID_ARGUMENT, "triplet normalisation needs num_pre <= num_post");
             // TripletPlasticity::initialize_data (cpp_src/plasticities/triplet_plasticity.cpp:21-31):
             // column sums in float, ascending pre; used as row targets.
+            // (rows in the outer loop: every column still adds in ascending pre order)
+            std::vector<float> fsum(c.n_post, 0.0f);
+            for (uint32_t i = 0; i < c.n_pre; ++i)
+                for (uint32_t q = 0; q < c.n_post; ++q)
+                    fsum[q] += static_cast<float>(c.w[static_cast<size_t>(i) * c.n_post + q]);
             std::vector<R> cols(c.n_post, R(0));
-            for (uint32_t q = 0; q < c.n_post; ++q) {
-                float sum = 0.0f;
-                for (uint32_t i = 0; i < c.n_pre; ++i)
-                    sum += static_cast<float>(c.w[static_cast<size_t>(i) * c.n_post + q]);
-                cols[q] = R(sum);
-            }
+            for (uint32_t q = 0; q < c.n_post; ++q) cols[q] = R(fsum[q]);
             pl.sums.assign(cols.begin(), cols.begin() + c.n_pre);
         }
         sim.plasts.push_back(std::move(pl));
