@@ -759,11 +759,15 @@ void finalize(bsnn_sim* s) {
         D.ts = conn_ts[c];
         D.plast = -1;
         D.w = F(o_w[c]);
-        std::vector<float> padded(static_cast<size_t>(D.n_pre) * D.ld, 0.0f);
-        for (uint32_t i = 0; i < D.n_pre; ++i)
-            std::memcpy(&padded[static_cast<size_t>(i) * D.ld], &C.w[static_cast<size_t>(i) * D.n_post],
-                        sizeof(float) * D.n_post);
-        cuda_check(cudaMemcpy(D.w, padded.data(), sizeof(float) * padded.size(), cudaMemcpyHostToDevice), "H2D w");
+        if (D.ld == D.n_post) {  // no padding columns: the rows are already laid out as on the device
+            cuda_check(cudaMemcpy(D.w, C.w.data(), sizeof(float) * C.w.size(), cudaMemcpyHostToDevice), "H2D w");
+        } else {
+            std::vector<float> padded(static_cast<size_t>(D.n_pre) * D.ld, 0.0f);
+            for (uint32_t i = 0; i < D.n_pre; ++i)
+                std::memcpy(&padded[static_cast<size_t>(i) * D.ld], &C.w[static_cast<size_t>(i) * D.n_post],
+                            sizeof(float) * D.n_post);
+            cuda_check(cudaMemcpy(D.w, padded.data(), sizeof(float) * padded.size(), cudaMemcpyHostToDevice), "H2D w");
+        }
         if (lazy) {
             const bool fp8 = s->weight_format == BSNN_WEIGHTS_FP8_E4M3;
             D.q = base + o_q[c];
