@@ -38,6 +38,7 @@ struct bsnn_batch {
     bool noise_on = true;
 
     bool finalized = false, failed = false;
+    uint64_t wait_limit_ns = kDefaultWaitLimitNs;  // bound of every device-side wait
     unsigned char* arena = nullptr;
     size_t arena_bytes = 0;
     BSim h{};
@@ -261,6 +262,7 @@ void batch_finalize(bsnn_batch* b) {
     h.partials = F(o_part);
     h.barrier = reinterpret_cast<unsigned long long*>(base + o_bar);
     h.error = reinterpret_cast<int32_t*>(base + o_err);
+    h.wait_limit_ns = b->wait_limit_ns;
     h.steps_done = reinterpret_cast<unsigned long long*>(base + o_sd);
     b->scratch = F(o_scr);
 
@@ -540,6 +542,20 @@ BSNN_API bsnn_status bsnn_batch_set_steps_per_launch(bsnn_batch* b, uint32_t ste
     return guarded_batch(b, [&] {
         require(steps > 0, BSNN_ERR_INVALID_ARGUMENT, "steps per launch must be > 0");
         b->steps_per_launch = steps;
+    });
+}
+
+BSNN_API bsnn_status bsnn_batch_set_device_wait_limit(bsnn_batch* b, uint64_t nanoseconds) {
+    if (!b) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded_batch(b, [&] {
+        require(nanoseconds >= 1000ull && nanoseconds <= 60000000000ull, BSNN_ERR_INVALID_ARGUMENT,
+                "device wait limit must be in [1 us, 60 s]");
+        b->wait_limit_ns = nanoseconds;
+        if (b->finalized) {
+            b->h.wait_limit_ns = nanoseconds;
+            cuda_check(cudaStreamSynchronize(b->stream), "stream synchronize");
+            cuda_check(cudaMemcpy(b->d_sim, &b->h, sizeof(BSim), cudaMemcpyHostToDevice), "H2D batch sim");
+        }
     });
 }
 

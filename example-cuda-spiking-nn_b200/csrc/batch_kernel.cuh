@@ -118,6 +118,7 @@ struct BSim {
     unsigned long long* barrier;
     int32_t* error;
     unsigned long long* steps_done;
+    unsigned long long wait_limit_ns;  // bound of every device-side wait of a launch
 };
 
 // ---- tcgen05 / tensor-memory wrappers ---------------------------------------------------------
@@ -471,6 +472,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
     __shared__ int s_ok;
     __shared__ unsigned long long s_bar0, s_t0;
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+    if (tid == 0) s_wait_limit_ns = S->wait_limit_ns;  // read after the first __syncthreads below
     // stage s: A tile at s * stage_bytes, B tile after it; then the instance table (when it is
     // kept in shared memory), then the neuron state (when it is kept in shared memory)
     const uint32_t stage_bytes = S->stage_bytes, n_stages = S->n_stages;
