@@ -315,6 +315,7 @@ SIGNATURES = {
                                        _U32, ctypes.POINTER(_U32)]),
     "bsnn_batch_set_noise": (_I32, [_P, _I32]),
     "bsnn_batch_set_steps_per_launch": (_I32, [_P, _U32]),
+    "bsnn_batch_set_device_wait_limit": (_I32, [_P, ctypes.c_uint64]),
     "bsnn_batch_run": (_I32, [_P, _U32]),
     "bsnn_batch_synchronize": (_I32, [_P]),
     "bsnn_batch_get_stream": (_I32, [_P, ctypes.POINTER(_P)]),
@@ -351,6 +352,9 @@ SIGNATURES = {
     "bsnn_synchronize": (_I32, [_P]),
     "bsnn_get_stream": (_I32, [_P, ctypes.POINTER(_P)]),
     "bsnn_set_steps_per_launch": (_I32, [_P, _U32]),
+    "bsnn_set_device_wait_limit": (_I32, [_P, ctypes.c_uint64]),
+    "bsnn_debug_skip_arrival": (_I32, [_P, _U32, ctypes.c_uint64]),
+    "bsnn_measure_exchange_floor": (_I32, [_P, _U32, ctypes.POINTER(ctypes.c_float)]),
     "bsnn_read_state": (_I32, [_P, _I32, _U32, _U32, _U32, _P]),
     "bsnn_write_state": (_I32, [_P, _I32, _U32, _U32, _U32, _P]),
     "bsnn_read_weights": (_I32, [_P, _U32, _FP]),
@@ -364,6 +368,8 @@ SIGNATURES = {
     "bsnn_record": (_I32, [_P, _U32]),
     "bsnn_flush_records": (_I32, [_P]),
     "bsnn_run_system": (_I32, [_P, _U32]),
+    "bsnn_set_progress_output": (_I32, [_P, _I32]),
+    "bsnn_memory_report": (_I32, [_P, ctypes.c_char_p, ctypes.c_uint64]),
     "bsnn_connection_propagate": (_I32, [ctypes.POINTER(ConnectionView), _P]),
     "bsnn_connection_propagate_noalloc": (_I32, [ctypes.POINTER(ConnectionView), _P]),
 }

@@ -56,6 +56,18 @@ class BatchSpec:
     classes: list = field(default_factory=list)
     instances: list = field(default_factory=list)
 
+    def subset(self, indices) -> "BatchSpec":
+        """The instances at `indices` (in that order) as a batch of their own: the same weight sets,
+        parameters, seeds and stimuli, so each runs exactly as it does in the full batch.  Classes
+        no listed instance uses are dropped."""
+        used = sorted({self.instances[b].cls for b in indices})
+        remap = {c: k for k, c in enumerate(used)}
+        out = BatchSpec(total_steps=self.total_steps, classes=[self.classes[c] for c in used])
+        for b in indices:
+            inst = self.instances[b]
+            out.instances.append(BatchInstance(remap[inst.cls], inst.e_group, inst.i_group, inst.seed, inst.stimulus))
+        return out
+
     def instance_network(self, b: int) -> NetworkSpec:
         inst = self.instances[b]
         c = self.classes[inst.cls]
@@ -165,6 +177,10 @@ class BatchSimulation:
 
     def set_steps_per_launch(self, steps: int):
         self._check(self._lib.bsnn_batch_set_steps_per_launch(self._h, steps))
+
+    def set_device_wait_limit(self, seconds: float):
+        """Bound of every device-side wait of the batch kernel (default 2 s)."""
+        self._check(self._lib.bsnn_batch_set_device_wait_limit(self._h, int(round(seconds * 1e9))))
 
     def synchronize(self):
         self._check(self._lib.bsnn_batch_synchronize(self._h))

@@ -153,6 +153,21 @@ class Simulation:
     def set_steps_per_launch(self, steps: int):
         self._check(self._lib.bsnn_set_steps_per_launch(self._h, steps))
 
+    def set_device_wait_limit(self, seconds: float):
+        """Bound of every device-side wait of the persistent kernel (default 2 s)."""
+        self._check(self._lib.bsnn_set_device_wait_limit(self._h, int(round(seconds * 1e9))))
+
+    def exchange_floor_us(self, steps: int = 2000) -> float:
+        """Latency floor of one clock step (microseconds): the partial-sum exchange and grid barrier
+        of the persistent kernel run alone, with this network's grid and plan."""
+        out = ctypes.c_float()
+        self._check(self._lib.bsnn_measure_exchange_floor(self._h, steps, ctypes.byref(out)))
+        return float(out.value)
+
+    def debug_skip_arrival(self, cta: int, step: int):
+        """Test switch: CTA `cta` skips its arrival at the grid barrier ending internal step `step`."""
+        self._check(self._lib.bsnn_debug_skip_arrival(self._h, cta, step))
+
     # -- state ------------------------------------------------------------------------------
     def _field_len(self, name: str, index: int) -> int:
         if name.startswith("connection_"):
@@ -239,6 +254,17 @@ class Simulation:
     def run_system(self, total_clock_steps: int) -> None:
         """System::run without callbacks: steps 0 .. total-1, recording at multiples of the interval."""
         self._check(self._lib.bsnn_run_system(self._h, total_clock_steps))
+
+    def set_progress_output(self, enabled: bool) -> None:
+        """run_system prints System::run's "Completed clock step: ... | elapsed: ...s" lines."""
+        self._check(self._lib.bsnn_set_progress_output(self._h, 1 if enabled else 0))
+
+    def memory_report(self) -> str:
+        """GpuSimulationState::memory_report: "Total GPU Memory Allocated: <bytes> bytes (<MB> MB)".
+        Finalises the network (allocates its device arena) when it has not run yet."""
+        buf = ctypes.create_string_buffer(256)
+        self._check(self._lib.bsnn_memory_report(self._h, buf, len(buf)))
+        return buf.value.decode()
 
     def device_pointer(self, name: str, index: int = 0) -> int:
         p = ctypes.c_void_p()

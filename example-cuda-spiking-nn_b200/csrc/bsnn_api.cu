@@ -9,11 +9,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <iostream>
 #include <map>
 #include <memory>
 #include <numeric>
@@ -121,6 +123,10 @@ struct bsnn_sim {
     uint32_t next_clock = 0;
     uint32_t steps_per_launch = 1000;
     uint64_t launches = 0;
+    bool progress = false;  // bsnn_run_system prints System::run's progress line
+    uint64_t wait_limit_ns = kDefaultWaitLimitNs;  // bound of every device-side wait
+    uint64_t skip_step = ~0ull;                      // test switch (bsnn_debug_skip_arrival)
+    uint32_t skip_cta = 0;
     bool graphs_ok = true;
     std::map<uint32_t, cudaGraphExec_t> graphs;
     std::vector<uint32_t> conn_ld;
@@ -713,7 +719,7 @@ void finalize(bsnn_sim* s) {
     size_t o_err = A.take(sizeof(int32_t));
     size_t o_sd = A.take(sizeof(unsigned long long));
     size_t o_clk = A.take(sizeof(uint32_t));
-    size_t o_pns = A.take(sizeof(unsigned long long) * 8 * std::max<uint32_t>(s->sm_count, 1));
+    size_t o_pns = A.take(sizeof(unsigned long long) * kPhaseSlots * std::max<uint32_t>(s->sm_count, 1));
     size_t o_sim = A.take(sizeof(DSim));
 
     cuda_check(cudaMalloc(&s->arena, A.size), "cudaMalloc arena");
@@ -905,6 +911,9 @@ void finalize(bsnn_sim* s) {
     h.steps_done = reinterpret_cast<unsigned long long*>(base + o_sd);
     h.clock = U(o_clk);
     h.phase_ns = reinterpret_cast<unsigned long long*>(base + o_pns);
+    h.wait_limit_ns = s->wait_limit_ns;
+    h.skip_step = s->skip_step;
+    h.skip_cta = s->skip_cta;
     s->d_sim = reinterpret_cast<DSim*>(base + o_sim);
     cuda_check(cudaMemcpy(s->d_sim, &h, sizeof(DSim), cudaMemcpyHostToDevice), "H2D sim");
 
@@ -1436,6 +1445,87 @@ BSNN_API bsnn_status bsnn_set_steps_per_launch(bsnn_sim* sim, uint32_t steps) {
     });
 }
 
+// Re-uploads the launch descriptor after a host-side change of one of its scalar fields (the next
+// launch reads it; queued launches finish first).
+static void upload_descriptor(bsnn_sim* sim) {
+    if (!sim->finalized) return;
+    sim->h.wait_limit_ns = sim->wait_limit_ns;
+    sim->h.skip_step = sim->skip_step;
+    sim->h.skip_cta = sim->skip_cta;
+    cuda_check(cudaStreamSynchronize(sim->stream), "stream synchronize");
+    cuda_check(cudaMemcpy(sim->d_sim, &sim->h, sizeof(DSim), cudaMemcpyHostToDevice), "H2D descriptor");
+}
+
+BSNN_API bsnn_status bsnn_set_device_wait_limit(bsnn_sim* sim, uint64_t nanoseconds) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        require(nanoseconds >= 1000ull && nanoseconds <= 60000000000ull, BSNN_ERR_INVALID_ARGUMENT,
+                "device wait limit must be in [1 us, 60 s]");
+        sim->wait_limit_ns = nanoseconds;
+        upload_descriptor(sim);
+    });
+}
+
+BSNN_API bsnn_status bsnn_measure_exchange_floor(bsnn_sim* sim, uint32_t num_steps, float* out_us_per_step) {
+    if (!sim || !out_us_per_step) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        require(num_steps >= 1 && num_steps <= 1000000, BSNN_ERR_INVALID_ARGUMENT, "num_steps must be in [1, 1e6]");
+        finalize(sim);
+        require(!sim->failed, BSNN_ERR_STATE, "simulation failed earlier (device timeout)");
+        const size_t smem = align16(sizeof(float) * 2u * sim->h.max_own) + align16(sizeof(DGroup) * sim->h.n_groups) +
+                            sizeof(uint32_t) * sim->h.n_red;
+        const void* fn = reinterpret_cast<const void*>(&bsnn_exchange_floor_kernel);
+        cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+                   "cudaFuncSetAttribute smem (exchange floor)");
+        int per_sm = 0;
+        cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, static_cast<int>(sim->block), smem),
+                   "occupancy (exchange floor)");
+        require(static_cast<uint64_t>(per_sm) * sim->sm_count >= sim->grid, BSNN_ERR_RUNTIME,
+                "exchange-floor kernel cannot be co-resident with the step kernel's grid");
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(sim->grid);
+        cfg.blockDim = dim3(sim->block);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = sim->stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        const DSim* arg0 = sim->d_sim;
+        uint32_t n = num_steps;
+        void* args[2] = {&arg0, &n};
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        cuda_check(cudaEventCreate(&e0), "event");
+        cuda_check(cudaEventCreate(&e1), "event");
+        // a warm-up launch, then the timed one
+        cudaError_t le = cudaLaunchKernelExC(&cfg, fn, args);
+        if (le == cudaSuccess) le = cudaEventRecord(e0, sim->stream);
+        if (le == cudaSuccess) le = cudaLaunchKernelExC(&cfg, fn, args);
+        if (le == cudaSuccess) le = cudaEventRecord(e1, sim->stream);
+        float ms = 0.0f;
+        if (le == cudaSuccess) le = cudaEventSynchronize(e1);
+        if (le == cudaSuccess) le = cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cuda_check(le, "exchange floor launch");
+        check_device_error(sim);
+        *out_us_per_step = 1000.0f * ms / static_cast<float>(num_steps);
+    });
+}
+
+BSNN_API bsnn_status bsnn_debug_skip_arrival(bsnn_sim* sim, uint32_t cta, uint64_t step) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        finalize(sim);
+        require(cta < sim->grid, BSNN_ERR_OUT_OF_RANGE,
+                "cta " + std::to_string(cta) + " is not in the grid of " + std::to_string(sim->grid));
+        sim->skip_cta = cta;
+        sim->skip_step = step;
+        upload_descriptor(sim);
+    });
+}
+
 // ---- checkpoint / resume ---------------------------------------------------------------------
 // A checkpoint is the simulation's whole device arena (neuron state, traces, weights and their
 // copies, plasticity traces, monitor rings, the step counters, the planned work lists) plus the
@@ -1736,15 +1826,42 @@ BSNN_API bsnn_status bsnn_run_system(bsnn_sim* sim, uint32_t total_clock_steps) 
     if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
     return guarded(sim, [&] {
         const uint32_t interval = sim->desc.recording_interval_steps;
+        const auto start_time = std::chrono::steady_clock::now();
         uint32_t step = 0;
         while (step < total_clock_steps) {
             // record after every step that is a multiple of the interval (system.cpp:71-76)
             const uint64_t next = (static_cast<uint64_t>(step) + interval - 1u) / interval * interval;
             const uint32_t end = static_cast<uint32_t>(std::min<uint64_t>(total_clock_steps, next + 1u));
             run_steps(sim, step, end - step);
-            if (end == next + 1u) record_all(sim, static_cast<uint32_t>(next));
+            if (end == next + 1u) {
+                record_all(sim, static_cast<uint32_t>(next));
+                if (sim->progress) {  // the progress line of system.cpp:78-81, after the record
+                    const std::chrono::duration<float> elapsed = std::chrono::steady_clock::now() - start_time;
+                    std::cout << "Completed clock step: " << next << " | elapsed: " << elapsed.count() << "s\n" << std::flush;
+                }
+            }
             step = end;
         }
+    });
+}
+
+BSNN_API bsnn_status bsnn_set_progress_output(bsnn_sim* sim, int32_t enabled) {
+    if (!sim) return BSNN_ERR_INVALID_ARGUMENT;
+    sim->progress = enabled != 0;
+    return BSNN_OK;
+}
+
+BSNN_API bsnn_status bsnn_memory_report(bsnn_sim* sim, char* buf, uint64_t capacity) {
+    if (!sim || (!buf && capacity)) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&] {
+        finalize(sim);
+        const uint64_t total = sim->arena_bytes;
+        char text[160];
+        std::snprintf(text, sizeof(text), "Total GPU Memory Allocated: %llu bytes (%f MB)",
+                      static_cast<unsigned long long>(total), static_cast<double>(total) / (1024.0 * 1024.0));
+        require(capacity > std::strlen(text), BSNN_ERR_OUT_OF_RANGE,
+                "memory report needs " + std::to_string(std::strlen(text) + 1) + " bytes of buffer");
+        std::memcpy(buf, text, std::strlen(text) + 1);
     });
 }
 
@@ -1790,16 +1907,15 @@ BSNN_API bsnn_status bsnn_connection_propagate_noalloc(const bsnn_connection_vie
 }  // extern "C"
 
 #ifdef BSNN_PHASE_TIMING
-// Profiling builds only (-DBSNN_PHASE_TIMING, `make libbsnn_phase.so`): SM clock cycles thread 0
-// of each CTA spent per phase of the step kernel (0 step inputs other than the partial sums,
-// 1 neuron phase beside the plasticity update and normalisation, 2 spike bits and row table,
-// 3 partial-sum loads, 4 weight pass, 5 grid barrier; 6 and 7 unused), accumulated since
-// creation; out[cta * 8 + phase] for every CTA of the grid.
+// Profiling builds only (-DBSNN_PHASE_TIMING, `make libbsnn_phase.so`): SM clock cycles per phase of
+// the step kernel (the slots listed beside BSNN_TMARK in step_kernel.cuh), accumulated since
+// creation; out[cta * kPhaseSlots + slot] for every CTA of the grid.
 extern "C" BSNN_API bsnn_status bsnn_debug_phase_ns(bsnn_sim* sim, unsigned long long* out) {
     if (!sim || !out) return BSNN_ERR_INVALID_ARGUMENT;
     return guarded(sim, [&] {
         check_device_error(sim);
-        cuda_check(cudaMemcpy(out, sim->h.phase_ns, 8 * sizeof(unsigned long long) * sim->grid, cudaMemcpyDeviceToHost),
+        cuda_check(cudaMemcpy(out, sim->h.phase_ns, kPhaseSlots * sizeof(unsigned long long) * sim->grid,
+                              cudaMemcpyDeviceToHost),
                    "D2H");
     });
 }

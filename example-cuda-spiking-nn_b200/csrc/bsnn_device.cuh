@@ -25,6 +25,7 @@ constexpr int kMaxMonitors = 16;
 constexpr int kMaxGroupRoles = 4;  // trace sets / plasticities / monitors per group and role
 constexpr int kMaxSegsPerCta = 2 * kMaxGroups;
 constexpr int kMaxBlksPerCta = kMaxConns;
+constexpr int kPhaseSlots = 16;  // per-CTA phase tallies of the step kernel (profiling builds)
 // Threads per CTA: the step-kernel instance that carries row sums needs up to 255 registers per
 // thread (256 threads); the others fit in 168 registers (three warps share one scheduler's
 // quarter of the register file): 288 threads for the reference form, 384 for the row-scaled
@@ -211,7 +212,12 @@ struct DSim {
     int32_t* error;
     unsigned long long* steps_done;  // internal step counter (stimulus / noise cursor)
     uint32_t* clock;                 // clock_step of the next step
-    unsigned long long* phase_ns;    // [8] per-phase time of CTA 0 (profiling builds only)
+    unsigned long long* phase_ns;    // [n_ctas][kPhaseSlots] phase clock tallies (profiling builds only)
+    unsigned long long wait_limit_ns;  // bound of every device-side wait of a launch
+    // Test switch (bsnn_debug_skip_arrival): CTA skip_cta does not arrive at the grid barrier that
+    // closes internal step skip_step, so every CTA's bounded wait runs out.  ~0 = off.
+    unsigned long long skip_step;
+    uint32_t skip_cta;
 };
 
 }  // namespace bsnn

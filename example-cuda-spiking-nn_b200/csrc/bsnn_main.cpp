@@ -216,6 +216,7 @@ int run(const bsnn::Config& cfg, const std::string& config_path, int32_t weight_
     system.add_monitor(std::make_unique<bsnn::VoltageRecorder>(e, cfg.voltage_recording_file,
                                                                cfg.voltage_recording_neuron_ids, interval, state));
     system.add_monitor(std::make_unique<bsnn::WeightRecorder>(ee, cfg.e_e_weight_recording_file, state));
+    std::cout << state.memory_report() << "\n";
     std::cout << "Running simulation...\n";
     system.run(cfg.simulation_steps);
     std::cout << "Simulation complete.\n";

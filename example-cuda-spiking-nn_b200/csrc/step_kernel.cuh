@@ -41,7 +41,11 @@
 
 namespace bsnn {
 
-constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;  // 2 s
+// Every device-side wait (the grid barrier, the staging mbarriers) gives up after the launch's wait
+// limit, a DSim field the host sets (2 s unless bsnn_set_device_wait_limit changed it).  Each
+// kernel that waits copies it into this shared variable before its first wait.
+constexpr unsigned long long kDefaultWaitLimitNs = 2000000000ull;  // 2 s
+__shared__ unsigned long long s_wait_limit_ns;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kRowBatch = 4;     // rows whose weights one thread loads before using them (plastic rows)
 constexpr int kStreamBatch = 4;  // same for read-only rows
@@ -129,14 +133,15 @@ __device__ __forceinline__ void red_release_add_u64(unsigned long long* p, unsig
 // After the CTA-wide sync, thread 0 arrives with a gpu-scope release reduction (no return value
 // to wait for) and spins with gpu-scope acquire loads until the counter reaches `target`, the
 // count at which every CTA has arrived; the closing CTA-wide sync extends the acquire to the
-// whole CTA.  Bounded: after kBarrierTimeoutNs (or when another CTA has already given up) it
-// records kErrBarrierTimeout and returns false so the kernel can exit.
+// whole CTA.  Bounded: after s_wait_limit_ns (or when another CTA has already given up) it
+// records kErrBarrierTimeout and returns false so the kernel can exit.  `arrive` false (a test
+// switch only) makes this CTA wait without arriving, so that every CTA's wait runs out.
 __device__ __forceinline__ bool grid_barrier(unsigned long long* barrier, int32_t* error, unsigned long long target,
-                                             int* s_ok) {
+                                             int* s_ok, bool arrive = true) {
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
-        red_release_add_u64(barrier, 1ull);
+        if (arrive) red_release_add_u64(barrier, 1ull);
         unsigned long long t_start = 0;
         uint32_t spins = 0;
         while (static_cast<long long>(ld_acquire_u64(barrier) - target) < 0) {
@@ -144,7 +149,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned long long* barrier, int32_
                 const unsigned long long now = globaltimer_ns();
                 if (t_start == 0) {
                     t_start = now;
-                } else if (now - t_start > kBarrierTimeoutNs) {
+                } else if (now - t_start > s_wait_limit_ns) {
                     atomicExch(error, kErrBarrierTimeout);
                     ok = 0;
                     break;
@@ -163,9 +168,12 @@ __device__ __forceinline__ bool grid_barrier(unsigned long long* barrier, int32_
 
 // Optional phase timing (profiling builds only, -DBSNN_PHASE_TIMING): thread 0 of every CTA adds
 // the SM clock cycles spent in each phase to a shared-memory tally (s_tally_[phase]) that the
-// kernel adds to S->phase_ns[cta * 8 + phase] when it ends: 3 partial-sum loads, 0 rest of the
-// step inputs, 1 neuron phase beside the plasticity update and normalisation, 2 spike bits and
-// row x, 4 weight pass, 5 grid barrier.
+// kernel adds to S->phase_ns[cta * kPhaseSlots + phase] when it ends: 3 partial-sum loads, 0 rest
+// of the step inputs, 1 neuron phase beside the plasticity update and normalisation, 2 spike bits
+// and row x, 4 weight pass, 5 grid barrier.  Spans of single threads inside those phases: 6 the
+// neuron warp's own neuron phase, 7 the update warps' update plus normalisation sums, 8 their
+// update alone, 9 thread 0's share of the weight pass, 10 the last warp's share of it, 11 thread
+// 0's share of the spike-bit merge.
 #ifdef BSNN_PHASE_TIMING
 #define BSNN_TMARK(slot)                                                                   \
     do {                                                                                   \
@@ -175,9 +183,19 @@ __device__ __forceinline__ bool grid_barrier(unsigned long long* barrier, int32_
             t_mark_ = now_;                                                                \
         }                                                                                  \
     } while (0)
+// Per-thread spans (same builds): the calling thread adds the cycles since its own start mark
+// to s_tally_[slot] (one thread per slot, so no two threads add to the same slot).
+#define BSNN_TSTART(var) const unsigned long long var = static_cast<unsigned long long>(clock64())
+#define BSNN_TSPAN(slot, var) (s_tally_[(slot)] += static_cast<unsigned long long>(clock64()) - (var))
 #else
 #define BSNN_TMARK(slot) \
     do {                 \
+    } while (0)
+#define BSNN_TSTART(var) \
+    do {                 \
+    } while (0)
+#define BSNN_TSPAN(slot, var) \
+    do {                      \
     } while (0)
 #endif
 
@@ -210,6 +228,8 @@ struct Desc {
     uint32_t stage_rows;  // rows per staging buffer (0 = streamed rows are loaded directly)
     int32_t wfmt;         // weight storage form (kFmt*)
     uint32_t q_nonneg;    // FP8 copy decoded by bit placement (non-negative weights)
+    unsigned long long skip_step;  // test switch (DSim::skip_step)
+    uint32_t skip_cta;
 };
 
 // Values produced and consumed by the same CTA stay in shared memory: x of the own neurons, the
@@ -780,7 +800,6 @@ __device__ __forceinline__ void sts4(uint32_t a, float4 v) {
 __device__ __forceinline__ uint32_t saddr(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
 
 // mbarrier and bulk asynchronous copy (global -> this CTA's shared memory, no multicast).
-constexpr unsigned long long kStageTimeoutNs = 2000000000ull;  // 2 s
 constexpr uint32_t kStageDead = 0x80000000u;  // staging gave up (stage_phase bit)
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
@@ -804,7 +823,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = globaltimer_ns();
     while (!mbar_try_wait(bar, parity))
-        if (globaltimer_ns() - t0 > kStageTimeoutNs) return false;
+        if (globaltimer_ns() - t0 > s_wait_limit_ns) return false;
     return true;
 }
 __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
@@ -1731,6 +1750,7 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : LAZY ? kMaxThreadsRows :
                                    S->max_trows * S->n_chunks, S->stage_warps, S->stage_rows,
                                    LAZY ? max_rows : 0u);
     if (threadIdx.x == 0) {
+        s_wait_limit_ns = S->wait_limit_ns;
         s_L = L0;
         unsigned char* p = smem_raw;
         sm.wres = reinterpret_cast<float*>(p);
@@ -1831,6 +1851,8 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : LAZY ? kMaxThreadsRows :
         s_d.stage_rows = S->stage_rows;
         s_d.wfmt = S->wfmt;
         s_d.q_nonneg = S->q_nonneg;
+        s_d.skip_step = S->skip_step;
+        s_d.skip_cta = S->skip_cta;
         uint32_t base = 0;
         for (uint32_t m = 0; m < S->n_mons; ++m) {
             s_d.bitbase[m] = base;
@@ -1916,9 +1938,10 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : LAZY ? kMaxThreadsRows :
     const uint32_t clock0 = s_clock0;
     bool ok = true;
 #ifdef BSNN_PHASE_TIMING
-    __shared__ unsigned long long s_tally_[8];
+    __shared__ unsigned long long s_tally_[kPhaseSlots];
     if (threadIdx.x == 0)
-        for (int i = 0; i < 8; ++i) s_tally_[i] = 0;
+        for (int i = 0; i < kPhaseSlots; ++i) s_tally_[i] = 0;
+    __syncthreads();
     unsigned long long t_mark_ = static_cast<unsigned long long>(clock64());
 #endif
     for (uint32_t k = 0; k < n_steps; ++k) {
@@ -1960,16 +1983,21 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : LAZY ? kMaxThreadsRows :
             // The neuron phase on the first warps; the plasticity update and then the normalisation
             // sums on the others (they touch no data of the neuron phase).
             if (tid < 32u * neuron_warps) {
+                BSNN_TSTART(t_nrn_);
                 neuron_phase(S, D, cta, t, clock, par, pending, sm, max_own, L, s_ev[0], s_ev[1]);
+                if (tid == 0) BSNN_TSPAN(6, t_nrn_);
             } else if (pending) {
+                BSNN_TSTART(t_upd_);
                 const uint32_t nw = nwarps - neuron_warps;
                 if constexpr (LAZY) apply_updates_rows(D, s_blk, s_nblk, ppar, sm, neuron_warps, nw);
                 else apply_updates(D, s_blk, s_nblk, ppar, sm, neuron_warps, nw);
+                if (tid == 32u * neuron_warps) BSNN_TSPAN(8, t_upd_);
                 if (norm_now) {
                     named_barrier_sync(1u, 32u * nw);
                     if constexpr (LAZY) norm_rows_lazy(D, sm, s_blk, s_nblk, neuron_warps, nw);
                     else norm_rows<CARRY>(D, sm, s_blk, s_nblk, neuron_warps, nw, n_chunks);
                 }
+                if (tid == 32u * neuron_warps) BSNN_TSPAN(7, t_upd_);
             }
             __syncthreads();
         } else {
@@ -1987,22 +2015,33 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : LAZY ? kMaxThreadsRows :
             }
         }
         BSNN_TMARK(1);
-        flush_spike_bits(S, D, cta, clock, par, sm);
+        {
+            BSNN_TSTART(t_fl_);
+            flush_spike_bits(S, D, cta, clock, par, sm);
+            if (tid == 0) BSNN_TSPAN(11, t_fl_);
+        }
         rows_x(D, cta, sm, max_own);
         __syncthreads();
         BSNN_TMARK(2);
-        weight_pass<CARRY, LAZY>(D, cta, pending, true, par, sm, s_seg, s_blk, n_seg, n_chunks);
+        {
+            BSNN_TSTART(t_wp_);
+            weight_pass<CARRY, LAZY>(D, cta, pending, true, par, sm, s_seg, s_blk, n_seg, n_chunks);
+            if (tid == 0) BSNN_TSPAN(9, t_wp_);
+            if (tid == blockDim.x - 32u) BSNN_TSPAN(10, t_wp_);
+        }
         __syncthreads();
         BSNN_TMARK(4);
-        if (!grid_barrier(D.barrier, D.error, bar0 + (k + 1ull) * gridDim.x, &s_ok)) {
+        if (!grid_barrier(D.barrier, D.error, bar0 + (k + 1ull) * gridDim.x, &s_ok,
+                          t != D.skip_step || blockIdx.x != D.skip_cta)) {
             ok = false;
             break;
         }
         BSNN_TMARK(5);
     }
 #ifdef BSNN_PHASE_TIMING
+    __syncthreads();
     if (threadIdx.x == 0)
-        for (int i = 0; i < 8; ++i) S->phase_ns[blockIdx.x * 8u + i] += s_tally_[i];
+        for (int i = 0; i < kPhaseSlots; ++i) S->phase_ns[blockIdx.x * kPhaseSlots + i] += s_tally_[i];
 #endif
     if (!ok) return;
 
@@ -2057,6 +2096,73 @@ __global__ void bsnn_fill_copy_kernel(DConn C, int32_t fmt) {
         const uint32_t i = static_cast<uint32_t>(tr % C.n_pre), q = static_cast<uint32_t>(tr / C.n_pre) * 128u + k;
         const float m = q < C.n_post ? C.w[static_cast<size_t>(i) * C.ld + q] : 0.0f;
         store_copy(fmt, C, i, q, m, C.qinv ? C.qinv[i] : 1.0f);
+    }
+}
+
+// The communication skeleton of bsnn_step_kernel's clock step, timed to give the step a latency
+// floor: per step every CTA stores its partial-sum slots (the weight pass's stores, without the
+// weights), crosses the grid barrier and gathers its own columns from every slot (load_partials,
+// the same code as the step kernel), with the same grid, block and plan.  Nothing else of a step
+// runs, so no step can be faster than this.  It writes only the partial-sum buffers (dead between
+// launches: each launch folds the pending partials into g before it ends) and the barrier counter
+// (left a multiple of the grid size, as every launch leaves it).
+__global__ void __launch_bounds__(kMaxThreadsRows, 1) bsnn_exchange_floor_kernel(const DSim* __restrict__ S,
+                                                                                 uint32_t n_steps) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ Desc s_d;
+    __shared__ DCta s_cta;
+    __shared__ DSeg s_seg[kMaxSegsPerCta];
+    __shared__ SmemLayout sm;
+    __shared__ int s_ok;
+    __shared__ unsigned long long s_bar0;
+    const uint32_t max_own = S->max_own;
+    const size_t red_bytes = align16(sizeof(float) * 2u * max_own);
+    const size_t grp_bytes = align16(sizeof(DGroup) * S->n_groups);
+    if (threadIdx.x == 0) {
+        s_wait_limit_ns = S->wait_limit_ns;
+        sm.red = reinterpret_cast<float*>(smem_raw);
+        s_d.groups = reinterpret_cast<const DGroup*>(smem_raw + red_bytes);
+        s_d.red_list = reinterpret_cast<const uint32_t*>(smem_raw + red_bytes + grp_bytes);
+        s_d.n_groups = S->n_groups;
+        s_d.partials = S->partials;
+        s_d.n_slots = S->n_slots;
+        s_d.N_pad = S->N_pad;
+        s_d.max_own = max_own;
+        s_d.barrier = S->barrier;
+        s_d.error = S->error;
+        for (uint32_t g = 0; g < S->n_groups; ++g) {
+            s_d.goff[g] = S->groups[g].off;
+            s_d.gn[g] = S->groups[g].n;
+        }
+        for (uint32_t T = 0; T < 2; ++T)
+            for (uint32_t g = 0; g < kMaxGroups; ++g) {
+                s_d.red_begin[T][g] = S->red_begin[T][g];
+                s_d.red_end[T][g] = S->red_end[T][g];
+            }
+        s_cta = S->ctas[blockIdx.x];
+        for (uint32_t s = s_cta.seg_begin; s < s_cta.seg_end; ++s) s_seg[s - s_cta.seg_begin] = S->segs[s];
+        const unsigned long long n = gridDim.x;
+        s_bar0 = ld_acquire_u64(S->barrier) / n * n;
+    }
+    __syncthreads();
+    copy_words(smem_raw + red_bytes, S->groups, sizeof(DGroup) * S->n_groups);
+    copy_words(smem_raw + red_bytes + grp_bytes, S->red_list, sizeof(uint32_t) * S->n_red);
+    __syncthreads();
+    const Desc& D = s_d;
+    const DCta& cta = s_cta;
+    const uint32_t n_seg = cta.seg_end - cta.seg_begin;
+    for (uint32_t k = 0; k < n_steps; ++k) {
+        const uint32_t par = k & 1u;
+        float* part_out = D.partials + static_cast<size_t>(par) * D.n_slots * D.N_pad;
+        const float v = sm.red[threadIdx.x % (2u * max_own > 0u ? 2u * max_own : 1u)];
+        for (uint32_t s = 0; s < n_seg; ++s) {
+            const DSeg& SG = s_seg[s];
+            float4* out = reinterpret_cast<float4*>(part_out + static_cast<size_t>(SG.slot) * D.N_pad + SG.pcol);
+            for (uint32_t u = threadIdx.x; u < SG.units; u += blockDim.x) __stcg(out + u, make_float4(v, v, v, v));
+        }
+        if (!grid_barrier(D.barrier, D.error, s_bar0 + (k + 1ull) * gridDim.x, &s_ok)) return;
+        load_partials(S, D, cta, par, sm, max_own);
+        __syncthreads();
     }
 }
 

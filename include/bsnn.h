@@ -260,6 +260,24 @@ BSNN_API bsnn_status bsnn_synchronize(bsnn_sim* sim);
 BSNN_API bsnn_status bsnn_get_stream(const bsnn_sim* sim, void** out_stream);
 /* Steps per persistent launch used by bsnn_run (default 1000; 1..65536). */
 BSNN_API bsnn_status bsnn_set_steps_per_launch(bsnn_sim* sim, uint32_t steps);
+/* Error contract of cpp_src/gpu_core/cuda_utils.h:10-20 for the persistent kernel's own waits.
+ * Every device-side wait (the grid barrier between steps, the staging copies) gives up after
+ * `nanoseconds` (default 2 s; 1 us .. 60 s): the kernel then records the failure and returns, the
+ * call that ran it (or bsnn_synchronize) returns BSNN_ERR_DEVICE_TIMEOUT, and later calls on that
+ * sim return BSNN_ERR_STATE.  Other sims on the device are unaffected. */
+BSNN_API bsnn_status bsnn_set_device_wait_limit(bsnn_sim* sim, uint64_t nanoseconds);
+/* Test switch, no reference counterpart: CTA `cta` of the persistent grid does not arrive at the
+ * grid barrier that ends internal step `step` (steps counted from 0 since creation), so every
+ * CTA's bounded wait runs out.  It exercises the timeout path above without a fault; finalises
+ * the network.  BSNN_ERR_OUT_OF_RANGE for a cta outside the grid. */
+BSNN_API bsnn_status bsnn_debug_skip_arrival(bsnn_sim* sim, uint32_t cta, uint64_t step);
+/* Measurement aid, no reference counterpart: the latency floor of one clock step of this network.
+ * Runs the step's communication skeleton alone -- every CTA stores its partial-sum slots, crosses
+ * the grid barrier and gathers its own columns from every slot, with the same grid, block and plan
+ * as bsnn_step / bsnn_run -- for num_steps steps after a warm-up launch, and writes its mean time
+ * per step (microseconds, CUDA events on the sim's stream).  The simulation's state is unchanged.
+ * Finalises the network. */
+BSNN_API bsnn_status bsnn_measure_exchange_floor(bsnn_sim* sim, uint32_t num_steps, float* out_us_per_step);
 
 /* ---- state access (GpuSimulationState download helpers) ------------------------------------ */
 
@@ -319,8 +337,18 @@ BSNN_API bsnn_status bsnn_record(bsnn_sim* sim, uint32_t clock_step);
 BSNN_API bsnn_status bsnn_flush_records(bsnn_sim* sim);
 /* System::run(total_clock_steps) (cpp_src/core/system.cpp:65-84) without step callbacks: clock
  * steps 0 .. total-1, with bsnn_record after every step that is a multiple of the state's
- * recording_interval_steps.  The reference's progress lines on stdout are not printed. */
+ * recording_interval_steps.  With progress output on (bsnn_set_progress_output) it prints the
+ * reference's line "Completed clock step: <step> | elapsed: <seconds>s" on stdout after each of
+ * those records (system.cpp:78-81), the seconds counted from the start of the call. */
 BSNN_API bsnn_status bsnn_run_system(bsnn_sim* sim, uint32_t total_clock_steps);
+/* Turns bsnn_run_system's progress line on (enabled != 0) or off (the default). */
+BSNN_API bsnn_status bsnn_set_progress_output(bsnn_sim* sim, int32_t enabled);
+/* GpuSimulationState::memory_report (cpp_src/gpu_core/gpu_simulation_state.cu:308-364): writes
+ * "Total GPU Memory Allocated: <bytes> bytes (<MB> MB)" with this sim's device arena into `buf`
+ * (NUL-terminated; BSNN_ERR_OUT_OF_RANGE when `capacity` is too small).  The reference allocates
+ * in its constructor; bsnn allocates when the network is complete, so this call finalises the
+ * network first (as the first bsnn_step or bsnn_run would): add every component before it. */
+BSNN_API bsnn_status bsnn_memory_report(bsnn_sim* sim, char* buf, uint64_t capacity);
 
 /* ---- one connection on caller-owned device buffers ------------------------------------------ */
 
@@ -362,15 +390,21 @@ typedef struct bsnn_connection_view {
  * (message in bsnn_last_error(NULL)). */
 BSNN_API bsnn_status bsnn_connection_propagate(const bsnn_connection_view* view, void* stream);
 
-/* No counterpart in the reference.  The same work and result as bsnn_connection_propagate, but the
- * call allocates no device memory: the GEMV scratch is a fixed module-scope device array of
+/* No counterpart in the reference.  The same work as bsnn_connection_propagate, but the call
+ * allocates no device memory: the GEMV scratch is a fixed module-scope device array of
  * 1,048,576 floats (4 MiB) per device, so post_group_num_neurons above 1,048,576 is rejected with
  * BSNN_ERR_OUT_OF_RANGE before anything is queued.  It is for callers that must not allocate per
  * call, e.g. a step loop inside an application whose device memory is already claimed by its own
  * caching allocator (PyTorch's), where a cudaMallocAsync can fail or grow a pool mid-run.
+ *  - Result: the same bits as bsnn_connection_propagate whenever both split the rows into the same
+ *    number of chunks, which holds for every post_group_num_neurons up to the limit on a 148-SM
+ *    B200.  On a GPU where the allocating path's chunks x post_group_num_neurons would not fit the
+ *    array, fewer chunks are used and the conductances agree with it to float rounding only.
  *  - The first call on each device does a one-time set-up with that device current (looking up the
  *    array's device address with cudaGetSymbolAddress, which may load this library's device code);
- *    make that first call before any stream capture.  A failed set-up returns BSNN_ERR_CUDA.
+ *    make that first call before any stream capture.  A failed set-up returns BSNN_ERR_CUDA.  The
+ *    address is kept with the context it came from and looked up again when the device's current
+ *    context changes (after cudaDeviceReset, for instance); the call that does so is a set-up call.
  *  - Nothing has to start at zero: each call writes every scratch value it reads.
  *  - All calls on one device share the array: calls that overlap in time (on different streams or
  *    from different host threads) race and give wrong results.  Order them (one stream, or events). */
@@ -447,6 +481,9 @@ BSNN_API bsnn_status bsnn_batch_add_instance(bsnn_batch* batch, uint32_t class_i
                                              uint32_t num_events, uint32_t* out_instance);
 BSNN_API bsnn_status bsnn_batch_set_noise(bsnn_batch* batch, int32_t on);
 BSNN_API bsnn_status bsnn_batch_set_steps_per_launch(bsnn_batch* batch, uint32_t steps);
+/* Bound of the batch kernel's device-side waits (default 2 s; 1 us .. 60 s), as
+ * bsnn_set_device_wait_limit. */
+BSNN_API bsnn_status bsnn_batch_set_device_wait_limit(bsnn_batch* batch, uint64_t nanoseconds);
 BSNN_API bsnn_status bsnn_batch_run(bsnn_batch* batch, uint32_t num_steps);
 BSNN_API bsnn_status bsnn_batch_synchronize(bsnn_batch* batch);
 BSNN_API bsnn_status bsnn_batch_get_stream(const bsnn_batch* batch, void** out_stream);

@@ -16,8 +16,10 @@
 //    work then); constructing one later throws std::runtime_error.
 #pragma once
 
+#include <chrono>
 #include <cstdint>
 #include <functional>
+#include <iostream>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -98,6 +100,13 @@ public:
         bsnn_info info{};
         check(bsnn_get_info(sim_, &info), sim_);
         return info.device_bytes;
+    }
+    // GpuSimulationState::memory_report (gpu_simulation_state.cu:357-362).  bsnn allocates once the
+    // network is complete, so call it after the components are added.
+    std::string memory_report() const {
+        char buf[256];
+        check(bsnn_memory_report(sim_, buf, sizeof(buf)), sim_);
+        return std::string(buf);
     }
     // GpuSimulationState::download_weight_matrix (gpu_simulation_state.cu:287-306), by the
     // ConnectionParams::weight_matrix_idx of the connection.
@@ -307,15 +316,22 @@ public:
     // System::run (system.cpp:65-84): callbacks before each step, Monitor::record after every step
     // that is a multiple of the recording interval.  Without callbacks the steps between records
     // run as batched persistent launches.
+    // Prints the reference's progress line after each record, as System::run does.
     void run(uint32_t total_clock_steps) {
         if (callbacks_.empty()) {
+            check(bsnn_set_progress_output(sim(), 1), sim());
             check(bsnn_run_system(sim(), total_clock_steps), sim());
         } else {
             const uint32_t interval = state_->recording_interval_steps();
+            const auto start_time = std::chrono::steady_clock::now();
             for (uint32_t s = 0; s < total_clock_steps; ++s) {
                 for (auto& cb : callbacks_) cb(s);
                 step_the_clock(s);
-                if (s % interval == 0) check(bsnn_record(sim(), s), sim());
+                if (s % interval == 0) {
+                    check(bsnn_record(sim(), s), sim());
+                    const std::chrono::duration<float> elapsed = std::chrono::steady_clock::now() - start_time;
+                    std::cout << "Completed clock step: " << s << " | elapsed: " << elapsed.count() << "s\n";
+                }
             }
         }
         check(bsnn_flush_records(sim()), sim());

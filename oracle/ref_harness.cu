@@ -11,6 +11,8 @@
 //       last), the full device state; plus, for every step, the background Poisson counts the
 //       reference drew (read with a copy of each neuron's curand state, so the reference's own
 //       draws are unchanged).  Weights of every connection are written after the last step.
+//   ref_harness <net.bin> bench <warm_steps> <samples> <steps_per_sample>
+//       the bench's reference arm: times each sample of steps separately, L2 flushed between them
 //   ref_harness <net.bin> time <warmup> <steps>
 //       times <steps> calls of System::step_the_clock (the hot path; Monitor::record's text
 //       output is not part of it) and prints one JSON line.
@@ -105,7 +107,7 @@ int main(int argc, char** argv) {
     try {
         if (argc < 3) {
             std::fprintf(stderr,
-                         "usage: %s net.bin dump <steps> <out.bin> <every> | time <warmup> <steps> | "
+                         "usage: %s net.bin dump <steps> <out.bin> <every> | time <warmup> <steps> | bench <warm> <samples> <per> | "
                          "record <steps> <outdir>\n",
                          argv[0]);
             return 2;
@@ -235,6 +237,34 @@ int main(int argc, char** argv) {
             }
             return 0;
         }
+        if (mode == "bench") {
+            if (argc < 6) throw std::runtime_error("bench mode needs <warm_steps> <samples> <steps_per_sample>");
+            // <warm_steps> <samples> <steps_per_sample>: after the warm-up steps, times each sample of
+            // consecutive steps separately (host wall clock around the reference's own synchronous
+            // step calls), with a 256 MB write between samples so no sample starts from a warm L2.
+            const uint32_t warm = static_cast<uint32_t>(std::atoi(argv[3]));
+            const uint32_t samples = static_cast<uint32_t>(std::atoi(argv[4]));
+            const uint32_t per = static_cast<uint32_t>(std::atoi(argv[5]));
+            void* flush = nullptr;
+            const size_t flush_bytes = size_t(256) << 20;
+            check(cudaMalloc(&flush, flush_bytes), "cudaMalloc flush");
+            uint32_t clock_step = 0;
+            for (; clock_step < warm; ++clock_step) system.step_the_clock(clock_step);
+            check(cudaDeviceSynchronize(), "sync");
+            std::printf("{\"steps_per_sample\": %u, \"neurons\": %u, \"seconds\": [", per, N);
+            for (uint32_t k = 0; k < samples; ++k) {
+                check(cudaMemset(flush, k & 0xff, flush_bytes), "flush L2");
+                check(cudaDeviceSynchronize(), "sync");
+                const auto t0 = std::chrono::steady_clock::now();
+                for (uint32_t s = 0; s < per; ++s) system.step_the_clock(clock_step++);
+                check(cudaDeviceSynchronize(), "sync");
+                const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+                std::printf("%s%.6f", k ? ", " : "", sec);
+            }
+            std::printf("]}\n");
+            cudaFree(flush);
+            return 0;
+        }
         if (mode == "time") {
             const uint32_t warm = static_cast<uint32_t>(std::atoi(argv[3]));
             const uint32_t steps = static_cast<uint32_t>(std::atoi(argv[4]));
@@ -260,6 +290,10 @@ int main(int argc, char** argv) {
         std::vector<uint8_t> all_counts;
         all_counts.reserve(static_cast<size_t>(steps) * N * 2);
         std::vector<uint8_t> h_counts(N * 2);
+        // every step's spike vector, packed 8 neurons per byte (bit 7 first), for the raster
+        const size_t row_bytes = (N + 7) / 8;
+        std::vector<uint8_t> raster(static_cast<size_t>(steps) * row_bytes, 0);
+        std::vector<uint32_t> h_spikes(N);
         for (uint32_t s = 0; s < steps; ++s) {
             for (const auto& g : ginfo) {
                 peek_poisson_counts<<<(g.n + 255) / 256, 256>>>(state.d_neuron_rng_states(), g.offset, g.n, g.mean_e,
@@ -269,6 +303,10 @@ int main(int argc, char** argv) {
             check(cudaMemcpy(h_counts.data(), d_counts, N * 2, cudaMemcpyDeviceToHost), "counts D2H");
             all_counts.insert(all_counts.end(), h_counts.begin(), h_counts.end());
             system.step_the_clock(s);
+            check(cudaMemcpy(h_spikes.data(), state.d_spikes(), N * sizeof(uint32_t), cudaMemcpyDeviceToHost),
+                  "spikes D2H");
+            for (uint32_t j = 0; j < N; ++j)
+                if (h_spikes[j]) raster[static_cast<size_t>(s) * row_bytes + j / 8] |= static_cast<uint8_t>(0x80u >> (j % 8));
             if ((s + 1) % every == 0 || s + 1 == steps) {
                 const uint32_t tag = s;
                 out.write("STEP", 4);
@@ -303,6 +341,8 @@ int main(int argc, char** argv) {
         }
         out.write("NOIS", 4);
         out.write(reinterpret_cast<const char*>(all_counts.data()), static_cast<std::streamsize>(all_counts.size()));
+        out.write("SPKS", 4);
+        out.write(reinterpret_cast<const char*>(raster.data()), static_cast<std::streamsize>(raster.size()));
         check(cudaFree(d_counts), "cudaFree");
         return 0;
     } catch (const std::exception& e) {

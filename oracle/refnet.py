@@ -55,12 +55,14 @@ def write_network(spec, path):
             f.write(ids.tobytes())
 
 
-def run_dump(spec, steps, every, workdir):
+def run_dump(spec, steps, every, workdir, raster=False):
+    """ref_harness dump mode: (states by step tag, final weights, Poisson counts [steps][N][2]) and,
+    with raster=True, also every step's spikes as uint8 [steps][N]."""
     workdir = Path(workdir)
     net, out = workdir / "net.bin", workdir / "dump.bin"
     write_network(spec, net)
     subprocess.run([str(HARNESS), str(net), "dump", str(steps), str(out), str(every)], check=True)
-    return read_dump(out, spec, steps)
+    return read_dump(out, spec, steps, raster=raster)
 
 
 def run_time(spec, warmup, steps, workdir):
@@ -72,7 +74,18 @@ def run_time(spec, warmup, steps, workdir):
     return json.loads(res.stdout.strip().splitlines()[-1])
 
 
-def read_dump(path, spec, steps):
+def run_bench(spec, warm_steps, samples, steps_per_sample, workdir):
+    """ref_harness bench mode: wall seconds of each sample of `steps_per_sample` consecutive
+    System::step_the_clock calls after `warm_steps`, with the L2 flushed between samples."""
+    import json
+    net = Path(workdir) / "net_bench.bin"
+    write_network(spec, net)
+    res = subprocess.run([str(HARNESS), str(net), "bench", str(warm_steps), str(samples), str(steps_per_sample)],
+                         check=True, capture_output=True, text=True)
+    return json.loads(res.stdout.strip().splitlines()[-1])
+
+
+def read_dump(path, spec, steps, raster=False):
     b = Path(path).read_bytes()
     assert b[:8] == b"BSNNDMP1"
     N, nsteps = struct.unpack_from("<II", b, 8)
@@ -111,7 +124,13 @@ def read_dump(path, spec, steps):
     assert b[pos:pos + 4] == b"NOIS"
     pos += 4
     noise = np.frombuffer(b, np.uint8, steps * N * 2, pos).copy().reshape(steps, N, 2)
-    return states, weights, noise
+    pos += steps * N * 2
+    if not raster:
+        return states, weights, noise
+    assert b[pos:pos + 4] == b"SPKS"
+    pos += 4
+    packed = np.frombuffer(b, np.uint8, steps * ((N + 7) // 8), pos).reshape(steps, (N + 7) // 8)
+    return states, weights, noise, np.unpackbits(packed, axis=1)[:, :N]
 
 
 def run_record(spec, steps, outdir):

@@ -66,6 +66,37 @@ def assert_close(a, b, rtol, what, scale=None):
                            f"got {a[bad[:5]]}, want {b[bad[:5]]}")
 
 
+# Absolute floors of the per-element comparison |a - b| <= rtol (|b| + floor), one per quantity.
+# Membrane potentials (|v| >= 0.04 V) and conductances (1e-10 .. 1e-8 S once driven, exactly 0
+# before) are held relative to themselves: their floors are far below any value they take.  A
+# weight is computed in steps of 1e-9 S scale (LTP and LTD increments, row rescaling), so one that
+# plasticity drove towards 0 keeps an absolute error of a few 1e-16 S, the rounding unit of that
+# arithmetic: weights are held relative to themselves down to 1e-11 S (1/150 of the smallest
+# connection's largest weight) and to 1e-16 S absolute below it.
+ELEMENT_FLOORS = {"membrane_potentials": 1e-9, "g_excitatory": 1e-16, "g_inhibitory": 1e-16, "weights": 1e-11}
+
+
+def elementwise_error(a, b, floor):
+    """The largest per-element relative error with an absolute floor, max |a - b| / (|b| + floor),
+    and the index where it occurs."""
+    a = np.asarray(a, dtype=np.float64).ravel()
+    b = np.asarray(b, dtype=np.float64).ravel()
+    if a.size == 0:
+        return 0.0, -1
+    e = np.abs(a - b) / (np.abs(b) + floor)
+    k = int(np.argmax(e))
+    return float(e[k]), k
+
+
+def assert_close_elementwise(a, b, rtol, floor, what):
+    """Every element within rtol of itself: |a - b| <= rtol (|b| + floor)."""
+    a = np.asarray(a, dtype=np.float64).ravel()
+    b = np.asarray(b, dtype=np.float64).ravel()
+    bad = np.flatnonzero(np.abs(a - b) > rtol * (np.abs(b) + floor))
+    assert bad.size == 0, (f"{what}: {bad.size} of {a.size} differ beyond {rtol:g} relative (floor {floor:g}); "
+                           f"first {bad[:5]}, got {a[bad[:5]]}, want {b[bad[:5]]}")
+
+
 def compare_state(g, o, spec, rtol=1e-5, weights=True, tag=""):
     """Compares every per-neuron field, the connection and plasticity traces and the weights."""
     np.testing.assert_array_equal(g.read("spikes"), o.read("spikes"), err_msg=f"{tag} spikes")

@@ -50,6 +50,64 @@ def test_replica_reduction_two_gloo_ranks():
         assert dict(results) == {0: (30.25, 300, 15), 1: (30.25, 300, 15)}
 
 
+def _shard_rank(rank, world, port, results):
+    import datetime
+
+    import numpy as np
+    import torch
+    sys.path.insert(0, str(ROOT))
+    import bench
+    import bsnn
+    torch.distributed.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                                         world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        full = bsnn.config4_batch(24, steps=50, seed=5)
+        mine = bench.shard_of(len(full.instances), rank, world)
+        part = full.subset(mine)
+        # what the shard would report: a per-instance count that identifies the instance
+        counts = np.array([[i.seed % 1000, i.seed % 7] for i in part.instances])
+        gathered = bench.gather_instance_counts(counts, mine, len(full.instances), "cpu")
+        results[rank] = (mine, [i.seed for i in part.instances], gathered.tolist())
+    finally:
+        torch.distributed.destroy_process_group()
+
+
+def test_batch_sharding_two_gloo_ranks():
+    """The batched workload over two ranks: the shards' instances are disjoint, their union is the
+    one-GPU spec (same seeds, parameters and weight sets), and the single all-reduce at the end gives
+    every rank every instance's counts at its global index."""
+    import numpy as np
+
+    import bsnn
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as mgr:
+        results = mgr.dict()
+        port = _free_port()
+        procs = [ctx.Process(target=_shard_rank, args=(r, 2, port, results)) for r in range(2)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(120)
+            assert p.exitcode == 0
+        res = dict(results)
+    full = bsnn.config4_batch(24, steps=50, seed=5)
+    seeds = {}
+    for r in range(2):
+        mine, shard_seeds, _ = res[r]
+        seeds.update(zip(mine, shard_seeds))
+    assert sorted(res[0][0] + res[1][0]) == list(range(24)) and not set(res[0][0]) & set(res[1][0])
+    assert [seeds[b] for b in range(24)] == [i.seed for i in full.instances]
+    want = np.array([[i.seed % 1000, i.seed % 7] for i in full.instances])
+    for r in range(2):
+        np.testing.assert_array_equal(np.array(res[r][2]), want)
+    part = full.subset([3, 1])
+    for k, b in enumerate((3, 1)):
+        a, c = part.instance_network(k), full.instance_network(b)
+        assert a.groups == c.groups and a.rng_seed == c.rng_seed
+        for x, y in zip(a.conns, c.conns):
+            np.testing.assert_array_equal(x.weights, y.weights)
+
+
 @pytest.mark.parametrize("rank,expect_line", [(0, True), (1, False)])
 def test_reference_arm_prints_on_rank_zero_only(rank, expect_line):
     env = dict(os.environ, RANK=str(rank), WORLD_SIZE="2", LOCAL_RANK=str(rank), CUDA_VISIBLE_DEVICES="")

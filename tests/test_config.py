@@ -20,7 +20,7 @@ import pytest
 ROOT = Path(__file__).resolve().parents[1]
 MAIN = ROOT / "example-cuda-spiking-nn_b200" / "bsnn_main"
 REF = ROOT / "oracle" / "_ref" / "ref_config"
-REF_EXAMPLE = Path("/root/reference/configs_to_run/config01.json")
+REF_EXAMPLE = Path(os.environ.get("BSNN_REFERENCE_ROOT", ROOT.parent / "reference")) / "configs_to_run" / "config01.json"
 
 needs_main = pytest.mark.skipif(not MAIN.exists(), reason="bsnn_main not built")
 needs_ref = pytest.mark.skipif(not REF.exists(), reason="reference loader not built (make -C oracle refcfg)")

@@ -7,8 +7,9 @@ replayed every input is identical and the comparison is step by step:
   * background traces and conductances, stimulus current, refractory counters, connection traces
     (x = d - r) and plasticity traces: bit-identical (they depend on spikes and noise only);
   * membrane potentials, conductances and the final weights: within 1e-5 x max|reference| of the
-    field (the reference's cublasSgemv sums in float in its own order; the oracle sums in double,
-    the CUDA path in float in a fixed order).
+    field, and element by element within 1e-5 of each value (|a - b| <= 1e-5 (|b| + floor), the
+    floors of conftest.ELEMENT_FLOORS) (the reference's cublasSgemv sums in float in its own
+    order; the oracle sums in double, the CUDA path in float in a fixed order).
 
 The CPU test pins the oracle to the reference; the GPU test runs the CUDA path through the C-ABI.
 """
@@ -21,7 +22,7 @@ import numpy as np
 import pytest
 
 import bsnn
-from conftest import ROOT, assert_close
+from conftest import ELEMENT_FLOORS, ROOT, assert_close, assert_close_elementwise
 
 sys.path.insert(0, str(ROOT / "tests" / "golden"))
 from specs import CHECK_STEPS, GOLDEN_STEPS, golden_specs, spec_digest  # noqa: E402
@@ -70,6 +71,7 @@ def compare(sim, spec, fx, name):
             assert bad.size == 0, f"{tag} {f}: {bad.size} differ, first {bad[:5]}: {got[bad[:5]]} vs {want[bad[:5]]}"
         for f in CLOSE_FIELDS:
             assert_close(sim.read(f), fx[f"state_{f}"][k], RTOL, f"{tag} {f}")
+            assert_close_elementwise(sim.read(f), fx[f"state_{f}"][k], RTOL, ELEMENT_FLOORS[f], f"{tag} {f}")
         for c in range(len(spec.conns)):
             got, want = sim.read("connection_summed", c), fx[f"summed_{c}"][k]
             assert np.array_equal(got, want), f"{tag} summed[{c}] differs"
@@ -88,6 +90,8 @@ def compare(sim, spec, fx, name):
     assert want_raster.sum() > 0, "fixture has no spikes"
     for c in range(len(spec.conns)):
         assert_close(sim.read_weights(c), fx[f"weights_{c}"], RTOL, f"{name} weights[{c}]")
+        assert_close_elementwise(sim.read_weights(c), fx[f"weights_{c}"], RTOL, ELEMENT_FLOORS["weights"],
+                                 f"{name} weights[{c}]")
 
 
 @pytest.mark.parametrize("name", NAMES)

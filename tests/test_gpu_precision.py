@@ -124,54 +124,90 @@ def test_copy_is_the_rounded_masters(form):
     g.close()
 
 
-def _run_form(spec, steps, form):
+def _run_form(spec, steps, form, v_step=20):
     g = bsnn.Simulation(spec.num_excitatory, spec.num_inhibitory, **spec.sim_kwargs())
     spec.build(g)
     if form != "f32":
         g.set_weight_format(form)
-    g.run(0, 20)
-    v20 = g.read("membrane_potentials").astype(np.float64)
-    g.run(20, steps - 20)
+    g.run(0, v_step)
+    v = g.read("membrane_potentials").astype(np.float64)
+    g.run(v_step, steps - v_step)
     spk = [g.read_spike_history(m) for m in (0, 1)]
     w = [g.read_weights(c).astype(np.float64) for c in range(len(spec.conns))]
     g.close()
-    return v20, spk, w
+    return v, spk, w
+
+
+def _errors_vs_fp64(spec, steps, forms, v_step=20):
+    """Per form: (voltage error at step v_step relative to the largest |v|, the larger relative
+    spike-count error of the two populations over the run, the larger relative drift of the
+    plastic matrices mean |w - w64| / mean |w64|) against the FP64 oracle with the same seed and
+    Poisson draws; and the FP64 run's spike counts."""
+    o = oracle.OracleSimulation(spec.num_excitatory, spec.num_inhibitory, precision=oracle.PREC_F64, **spec.sim_kwargs())
+    spec.build(o)
+    o.run(0, v_step)
+    v_ref = o.read_f64("membrane_potentials")
+    o.run(v_step, steps - v_step)
+    n_ref = [int(o.read_spike_history(m).sum()) for m in (0, 1)]
+    plastic = sorted({p.conn for p in spec.plasts})
+    w_ref = {c: o.read_weights_f64(c) for c in plastic}
+    o.close()
+    vscale = float(np.max(np.abs(v_ref)))
+    results = {}
+    for form in forms:
+        v, spk, w = _run_form(spec, steps, form, v_step)
+        ev = float(np.max(np.abs(v - v_ref))) / vscale
+        n = [int(spk[m].sum()) for m in (0, 1)]
+        er = max(abs(n[m] - n_ref[m]) / max(n_ref[m], 1) for m in (0, 1))
+        ew = max(float(np.mean(np.abs(w[c] - w_ref[c]))) / float(np.mean(np.abs(w_ref[c]))) for c in plastic)
+        results[form] = (ev, er, ew)
+        print(f"{spec.name} {form:>14}: voltage err (step {v_step}) {ev:.2e}, rate err {er:.3e} "
+              f"(E {n[0]} vs {n_ref[0]}, I {n[1]} vs {n_ref[1]} spikes), weight drift {ew:.2e}")
+    return results, n_ref
+
+
+def _check_bounds(results, bounds):
+    for form, (b_v, b_r, b_w) in bounds.items():
+        ev, er, ew = results[form]
+        assert ev <= b_v, (form, "voltage", ev, b_v)
+        assert er <= b_r, (form, "rate", er, b_r)
+        assert ew <= b_w, (form, "weights", ew, b_w)
+
+
+# Bounds per form: (voltage error at step 20, rate error, plastic weight drift), about twice the
+# values measured on B200 (printed by the tests), with a floor of 2e-3 on the rate error.  Past a
+# few hundred steps the trajectories of any two precisions part (the network is chaotic), so the
+# FP32 reference form's own rate and drift set the scale the others are held to.  Measured,
+# 400 E + 100 I over 3,000 steps: f32 4.4e-7 / 6.5e-4 / 1.6e-2; f32_rowscaled 4.4e-7 / 0 / 4.4e-7;
+# bf16 4.4e-7 / 1.3e-3 / 2.7e-2; fp8_e4m3 4.4e-7 / 3.5e-2 / 3.9e-2.
+SMALL_BOUNDS = {"f32": (1e-6, 2e-3, 3.2e-2), "f32_rowscaled": (1e-6, 2e-3, 1e-6), "bf16": (1e-6, 3e-3, 5.4e-2),
+                "fp8_e4m3": (1e-6, 7e-2, 8e-2)}
 
 
 def test_precision_forms_against_fp64():
     steps = 3000
     spec = bsnn.synthetic_network("small_plastic_500", steps=steps + 1, weight_values="uniform")
-    o = oracle.OracleSimulation(spec.num_excitatory, spec.num_inhibitory, precision=oracle.PREC_F64, **spec.sim_kwargs())
-    spec.build(o)
-    o.run(0, 20)
-    v20_ref = o.read_f64("membrane_potentials")
-    o.run(20, steps - 20)
-    spk_ref = [o.read_spike_history(m) for m in (0, 1)]
-    w_ref = [o.read_weights_f64(c) for c in range(len(spec.conns))]
-    plastic = sorted({p.conn for p in spec.plasts})
-    n_ref = [int(s.sum()) for s in spk_ref]
+    results, n_ref = _errors_vs_fp64(spec, steps, list(SMALL_BOUNDS))
     assert min(n_ref) > 200, n_ref
-    vscale = float(np.max(np.abs(v20_ref)))
-    # Bounds per form: voltage error at step 20 (relative to the largest |v|), relative rate error
-    # over the run, relative drift of the plastic weights (mean |w - w64| / mean |w64|).  Past a few
-    # hundred steps the trajectories of any two precisions part (the network is chaotic), so the
-    # FP32 reference form's own rate and drift set the scale the others are held to.
-    bounds = {"f32": (1e-5, 0.02, 0.05), "f32_rowscaled": (1e-5, 0.02, 0.05), "bf16": (1e-2, 0.05, 0.10),
-              "fp8_e4m3": (5e-2, 0.10, 0.25)}
-    results = {}
-    for form in bounds:
-        v20, spk, w = _run_form(spec, steps, form)
-        ev = float(np.max(np.abs(v20 - v20_ref))) / vscale
-        er = max(abs(int(spk[m].sum()) - n_ref[m]) / n_ref[m] for m in (0, 1))
-        ew = max(float(np.mean(np.abs(w[c] - w_ref[c]))) / float(np.mean(np.abs(w_ref[c]))) for c in plastic)
-        results[form] = (ev, er, ew)
-        print(f"{form:>14}: voltage err (step 20) {ev:.2e}, rate err {er:.3e} "
-              f"(E {int(spk[0].sum())} vs {n_ref[0]}, I {int(spk[1].sum())} vs {n_ref[1]} spikes), weight drift {ew:.2e}")
-    for form, (b_v, b_r, b_w) in bounds.items():
-        ev, er, ew = results[form]
-        assert ev <= b_v, (form, "voltage", ev)
-        assert er <= b_r, (form, "rate", er)
-        assert ew <= b_w, (form, "weights", ew)
+    _check_bounds(results, SMALL_BOUNDS)
+
+
+# The precision form's own configuration: 8,100 E + 2,025 I (~102 M synapse entries, rows of 8,100
+# weights, so the normalisation sums and the FP8 row scales act on rows 20x longer than above), 600
+# steps (the FP64 oracle takes ~0.1 s per step on the host).  The network is nearly silent in
+# these steps (background drive only), so the rate error rests on few spikes; the voltage error
+# and the weight drift are the sharper measures.  Bounds as above: about twice the measured values.
+LARGE_STEPS = 600
+LARGE_BOUNDS = {"f32": (1e-6, 0.5, 5e-2), "f32_rowscaled": (1e-6, 0.5, 5e-2), "bf16": (1e-2, 0.5, 0.1),
+                "fp8_e4m3": (5e-2, 0.5, 0.25)}
+
+
+def test_precision_forms_against_fp64_at_the_large_size():
+    spec = bsnn.synthetic_network("large_plastic_10125", steps=LARGE_STEPS + 1, weight_values="uniform",
+                                  recording_interval_steps=LARGE_STEPS)
+    results, n_ref = _errors_vs_fp64(spec, LARGE_STEPS, list(LARGE_BOUNDS))
+    print("FP64 spikes", n_ref)
+    _check_bounds(results, LARGE_BOUNDS)
 
 
 def test_fp8_decode_paths_agree_bit_for_bit(monkeypatch):

@@ -4,6 +4,7 @@ the reference generator's weights, triplet STDP + iSTDP) over 20,001 clock steps
 seconds), with the reference's Poisson counts replayed.  Individual spikes diverge once the
 network's chaotic dynamics amplify last-bit differences, so the run is compared through:
 
+  * the spike rows of the first 1,000 steps: identical, neuron for neuron;
   * per-population firing rates: within 10 % of the reference's;
   * the coefficient of variation of the inter-spike intervals (pooled per population): within 15 %;
   * the histogram of the final plastic weights (E->E, I->E): total-variation distance < 0.02 over
@@ -64,6 +65,10 @@ def test_long_run_statistics_match_reference(tmp_path):
         ref_rows = refnet.read_spike_rows(ref_dir / f"spikes_m{m}.txt")
         our_rows = refnet.read_spike_rows(ours / f"spikes_m{m}.txt")
         assert sorted(ref_rows) == sorted(our_rows) == list(range(STEPS - 1))
+        # the first 1,000 steps spike for spike, before chaos can part the runs
+        first = [t for t in range(1000) if ref_rows[t] != our_rows[t]]
+        assert not first, f"population {m}: spike rows differ at steps {first[:5]}"
+        assert sum(len(ref_rows[t]) for t in range(1000)) > 0
         r_ref, cv_ref, n_ref = rates_and_cv(ref_rows, n, STEPS)
         r_our, cv_our, n_our = rates_and_cv(our_rows, n, STEPS)
         print(f"population {m}: rate {r_our:.4f} Hz vs reference {r_ref:.4f} Hz ({n_our} vs {n_ref} spikes), "

@@ -80,3 +80,31 @@ def test_recorder_files_match_the_reference(tmp_path):
             assert ka == kb, (name, a, b)
             assert abs(float(va) - float(vb)) <= 1e-5 * scale, (name, a, b)
     assert n_spike_rows == 2 * 5 * spec.recording_interval_steps
+
+
+@pytest.mark.gpu
+def test_run_system_prints_the_progress_line_and_memory_report(capfd):
+    """System::run's console line after each record (cpp_src/core/system.cpp:78-81) and
+    GpuSimulationState::memory_report (cpp_src/gpu_core/gpu_simulation_state.cu:357-362)."""
+    import re
+    spec = bsnn.random_network(48, 12, steps=200, seed=3)
+    sim = bsnn.Simulation(spec.num_excitatory, spec.num_inhibitory, **spec.sim_kwargs())
+    spec.build(sim)
+    report = sim.memory_report()
+    m = re.fullmatch(r"Total GPU Memory Allocated: (\d+) bytes \((\d+\.\d{6}) MB\)", report)
+    assert m, report
+    assert int(m.group(1)) == sim.info().device_bytes > 0
+    assert abs(float(m.group(2)) - int(m.group(1)) / 2 ** 20) < 1e-6
+    sim.run_system(10)  # progress off (the default): nothing printed
+    assert "Completed clock step" not in capfd.readouterr().out
+    sim.close()
+    sim = bsnn.Simulation(spec.num_excitatory, spec.num_inhibitory, **spec.sim_kwargs())
+    spec.build(sim)
+    sim.set_progress_output(True)
+    interval = spec.recording_interval_steps  # 64
+    sim.run_system(2 * interval + 5)
+    sim.flush_records()
+    sim.close()
+    lines = [ln for ln in capfd.readouterr().out.splitlines() if ln.startswith("Completed clock step")]
+    steps = [int(re.fullmatch(r"Completed clock step: (\d+) \| elapsed: ([0-9.e+-]+)s", ln).group(1)) for ln in lines]
+    assert steps == [0, interval, 2 * interval], lines
