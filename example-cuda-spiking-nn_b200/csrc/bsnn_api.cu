@@ -517,7 +517,7 @@ void finalize(bsnn_sim* s) {
         o_ts[3 * t + 1] = A.take(n);
         o_ts[3 * t + 2] = A.take(n);
     }
-    std::vector<size_t> o_w(h.n_conns), o_q(h.n_conns, 0), o_rowv(h.n_conns, 0);
+    std::vector<size_t> o_w(h.n_conns), o_q(h.n_conns, 0), o_rowv(h.n_conns, 0), o_rsum(h.n_conns, 0);
     const bool lazy = s->weight_format != BSNN_WEIGHTS_F32;
     s->conn_ld.assign(h.n_conns, 0);
     size_t wbytes = 0;
@@ -534,6 +534,10 @@ void finalize(bsnn_sim* s) {
             o_q[c] = A.take(eb * tiles * n_pre * 128);
             wbytes += eb * tiles * n_pre * 128;
             o_rowv[c] = A.take(sizeof(float) * 4 * static_cast<size_t>(n_pre));  // s, M, qs, 1/qs
+        } else {
+            bool triplet = false;
+            for (const auto& PL : s->plasts) triplet |= PL.conn == c && PL.kind == BSNN_PLASTICITY_TRIPLET;
+            if (triplet) o_rsum[c] = A.take(sizeof(float) * static_cast<size_t>(n_pre));  // running row sums
         }
     }
     struct PlOff { size_t pre, post, tpre, tpost, colA[2], colB[2], sums; };
@@ -765,6 +769,7 @@ void finalize(bsnn_sim* s) {
         D.ts = conn_ts[c];
         D.plast = -1;
         D.w = F(o_w[c]);
+        D.rowsum = o_rsum[c] ? F(o_rsum[c]) : nullptr;  // written by the first launch (from step 0)
         if (D.ld == D.n_post) {  // no padding columns: the rows are already laid out as on the device
             cuda_check(cudaMemcpy(D.w, C.w.data(), sizeof(float) * C.w.size(), cudaMemcpyHostToDevice), "H2D w");
         } else {

@@ -94,6 +94,9 @@ struct DConn {
     float* qinv;      // [n_pre] its reciprocal
     float* lz_s;      // [n_pre] normalisation scale s of each row
     float* lz_m;      // [n_pre] sum of the row's masters
+    // Reference form, triplet connections: [n_pre] running sum of each row's weights between
+    // launches (rows resident in shared memory keep it in step; see norm_rows), else null.
+    float* rowsum;
 };
 
 // PlasticityView (cpp_src/plasticities/plasticity_view.h:8-38) plus per-step factor buffers.

@@ -166,6 +166,42 @@ __device__ __forceinline__ bool grid_barrier(unsigned long long* barrier, int32_
     return *s_ok != 0;
 }
 
+// The same barrier in two halves, so a CTA can do work that needs nothing from other CTAs between
+// its arrival and its wait: grid_arrive (after the CTA-wide sync, thread 0's release reduction)
+// and grid_wait (thread 0's bounded acquire spin, then the CTA-wide sync that extends it).
+__device__ __forceinline__ void grid_arrive(unsigned long long* barrier, bool arrive) {
+    __syncthreads();
+    if (threadIdx.x == 0 && arrive) red_release_add_u64(barrier, 1ull);
+}
+
+__device__ __forceinline__ bool grid_wait(unsigned long long* barrier, int32_t* error, unsigned long long target,
+                                          int* s_ok) {
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        unsigned long long t_start = 0;
+        uint32_t spins = 0;
+        while (static_cast<long long>(ld_acquire_u64(barrier) - target) < 0) {
+            if ((++spins & 255u) == 0u) {
+                const unsigned long long now = globaltimer_ns();
+                if (t_start == 0) {
+                    t_start = now;
+                } else if (now - t_start > s_wait_limit_ns) {
+                    atomicExch(error, kErrBarrierTimeout);
+                    ok = 0;
+                    break;
+                }
+                if (ld_relaxed_s32(error) != kErrNone) {
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+        *s_ok = ok;
+    }
+    __syncthreads();
+    return *s_ok != 0;
+}
+
 // Optional phase timing (profiling builds only, -DBSNN_PHASE_TIMING): thread 0 of every CTA adds
 // the SM clock cycles spent in each phase to a shared-memory tally (s_tally_[phase]) that the
 // kernel adds to S->phase_ns[cta * kPhaseSlots + phase] when it ends: 3 partial-sum loads, 0 rest
@@ -173,7 +209,8 @@ __device__ __forceinline__ bool grid_barrier(unsigned long long* barrier, int32_
 // and row x, 4 weight pass, 5 grid barrier.  Spans of single threads inside those phases: 6 the
 // neuron warp's own neuron phase, 7 the update warps' update plus normalisation sums, 8 their
 // update alone, 9 thread 0's share of the weight pass, 10 the last warp's share of it, 11 thread
-// 0's share of the spike-bit merge.
+// 0's share of the spike-bit merge, 12 the normalisation sums alone, 13 the last warp's update,
+// 14 the work done between arrival and wait (warp 1), 15 arrival to release (thread 0).
 #ifdef BSNN_PHASE_TIMING
 #define BSNN_TMARK(slot)                                                                   \
     do {                                                                                   \
@@ -241,6 +278,7 @@ struct SmemLayout {
     DRowMeta* meta;     // [max_rows]
     uint32_t* rowflag;  // [max_rows] presynaptic neuron spiked at the step being applied
     float* rowtgt;      // [max_rows] triplet normalisation target of the row
+    float* rowsum;      // [max_rows] running sum of each resident triplet row (see norm_rows)
     uint32_t* sbits;    // [spk_words] spike bitmask of the step whose plasticity is being applied
     uint32_t* gbits;    // [2][max_own/32 + 2] this CTA's spike bits, by step parity
     float* xown;        // [n_ts][max_own] x = d - r of the own neurons (this step)
@@ -266,6 +304,7 @@ struct SmemLayout {
 // side (post, triplet post) and one per voltage monitor (the neuron's ring column, or -1).
 enum : uint32_t {
     kNsV = 0, kNsGe, kNsGi, kNsIstim, kNsEr, kNsEd, kNsIr, kNsId, kNsBgGe, kNsBgGi, kNsRefrac, kNsSpike,
+    kNsNoise,  // the step's background Poisson counts, excitatory | inhibitory << 16 (drawn ahead)
     kNsFixed
 };
 struct NsLayout {
@@ -285,7 +324,7 @@ __host__ __device__ __forceinline__ size_t align16(size_t x) { return (x + 15) &
 
 // Byte layout of the dynamic shared memory; the host sizes the launch with the same function.
 struct SmemSizes {
-    size_t wres, row, meta, rowflag, rowtgt, sbits, gbits, xown, rowfac, ns, rsum, redscr, stage, lz, bits, groups, ts,
+    size_t wres, row, meta, rowflag, rowtgt, rowsum, sbits, gbits, xown, rowfac, ns, rsum, redscr, stage, lz, bits, groups, ts,
         conns, plast, mons, red, total;
 };
 __host__ __device__ __forceinline__ SmemSizes smem_sizes(uint32_t resident_floats, uint32_t max_rows, uint32_t max_own,
@@ -300,6 +339,7 @@ __host__ __device__ __forceinline__ SmemSizes smem_sizes(uint32_t resident_float
     z.meta = align16(sizeof(DRowMeta) * max_rows);
     z.rowflag = align16(sizeof(uint32_t) * max_rows);
     z.rowtgt = align16(sizeof(float) * max_rows);
+    z.rowsum = align16(sizeof(float) * max_rows);
     z.sbits = align16(sizeof(uint32_t) * spk_words);
     z.gbits = align16(sizeof(uint32_t) * 2 * (max_own / 32 + 2));
     z.xown = align16(sizeof(float) * n_ts * max_own);
@@ -318,7 +358,7 @@ __host__ __device__ __forceinline__ SmemSizes smem_sizes(uint32_t resident_float
     z.plast = align16(sizeof(DPlast) * n_plast);
     z.mons = align16(sizeof(DMon) * n_mons);
     z.red = align16(sizeof(uint32_t) * n_red);
-    z.total = z.wres + z.row + z.meta + z.rowflag + z.rowtgt + z.sbits + z.gbits + z.xown + z.rowfac + z.ns + z.rsum + z.redscr + z.stage + z.lz +
+    z.total = z.wres + z.row + z.meta + z.rowflag + z.rowtgt + z.rowsum + z.sbits + z.gbits + z.xown + z.rowfac + z.ns + z.rsum + z.redscr + z.stage + z.lz +
               z.bits + z.groups + z.ts + z.conns + z.plast + z.mons + z.red;
     return z;
 }
@@ -445,15 +485,8 @@ __device__ __forceinline__ void neuron_phase(const DSim* S, const Desc& D, const
     float ir = flush_tiny(ir0 * G.bg_ir_decay);
     float ed = flush_tiny(ed0 * G.bg_ed_decay);
     float id = flush_tiny(id0 * G.bg_id_decay);
-    uint32_t ne = 0, ni = 0;
-    if (D.noise_mode == kNoisePhilox) {
-        if (G.has_bg_e) ne = poisson_knuth(G.exp_neg_mean_e, D.seed, j, t, 0u);
-        if (G.has_bg_i) ni = poisson_knuth(G.exp_neg_mean_i, D.seed, j, t, 1u);
-    } else if (D.noise_mode == kNoiseReplay && t < D.replay_steps) {
-        const size_t base = (static_cast<size_t>(t) * D.N + j) * 2u;
-        ne = D.replay[base];
-        ni = D.replay[base + 1];
-    }
+    const uint32_t noise = __float_as_uint(ns[kNsNoise * MO]);
+    const uint32_t ne = noise & 0xffffu, ni = noise >> 16;
     if (ne > 0u) {
         const float inc = static_cast<float>(ne);
         er += inc;
@@ -595,6 +628,31 @@ __device__ __forceinline__ void neuron_phase(const DSim* S, const Desc& D, const
             ++vk;
             if (col >= 0) M.vh[static_cast<size_t>(clock % M.interval) * M.n_sel + col] = v;
         }
+    }
+}
+
+// The background Poisson counts of step t for the own neurons (kernel_neuron_group_evolve.cu:49-56:
+// one excitatory and one inhibitory count per neuron and step), into the kNsNoise field.  They
+// depend only on (seed, neuron, step) -- or on the replayed counts -- so they are drawn ahead, by
+// threads [first_thread, blockDim), while the CTA waits at the grid barrier before step t.
+__device__ __forceinline__ void draw_noise(const Desc& D, const DCta& cta, unsigned long long t, const SmemLayout& sm,
+                                           uint32_t max_own, uint32_t first_thread) {
+    if (threadIdx.x < first_thread) return;
+    for (uint32_t i = threadIdx.x - first_thread; i < cta.n1 - cta.n0; i += blockDim.x - first_thread) {
+        const uint32_t j = cta.n0 + i;
+        const int g = group_of(D, j);
+        if (g < 0) continue;
+        const DGroup& G = D.groups[g];
+        uint32_t ne = 0, ni = 0;
+        if (D.noise_mode == kNoisePhilox) {
+            if (G.has_bg_e) ne = poisson_knuth(G.exp_neg_mean_e, D.seed, j, t, 0u);
+            if (G.has_bg_i) ni = poisson_knuth(G.exp_neg_mean_i, D.seed, j, t, 1u);
+        } else if (D.noise_mode == kNoiseReplay && t < D.replay_steps) {
+            const size_t base = (static_cast<size_t>(t) * D.N + j) * 2u;
+            ne = D.replay[base];
+            ni = D.replay[base + 1];
+        }
+        sm.ns[kNsNoise * max_own + i] = __uint_as_float(ne | (ni << 16));
     }
 }
 
@@ -869,6 +927,7 @@ __device__ __forceinline__ void apply_updates(const Desc& D, const DBlk* s_blk, 
         const uint32_t nrows = B.row_end - B.row_begin, n_post = C.n_post, post_off = C.post_off;
         const float* colA = P.colA[ppar];
         const float* colB = P.colB[ppar];
+        const bool carry_sum = B.resident && P.kind == kKindTriplet;  // keep rowsum in step (see norm_rows)
         // column pass: lanes scan the bitmask words of the postsynaptic group
         const uint32_t w0 = post_off >> 5, w1 = (post_off + n_post - 1u) >> 5;
         for (uint32_t wb = w0; wb <= w1; wb += 32u) {
@@ -894,8 +953,12 @@ __device__ __forceinline__ void apply_updates(const Desc& D, const DBlk* s_blk, 
                         if (sm.rowflag[r]) continue;  // the row pass owns this weight
                         float* wp = weight_ptr(B, C, sm, i, q);
                         const float4 rw = sm.row[r];
-                        *wp = plastic_update(*wp, q, B.row_begin + i, n_post, 1u, 0u, rw.z, cA, cB, rw.w, P.wmin,
-                                             P.wmax);
+                        const float w0 = *wp;
+                        const float w1 = plastic_update(w0, q, B.row_begin + i, n_post, 1u, 0u, rw.z, cA, cB, rw.w,
+                                                        P.wmin, P.wmax);
+                        *wp = w1;
+                        // one thread per row, columns in ascending order: a fixed summation order
+                        if (carry_sum) sm.rowsum[r] += w1 - w0;
                     }
                 }
             }
@@ -999,14 +1062,67 @@ __device__ __forceinline__ void chunk_sums8(const DBlk& B, const DConn& C, const
 }
 
 // Pass 1 of the triplet normalisation (after apply_updates), on warps [w_first, w_first + nwarps).
-// Resident rows: each warp sums two rows at a time, each lane its units, then an xor-butterfly.
+// Resident rows keep a running sum (rowsum): summed exactly at the start of each launch, then
+// carried from step to step -- the column pass adds each weight change (one thread per row, the
+// columns in ascending order), the normalisation multiplies it by the row's scale as the weight
+// pass rescales the row -- and summed again (each lane its units, then an xor-butterfly) for rows
+// whose presynaptic neuron spiked, where the row pass rewrote every weight, and for every row each
+// kRowSumResync steps.  Between those its rounding departs from the stored row's exact sum by
+// about 1e-8 relative (the reference itself sums sequentially in float, 1e-6 from exact), so the
+// scale target / sum agrees with the reference's to the comparison tolerance, and the rows are not
+// read again for their sums each step.
 // Streamed rows: the carried chunk sums are used; the chunks the update touched are recomputed
 // first (all chunks of a row whose presynaptic neuron spiked; for a spiking postsynaptic neuron,
 // its chunk in every row), then the lanes add the chunks c = lane, lane + 32, ... in order and an
 // xor-butterfly adds the lanes.  Lane 0 forms target / sum.
+// Steps between the exact re-summations of the resident triplet rows' running sums: the
+// normalisation applied at internal step t sums every row again when t is a multiple of this, at
+// a fixed step whatever the launch boundaries (results do not depend on how steps are split
+// into launches).
+constexpr unsigned long long kRowSumResync = 1000ull;
+
+// The exact sum of every resident triplet row (each warp two rows at a time), into rowsum: when a
+// launch starts at step 0.  Between launches the sums are kept in DConn::rowsum.
+__device__ __noinline__ void resident_row_sums(const Desc& D, const SmemLayout& sm, const DBlk* s_blk,
+                                                  uint32_t nblk) {
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u, nwarps = blockDim.x >> 5;
+    for (uint32_t bk = 0; bk < nblk; ++bk) {
+        const DBlk B = s_blk[bk];
+        const DConn& C = D.conns[B.conn];
+        if (!B.resident || C.plast < 0 || D.plast[C.plast].kind != kKindTriplet) continue;
+        const uint32_t nrows = B.row_end - B.row_begin, base = saddr(sm.wres + B.sm_off), ld = C.ld;
+        for (uint32_t i = warp; i < nrows; i += 2u * nwarps) {
+            const uint32_t i2 = i + nwarps;
+            const bool two = i2 < nrows;
+            float sum0, sum1;
+            row_pair_sums(base + 4u * ld * i, base + 4u * ld * (two ? i2 : i), C.units, lane, two, sum0, sum1);
+            sum0 = warp_sum(sum0);
+            sum1 = warp_sum(sum1);
+            if (lane == 0) {
+                sm.rowsum[B.srow + i] = sum0;
+                if (two) sm.rowsum[B.srow + i2] = sum1;
+            }
+        }
+    }
+}
+
+// Copies the running sums of the resident triplet rows between shared memory and DConn::rowsum.
+__device__ __forceinline__ void move_row_sums(const Desc& D, const SmemLayout& sm, const DBlk* s_blk, uint32_t nblk,
+                                              bool to_smem) {
+    for (uint32_t bk = 0; bk < nblk; ++bk) {
+        const DBlk& B = s_blk[bk];
+        const DConn& C = D.conns[B.conn];
+        if (!B.resident || C.rowsum == nullptr) continue;
+        for (uint32_t i = threadIdx.x; i < B.row_end - B.row_begin; i += blockDim.x) {
+            if (to_smem) sm.rowsum[B.srow + i] = __ldcg(C.rowsum + B.row_begin + i);
+            else C.rowsum[B.row_begin + i] = sm.rowsum[B.srow + i];
+        }
+    }
+}
+
 template <bool CARRY>
 __device__ __forceinline__ void norm_rows(const Desc& D, const SmemLayout& sm, const DBlk* s_blk, uint32_t nblk,
-                                       uint32_t w_first, uint32_t nwarps, uint32_t n_chunks) {
+                                       uint32_t w_first, uint32_t nwarps, uint32_t n_chunks, bool resync) {
     const uint32_t warp = (threadIdx.x >> 5) - w_first, lane = threadIdx.x & 31u;
     uint32_t k = 0;  // running index over the CTA's normalised rows
     for (uint32_t bk = 0; bk < nblk; ++bk) {
@@ -1018,20 +1134,18 @@ __device__ __forceinline__ void norm_rows(const Desc& D, const SmemLayout& sm, c
         k += nrows;
         if (!CARRY || B.resident) {
             const uint32_t base = saddr(sm.wres + B.sm_off), ld = C.ld;
-            for (uint32_t i = first; i < nrows; i += 2u * nwarps) {
-                const uint32_t i2 = i + nwarps;
-                const bool two = i2 < nrows;
-                float sum0, sum1;
-                row_pair_sums(base + 4u * ld * i, base + 4u * ld * (two ? i2 : i), units, lane, two, sum0, sum1);
-                sum0 = warp_sum(sum0);
-                sum1 = warp_sum(sum1);
+            for (uint32_t i = first; i < nrows; i += nwarps) {
+                const uint32_t r = B.srow + i;
+                float sum = sm.rowsum[r];
+                if (resync || sm.rowflag[r]) {  // every kRowSumResync steps, or after the row pass: sum again
+                    float unused;
+                    row_pair_sums(base + 4u * ld * i, base + 4u * ld * i, units, lane, false, sum, unused);
+                    sum = warp_sum(sum);
+                }
                 if (lane == 0) {
-                    const uint32_t r = B.srow + i;
-                    sm.row[r].y = sum0 <= 0.0f ? 1.0f : __fdiv_rn(sm.rowtgt[r], sum0);
-                    if (two) {
-                        const uint32_t r2 = B.srow + i2;
-                        sm.row[r2].y = sum1 <= 0.0f ? 1.0f : __fdiv_rn(sm.rowtgt[r2], sum1);
-                    }
+                    const float scale = sum <= 0.0f ? 1.0f : __fdiv_rn(sm.rowtgt[r], sum);
+                    sm.row[r].y = scale;
+                    sm.rowsum[r] = sum <= 0.0f ? sum : sum * scale;  // the sum the rescaled row will have
                 }
             }
             continue;
@@ -1763,6 +1877,8 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : LAZY ? kMaxThreadsRows :
         p += z.rowflag;
         sm.rowtgt = reinterpret_cast<float*>(p);
         p += z.rowtgt;
+        sm.rowsum = reinterpret_cast<float*>(p);
+        p += z.rowsum;
         sm.sbits = reinterpret_cast<uint32_t*>(p);
         p += z.sbits;
         sm.gbits = reinterpret_cast<uint32_t*>(p);
@@ -1937,6 +2053,15 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : LAZY ? kMaxThreadsRows :
     const unsigned long long t0 = s_t0, bar0 = s_bar0;
     const uint32_t clock0 = s_clock0;
     bool ok = true;
+    if constexpr (!LAZY) {
+        if (t0 == 0ull) {
+            resident_row_sums(D, sm, s_blk, s_nblk);
+        } else {
+            move_row_sums(D, sm, s_blk, s_nblk, true);
+        }
+    }
+    draw_noise(D, cta, t0, sm, max_own, 0u);
+    __syncthreads();
 #ifdef BSNN_PHASE_TIMING
     __shared__ unsigned long long s_tally_[kPhaseSlots];
     if (threadIdx.x == 0)
@@ -1992,10 +2117,13 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : LAZY ? kMaxThreadsRows :
                 if constexpr (LAZY) apply_updates_rows(D, s_blk, s_nblk, ppar, sm, neuron_warps, nw);
                 else apply_updates(D, s_blk, s_nblk, ppar, sm, neuron_warps, nw);
                 if (tid == 32u * neuron_warps) BSNN_TSPAN(8, t_upd_);
+                if (tid == blockDim.x - 32u) BSNN_TSPAN(13, t_upd_);
                 if (norm_now) {
                     named_barrier_sync(1u, 32u * nw);
+                    BSNN_TSTART(t_nrm_);
                     if constexpr (LAZY) norm_rows_lazy(D, sm, s_blk, s_nblk, neuron_warps, nw);
-                    else norm_rows<CARRY>(D, sm, s_blk, s_nblk, neuron_warps, nw, n_chunks);
+                    else norm_rows<CARRY>(D, sm, s_blk, s_nblk, neuron_warps, nw, n_chunks, t % kRowSumResync == 0ull);
+                    if (tid == 32u * neuron_warps) BSNN_TSPAN(12, t_nrm_);
                 }
                 if (tid == 32u * neuron_warps) BSNN_TSPAN(7, t_upd_);
             }
@@ -2010,7 +2138,7 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : LAZY ? kMaxThreadsRows :
             __syncthreads();
             if (norm_now) {
                 if constexpr (LAZY) norm_rows_lazy(D, sm, s_blk, s_nblk, 0u, nwarps);
-                else norm_rows<CARRY>(D, sm, s_blk, s_nblk, 0u, nwarps, n_chunks);
+                else norm_rows<CARRY>(D, sm, s_blk, s_nblk, 0u, nwarps, n_chunks, t % kRowSumResync == 0ull);
                 __syncthreads();
             }
         }
@@ -2031,11 +2159,16 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : LAZY ? kMaxThreadsRows :
         }
         __syncthreads();
         BSNN_TMARK(4);
-        if (!grid_barrier(D.barrier, D.error, bar0 + (k + 1ull) * gridDim.x, &s_ok,
-                          t != D.skip_step || blockIdx.x != D.skip_cta)) {
+        grid_arrive(D.barrier, t != D.skip_step || blockIdx.x != D.skip_cta);
+        BSNN_TSTART(t_win_);
+        // the next step's Poisson counts while the other CTAs finish (warp 0 waits)
+        if (k + 1u < n_steps) draw_noise(D, cta, t + 1ull, sm, max_own, nwarps > 1u ? 32u : 0u);
+        if (tid == 32u) BSNN_TSPAN(14, t_win_);
+        if (!grid_wait(D.barrier, D.error, bar0 + (k + 1ull) * gridDim.x, &s_ok)) {
             ok = false;
             break;
         }
+        if (tid == 0) BSNN_TSPAN(15, t_win_);
         BSNN_TMARK(5);
     }
 #ifdef BSNN_PHASE_TIMING
@@ -2069,13 +2202,14 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : LAZY ? kMaxThreadsRows :
         apply_updates(D, s_blk, s_nblk, lpar, sm, 0u, nwarps);
         __syncthreads();
         if (s_has_norm) {
-            norm_rows<CARRY>(D, sm, s_blk, s_nblk, 0u, nwarps, n_chunks);
+            norm_rows<CARRY>(D, sm, s_blk, s_nblk, 0u, nwarps, n_chunks, (t_last + 1ull) % kRowSumResync == 0ull);
             __syncthreads();
         }
         weight_pass<CARRY, LAZY>(D, cta, true, false, lpar, sm, s_seg, s_blk, n_seg, n_chunks);
     }
     __syncthreads();
     move_resident(D, s_blk, s_nblk, sm, false);
+    if constexpr (!LAZY) move_row_sums(D, sm, s_blk, s_nblk, false);
     load_partials(S, D, cta, lpar, sm, max_own);
     __syncthreads();
     move_neuron_state(S, D, cta, sm, max_own, L, false, lpar, true);
