@@ -325,13 +325,20 @@ void batch_finalize(bsnn_batch* b) {
     const size_t state_bytes = (static_cast<size_t>(h.per_cta) * (9u * 4u + 1u) + 15u) & ~size_t(15);
     const size_t noise_bytes = sizeof(uint16_t) * h.per_cta;  // the next step's Poisson counts
     const char* env_state = std::getenv("BSNN_BATCH_STATE");    // "global": keep the state in global memory
-    const char* env_stages = std::getenv("BSNN_BATCH_STAGES");  // 2 .. 4
+    const char* env_stages = std::getenv("BSNN_BATCH_STAGES");  // 2 .. kBatchStages
     const bool allow_smem_state = !(env_state && std::string(env_state) == "global");
     const uint32_t forced_stages =
         b->tune_stages ? b->tune_stages : env_stages ? static_cast<uint32_t>(std::atoi(env_stages)) : 0u;
     struct Choice { uint32_t state, stages, table; };
-    const Choice choices[] = {{1, 4, 1}, {1, 3, 1}, {1, 4, 0}, {1, 3, 0}, {1, 2, 1}, {1, 2, 0},
-                              {0, 4, 1}, {0, 3, 1}, {0, 4, 0}, {0, 3, 0}, {0, 2, 1}, {0, 2, 0}};
+    // Preference without a forced depth: the state resident with 4 or 3 stages, then fewer stages,
+    // then the state in global memory with 4 or 3 stages.  A forced depth (the autotuner tries
+    // every depth up to kBatchStages) takes the first placement that fits it: deep rings leave no
+    // room for the state, so they trade phase A's state traffic for more operand tiles in flight.
+    std::vector<Choice> choices = {{1, 4, 1}, {1, 3, 1}, {1, 4, 0}, {1, 3, 0}, {1, 2, 1}, {1, 2, 0},
+                                   {0, 4, 1}, {0, 3, 1}, {0, 4, 0}, {0, 3, 0}, {0, 2, 1}, {0, 2, 0}};
+    for (uint32_t st = kBatchStages; st > 4; --st)
+        for (uint32_t state = 2; state-- > 0;)
+            for (uint32_t table = 2; table-- > 0;) choices.push_back({state, st, table});
     bool placed = false;
     for (const Choice& ch : choices) {
         if (ch.state && !allow_smem_state) continue;
@@ -656,7 +663,7 @@ BSNN_API bsnn_status bsnn_batch_read_spike_counts(bsnn_batch* b, uint64_t* host_
 }
 
 // Times candidate GEMM unit sizes (K tiles per unit, around the default rule) with the placement's
-// ring depth, then ring depths of 2, 3 and 4 stages for the best unit size, each over
+// ring depth, then ring depths of 2 to 8 stages for the best unit size, each over
 // `trial_steps` clock steps after a warm-up, and keeps the fastest.  Only before the first step:
 // the batch is left at step 0 with the chosen shapes.  The unit size sets how many K chunks a
 // neuron's partial sums add up, so it is part of the batch's arithmetic (results stay
@@ -745,7 +752,7 @@ BSNN_API bsnn_status bsnn_batch_set_tuning(bsnn_batch* b, const bsnn_batch_tunin
     return guarded_batch(b, [&] {
         require(b->steps_done == 0, BSNN_ERR_STATE, "shapes are set before the first step");
         require(t->operand_stages == 0 || (t->operand_stages >= 2 && t->operand_stages <= kBatchStages),
-                BSNN_ERR_INVALID_ARGUMENT, "operand_stages must be 0 or 2..4");
+                BSNN_ERR_INVALID_ARGUMENT, "operand_stages must be 0 or 2..8");
         batch_teardown(b);
         b->tune_kc = t->k_tiles_per_unit;
         b->tune_stages = t->operand_stages;

@@ -48,7 +48,7 @@
 namespace bsnn {
 
 constexpr uint32_t kBatchMaxClasses = 8;
-constexpr uint32_t kBatchStages = 4;        // the largest shared-memory ring of operand stages
+constexpr uint32_t kBatchStages = 8;        // the largest shared-memory ring of operand stages
 constexpr uint32_t kBatchTmemCols = 256;    // accumulator columns (N <= 256)
 constexpr uint32_t kBatchThreads = 512;
 constexpr uint32_t kATileBytes = 128u * 64u * 2u;  // one 128 x 64 BF16 A tile
@@ -544,7 +544,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
     const uint32_t n_units = S->n_units;
     // producer / MMA state (thread 0 only)
     uint32_t full_ph = 0, empty_ph = 0, accum_ph = 0, tfree_ph = 0;
-    uint32_t empty_pend[kBatchStages] = {0, 0, 0, 0};
+    uint32_t empty_pend = 0;  // bit s: stage s holds tiles whose MMAs may still read it
     uint32_t load_s = 0, use_s = 0, units_issued = 0;
     uint32_t ready_slot = 0, ready_ph = 0;  // the unit ring (producer and epilogue alike)
     const bool producer = tid == 128u;  // warp 4: loads and MMAs; warps 0-3: the epilogue
@@ -604,10 +604,10 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
                 // are done
                 auto load = [&](uint32_t i) {
                     const uint32_t s = load_s;
-                    if (empty_pend[s]) {
+                    if ((empty_pend >> s) & 1u) {
                         if (!mbar_wait(saddr(&bs.empty[s]), (empty_ph >> s) & 1u)) good = false;
                         empty_ph ^= 1u << s;
-                        empty_pend[s] = 0;
+                        empty_pend &= ~(1u << s);
                     }
                     const uint32_t bar = saddr(&bs.full[s]);
                     const uint32_t dst = smem_base + s * stage_bytes;
@@ -638,7 +638,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
                         tc_mma_bf16(tmem, smem_desc(a + ks * 2u * 2048u, 2048u, 128u),
                                     smem_desc(b + ks * 2u * (N * 16u), N * 16u, 128u), idesc, (i | ks) != 0u);
                     tc_commit(saddr(&bs.empty[s]));
-                    empty_pend[s] = 1u;
+                    empty_pend |= 1u << s;
                     use_s = use_s + 1u == n_stages ? 0u : use_s + 1u;
                     // refill the stage of the previous iteration (its MMAs have had an MMA's time to
                     // finish; load() waits for them)

@@ -756,12 +756,13 @@ __device__ __forceinline__ uint32_t range_mask(uint32_t w, uint32_t w0, uint32_t
     return (hi == 31u ? 0xffffffffu : ((1u << (hi + 1u)) - 1u)) & ~((1u << lo) - 1u);
 }
 
+// Runs on threads [0, nthreads) of the CTA.
 __device__ __forceinline__ void flush_spike_bits(const DSim* S, const Desc& D, const DCta& cta, uint32_t clock,
-                                              uint32_t par, const SmemLayout& sm) {
+                                              uint32_t par, const SmemLayout& sm, uint32_t nthreads) {
     // the network-wide spike bitmask of this step (read by every CTA's next weight pass)
     if (cta.n1 > cta.n0) {
         const uint32_t w0 = cta.n0 >> 5, w1 = (cta.n1 - 1) >> 5;
-        for (uint32_t w = w0 + threadIdx.x; w <= w1; w += blockDim.x)
+        for (uint32_t w = w0 + threadIdx.x; w <= w1; w += nthreads)
             merge_bits(D.spk_bits[par] + w, range_mask(w, w0, w1, cta.n0, cta.n1),
                        sm.gbits[par * (D.max_own / 32u + 2u) + w - w0]);
     }
@@ -773,7 +774,7 @@ __device__ __forceinline__ void flush_spike_bits(const DSim* S, const Desc& D, c
         const uint32_t b_end = cta.n1 - G.off < G.n ? cta.n1 - G.off : G.n;
         if (cta.n1 <= G.off || a >= b_end) continue;
         const uint32_t w0 = a >> 5, w1 = (b_end - 1) >> 5;
-        for (uint32_t w = w0 + threadIdx.x; w <= w1; w += blockDim.x) {
+        for (uint32_t w = w0 + threadIdx.x; w <= w1; w += nthreads) {
             const uint32_t lo = w == w0 ? (a & 31u) : 0u;
             const uint32_t hi = w == w1 ? ((b_end - 1) & 31u) : 31u;
             const uint32_t mask = (hi == 31u ? 0xffffffffu : ((1u << (hi + 1u)) - 1u)) & ~((1u << lo) - 1u);
@@ -811,8 +812,10 @@ __device__ __forceinline__ void rows_pending(const Desc& D, const DCta& cta, boo
 
 // x = d - r of this step into the row table (after the neuron phase).
 // (Row-scaled forms: also the row's GEMV weight x s qs, with s qs from the row table.)
-__device__ __forceinline__ void rows_x(const Desc& D, const DCta& cta, const SmemLayout& sm, uint32_t max_own) {
-    for (uint32_t r = threadIdx.x; r < cta.n_rows; r += blockDim.x) {
+// Runs on threads [0, nthreads) of the CTA.
+__device__ __forceinline__ void rows_x(const Desc& D, const DCta& cta, const SmemLayout& sm, uint32_t max_own,
+                                       uint32_t nthreads) {
+    for (uint32_t r = threadIdx.x; r < cta.n_rows; r += nthreads) {
         const DRowMeta meta = sm.meta[r];
         const DConn& C = D.conns[meta.conn];
         const float x = sm.xown[static_cast<uint32_t>(C.ts) * max_own + (meta.j - cta.n0)];
@@ -2111,6 +2114,17 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : LAZY ? kMaxThreadsRows :
                 BSNN_TSTART(t_nrn_);
                 neuron_phase(S, D, cta, t, clock, par, pending, sm, max_own, L, s_ev[0], s_ev[1]);
                 if (tid == 0) BSNN_TSPAN(6, t_nrn_);
+                if constexpr (!LAZY) {
+                    // The neuron warps go on to publish the step's spikes and put x into the row
+                    // table while the update warps still work (the normalisation writes only the
+                    // rows' scales).
+                    if (neuron_warps > 1u) named_barrier_sync(3u, 32u * neuron_warps);
+                    else __syncwarp();
+                    BSNN_TSTART(t_fl_);
+                    flush_spike_bits(S, D, cta, clock, par, sm, 32u * neuron_warps);
+                    if (tid == 0) BSNN_TSPAN(11, t_fl_);
+                    rows_x(D, cta, sm, max_own, 32u * neuron_warps);
+                }
             } else if (pending) {
                 BSNN_TSTART(t_upd_);
                 const uint32_t nw = nwarps - neuron_warps;
@@ -2143,13 +2157,13 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : LAZY ? kMaxThreadsRows :
             }
         }
         BSNN_TMARK(1);
-        {
+        if (LAZY || !norm_beside) {
             BSNN_TSTART(t_fl_);
-            flush_spike_bits(S, D, cta, clock, par, sm);
+            flush_spike_bits(S, D, cta, clock, par, sm, blockDim.x);
             if (tid == 0) BSNN_TSPAN(11, t_fl_);
+            rows_x(D, cta, sm, max_own, blockDim.x);
+            __syncthreads();
         }
-        rows_x(D, cta, sm, max_own);
-        __syncthreads();
         BSNN_TMARK(2);
         {
             BSNN_TSTART(t_wp_);
