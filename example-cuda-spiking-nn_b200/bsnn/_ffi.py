@@ -270,6 +270,7 @@ class BatchInfo(ctypes.Structure):
         ("smem_bytes", ctypes.c_uint64),
         ("state_in_smem", ctypes.c_uint32),
         ("operand_stages", ctypes.c_uint32),
+        ("form", ctypes.c_int32),
     ]
 
 
@@ -315,6 +316,7 @@ SIGNATURES = {
                                        _U32, ctypes.POINTER(_U32)]),
     "bsnn_batch_set_noise": (_I32, [_P, _I32]),
     "bsnn_batch_set_steps_per_launch": (_I32, [_P, _U32]),
+    "bsnn_batch_set_form": (_I32, [_P, _I32]),
     "bsnn_batch_set_device_wait_limit": (_I32, [_P, ctypes.c_uint64]),
     "bsnn_batch_run": (_I32, [_P, _U32]),
     "bsnn_batch_synchronize": (_I32, [_P]),

@@ -139,7 +139,9 @@ def _ptr(a, t):
 class BatchSimulation:
     """One batch on one GPU, built from a BatchSpec."""
 
-    def __init__(self, spec: BatchSpec, device: int = 0, noise: bool = True, library=None):
+    FORMS = {"flow": 0, "phased": 1}
+
+    def __init__(self, spec: BatchSpec, device: int = 0, noise: bool = True, library=None, form: str = "phased"):
         self._lib = library if library is not None else load_library()
         self._h = ctypes.c_void_p()
         self._check(self._lib.bsnn_batch_create(device, ctypes.byref(self._h)), creating=True)
@@ -166,6 +168,15 @@ class BatchSimulation:
             self._sizes.append(C.num_e + C.num_i)
         if not noise:
             self._check(self._lib.bsnn_batch_set_noise(self._h, 0))
+        self.set_form(form)
+
+    def set_form(self, form: str):
+        """How the kernel orders a clock step's work, before the first step: "flow" (each size
+        class its own chain of neuron updates and GEMM units, overlapping) or "phased" (all
+        neurons, grid barrier, all GEMM units, grid barrier).  Results are bit-identical."""
+        if form not in self.FORMS:
+            raise ValueError(f"unknown batch form {form!r}")
+        self._check(self._lib.bsnn_batch_set_form(self._h, self.FORMS[form]))
 
     def _check(self, st, creating=False):
         if st != 0:

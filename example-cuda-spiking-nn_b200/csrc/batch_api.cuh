@@ -43,15 +43,17 @@ struct bsnn_batch {
     size_t arena_bytes = 0;
     BSim h{};
     BSim* d_sim = nullptr;
-    std::vector<uint32_t> inst_order;  // instance id -> position in the class-sorted order
-    std::vector<uint32_t> nbase;       // per instance id: first neuron
+    std::vector<uint32_t> pos;    // instance id -> position in the class-sorted order (the device's
+                                  // instance table is in this order)
+    std::vector<uint32_t> nbase;  // per instance id: first neuron (neurons are numbered class by class)
     uint32_t grid = 0;
     size_t smem = 0;
     uint64_t steps_done = 0, launches = 0;
     uint32_t steps_per_launch = 1000;
     std::map<uint32_t, cudaGraphExec_t> graphs;
     float* scratch = nullptr;  // [2][max N] for reads of g with the pending propagation
-    const void* kernel = nullptr;  // bsnn_batch_kernel<state in shared memory or not>
+    const void* kernel = nullptr;  // the flow or phased kernel, state in shared memory or not
+    int32_t form = BSNN_BATCH_FORM_PHASED;
     uint32_t tune_kc = 0;          // K tiles per GEMM unit (0: the default rule)
     uint32_t tune_stages = 0;      // operand stages (0: the placement's choice)
     uint32_t kc = 0;               // the unit size in use
@@ -128,18 +130,25 @@ void batch_finalize(bsnn_batch* b) {
     h.n_inst = static_cast<uint32_t>(b->insts.size());
     h.noise_on = b->noise_on ? 1 : 0;
 
-    // Instances in class order: the instance's row in its class's B operand is its rank there.
-    std::vector<uint32_t> row(h.n_inst);
+    // Instances in class order: the instance's row in its class's B operand is its rank there, and
+    // neurons are numbered class by class (a class's neurons are contiguous).
+    std::vector<uint32_t> row(h.n_inst), by_pos;
     b->nbase.assign(h.n_inst, 0);
+    b->pos.assign(h.n_inst, 0);
     uint32_t n_neurons = 0;
+    std::vector<uint32_t> cls_nbase(h.n_classes), cls_nlen(h.n_classes);
     for (uint32_t c = 0; c < h.n_classes; ++c) {
         const auto& HC = b->classes[c];
-        for (uint32_t r = 0; r < HC.instances.size(); ++r) row[HC.instances[r]] = r;
-    }
-    for (uint32_t i = 0; i < h.n_inst; ++i) {
-        const auto& HC = b->classes[b->insts[i].cls];
-        b->nbase[i] = n_neurons;
-        n_neurons += HC.E + HC.I;
+        cls_nbase[c] = n_neurons;
+        for (uint32_t r = 0; r < HC.instances.size(); ++r) {
+            const uint32_t i = HC.instances[r];
+            row[i] = r;
+            b->pos[i] = static_cast<uint32_t>(by_pos.size());
+            by_pos.push_back(i);
+            b->nbase[i] = n_neurons;
+            n_neurons += HC.E + HC.I;
+        }
+        cls_nlen[c] = n_neurons - cls_nbase[c];
     }
     h.n_neurons = n_neurons;
 
@@ -165,7 +174,8 @@ void batch_finalize(bsnn_batch* b) {
         C.n_inst = static_cast<uint32_t>(HC.instances.size());
         C.NP = std::max<uint32_t>(8u, round_up(C.n_inst, 8));
         require(C.NP <= 128, BSNN_ERR_INVALID_ARGUMENT, "at most 128 instances per size class");
-        C.inst0 = HC.instances.empty() ? 0u : HC.instances[0];
+        C.nbase = cls_nbase[c];
+        C.nlen = cls_nlen[c];
         C.MT = (C.N + 127) / 128;
         for (int sd = 0; sd < 2; ++sd) {
             const uint32_t K = sd == 0 ? C.E : C.I;
@@ -190,11 +200,30 @@ void batch_finalize(bsnn_batch* b) {
         }
     }
     h.n_units = static_cast<uint32_t>(units.size());
-    // longest first: CTAs take units from a shared dispenser in this order
+    // Class processing order of the flow form: the classes with the most GEMM work first (their
+    // chains are the longest).
+    std::vector<double> cls_work(h.n_classes, 0.0);
+    for (const BUnit& U : units) cls_work[U.cls] += static_cast<double>(U.k1 - U.k0);
+    std::vector<uint32_t> cls_order(h.n_classes);
+    std::iota(cls_order.begin(), cls_order.end(), 0u);
+    std::stable_sort(cls_order.begin(), cls_order.end(), [&](uint32_t a, uint32_t c) { return cls_work[a] > cls_work[c]; });
+    std::vector<uint32_t> cls_rank(h.n_classes);
+    for (uint32_t p = 0; p < h.n_classes; ++p) {
+        h.order[p] = cls_order[p];
+        cls_rank[cls_order[p]] = p;
+    }
+    for (const BUnit& U : units) ++h.units_of[U.cls];
+    const bool flow = b->form == BSNN_BATCH_FORM_FLOW;
+    // The dispenser's order: longest first (phased form), or by class processing order and longest
+    // first within a class (flow form: a step's units are taken in the order its classes become
+    // ready).
     std::vector<uint32_t> order(units.size());
     std::iota(order.begin(), order.end(), 0u);
     auto cost = [&](uint32_t u) { return static_cast<double>(units[u].k1 - units[u].k0) + 2.0; };
-    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t c) { return cost(a) > cost(c); });
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t c) {
+        if (flow && units[a].cls != units[c].cls) return cls_rank[units[a].cls] < cls_rank[units[c].cls];
+        return cost(a) > cost(c);
+    });
     std::vector<BUnit> units_sorted;
     units_sorted.reserve(units.size());
     for (uint32_t u : order) units_sorted.push_back(units[u]);
@@ -232,6 +261,8 @@ void batch_finalize(bsnn_batch* b) {
     const size_t o_inst = A.take(sizeof(BInst) * h.n_inst);
     const size_t o_units = A.take(sizeof(BUnit) * units_sorted.size());
     const size_t o_ctr = A.take(sizeof(unsigned long long));
+    const size_t o_nready = A.take(sizeof(unsigned long long) * kBatchMaxClasses);
+    const size_t o_udone = A.take(sizeof(unsigned long long) * kBatchMaxClasses);
     const size_t o_part = A.take(sizeof(float) * std::max<size_t>(part_floats, 1));
     size_t o_a[kBatchMaxClasses][2], o_x[kBatchMaxClasses][2];
     for (uint32_t c = 0; c < h.n_classes; ++c)
@@ -268,12 +299,13 @@ void batch_finalize(bsnn_batch* b) {
 
     // neuron -> instance, instance table, initial voltages and refractory counters
 
-    std::vector<BInst> inst(h.n_inst);
+    std::vector<BInst> inst(h.n_inst);  // in position order
     std::vector<float> v0(n_neurons);
     for (uint32_t i = 0; i < h.n_inst; ++i) {
         const auto& I = b->insts[i];
         const auto& HC = b->classes[I.cls];
-        BInst& BI = inst[i];
+        BInst& BI = inst[b->pos[i]];
+        BI.id = i;
         BI.cls = I.cls;
         BI.row = row[i];
         BI.nbase = b->nbase[i];
@@ -287,6 +319,8 @@ void batch_finalize(bsnn_batch* b) {
     h.inst = reinterpret_cast<const BInst*>(base + o_inst);
     h.units = reinterpret_cast<const BUnit*>(base + o_units);
     h.unit_ctr = reinterpret_cast<unsigned long long*>(base + o_ctr);
+    h.nready = reinterpret_cast<unsigned long long*>(base + o_nready);
+    h.udone = reinterpret_cast<unsigned long long*>(base + o_udone);
     cuda_check(cudaMemcpy(base + o_inst, inst.data(), sizeof(BInst) * inst.size(), cudaMemcpyHostToDevice), "H2D");
     cuda_check(cudaMemcpy(h.v, v0.data(), fN, cudaMemcpyHostToDevice), "H2D v");
     cuda_check(cudaMemcpy(base + o_units, units_sorted.data(), sizeof(BUnit) * units_sorted.size(),
@@ -317,7 +351,12 @@ void batch_finalize(bsnn_batch* b) {
     uint32_t max_b = 0;
     for (uint32_t c = 0; c < h.n_classes; ++c) max_b = std::max(max_b, 2u * h.cls[c].NP * 128u);
     h.stage_bytes = (kATileBytes + max_b + 1023u) & ~1023u;
+    // Neurons per CTA: a contiguous range (phased form), or a slice of every class (flow form).
     h.per_cta = (n_neurons + n_ctas - 1) / n_ctas;
+    if (flow) {
+        h.per_cta = 0;
+        for (uint32_t c = 0; c < h.n_classes; ++c) h.per_cta += (cls_nlen[c] + n_ctas - 1) / n_ctas;
+    }
     int optin = 0;
     cuda_check(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device), "smem attr");
     const size_t avail = static_cast<size_t>(optin) - 4096;  // the kernel's static shared memory
@@ -359,8 +398,12 @@ void batch_finalize(bsnn_batch* b) {
     }
     require(placed, BSNN_ERR_INVALID_ARGUMENT, "batch too large: the operand stages do not fit in shared memory");
     cuda_check(cudaMemcpy(b->d_sim, &h, sizeof(BSim), cudaMemcpyHostToDevice), "H2D batch sim");
-    b->kernel = h.state_in_smem ? reinterpret_cast<const void*>(&bsnn_batch_kernel<true>)
-                                : reinterpret_cast<const void*>(&bsnn_batch_kernel<false>);
+    if (flow)
+        b->kernel = h.state_in_smem ? reinterpret_cast<const void*>(&bsnn_batch_flow_kernel<true>)
+                                    : reinterpret_cast<const void*>(&bsnn_batch_flow_kernel<false>);
+    else
+        b->kernel = h.state_in_smem ? reinterpret_cast<const void*>(&bsnn_batch_kernel<true>)
+                                    : reinterpret_cast<const void*>(&bsnn_batch_kernel<false>);
     // the limit is per function and shared by every batch in the process: allow the most any
     // batch may use, so one batch's smaller setting never invalidates another's launches
     cuda_check(cudaFuncSetAttribute(b->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(avail)),
@@ -544,6 +587,19 @@ BSNN_API bsnn_status bsnn_batch_set_noise(bsnn_batch* b, int32_t on) {
     });
 }
 
+BSNN_API bsnn_status bsnn_batch_set_form(bsnn_batch* b, int32_t form) {
+    if (!b) return BSNN_ERR_INVALID_ARGUMENT;
+    return guarded_batch(b, [&] {
+        require(form == BSNN_BATCH_FORM_FLOW || form == BSNN_BATCH_FORM_PHASED, BSNN_ERR_INVALID_ARGUMENT,
+                "unknown batch form");
+        require(b->steps_done == 0, BSNN_ERR_STATE, "the form is set before the first step");
+        if (form != b->form) {
+            batch_teardown(b);
+            b->form = form;
+        }
+    });
+}
+
 BSNN_API bsnn_status bsnn_batch_set_steps_per_launch(bsnn_batch* b, uint32_t steps) {
     if (!b) return BSNN_ERR_INVALID_ARGUMENT;
     return guarded_batch(b, [&] {
@@ -637,7 +693,7 @@ BSNN_API bsnn_status bsnn_batch_read_state(bsnn_batch* b, uint32_t instance, int
             case BSNN_FIELD_BG_G_INHIBITORY: {
                 const bool with_pending = field == BSNN_FIELD_G_EXCITATORY || field == BSNN_FIELD_G_INHIBITORY;
                 const bool exc = field == BSNN_FIELD_G_EXCITATORY || field == BSNN_FIELD_BG_G_EXCITATORY;
-                bsnn_batch_g_kernel<<<(n + 255) / 256, 256, 0, b->stream>>>(b->d_sim, instance, with_pending ? 1 : 0,
+                bsnn_batch_g_kernel<<<(n + 255) / 256, 256, 0, b->stream>>>(b->d_sim, b->pos[instance], with_pending ? 1 : 0,
                                                                             b->scratch, b->scratch + n);
                 cuda_check(cudaGetLastError(), "batch g read");
                 cuda_check(cudaMemcpyAsync(host_out, b->scratch + (exc ? 0 : n), 4ull * n, cudaMemcpyDeviceToHost,
@@ -779,6 +835,7 @@ BSNN_API bsnn_status bsnn_batch_get_info(bsnn_batch* b, bsnn_batch_info* out) {
         i.smem_bytes = b->smem;
         i.state_in_smem = b->h.state_in_smem;
         i.operand_stages = b->h.n_stages;
+        i.form = b->form;
         *out = i;
     });
 }

@@ -57,7 +57,8 @@ constexpr uint32_t kATileBytes = 128u * 64u * 2u;  // one 128 x 64 BF16 A tile
 struct BClass {
     uint32_t E, I, N;        // neurons per instance (N = E + I)
     uint32_t n_inst, NP;     // instances; NP = n_inst rounded up to 8 (B has 2 NP rows: hi, lo)
-    uint32_t inst0;          // first instance id of the class
+    uint32_t nbase, nlen;    // the class's neurons: [nbase, nbase + nlen) (instances are numbered
+                             // class by class, so a class's neurons are contiguous)
     uint32_t MT;             // 128-post tiles
     uint32_t KT[2];          // 64-pre K tiles of the E and I sides
     uint32_t nkc[2];         // K chunks per post tile (one unit each)
@@ -78,9 +79,11 @@ struct BGroupP {
     uint32_t refractory_steps, has_bg_e, has_bg_i;
 };
 
-// One instance: its class, its row in the class's B operand, its first neuron, seed and groups.
+// One instance: its class, its row in the class's B operand, its first neuron, seed, its index in
+// the order the instances were added (`id`, which indexes the spike counts) and its groups.  The
+// table is sorted by first neuron.
 struct BInst {
-    uint32_t cls, row, nbase, seed;
+    uint32_t cls, row, nbase, seed, id, pad_;
     BGroupP g[2];  // E, I
 };
 
@@ -119,6 +122,11 @@ struct BSim {
     int32_t* error;
     unsigned long long* steps_done;
     unsigned long long wait_limit_ns;  // bound of every device-side wait of a launch
+    // the flow form (bsnn_batch_flow_kernel)
+    uint32_t order[kBatchMaxClasses];     // classes in processing order (most GEMM work first)
+    uint32_t units_of[kBatchMaxClasses];  // GEMM units per class
+    unsigned long long* nready;           // [kBatchMaxClasses] CTA slices stepped (+1 per CTA per step)
+    unsigned long long* udone;            // [kBatchMaxClasses] unit epilogue warps done (+4 per unit per step)
 };
 
 // ---- tcgen05 / tensor-memory wrappers ---------------------------------------------------------
@@ -343,7 +351,7 @@ __device__ __forceinline__ void neuron_step(const BSim* S, const BInst* P, const
     X.refrac[i] = refrac;
     if constexpr (SMEM) X.spike8[i] = static_cast<uint8_t>(spike);
     else X.spike32[i] = spike;
-    if (spike) atomicAdd(S->spike_counts + 2u * a.inst + side, 1ull);
+    if (spike) atomicAdd(S->spike_counts + 2u * B.id + side, 1ull);
 
     // stimulus events of this step act from the next step
     if (t < S->stim_len) {
@@ -385,15 +393,17 @@ __device__ __forceinline__ void neuron_step(const BSim* S, const BInst* P, const
 #endif
 constexpr uint32_t kNeuronsInFlight = BSNN_BATCH_NEURONS_IN_FLIGHT;
 
+// Neurons [n0, n1), by `count` threads of the CTA, this one being number `me`.
 template <bool SMEM>
 __device__ __forceinline__ void batch_neurons(const BSim* S, const BInst* P, const BClass* s_cls, const BState& X,
-                                              const uint16_t* nz, uint32_t n0, uint32_t n1, unsigned long long t) {
-    uint32_t cur = instance_of(P, S->n_inst, n0 + threadIdx.x < n1 ? n0 + threadIdx.x : n0);
-    for (uint32_t n = n0 + threadIdx.x; n < n1; n += kNeuronsInFlight * blockDim.x) {
+                                              const uint16_t* nz, uint32_t n0, uint32_t n1, unsigned long long t,
+                                              uint32_t me, uint32_t count) {
+    uint32_t cur = instance_of(P, S->n_inst, n0 + me < n1 ? n0 + me : n0);
+    for (uint32_t n = n0 + me; n < n1; n += kNeuronsInFlight * count) {
         NeuronIn a[kNeuronsInFlight];
 #pragma unroll
         for (uint32_t q = 0; q < kNeuronsInFlight; ++q)
-            neuron_load<SMEM>(S, P, s_cls, X, n + q * blockDim.x, n + q * blockDim.x < n1, t, cur, a[q]);
+            neuron_load<SMEM>(S, P, s_cls, X, n + q * count, n + q * count < n1, t, cur, a[q]);
 #pragma unroll
         for (uint32_t q = 0; q < kNeuronsInFlight; ++q) neuron_step<SMEM>(S, P, s_cls, X, nz, n0, t, a[q]);
     }
@@ -401,14 +411,14 @@ __device__ __forceinline__ void batch_neurons(const BSim* S, const BInst* P, con
 
 // The background Poisson counts of step t for neurons [n0, n1), drawn by `count` threads of the
 // CTA, this one being number `me`: nz[n - n0] = n_e | n_i << 8 (each saturates at 255).
-__device__ __forceinline__ void noise_ahead(const BSim* S, const BInst* P, uint16_t* nz, uint32_t n0, uint32_t n1,
-                                            unsigned long long t, uint32_t me, uint32_t count) {
+__device__ __forceinline__ void noise_ahead(const BSim* S, const BInst* P, const BClass* s_cls, uint16_t* nz, uint32_t n0,
+                                            uint32_t n1, unsigned long long t, uint32_t me, uint32_t count) {
     uint32_t cur = instance_of(P, S->n_inst, n0 + me < n1 ? n0 + me : n0);
     for (uint32_t n = n0 + me; n < n1; n += count) {
         while (cur + 1u < S->n_inst && P[cur + 1u].nbase <= n) ++cur;
         const BInst& B = P[cur];
         const uint32_t j = n - B.nbase;
-        const BGroupP& G = B.g[j < S->cls[B.cls].E ? 0 : 1];
+        const BGroupP& G = B.g[j < s_cls[B.cls].E ? 0 : 1];
         const uint32_t ne = G.has_bg_e ? poisson_knuth(G.exp_neg_mean_e, B.seed, j, t, 0u) : 0u;
         const uint32_t ni = G.has_bg_i ? poisson_knuth(G.exp_neg_mean_i, B.seed, j, t, 1u) : 0u;
         nz[n - n0] = static_cast<uint16_t>(ne | (ni << 8));
@@ -431,7 +441,42 @@ __device__ __forceinline__ uint32_t noise_rank(uint32_t warp) {  // among the no
 }
 constexpr uint32_t kNoiseWarps = BSNN_BATCH_NOISE_WARPS == 1 ? 9u : 11u;
 
-// Copies the CTA's state between global memory and its shared-memory arrays.
+// The CTA's shared-memory state arrays (`per` neurons each, from `raw` on), from index `soff` on,
+// for neurons numbered from `base`.
+__device__ __forceinline__ BState smem_state(unsigned char* raw, uint32_t per, uint32_t soff, uint32_t base) {
+    float* f = reinterpret_cast<float*>(raw);
+    BState X{};
+    X.v = f + soff;
+    X.istim = f + per + soff;
+    X.er = f + 2 * per + soff;
+    X.ed = f + 3 * per + soff;
+    X.ir = f + 4 * per + soff;
+    X.id = f + 5 * per + soff;
+    X.tr = f + 6 * per + soff;
+    X.td = f + 7 * per + soff;
+    X.refrac = reinterpret_cast<uint32_t*>(f + 8 * per) + soff;
+    X.spike8 = reinterpret_cast<uint8_t*>(f + 9 * per) + soff;
+    X.base = base;
+    return X;
+}
+__device__ __forceinline__ BState global_state(const BSim* S) {
+    BState X{};
+    X.v = S->v;
+    X.istim = S->istim;
+    X.er = S->er;
+    X.ed = S->ed;
+    X.ir = S->ir;
+    X.id = S->id;
+    X.tr = S->tr;
+    X.td = S->td;
+    X.refrac = S->refrac;
+    X.spike32 = S->spikes;
+    X.base = 0;
+    return X;
+}
+
+// Copies the state of neurons [n0, n1) between global memory and shared-memory arrays indexed by
+// n - n0.
 __device__ __forceinline__ void state_copy(const BSim* S, const BState& X, uint32_t n0, uint32_t n1, bool to_smem) {
     float* g[8] = {S->v, S->istim, S->er, S->ed, S->ir, S->id, S->tr, S->td};
     float* sm[8] = {X.v, X.istim, X.er, X.ed, X.ir, X.id, X.tr, X.td};
@@ -464,6 +509,140 @@ struct BatchSmem {
     uint64_t tfree;   // the 4 epilogue warps: the accumulator has been read
 };
 
+// The producer's ring and accumulator state (one thread).
+struct ProducerState {
+    uint32_t full_ph = 0, empty_ph = 0, tfree_ph = 0;
+    uint32_t empty_pend = 0;  // bit s: stage s holds tiles whose MMAs may still read it
+    uint32_t full_pend = 0;   // bit s: stage s has copies in flight not yet waited for
+    uint32_t load_s = 0, use_s = 0, units_issued = 0;
+};
+
+// One GEMM unit on the producer thread: streams the unit's A and B tiles into the ring of
+// shared-memory stages (one bulk copy per operand tile), issues the MMAs into the accumulator
+// (after the epilogue has read the previous unit's), and commits the accumulator.  Returns false
+// when a wait timed out (the accumulator is committed all the same, to release the epilogue).
+__device__ __forceinline__ bool issue_unit(BatchSmem& bs, ProducerState& ps, const BUnit& U, const BClass& C,
+                                           uint32_t tmem, uint32_t smem_base, uint32_t stage_bytes, uint32_t n_stages,
+                                           uint64_t keep) {
+    const uint32_t N = 2u * C.NP, b_bytes = N * 128u, nk = U.k1 - U.k0;
+    const unsigned char* a_src =
+        reinterpret_cast<const unsigned char*>(C.A[U.side]) + (static_cast<size_t>(U.mt) * C.KT[U.side] + U.k0) * kATileBytes;
+    const unsigned char* b_src = reinterpret_cast<const unsigned char*>(C.X[U.side]) + static_cast<size_t>(U.k0) * b_bytes;
+    bool good = true;
+    // K tile i of the unit into stage load_s, once the MMAs that read the stage last are done
+    auto load = [&](uint32_t i) {
+        const uint32_t s = ps.load_s;
+        if ((ps.empty_pend >> s) & 1u) {
+            if (!mbar_wait(saddr(&bs.empty[s]), (ps.empty_ph >> s) & 1u)) good = false;
+            ps.empty_ph ^= 1u << s;
+            ps.empty_pend &= ~(1u << s);
+        }
+        const uint32_t bar = saddr(&bs.full[s]);
+        const uint32_t dst = smem_base + s * stage_bytes;
+        mbar_expect_tx(bar, kATileBytes + b_bytes);
+        bulk_load_keep(dst, a_src + static_cast<size_t>(i) * kATileBytes, kATileBytes, bar, keep);
+        bulk_load(dst + kATileBytes, b_src + static_cast<size_t>(i) * b_bytes, b_bytes, bar);
+        ps.full_pend |= 1u << s;
+        ps.load_s = ps.load_s + 1u == n_stages ? 0u : ps.load_s + 1u;
+    };
+    const uint32_t idesc = idesc_bf16_m128(N);
+    uint32_t next = 0;
+    for (; next < nk && next < n_stages; ++next) load(next);
+    // the epilogue of the previous unit has read the accumulator
+    if (ps.units_issued > 0u) {
+        if (!mbar_wait(saddr(&bs.tfree), ps.tfree_ph & 1u)) good = false;
+        ps.tfree_ph ^= 1u;
+    }
+    for (uint32_t i = 0; i < nk && good; ++i) {
+        const uint32_t s = ps.use_s;
+        if (!mbar_wait(saddr(&bs.full[s]), (ps.full_ph >> s) & 1u)) {
+            good = false;
+            break;
+        }
+        ps.full_ph ^= 1u << s;
+        ps.full_pend &= ~(1u << s);
+        tc_fence_after();
+        const uint32_t a = smem_base + s * stage_bytes, b = a + kATileBytes;
+#pragma unroll
+        for (uint32_t ks = 0; ks < 4; ++ks)
+            tc_mma_bf16(tmem, smem_desc(a + ks * 2u * 2048u, 2048u, 128u), smem_desc(b + ks * 2u * (N * 16u), N * 16u, 128u),
+                        idesc, (i | ks) != 0u);
+        tc_commit(saddr(&bs.empty[s]));
+        ps.empty_pend |= 1u << s;
+        ps.use_s = ps.use_s + 1u == n_stages ? 0u : ps.use_s + 1u;
+        // refill the stage of the previous iteration (its MMAs have had an MMA's time to finish;
+        // load() waits for them)
+        if (i > 0u && next < nk) load(next++);
+    }
+    tc_commit(saddr(&bs.accum));
+    ++ps.units_issued;
+    return good;
+}
+
+// After a timeout, on the producer thread: waits (each wait bounded) for the copies it issued and
+// for its last MMAs, so that none is in flight when the CTA frees its tensor memory and exits.
+__device__ __forceinline__ void producer_quiesce(BatchSmem& bs, ProducerState& ps, uint32_t n_stages) {
+    for (uint32_t s = 0; s < n_stages; ++s)
+        if ((ps.full_pend >> s) & 1u) mbar_wait(saddr(&bs.full[s]), (ps.full_ph >> s) & 1u);
+    if (ps.units_issued > 0u) mbar_wait(saddr(&bs.accum), (ps.units_issued - 1u) & 1u);
+}
+
+// One GEMM unit on the epilogue warps 0-3 (warp w reads accumulator lanes 32w .. 32w + 31, one
+// post each): waits for the accumulator, adds its hi and lo halves, writes the class's instances'
+// partial sums of the unit, and frees the accumulator.
+__device__ __forceinline__ void drain_unit(const BSim* S, BatchSmem& bs, const BUnit& U, const BClass& C, uint32_t tmem,
+                                           uint32_t& accum_ph, uint32_t warp, uint32_t lane) {
+    const uint32_t row = 32u * warp + lane;
+    const bool got = mbar_wait(saddr(&bs.accum), accum_ph & 1u);
+    accum_ph ^= 1u;
+    if (!got) {
+        atomicExch(S->error, kErrStageTimeout);
+        bs.ok = 0u;
+    }
+    tc_fence_after();
+    float* part = S->partials + U.part;
+    for (uint32_t c0 = 0; c0 < C.NP; c0 += 16u) {
+        float hi[16], lo[16];
+        tmem_ld16(tmem + ((32u * warp) << 16) + c0, hi);
+        tmem_ld16(tmem + ((32u * warp) << 16) + C.NP + c0, lo);
+#pragma unroll
+        for (uint32_t q = 0; q < 16; ++q)
+            if (c0 + q < C.n_inst) part[static_cast<size_t>(c0 + q) * 128u + row] = hi[q] + lo[q];
+    }
+    tc_fence_before();
+    __syncwarp();
+    if (lane == 0) mbar_arrive(saddr(&bs.tfree));
+}
+
+// Copies the launch-invariant tables into shared memory: the class table, and the instance table
+// when the placement keeps it there (returned; else the global one).
+__device__ __forceinline__ const BInst* batch_tables(const BSim* S, unsigned char* table_smem, BClass* s_cls) {
+    const BInst* P = S->inst;
+    if (S->inst_in_smem) {
+        BInst* s_inst = reinterpret_cast<BInst*>(table_smem);
+        for (uint32_t i = threadIdx.x; i < S->n_inst * (sizeof(BInst) / 4u); i += blockDim.x)
+            reinterpret_cast<uint32_t*>(s_inst)[i] = reinterpret_cast<const uint32_t*>(S->inst)[i];
+        P = s_inst;
+    }
+    for (uint32_t i = threadIdx.x; i < S->n_classes * (sizeof(BClass) / 4u); i += blockDim.x)
+        reinterpret_cast<uint32_t*>(s_cls)[i] = reinterpret_cast<const uint32_t*>(S->cls)[i];
+    return P;
+}
+
+// Thread 0: the ring's, the accumulator's and the unit ring's mbarriers.
+__device__ __forceinline__ void batch_init_barriers(BatchSmem& bs, uint32_t n_stages) {
+    bs.ok = 1u;
+    for (uint32_t s = 0; s < n_stages; ++s) {
+        mbar_init(saddr(&bs.full[s]), 1u);
+        mbar_init(saddr(&bs.empty[s]), 1u);
+    }
+    mbar_init(saddr(&bs.accum), 1u);
+    mbar_init(saddr(&bs.ready[0]), 1u);
+    mbar_init(saddr(&bs.ready[1]), 1u);
+    mbar_init(saddr(&bs.tfree), 4u);
+    fence_mbar_init();
+}
+
 template <bool SMEM_STATE>
 __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim* __restrict__ S, uint32_t n_steps) {
     extern __shared__ __align__(1024) unsigned char bsm_raw[];
@@ -477,58 +656,19 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
     // kept in shared memory), then the neuron state (when it is kept in shared memory)
     const uint32_t stage_bytes = S->stage_bytes, n_stages = S->n_stages;
     const uint32_t smem_base = saddr(bsm_raw);
-    const BInst* P = S->inst;
-    if (S->inst_in_smem) {
-        BInst* s_inst = reinterpret_cast<BInst*>(bsm_raw + n_stages * stage_bytes);
-        for (uint32_t i = tid; i < S->n_inst * (sizeof(BInst) / 4u); i += blockDim.x)
-            reinterpret_cast<uint32_t*>(s_inst)[i] = reinterpret_cast<const uint32_t*>(S->inst)[i];
-        P = s_inst;
-    }
+    const BInst* P = batch_tables(S, bsm_raw + n_stages * stage_bytes, s_cls);
     const uint32_t n0 = min(blockIdx.x * S->per_cta, S->n_neurons);
     const uint32_t n1 = min(n0 + S->per_cta, S->n_neurons);
     BState X{};
     if constexpr (SMEM_STATE) {
-        const uint32_t per = S->per_cta;
-        float* f = reinterpret_cast<float*>(bsm_raw + S->state_off);
-        X.v = f;
-        X.istim = f + per;
-        X.er = f + 2 * per;
-        X.ed = f + 3 * per;
-        X.ir = f + 4 * per;
-        X.id = f + 5 * per;
-        X.tr = f + 6 * per;
-        X.td = f + 7 * per;
-        X.refrac = reinterpret_cast<uint32_t*>(f + 8 * per);
-        X.spike8 = reinterpret_cast<uint8_t*>(f + 9 * per);
-        X.base = n0;
+        X = smem_state(bsm_raw + S->state_off, S->per_cta, 0u, n0);
         state_copy(S, X, n0, n1, true);
     } else {
-        X.v = S->v;
-        X.istim = S->istim;
-        X.er = S->er;
-        X.ed = S->ed;
-        X.ir = S->ir;
-        X.id = S->id;
-        X.tr = S->tr;
-        X.td = S->td;
-        X.refrac = S->refrac;
-        X.spike32 = S->spikes;
-        X.base = 0;
+        X = global_state(S);
     }
-    for (uint32_t i = tid; i < S->n_classes * (sizeof(BClass) / 4u); i += blockDim.x)
-        reinterpret_cast<uint32_t*>(s_cls)[i] = reinterpret_cast<const uint32_t*>(S->cls)[i];
 
     if (tid == 0) {
-        bs.ok = 1u;
-        for (uint32_t s = 0; s < n_stages; ++s) {
-            mbar_init(saddr(&bs.full[s]), 1u);
-            mbar_init(saddr(&bs.empty[s]), 1u);
-        }
-        mbar_init(saddr(&bs.accum), 1u);
-        mbar_init(saddr(&bs.ready[0]), 1u);
-        mbar_init(saddr(&bs.ready[1]), 1u);
-        mbar_init(saddr(&bs.tfree), 4u);
-        fence_mbar_init();
+        batch_init_barriers(bs, n_stages);
         s_bar0 = ld_acquire_u64(S->barrier) / gridDim.x * gridDim.x;
         s_t0 = *S->steps_done;
     }
@@ -542,10 +682,8 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
     const uint32_t tmem = bs.tmem;
     const unsigned long long bar0 = s_bar0, t0 = s_t0;
     const uint32_t n_units = S->n_units;
-    // producer / MMA state (thread 0 only)
-    uint32_t full_ph = 0, empty_ph = 0, accum_ph = 0, tfree_ph = 0;
-    uint32_t empty_pend = 0;  // bit s: stage s holds tiles whose MMAs may still read it
-    uint32_t load_s = 0, use_s = 0, units_issued = 0;
+    ProducerState ps;              // the producer's ring state
+    uint32_t accum_ph = 0;         // the epilogue's accumulator phase
     uint32_t ready_slot = 0, ready_ph = 0;  // the unit ring (producer and epilogue alike)
     const bool producer = tid == 128u;  // warp 4: loads and MMAs; warps 0-3: the epilogue
     bool ok = true;
@@ -557,12 +695,12 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
 #endif
 
     uint16_t* s_nz = reinterpret_cast<uint16_t*>(bsm_raw + S->noise_off);
-    if (S->noise_on) noise_ahead(S, P, s_nz, n0, n1, t0, tid, blockDim.x);
+    if (S->noise_on) noise_ahead(S, P, s_cls, s_nz, n0, n1, t0, tid, blockDim.x);
     __syncthreads();
 
     for (uint32_t k = 0; k < n_steps && ok; ++k) {
         const unsigned long long t = t0 + k;
-        batch_neurons<SMEM_STATE>(S, P, s_cls, X, s_nz, n0, n1, t);
+        batch_neurons<SMEM_STATE>(S, P, s_cls, X, s_nz, n0, n1, t, tid, blockDim.x);
         fence_proxy_async_global();
         __syncthreads();
         BSNN_TMARK(0);
@@ -588,72 +726,15 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
                 ready_slot ^= 1u;
                 if (none) break;
                 const BUnit U = S->units[ui];
-                const BClass& C = s_cls[U.cls];
-                const uint32_t N = 2u * C.NP, b_bytes = N * 128u, nk = U.k1 - U.k0;
                 if (bs.ok == 0u) {  // after a timeout: only release the epilogue
                     tc_commit(saddr(&bs.accum));
-                    ui = take();
-                    continue;
-                }
-                const unsigned char* a_src = reinterpret_cast<const unsigned char*>(C.A[U.side]) +
-                                             (static_cast<size_t>(U.mt) * C.KT[U.side] + U.k0) * kATileBytes;
-                const unsigned char* b_src =
-                    reinterpret_cast<const unsigned char*>(C.X[U.side]) + static_cast<size_t>(U.k0) * b_bytes;
-                bool good = true;
-                // K tile i of the unit into stage load_s, once the MMAs that read the stage last
-                // are done
-                auto load = [&](uint32_t i) {
-                    const uint32_t s = load_s;
-                    if ((empty_pend >> s) & 1u) {
-                        if (!mbar_wait(saddr(&bs.empty[s]), (empty_ph >> s) & 1u)) good = false;
-                        empty_ph ^= 1u << s;
-                        empty_pend &= ~(1u << s);
-                    }
-                    const uint32_t bar = saddr(&bs.full[s]);
-                    const uint32_t dst = smem_base + s * stage_bytes;
-                    mbar_expect_tx(bar, kATileBytes + b_bytes);
-                    bulk_load_keep(dst, a_src + static_cast<size_t>(i) * kATileBytes, kATileBytes, bar, keep);
-                    bulk_load(dst + kATileBytes, b_src + static_cast<size_t>(i) * b_bytes, b_bytes, bar);
-                    load_s = load_s + 1u == n_stages ? 0u : load_s + 1u;
-                };
-                const uint32_t idesc = idesc_bf16_m128(N);
-                uint32_t next = 0;
-                for (; next < nk && next < n_stages; ++next) load(next);
-                // the epilogue of the previous unit has read the accumulator
-                if (units_issued > 0u) {
-                    if (!mbar_wait(saddr(&bs.tfree), tfree_ph & 1u)) good = false;
-                    tfree_ph ^= 1u;
-                }
-                for (uint32_t i = 0; i < nk && good; ++i) {
-                    const uint32_t s = use_s;
-                    if (!mbar_wait(saddr(&bs.full[s]), (full_ph >> s) & 1u)) {
-                        good = false;
-                        break;
-                    }
-                    full_ph ^= 1u << s;
-                    tc_fence_after();
-                    const uint32_t a = smem_base + s * stage_bytes, b = a + kATileBytes;
-#pragma unroll
-                    for (uint32_t ks = 0; ks < 4; ++ks)
-                        tc_mma_bf16(tmem, smem_desc(a + ks * 2u * 2048u, 2048u, 128u),
-                                    smem_desc(b + ks * 2u * (N * 16u), N * 16u, 128u), idesc, (i | ks) != 0u);
-                    tc_commit(saddr(&bs.empty[s]));
-                    empty_pend |= 1u << s;
-                    use_s = use_s + 1u == n_stages ? 0u : use_s + 1u;
-                    // refill the stage of the previous iteration (its MMAs have had an MMA's time to
-                    // finish; load() waits for them)
-                    if (i > 0u && next < nk) load(next++);
-                }
-                tc_commit(saddr(&bs.accum));
-                ++units_issued;
-                if (!good) {
+                } else if (!issue_unit(bs, ps, U, s_cls[U.cls], tmem, smem_base, stage_bytes, n_stages, keep)) {
                     atomicExch(S->error, kErrStageTimeout);
                     bs.ok = 0u;
                 }
                 ui = take();
             }
         } else if (warp < 4) {
-            const uint32_t row = 32u * warp + lane;
             for (;;) {
                 // the unit the producer took (or the end of the step's units)
                 if (!mbar_wait(saddr(&bs.ready[ready_slot]), (ready_ph >> ready_slot) & 1u)) {
@@ -666,29 +747,10 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
                 ready_slot ^= 1u;
                 if (ui == 0xFFFFFFFFu) break;
                 const BUnit U = S->units[ui];
-                const BClass& C = s_cls[U.cls];
-                const bool got = mbar_wait(saddr(&bs.accum), accum_ph & 1u);
-                accum_ph ^= 1u;
-                if (!got) {
-                    atomicExch(S->error, kErrStageTimeout);
-                    bs.ok = 0u;
-                }
-                tc_fence_after();
-                float* part = S->partials + U.part;
-                for (uint32_t c0 = 0; c0 < C.NP; c0 += 16u) {
-                    float hi[16], lo[16];
-                    tmem_ld16(tmem + ((32u * warp) << 16) + c0, hi);
-                    tmem_ld16(tmem + ((32u * warp) << 16) + C.NP + c0, lo);
-#pragma unroll
-                    for (uint32_t q = 0; q < 16; ++q)
-                        if (c0 + q < C.n_inst) part[static_cast<size_t>(c0 + q) * 128u + row] = hi[q] + lo[q];
-                }
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(saddr(&bs.tfree));
+                drain_unit(S, bs, U, s_cls[U.cls], tmem, accum_ph, warp, lane);
             }
         } else if (noise_warp(warp) && S->noise_on && k + 1u < n_steps) {
-            noise_ahead(S, P, s_nz, n0, n1, t + 1ull, 32u * noise_rank(warp) + lane, 32u * kNoiseWarps);
+            noise_ahead(S, P, s_cls, s_nz, n0, n1, t + 1ull, 32u * noise_rank(warp) + lane, 32u * kNoiseWarps);
         }
         __syncthreads();
         ok = bs.ok != 0u;  // the same for every thread of the CTA
@@ -704,6 +766,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
     if (tid == 0)
         for (int i = 0; i < 8; ++i) S->phase_ns[blockIdx.x * 8u + i] += s_tally_[i];
 #endif
+    if (producer && bs.ok == 0u) producer_quiesce(bs, ps, n_stages);
     tc_fence_before();
     __syncthreads();
     if constexpr (SMEM_STATE) state_copy(S, X, n0, n1, false);
@@ -711,9 +774,244 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
     if (blockIdx.x == 0 && tid == 0 && ok) *S->steps_done = t0 + n_steps;
 }
 
+// ---- the flow form -------------------------------------------------------------------------------
+// The same per-neuron arithmetic and the same GEMM units as bsnn_batch_kernel, without grid
+// barriers.  Each size class is a chain of its own (its neurons of step t, then its GEMM units of
+// step t, then its neurons of step t + 1, ...), and the chains of different classes overlap, as
+// do the neuron updates and the GEMMs inside a CTA.  Two monotonically increasing counters per
+// class in global memory carry the dependencies:
+//   nready[c]: +1 when a CTA has stepped its slice of class c (every CTA, every step, an empty
+//              slice too), so the class's neurons of step t are all done at (t + 1) * grid;
+//   udone[c]:  +1 when an epilogue warp has written its 32 posts of a GEMM unit of class c, so
+//              the class's propagation of step t is complete at 4 * (t + 1) * units_of[c].
+// Roles in a CTA:
+//   warps 5-15, the neuron side: per step, per class in processing order (the classes with the
+//     most GEMM work first), draw the Poisson counts of the CTA's slice of the class, wait until
+//     the class's propagation of the previous step is complete, step the slice (its state in
+//     shared memory for the launch, as in the phased form), and count the slice in nready[c];
+//   thread 128, the producer: takes GEMM units from one dispenser over all steps of the launch
+//     (ticket q is unit q mod n_units of step q / n_units; units in class processing order,
+//     longest first within a class), waits until every CTA has stepped the unit's class at that
+//     step, then streams the operands and issues the MMAs as in the phased form;
+//   warps 0-3, the epilogue: drain the accumulator, write the unit's partial sums, and count them
+//     in udone[c].
+// Every role takes its work in one order (step, then class processing order) and every wait is
+// for work earlier in that order, so the earliest unfinished piece of work can always run: with
+// all CTAs resident (a cooperative launch) the chains cannot deadlock.  The write-after-read
+// hazards are covered by the same counters: a class's neurons of step t + 1 (which overwrite its
+// x tiles and read its partial sums) wait for all its units of step t (which read those tiles and
+// wrote those sums), and its units of step t + 1 (which overwrite the sums) wait for all its
+// neurons of step t + 1.  The dispenser ends a launch at exactly (t0 + n_steps) * n_units: each
+// producer's last take is past the end and is given back.
+constexpr uint32_t kFlowNeuronWarp0 = 5;
+constexpr uint32_t kFlowNeuronThreads = kBatchThreads - 32u * kFlowNeuronWarp0;
+
+// One thread: bounded wait until the counter reaches `target` (gpu-scope acquire loads).  Gives up
+// after s_wait_limit_ns, recording kErrBarrierTimeout, or when another CTA has given up.
+__device__ __forceinline__ bool count_wait(const unsigned long long* ctr, int32_t* error, unsigned long long target) {
+    unsigned long long t_start = 0;
+    uint32_t spins = 0;
+    while (static_cast<long long>(ld_acquire_u64(ctr) - target) < 0) {
+        if ((++spins & 63u) == 0u) {
+            const unsigned long long now = globaltimer_ns();
+            if (t_start == 0) {
+                t_start = now;
+            } else if (now - t_start > s_wait_limit_ns) {
+                atomicExch(error, kErrBarrierTimeout);
+                return false;
+            }
+            if (ld_relaxed_s32(error) != kErrNone) return false;
+        }
+    }
+    return true;
+}
+
+// Bounded wait for an mbarrier phase with an explicit limit.
+__device__ __forceinline__ bool mbar_wait_for(uint32_t bar, uint32_t parity, unsigned long long limit_ns) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    while (!mbar_try_wait(bar, parity))
+        if (globaltimer_ns() - t0 > limit_ns) return false;
+    return true;
+}
+
+template <bool SMEM_STATE>
+__global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_flow_kernel(const BSim* __restrict__ S, uint32_t n_steps) {
+    extern __shared__ __align__(1024) unsigned char bsm_raw[];
+    __shared__ BatchSmem bs;
+    __shared__ BClass s_cls[kBatchMaxClasses];
+    __shared__ uint32_t s_order[kBatchMaxClasses];
+    __shared__ uint32_t s_slice[kBatchMaxClasses][3];  // per processing position: first neuron, end, state index
+    __shared__ int s_nok;
+    __shared__ unsigned long long s_t0;
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+    const uint32_t stage_bytes = S->stage_bytes, n_stages = S->n_stages, nc = S->n_classes;
+    const uint32_t smem_base = saddr(bsm_raw);
+    const BInst* P = batch_tables(S, bsm_raw + n_stages * stage_bytes, s_cls);
+    unsigned char* state_raw = bsm_raw + S->state_off;
+    uint16_t* s_nz = reinterpret_cast<uint16_t*>(bsm_raw + S->noise_off);
+    if (tid == 0) {
+        s_wait_limit_ns = S->wait_limit_ns;
+        // the CTA's slice of each class: an even share of the class's contiguous neurons
+        uint32_t soff = 0;
+        for (uint32_t p = 0; p < nc; ++p) {
+            const uint32_t c = S->order[p];
+            const BClass& C = S->cls[c];
+            const uint32_t a = C.nbase + static_cast<uint32_t>((static_cast<unsigned long long>(blockIdx.x) * C.nlen) / gridDim.x);
+            const uint32_t e =
+                C.nbase + static_cast<uint32_t>((static_cast<unsigned long long>(blockIdx.x + 1u) * C.nlen) / gridDim.x);
+            s_order[p] = c;
+            s_slice[p][0] = a;
+            s_slice[p][1] = e;
+            s_slice[p][2] = soff;
+            soff += e - a;
+        }
+        batch_init_barriers(bs, n_stages);
+        s_t0 = *S->steps_done;
+        s_nok = 1;
+    }
+    if (warp == 0) {
+        tmem_alloc(saddr(&bs.tmem), kBatchTmemCols);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if constexpr (SMEM_STATE) {
+        for (uint32_t p = 0; p < nc; ++p)
+            state_copy(S, smem_state(state_raw, S->per_cta, s_slice[p][2], s_slice[p][0]), s_slice[p][0], s_slice[p][1], true);
+    }
+#ifdef BSNN_PHASE_TIMING
+    __shared__ unsigned long long s_tally_[8];
+    if (tid < 8) s_tally_[tid] = 0;
+#endif
+    __syncthreads();
+    const uint32_t tmem = bs.tmem;
+    const unsigned long long t0 = s_t0;
+    const uint32_t n_units = S->n_units;
+
+    if (tid == 128u) {
+        // the producer
+        ProducerState ps;
+        uint32_t ready_slot = 0;
+        const uint64_t keep = l2_evict_last_policy();
+        const unsigned long long end = (t0 + n_steps) * n_units;
+        for (;;) {
+            BSNN_TSTART(t_take_);
+            uint32_t ui = 0xFFFFFFFFu;
+            unsigned long long tq = 0;
+            if (bs.ok != 0u) {
+                const unsigned long long q = atomicAdd(S->unit_ctr, 1ull);
+                if (q >= end) {
+                    atomicAdd(S->unit_ctr, ~0ull);  // the take past the launch's end is given back
+                } else {
+                    tq = q / n_units;
+                    ui = static_cast<uint32_t>(q - tq * n_units);
+                }
+            }
+            BSNN_TSPAN(6, t_take_);
+            if (ui != 0xFFFFFFFFu) {
+                BSNN_TSTART(t_wait_);
+                // every CTA has stepped its slice of the unit's class at step tq
+                if (!count_wait(S->nready + S->units[ui].cls, S->error, (tq + 1ull) * gridDim.x)) {
+                    bs.ok = 0u;
+                    ui = 0xFFFFFFFFu;
+                }
+                BSNN_TSPAN(4, t_wait_);
+            }
+            bs.unit[ready_slot] = ui;
+            mbar_arrive(saddr(&bs.ready[ready_slot]));
+            ready_slot ^= 1u;
+            if (ui == 0xFFFFFFFFu) break;
+            BSNN_TSTART(t_issue_);
+            fence_proxy_async_global();  // x tiles written by generic stores, read by the bulk copies
+            const BUnit U = S->units[ui];
+            if (!issue_unit(bs, ps, U, s_cls[U.cls], tmem, smem_base, stage_bytes, n_stages, keep)) {
+                atomicExch(S->error, kErrStageTimeout);
+                bs.ok = 0u;
+            }
+            BSNN_TSPAN(5, t_issue_);
+        }
+        if (bs.ok == 0u) producer_quiesce(bs, ps, n_stages);
+    } else if (warp < 4) {
+        // the epilogue; its wait for the next unit spans the producer's wait for the unit's class,
+        // so it is bounded by twice the limit
+        uint32_t accum_ph = 0, ready_slot = 0, ready_ph = 0;
+        for (;;) {
+            if (!mbar_wait_for(saddr(&bs.ready[ready_slot]), (ready_ph >> ready_slot) & 1u, 2ull * s_wait_limit_ns)) {
+                atomicExch(S->error, kErrStageTimeout);
+                bs.ok = 0u;
+                break;
+            }
+            ready_ph ^= 1u << ready_slot;
+            const uint32_t ui = bs.unit[ready_slot];
+            ready_slot ^= 1u;
+            if (ui == 0xFFFFFFFFu) break;
+            const BUnit U = S->units[ui];
+            BSNN_TSTART(t_drain_);
+            drain_unit(S, bs, U, s_cls[U.cls], tmem, accum_ph, warp, lane);
+            // each epilogue warp counts its own 32 posts (no barrier across the warps, whose waits
+            // may end differently after a timeout)
+            if (lane == 0) red_release_add_u64(S->udone + U.cls, 1ull);
+            if (tid == 0) BSNN_TSPAN(7, t_drain_);
+        }
+    } else if (warp >= kFlowNeuronWarp0) {
+        // the neuron side
+        const uint32_t me = tid - 32u * kFlowNeuronWarp0;
+        bool nok = true;
+        for (uint32_t k = 0; k < n_steps && nok; ++k) {
+            const unsigned long long t = t0 + k;
+            for (uint32_t p = 0; p < nc; ++p) {
+                const uint32_t c = s_order[p];
+                const uint32_t s0 = s_slice[p][0], s1 = s_slice[p][1], soff = s_slice[p][2];
+                BSNN_TSTART(t_noise_);
+                // the slice's Poisson counts of step t (they need no propagation: drawn while the
+                // class's GEMM of the previous step may still run)
+                if (S->noise_on) noise_ahead(S, P, s_cls, s_nz + soff, s0, s1, t, me, kFlowNeuronThreads);
+                if (me == 0) {
+                    BSNN_TSPAN(0, t_noise_);
+                    BSNN_TSTART(t_wait_);
+                    // the class's propagation of step t - 1 is complete (4 counts per unit)
+                    s_nok = count_wait(S->udone + c, S->error, 4ull * t * S->units_of[c]) ? 1 : 0;
+                    BSNN_TSPAN(1, t_wait_);
+                }
+                named_barrier_sync(2, kFlowNeuronThreads);
+                if (s_nok == 0) {
+                    nok = false;
+                    break;
+                }
+                BSNN_TSTART(t_nrn_);
+                BState X;
+                if constexpr (SMEM_STATE) X = smem_state(state_raw, S->per_cta, soff, s0);
+                else X = global_state(S);
+                batch_neurons<SMEM_STATE>(S, P, s_cls, X, s_nz + soff, s0, s1, t, me, kFlowNeuronThreads);
+                fence_proxy_async_global();
+                named_barrier_sync(2, kFlowNeuronThreads);
+                if (me == 0) {
+                    red_release_add_u64(S->nready + c, 1ull);
+                    BSNN_TSPAN(2, t_nrn_);
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+#ifdef BSNN_PHASE_TIMING
+    if (tid == 0)
+        for (int i = 0; i < 8; ++i) S->phase_ns[blockIdx.x * 8u + i] += s_tally_[i];
+#endif
+    if constexpr (SMEM_STATE) {
+        for (uint32_t p = 0; p < nc; ++p)
+            state_copy(S, smem_state(state_raw, S->per_cta, s_slice[p][2], s_slice[p][0]), s_slice[p][0], s_slice[p][1], false);
+    }
+    if (warp == 0) tmem_dealloc(tmem, kBatchTmemCols);
+    if (blockIdx.x == 0 && tid == 0 && ld_relaxed_s32(S->error) == kErrNone) *S->steps_done = t0 + n_steps;
+}
+
 // g of one instance's neurons: the background conductance (d - r) * scale of the background
 // traces, plus, with `pending`, the propagation still pending in the partial sums (the value the
-// reference holds after step_the_clock).  Reads only.
+// reference holds after step_the_clock).  Reads only.  `instance` is the instance's position in the
+// device's instance table.
 __global__ void bsnn_batch_g_kernel(const BSim* __restrict__ S, uint32_t instance, int with_pending, float* out_ge,
                                     float* out_gi) {
     const BInst& B = S->inst[instance];

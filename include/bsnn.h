@@ -458,6 +458,7 @@ typedef struct bsnn_batch_info {
     uint64_t smem_bytes;
     uint32_t state_in_smem;    /* 1: each CTA's neuron state stays in shared memory      */
     uint32_t operand_stages;   /* shared-memory operand stages of the GEMM ring           */
+    int32_t form;              /* BSNN_BATCH_FORM_*                                       */
 } bsnn_batch_info;
 
 BSNN_API bsnn_status bsnn_batch_create(int32_t device, bsnn_batch** out_batch);
@@ -481,6 +482,13 @@ BSNN_API bsnn_status bsnn_batch_add_instance(bsnn_batch* batch, uint32_t class_i
                                              uint32_t num_events, uint32_t* out_instance);
 BSNN_API bsnn_status bsnn_batch_set_noise(bsnn_batch* batch, int32_t on);
 BSNN_API bsnn_status bsnn_batch_set_steps_per_launch(bsnn_batch* batch, uint32_t steps);
+/* How the kernel orders a clock step's work (before the first step; results are bit-identical):
+ * FLOW runs each size class as its own chain, its GEMM units starting when its neurons are
+ * stepped and its neurons when its units are done, neuron updates and GEMMs overlapping inside a
+ * CTA; PHASED steps all neurons, then runs all GEMM units, with a grid barrier after each. */
+#define BSNN_BATCH_FORM_FLOW 0
+#define BSNN_BATCH_FORM_PHASED 1
+BSNN_API bsnn_status bsnn_batch_set_form(bsnn_batch* batch, int32_t form);
 /* Bound of the batch kernel's device-side waits (default 2 s; 1 us .. 60 s), as
  * bsnn_set_device_wait_limit. */
 BSNN_API bsnn_status bsnn_batch_set_device_wait_limit(bsnn_batch* batch, uint64_t nanoseconds);

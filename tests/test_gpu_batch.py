@@ -157,6 +157,38 @@ def test_batch_placements_are_bit_exact(env):
     b.close()
 
 
+@pytest.mark.parametrize("env", [{}, {"BSNN_BATCH_STATE": "global"}, {"BSNN_BATCH_STAGES": "2"}])
+def test_batch_forms_are_bit_exact(env):
+    """The flow form (each size class its own chain of neuron updates and GEMM units, no grid
+    barriers) and the phased form do the same arithmetic in another order of work: states and
+    spike counts are identical, over launches that end in the middle of the classes' chains."""
+    spec = bsnn.config4_batch(n_instances=9, steps=200, seed=10, sizes=(400, 900, 1600), stim_window=(10, 150))
+    assert len({i.cls for i in spec.instances}) == 3
+    a = bsnn.BatchSimulation(spec, form="phased")
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
+    try:
+        b = bsnn.BatchSimulation(spec, form="flow")
+        ib = b.info()
+    finally:
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    assert a.info().form == 1 and ib.form == 0
+    for sim, per in ((a, 150), (b, 23)):
+        sim.set_steps_per_launch(per)
+        sim.run(150)
+    for k in range(len(spec.instances)):
+        for f in FIELDS + ["spikes", "refractory_counter"]:
+            np.testing.assert_array_equal(a.read(k, f), b.read(k, f), err_msg=f"instance {k} {f}")
+    np.testing.assert_array_equal(a.spike_counts(), b.spike_counts())
+    assert b.spike_counts().sum() > 0
+    a.close()
+    b.close()
+
+
 def test_batch_rate_error_over_a_simulated_second():
     """10,000 clock steps (1 simulated second) of four instances against the FP64 oracle on the same
     BF16-valued weights: the aggregate spike count of the populations is within 1e-3 relative,
