@@ -723,13 +723,15 @@ def form_batched(args, dev):
 
 
 ADJOINT_WORKLOADS = {"config5_adjoint_3125": 2000}
+ADJOINT_CHECKPOINT = 2000  # one segment: the whole tape in HBM, no recomputation
 
 
 def run_adjoint(args, rank, world, K=None, W=None):
     """The differentiation form: one bench step is one gradient of the rate loss with respect to
-    W_EE and g_leak (forward pass over 2,000 clock steps with checkpoints every 100, then the
-    checkpointed backward pass) on the example network (2,500 E + 625 I, plasticity off), the
-    target rate trace made by the same network with perturbed W_EE."""
+    W_EE and g_leak (forward pass over 2,000 clock steps, then the backward pass) on the example
+    network (2,500 E + 625 I, plasticity off), the target rate trace made by the same network with
+    perturbed W_EE.  One checkpoint segment: the forward pass keeps the whole run's tape in HBM
+    (about 160 MB), so the backward pass recomputes nothing."""
     import torch
 
     import bsnn
@@ -739,7 +741,8 @@ def run_adjoint(args, rank, world, K=None, W=None):
     K = args.steps if K is None else K
     W = args.warmup if W is None else W
     spec, w_target = bsnn.config5_network(steps=T, seed=11 + rank)
-    net = bsnn.AdjointNetwork(spec, T, checkpoint=100, noise=True, beta=0.5e-3, rate_weight=1.0, device=dev)
+    net = bsnn.AdjointNetwork(spec, T, checkpoint=ADJOINT_CHECKPOINT, noise=True, beta=0.5e-3, rate_weight=1.0,
+                              device=dev)
     net.set_params(w_target, None)
     _, target, _ = net.forward(np.zeros(T, np.float32))
     net.set_params(spec.conns[0].weights, None)
@@ -781,7 +784,7 @@ def run_adjoint(args, rank, world, K=None, W=None):
         "ms_per_step": t_ms / K, "ms_per_gradient": t_ms / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded; reference example shapes, uniform[0, max_weight] weights)",
-        "config": {"workload": "config5_adjoint_3125", "neurons": N, "clock_steps": T, "checkpoint_interval": 100,
+        "config": {"workload": "config5_adjoint_3125", "neurons": N, "clock_steps": T, "checkpoint_interval": ADJOINT_CHECKPOINT,
                    "dt_s": DT, "plasticity": "off", "loss": "MSE of the 5 ms-smoothed E rate vs a target trace",
                    "surrogate": "fast sigmoid, beta 0.5 mV", "parallelism": f"replicas x{world}",
                    "l2": "W (39 MB) is L2-resident by design; no flush"},

@@ -7,7 +7,10 @@
 // with rho_t = a rho_{t-1} + (1 - a) n_E(t) / (N_E dt), a = exp(-dt / rate_tau) (the smoothed
 // excitatory population rate) and vbar the mean excitatory membrane potential after the step.
 // bsnn_adjoint_backward replays each segment from its checkpoint and propagates the adjoints back
-// (adjoint_kernel.cuh), returning dL/dW_EE and dL/dg_leak (one g_leak shared by both groups).
+// (adjoint_kernel.cuh), returning dL/dW_EE and dL/dg_leak (one g_leak shared by both groups).  The
+// forward pass runs its last segment the way the backward pass replays it (from the restored
+// checkpoint, keeping the tape), so the backward pass starts on that tape without a replay; with
+// one segment (checkpoint interval >= num_steps) nothing is recomputed.
 #pragma once
 
 #include "adjoint_kernel.cuh"
@@ -35,7 +38,10 @@ struct bsnn_adjoint {
     // one captured graph per checkpoint segment for each pass (captured on first use, dropped when
     // g_leak changes, since the group parameters are kernel arguments)
     std::vector<cudaGraphExec_t> fwd_graphs, bwd_graphs;
+    cudaGraphExec_t replay_graph = nullptr;    // the last segment's replay, when its tape is stale
+    bool tape_last = false;                    // the tape holds the last segment of the last forward pass
     std::vector<size_t> fwd_nodes, bwd_nodes;  // kernels per graph
+    size_t replay_nodes = 0;
     uint64_t launches = 0;                     // kernels run (graph nodes included)
     // forward results
     std::vector<double> rho, vbar;
@@ -48,6 +54,8 @@ struct bsnn_adjoint {
             if (g) cudaGraphExecDestroy(g);
         for (auto g : bwd_graphs)
             if (g) cudaGraphExecDestroy(g);
+        if (replay_graph) cudaGraphExecDestroy(replay_graph);
+        replay_graph = nullptr;
         fwd_graphs.clear();
         bwd_graphs.clear();
     }
@@ -116,27 +124,41 @@ void adj_step(bsnn_adjoint* a, uint32_t t, size_t tape_row, bool tape, float* x_
     bsnn_adj_propagate<<<pg, kAdjBlock, 0, a->stream>>>(a->WE, a->WI, a->h.E, a->h.I, N, a->ld, x_next, a->part);
 }
 
-// Forward segment c: save the checkpoint, then run its steps.
+// The last segment's steps from its restored checkpoint, keeping the tape (x_t in tape row k of
+// tx, x_{t+1} in row k + 1); `forward` adds the forward pass's per-step outputs.  Restoring the
+// checkpoint just saved changes no bit: the saved g is g_base plus the chunk sums, restored as
+// g_base with zero chunks.
+void adj_tape_segment(bsnn_adjoint* a, uint32_t c, bool forward) {
+    const uint32_t T = a->d.num_steps, C = a->d.checkpoint_interval, N = a->h.N;
+    const uint32_t t0 = c * C, t1 = std::min(T, t0 + C);
+    const float* slot = a->ckpt + static_cast<size_t>(c) * kAdjCkptArrays * N;
+    bsnn_adj_restore<<<a->nb, kAdjBlock, 0, a->stream>>>(a->h, a->part, a->tx, slot);
+    for (uint32_t k = 0; k < t1 - t0; ++k) {
+        const size_t o = static_cast<size_t>(k) * N;
+        adj_step(a, t0 + k, o, true, a->tx + o + N, forward);
+    }
+}
+
+// Forward segment c: save the checkpoint, then run its steps (the last one keeping the tape).
 void adj_forward_segment(bsnn_adjoint* a, uint32_t c) {
     const uint32_t T = a->d.num_steps, C = a->d.checkpoint_interval;
     const uint32_t t0 = c * C, t1 = std::min(T, t0 + C);
     float* slot = a->ckpt + static_cast<size_t>(c) * kAdjCkptArrays * a->h.N;
     bsnn_adj_save<<<a->nb, kAdjBlock, 0, a->stream>>>(a->h, a->part, a->x_cur, slot);
+    if (c + 1 == a->n_ckpt) {
+        adj_tape_segment(a, c, true);
+        return;
+    }
     for (uint32_t t = t0; t < t1; ++t) adj_step(a, t, 0, false, a->x_cur, true);
 }
 
-// Backward segment c: restore its checkpoint, replay its steps keeping the tape, then walk them
-// backwards (neuron adjoints, pull-back of the g adjoints through the weights), then add the
-// segment's x_t lambda_ge(t)^T to dW_EE.
+// Backward segment c: restore its checkpoint and replay its steps keeping the tape (the last
+// segment's tape is the forward pass's), then walk them backwards (neuron adjoints, pull-back of
+// the g adjoints through the weights), then add the segment's x_t lambda_ge(t)^T to dW_EE.
 void adj_backward_segment(bsnn_adjoint* a, uint32_t c) {
     const uint32_t T = a->d.num_steps, C = a->d.checkpoint_interval, N = a->h.N, E = a->h.E;
     const uint32_t t0 = c * C, t1 = std::min(T, t0 + C), steps = t1 - t0;
-    const float* slot = a->ckpt + static_cast<size_t>(c) * kAdjCkptArrays * N;
-    bsnn_adj_restore<<<a->nb, kAdjBlock, 0, a->stream>>>(a->h, a->part, a->tx, slot);
-    for (uint32_t k = 0; k < steps; ++k) {
-        const size_t o = static_cast<size_t>(k) * N;
-        adj_step(a, t0 + k, o, true, a->tx + o + N, false);
-    }
+    if (c + 1 != a->n_ckpt) adj_tape_segment(a, c, false);
     const float beta = a->d.surrogate_beta;
     for (uint32_t k = steps; k-- > 0;) {
         const size_t o = static_cast<size_t>(k) * N;
@@ -256,9 +278,10 @@ BSNN_API bsnn_status bsnn_adjoint_create(const bsnn_adjoint_desc* desc, const bs
         const size_t o_cs = A.take(4ull * T), o_cv = A.take(4ull * T);
         const size_t o_we = A.take(4ull * E * ld), o_wi = A.take(4ull * I * ld);
         const size_t o_part = A.take(4ull * 2 * kAdjChunks * N), o_x = A.take(fN);
-        const size_t o_tv = A.take(fN * C), o_tu = A.take(fN * C), o_tge = A.take(fN * C), o_tgi = A.take(fN * C);
-        const size_t o_tx = A.take(fN * (C + 1)), o_lge = A.take(4ull * ld * C);
-        const size_t o_ts = A.take(static_cast<size_t>(N) * C), o_tref = A.take(static_cast<size_t>(N) * C);
+        const size_t Ct = std::min(C, T);  // tape rows: one segment's steps
+        const size_t o_tv = A.take(fN * Ct), o_tu = A.take(fN * Ct), o_tge = A.take(fN * Ct), o_tgi = A.take(fN * Ct);
+        const size_t o_tx = A.take(fN * (Ct + 1)), o_lge = A.take(4ull * ld * Ct);
+        const size_t o_ts = A.take(static_cast<size_t>(N) * Ct), o_tref = A.take(static_cast<size_t>(N) * Ct);
         const size_t o_lv = A.take(fN), o_ld = A.take(fN), o_lr = A.take(fN), o_lx = A.take(fN), o_lgi = A.take(4ull * ld);
         const size_t o_dw = A.take(4ull * E * E);
         const size_t o_gl = A.take(8ull * a->nb);
@@ -385,6 +408,7 @@ BSNN_API bsnn_status bsnn_adjoint_forward(bsnn_adjoint* a, const float* rate_tar
         a->launches += 1;
         adj_run_graphs(a, a->fwd_graphs, a->fwd_nodes, false, [&](uint32_t c) { adj_forward_segment(a, c); },
                        "adjoint forward");
+        a->tape_last = true;
         std::vector<uint32_t> cnt(T);
         std::vector<double> vs(static_cast<size_t>(T) * a->nb);
         cuda_check(cudaMemcpyAsync(cnt.data(), a->counts, 4ull * T, cudaMemcpyDeviceToHost, a->stream), "D2H counts");
@@ -435,8 +459,26 @@ BSNN_API bsnn_status bsnn_adjoint_backward(bsnn_adjoint* a, float* grad_w_ee, do
             cuda_check(cudaMemsetAsync(p, 0, fN, a->stream), "memset adjoints");
         cuda_check(cudaMemsetAsync(a->dW, 0, 4ull * E * E, a->stream), "memset dW");
         cuda_check(cudaMemsetAsync(a->gl_acc, 0, 8ull * a->nb, a->stream), "memset g_leak");
+        if (!a->tape_last) {  // an earlier backward pass replayed other segments over the tape
+            if (!a->replay_graph) {
+                cudaGraph_t g = nullptr;
+                cuda_check(cudaStreamBeginCapture(a->stream, cudaStreamCaptureModeThreadLocal), "adjoint replay");
+                adj_tape_segment(a, a->n_ckpt - 1, false);
+                const cudaError_t launch_err = cudaGetLastError();
+                cuda_check(cudaStreamEndCapture(a->stream, &g), "adjoint replay");
+                cuda_check(launch_err, "adjoint replay");
+                cudaGraphGetNodes(g, nullptr, &a->replay_nodes);
+                const cudaError_t ie = cudaGraphInstantiate(&a->replay_graph, g, 0);
+                cudaGraphDestroy(g);
+                cuda_check(ie, "adjoint replay");
+            }
+            cuda_check(cudaGraphLaunch(a->replay_graph, a->stream), "adjoint replay");
+            a->launches += a->replay_nodes;
+            a->tape_last = true;
+        }
         adj_run_graphs(a, a->bwd_graphs, a->bwd_nodes, true, [&](uint32_t c) { adj_backward_segment(a, c); },
                        "adjoint backward");
+        if (a->n_ckpt > 1) a->tape_last = false;
         std::vector<double> gl(a->nb);
         cuda_check(cudaMemcpyAsync(gl.data(), a->gl_acc, 8ull * a->nb, cudaMemcpyDeviceToHost, a->stream), "D2H g_leak");
         if (grad_w_ee)

@@ -806,12 +806,20 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
 constexpr uint32_t kFlowNeuronWarp0 = 5;
 constexpr uint32_t kFlowNeuronThreads = kBatchThreads - 32u * kFlowNeuronWarp0;
 
-// One thread: bounded wait until the counter reaches `target` (gpu-scope acquire loads).  Gives up
-// after s_wait_limit_ns, recording kErrBarrierTimeout, or when another CTA has given up.
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// One thread: bounded wait until the counter reaches `target`.  It polls with gpu-scope relaxed
+// loads and makes one acquire load once the target is reached: these waits run beside the other
+// roles' work, and an acquire load per poll would keep invalidating the SM's L1 under them.  Gives
+// up after s_wait_limit_ns, recording kErrBarrierTimeout, or when another CTA has given up.
 __device__ __forceinline__ bool count_wait(const unsigned long long* ctr, int32_t* error, unsigned long long target) {
     unsigned long long t_start = 0;
     uint32_t spins = 0;
-    while (static_cast<long long>(ld_acquire_u64(ctr) - target) < 0) {
+    while (static_cast<long long>(ld_relaxed_u64(ctr) - target) < 0) {
         if ((++spins & 63u) == 0u) {
             const unsigned long long now = globaltimer_ns();
             if (t_start == 0) {
@@ -823,6 +831,7 @@ __device__ __forceinline__ bool count_wait(const unsigned long long* ctr, int32_
             if (ld_relaxed_s32(error) != kErrNone) return false;
         }
     }
+    ld_acquire_u64(ctr);  // orders this thread's later reads after the counted work
     return true;
 }
 

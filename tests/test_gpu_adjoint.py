@@ -138,6 +138,21 @@ def test_surrogate_rate_gradient_matches_fp64_and_checkpoints():
         assert abs(dgl - grads[0][1]) <= 1e-5 * abs(grads[0][1])
 
 
+@pytest.mark.parametrize("ckpt", [64, T])
+def test_backward_twice_gives_the_same_gradient(ckpt):
+    """The forward pass leaves the last segment's tape for the backward pass; a second backward
+    pass of the same forward pass (after the first replayed the other segments over that tape)
+    replays it again and gives the same bits."""
+    spec = network(4)
+    net = bsnn.AdjointNetwork(spec, T, checkpoint=ckpt, noise=True, beta=0.5e-3, rate_weight=1.0, voltage_weight=1e3)
+    net.forward(RT, VT)
+    dW1, dgl1 = net.backward()
+    dW2, dgl2 = net.backward()
+    np.testing.assert_array_equal(dW1, dW2)
+    assert dgl1 == dgl2
+    net.close()
+
+
 def test_set_params_and_errors():
     spec = network(4)
     net = bsnn.AdjointNetwork(spec, T, checkpoint=50, noise=False, beta=0.5e-3, voltage_weight=1e3)
