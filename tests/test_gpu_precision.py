@@ -14,13 +14,19 @@ scales).
 """
 from __future__ import annotations
 
+import sys
+from pathlib import Path
+
 import numpy as np
 import pytest
 import torch
 
 import bsnn
 import oracle
-from conftest import FLOAT_FIELDS, compare_state, make_pair
+from conftest import FLOAT_FIELDS, ROOT, compare_state, make_pair
+
+sys.path.insert(0, str(ROOT / "tests" / "golden"))
+from specs import spec_digest  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
@@ -193,20 +199,68 @@ def test_precision_forms_against_fp64():
 
 
 # The precision form's own configuration: 8,100 E + 2,025 I (~102 M synapse entries, rows of 8,100
-# weights, so the normalisation sums and the FP8 row scales act on rows 20x longer than above), 600
-# steps (the FP64 oracle takes ~0.1 s per step on the host).  The network is nearly silent in
-# these steps (background drive only), so the rate error rests on few spikes; the voltage error
-# and the weight drift are the sharper measures.  Bounds as above: about twice the measured values.
-LARGE_STEPS = 600
+# weights, so the normalisation sums and the FP8 row scales act on rows 20x longer than above), seed
+# 751, against an FP64 oracle run of the same network, seed and Poisson draws recorded once on the
+# host (tests/golden/make_fp64_large.py; ~0.1 s per step): the voltages after steps 20, 100 and
+# 1,000, the spikes of each population per 1,000-step bin, and a fixed random sample of 200,000
+# weights of each plastic matrix after the last step.
+LARGE_FIXTURE = Path(__file__).resolve().parent / "golden" / "fp64_large_plastic_10125.npz"
+# Bounds per form: (voltage error after step 20 relative to the largest |v|, the larger relative
+# spike-count error of the two populations over the run, the larger plastic-weight drift
+# mean |w - w64| / mean |w64| over the sample): about twice the values measured on B200.
 LARGE_BOUNDS = {"f32": (1e-6, 0.5, 5e-2), "f32_rowscaled": (1e-6, 0.5, 5e-2), "bf16": (1e-2, 0.5, 0.1),
                 "fp8_e4m3": (5e-2, 0.5, 0.25)}
 
 
+def _large_form_run(spec, ref, form):
+    """The form's voltages at the fixture's steps, its spikes per 1,000-step bin and its weights at
+    the fixture's sample indices, stepping in the same stretches as the FP64 recording."""
+    T = int(ref["steps"])
+    v_steps = [int(x) for x in ref["v_steps"]]
+    g = bsnn.Simulation(spec.num_excitatory, spec.num_inhibitory, **spec.sim_kwargs())
+    spec.build(g)
+    if form != "f32":
+        g.set_weight_format(form)
+    v, bins, done = [], [], 0
+    while done < T:
+        n = min(1000 - done % 1000, T - done)
+        for vs in v_steps:
+            if done < vs <= done + n:
+                g.run(done, vs - done)
+                v.append(g.read("membrane_potentials").astype(np.float64))
+                n -= vs - done
+                done = vs
+        if n > 0:
+            g.run(done, n)
+            done += n
+        if done % 1000 == 0 or done == T:
+            filled = (done - 1) % 1000 + 1
+            bins.append([int(g.read_spike_history(m)[:, :filled].sum()) for m in (0, 1)])
+    w = {c: g.read_weights(c).astype(np.float64).ravel()[ref[f"w_index_{c}"]] for c in sorted({p.conn for p in spec.plasts})}
+    g.close()
+    return np.array(v), np.array(bins, np.int64), w
+
+
 def test_precision_forms_against_fp64_at_the_large_size():
-    spec = bsnn.synthetic_network("large_plastic_10125", steps=LARGE_STEPS + 1, weight_values="uniform",
-                                  recording_interval_steps=LARGE_STEPS)
-    results, n_ref = _errors_vs_fp64(spec, LARGE_STEPS, list(LARGE_BOUNDS))
-    print("FP64 spikes", n_ref)
+    ref = np.load(LARGE_FIXTURE)
+    T = int(ref["steps"])
+    spec = bsnn.synthetic_network("large_plastic_10125", steps=T + 1, weight_values="uniform",
+                                  recording_interval_steps=1000, seed=751)
+    assert spec_digest(spec) == str(ref["digest"]), "the large network's inputs differ from the recorded run's"
+    v_ref, bins_ref = ref["v"], ref["spikes_per_bin"]
+    n_ref = bins_ref.sum(axis=0)
+    print(f"FP64 {T} steps: E {n_ref[0]}, I {n_ref[1]} spikes")
+    results = {}
+    for form in LARGE_BOUNDS:
+        v, bins, w = _large_form_run(spec, ref, form)
+        ev = [float(np.max(np.abs(v[k] - v_ref[k]))) / float(np.max(np.abs(v_ref[k]))) for k in range(len(v_ref))]
+        n = bins.sum(axis=0)
+        er = max(abs(int(n[m]) - int(n_ref[m])) / max(int(n_ref[m]), 1) for m in (0, 1))
+        ew = max(float(np.mean(np.abs(w[c] - ref[f"w_sample_{c}"]))) / float(ref[f"w_abs_mean_{c}"]) for c in w)
+        results[form] = (ev[0], er, ew)
+        print(f"large_plastic_10125 {form:>14}: voltage err after steps {list(ref['v_steps'])}: "
+              f"{', '.join(f'{e:.2e}' for e in ev)}; rate err {er:.3e} (E {n[0]} vs {n_ref[0]}, I {n[1]} vs "
+              f"{n_ref[1]}); weight drift {ew:.2e}")
     _check_bounds(results, LARGE_BOUNDS)
 
 
