@@ -26,10 +26,16 @@ struct bsnn_adjoint {
     float *WE = nullptr, *WI = nullptr, *part = nullptr, *x_cur = nullptr;
     float *tv = nullptr, *tu = nullptr, *tge = nullptr, *tgi = nullptr, *tx = nullptr, *lge_all = nullptr;
     uint8_t *ts = nullptr, *tref = nullptr;
-    float *lam_v = nullptr, *lam_d = nullptr, *lam_r = nullptr, *lam_x = nullptr, *lam_gi = nullptr;
+    float *lam_v = nullptr, *lam_d = nullptr, *lam_r = nullptr, *lam_x = nullptr;
+    float* lam_gi = nullptr;      // [2][ld] lambda_gi by step parity
+    // the persistent backward kernel: CTAs, neurons per CTA at most, shared memory, grid barrier
+    uint32_t bwd_grid = 0, bwd_max_own = 0, bwd_res = 0;  // CTAs, own neurons at most, rows of W in smem
+    size_t bwd_smem = 0;
+    unsigned long long* barrier = nullptr;
+    int32_t* error = nullptr;
     float *c_s = nullptr, *c_v = nullptr;  // [T] loss sensitivities, uploaded before the backward pass
     float* dW = nullptr;
-    double* gl_acc = nullptr;
+    double* gl_acc = nullptr;     // [bwd_grid] per-CTA g_leak shares
     double* vsum = nullptr;       // [T][nb] per-block sums of the E voltages after each step
     uint32_t* counts = nullptr;   // [T] E spikes per step
     float* ckpt = nullptr;        // [n_ckpt][kAdjCkptArrays][N]
@@ -153,23 +159,49 @@ void adj_forward_segment(bsnn_adjoint* a, uint32_t c) {
 }
 
 // Backward segment c: restore its checkpoint and replay its steps keeping the tape (the last
-// segment's tape is the forward pass's), then walk them backwards (neuron adjoints, pull-back of
-// the g adjoints through the weights), then add the segment's x_t lambda_ge(t)^T to dW_EE.
+// segment's tape is the forward pass's), then walk them backwards in one persistent launch
+// (bsnn_adj_backward_kernel: neuron adjoints, pull-back of the g adjoints through the weights),
+// then add the segment's x_t lambda_ge(t)^T to dW_EE.
 void adj_backward_segment(bsnn_adjoint* a, uint32_t c) {
     const uint32_t T = a->d.num_steps, C = a->d.checkpoint_interval, N = a->h.N, E = a->h.E;
     const uint32_t t0 = c * C, t1 = std::min(T, t0 + C), steps = t1 - t0;
     if (c + 1 != a->n_ckpt) adj_tape_segment(a, c, false);
-    const float beta = a->d.surrogate_beta;
-    for (uint32_t k = steps; k-- > 0;) {
-        const size_t o = static_cast<size_t>(k) * N;
-        float* lge = a->lge_all + static_cast<size_t>(k) * a->ld;
-        bsnn_adj_neuron_bwd<<<a->nb, kAdjBlock, 0, a->stream>>>(
-            a->h, a->tv + o, a->tu + o, a->tge + o, a->tgi + o, a->ts + o, a->tref + o, a->lam_v, a->lam_d, a->lam_r,
-            a->lam_x, a->c_s + t0 + k, a->c_v + t0 + k, beta, lge, a->lam_gi, a->gl_acc);
-        // lambda_x(t) = W lambda_g(t), used by step t - 1
-        bsnn_adj_pullback<<<(N * 32 + 255) / 256, 256, 0, a->stream>>>(a->WE, a->WI, E, N, a->ld, lge, a->lam_gi,
-                                                                       a->lam_x);
-    }
+    AdjBwd B{};
+    B.tv = a->tv;
+    B.tu = a->tu;
+    B.tge = a->tge;
+    B.tgi = a->tgi;
+    B.ts = a->ts;
+    B.tref = a->tref;
+    B.lam_v = a->lam_v;
+    B.lam_d = a->lam_d;
+    B.lam_r = a->lam_r;
+    B.lam_x = a->lam_x;
+    B.c_s = a->c_s;
+    B.c_v = a->c_v;
+    B.lge_all = a->lge_all;
+    B.lgi2 = a->lam_gi;
+    B.gl_acc = a->gl_acc;
+    B.barrier = a->barrier;
+    B.error = a->error;
+    B.wait_limit_ns = kDefaultWaitLimitNs;
+    B.t0 = t0;
+    B.steps = steps;
+    B.ld = a->ld;
+    B.max_own = a->bwd_max_own;
+    B.n_res = a->bwd_res;
+    B.beta = a->d.surrogate_beta;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(a->bwd_grid);
+    cfg.blockDim = dim3(kAdjBwdThreads);
+    cfg.dynamicSmemBytes = a->bwd_smem;
+    cfg.stream = a->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cuda_check(cudaLaunchKernelEx(&cfg, bsnn_adj_backward_kernel, a->h, B), "adjoint backward launch");
     const dim3 og((E + 31) / 32, (E + 31) / 32);
     bsnn_adj_outer<<<og, 256, 0, a->stream>>>(a->tx, N, a->lge_all, a->ld, steps, E, a->dW);
 }
@@ -282,9 +314,32 @@ BSNN_API bsnn_status bsnn_adjoint_create(const bsnn_adjoint_desc* desc, const bs
         const size_t o_tv = A.take(fN * Ct), o_tu = A.take(fN * Ct), o_tge = A.take(fN * Ct), o_tgi = A.take(fN * Ct);
         const size_t o_tx = A.take(fN * (Ct + 1)), o_lge = A.take(4ull * ld * Ct);
         const size_t o_ts = A.take(static_cast<size_t>(N) * Ct), o_tref = A.take(static_cast<size_t>(N) * Ct);
-        const size_t o_lv = A.take(fN), o_ld = A.take(fN), o_lr = A.take(fN), o_lx = A.take(fN), o_lgi = A.take(4ull * ld);
+        const size_t o_lv = A.take(fN), o_ld = A.take(fN), o_lr = A.take(fN), o_lx = A.take(fN),
+                     o_lgi = A.take(4ull * 2 * ld);
         const size_t o_dw = A.take(4ull * E * E);
-        const size_t o_gl = A.take(8ull * a->nb);
+        // the persistent backward kernel: one CTA per SM, at least 8 neurons each
+        int sms = 0, optin = 0;
+        cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
+        cuda_check(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device), "smem attr");
+        a->bwd_grid = std::max<uint32_t>(1u, std::min<uint32_t>(static_cast<uint32_t>(sms), (N + 7u) / 8u));
+        a->bwd_max_own = (N + a->bwd_grid - 1) / a->bwd_grid;
+        // lambda_g vectors, own state and row pieces, then as many own rows of W as fit
+        const size_t fixed = sizeof(float) * (2ull * ld + ((4ull * a->bwd_max_own + kPbChunks * a->bwd_max_own + 3u) & ~3ull));
+        require(fixed + 2048 <= static_cast<size_t>(optin), BSNN_ERR_INVALID_ARGUMENT,
+                "network too large for the adjoint's shared-memory lambda_g vectors");
+        const size_t room = static_cast<size_t>(optin) - 2048 - fixed;
+        a->bwd_res = static_cast<uint32_t>(std::min<size_t>(a->bwd_max_own, room / (sizeof(float) * ld)));
+        a->bwd_smem = fixed + sizeof(float) * ld * a->bwd_res;
+        cuda_check(cudaFuncSetAttribute(bsnn_adj_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(a->bwd_smem)),
+                   "adjoint backward smem");
+        int per_sm = 0;
+        cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bsnn_adj_backward_kernel, kAdjBwdThreads,
+                                                                 a->bwd_smem),
+                   "adjoint backward occupancy");
+        require(per_sm >= 1, BSNN_ERR_RUNTIME, "adjoint backward kernel does not fit on an SM");
+        const size_t o_gl = A.take(8ull * a->bwd_grid);
+        const size_t o_bar = A.take(sizeof(unsigned long long)), o_err = A.take(sizeof(int32_t));
         const size_t o_vs = A.take(8ull * a->nb * T);
         const size_t o_cnt = A.take(4ull * T);
         const size_t o_ck = A.take(fN * kAdjCkptArrays * a->n_ckpt);
@@ -320,6 +375,8 @@ BSNN_API bsnn_status bsnn_adjoint_create(const bsnn_adjoint_desc* desc, const bs
         a->lam_gi = F(o_lgi);
         a->dW = F(o_dw);
         a->gl_acc = reinterpret_cast<double*>(base + o_gl);
+        a->barrier = reinterpret_cast<unsigned long long*>(base + o_bar);
+        a->error = reinterpret_cast<int32_t*>(base + o_err);
         a->vsum = reinterpret_cast<double*>(base + o_vs);
         a->counts = reinterpret_cast<uint32_t*>(base + o_cnt);
         a->ckpt = F(o_ck);
@@ -458,7 +515,7 @@ BSNN_API bsnn_status bsnn_adjoint_backward(bsnn_adjoint* a, float* grad_w_ee, do
         for (float* p : {a->lam_v, a->lam_d, a->lam_r, a->lam_x})
             cuda_check(cudaMemsetAsync(p, 0, fN, a->stream), "memset adjoints");
         cuda_check(cudaMemsetAsync(a->dW, 0, 4ull * E * E, a->stream), "memset dW");
-        cuda_check(cudaMemsetAsync(a->gl_acc, 0, 8ull * a->nb, a->stream), "memset g_leak");
+        cuda_check(cudaMemsetAsync(a->gl_acc, 0, 8ull * a->bwd_grid, a->stream), "memset g_leak");
         if (!a->tape_last) {  // an earlier backward pass replayed other segments over the tape
             if (!a->replay_graph) {
                 cudaGraph_t g = nullptr;
@@ -479,11 +536,18 @@ BSNN_API bsnn_status bsnn_adjoint_backward(bsnn_adjoint* a, float* grad_w_ee, do
         adj_run_graphs(a, a->bwd_graphs, a->bwd_nodes, true, [&](uint32_t c) { adj_backward_segment(a, c); },
                        "adjoint backward");
         if (a->n_ckpt > 1) a->tape_last = false;
-        std::vector<double> gl(a->nb);
-        cuda_check(cudaMemcpyAsync(gl.data(), a->gl_acc, 8ull * a->nb, cudaMemcpyDeviceToHost, a->stream), "D2H g_leak");
+        std::vector<double> gl(a->bwd_grid);
+        int32_t err = 0;
+        cuda_check(cudaMemcpyAsync(gl.data(), a->gl_acc, 8ull * a->bwd_grid, cudaMemcpyDeviceToHost, a->stream),
+                   "D2H g_leak");
+        cuda_check(cudaMemcpyAsync(&err, a->error, sizeof(err), cudaMemcpyDeviceToHost, a->stream), "D2H error");
         if (grad_w_ee)
             cuda_check(cudaMemcpyAsync(grad_w_ee, a->dW, 4ull * E * E, cudaMemcpyDeviceToHost, a->stream), "D2H dW");
         cuda_check(cudaStreamSynchronize(a->stream), "adjoint backward");
+        if (err != kErrNone) {
+            a->have_forward = false;
+            throw ApiError(BSNN_ERR_DEVICE_TIMEOUT, "adjoint backward: a grid-barrier wait timed out");
+        }
         if (grad_g_leak) {
             double s = 0.0;
             for (double x : gl) s += x;

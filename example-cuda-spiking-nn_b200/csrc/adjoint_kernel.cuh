@@ -283,72 +283,89 @@ __device__ __forceinline__ float surrogate(float z, float beta) {
     return 1.0f / (a * a);
 }
 
-// One backward step t for every neuron.  In: lambda_v(t+1) (lam_v), the trace adjoints carried
-// from step t+1 (lam_d, lam_r: dL/dd_{t+1}, dL/dr_{t+1} before adding lambda_x(t+1)), lambda_x(t+1)
-// (lam_x, the pull-back of step t+1's g adjoints), *c_s_t (dL/ds_t from the rate loss, E neurons)
-// and *c_v_t (dL/dv_{t+1} from the voltage loss, E neurons).  Out: lambda_v(t), the carried trace
-// adjoints for step t, lambda_ge(t) / lambda_gi(t), and this block's share of dL/dg_leak.
-__global__ void bsnn_adj_neuron_bwd(ADev A, const float* tape_v, const float* tape_u, const float* tape_ge,
-                                    const float* tape_gi, const uint8_t* tape_s, const uint8_t* tape_ref,
-                                    float* lam_v, float* lam_d, float* lam_r, const float* lam_x,
-                                    const float* __restrict__ c_s_t, const float* __restrict__ c_v_t, float beta,
-                                    float* lam_ge, float* lam_gi, double* gleak_acc) {
-    const float c_s = *c_s_t, c_v = *c_v_t;
-    const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
+// One backward step t of neuron n.  In: lambda_v(t+1) (lv), the trace adjoints carried from step
+// t+1 (ld_, lr_: dL/dd_{t+1}, dL/dr_{t+1} before adding lambda_x(t+1)), lambda_x(t+1) (lx, the
+// pull-back of step t+1's g adjoints), c_s (dL/ds_t from the rate loss, E neurons) and c_v
+// (dL/dv_{t+1} from the voltage loss, E neurons), and the step's tape row.  Out: lambda_v(t), the
+// carried trace adjoints for step t, lambda_ge(t) / lambda_gi(t), and the neuron's share of
+// dL/dg_leak.
+__device__ __forceinline__ double adj_neuron_bwd_one(const ADev& A, uint32_t n, float tv, float tu, float tge, float tgi,
+                                                     uint8_t ts, uint8_t tref, float& lv_io, float& ld_io, float& lr_io,
+                                                     float lx, float c_s, float c_v, float beta, float& lge_out,
+                                                     float& lgi_out) {
+    const uint32_t side = n < A.E ? 0u : 1u;
+    const AdjGroupP& G = A.g[side];
+    // traces produced at step t (x_{t+1} = d_{t+1} - r_{t+1}); lx is dL/dx_{t+1}
+    const float Ld = ld_io + lx, Lr = lr_io - lx;
+    const float s = ts ? 1.0f : 0.0f;
+    float dLds = A.norm[side] * (Ld + Lr);
+    if (side == 0) dLds += c_s;
+    const float Lv_next = lv_io + (side == 0 ? c_v : 0.0f);
+    float lv = 0.0f, lge = 0.0f, lgi = 0.0f;
     double gl = 0.0;
-    if (n < A.N) {
-        const uint32_t side = n < A.E ? 0u : 1u;
-        const AdjGroupP& G = A.g[side];
-        // traces produced at step t (x_{t+1} = d_{t+1} - r_{t+1}); lam_x is dL/dx_{t+1}
-        const float Ld = lam_d[n] + lam_x[n], Lr = lam_r[n] - lam_x[n];
-        const float s = tape_s[n] ? 1.0f : 0.0f;
-        float dLds = A.norm[side] * (Ld + Lr);
-        if (side == 0) dLds += c_s;
-        float Lv_next = lam_v[n] + (side == 0 ? c_v : 0.0f);
-        float lv = 0.0f, lge = 0.0f, lgi = 0.0f;
-        if (!tape_ref[n]) {
-            const float v = tape_v[n], u = tape_u[n], ge = tape_ge[n], gi = tape_gi[n];
-            const float lu = Lv_next * (1.0f - s) + dLds * surrogate(u - G.v_th, beta);
-            const float k = G.timestep / G.cap;
-            const float ex = expf((v - G.v_eff) / G.delta_t);
-            lv = lu * (1.0f + k * (-G.g_leak + G.g_leak * ex - ge - gi));
-            lge = lu * k * (G.e_exc - v);
-            lgi = lu * k * (G.e_inh - v);
-            gl = static_cast<double>(lu) * static_cast<double>(k * (-(v - G.v_rest) + G.delta_t * ex));
-        }
-        lam_v[n] = lv;
-        lam_d[n] = A.d_decay[side] * Ld;  // dL/dd_t
-        lam_r[n] = A.r_decay[side] * Lr;
-        lam_ge[n] = lge;
-        lam_gi[n] = lgi;
+    if (!tref) {
+        const float v = tv, u = tu, ge = tge, gi = tgi;
+        const float lu = Lv_next * (1.0f - s) + dLds * surrogate(u - G.v_th, beta);
+        const float k = G.timestep / G.cap;
+        const float ex = expf((v - G.v_eff) / G.delta_t);
+        lv = lu * (1.0f + k * (-G.g_leak + G.g_leak * ex - ge - gi));
+        lge = lu * k * (G.e_exc - v);
+        lgi = lu * k * (G.e_inh - v);
+        gl = static_cast<double>(lu) * static_cast<double>(k * (-(v - G.v_rest) + G.delta_t * ex));
     }
-    // block reduction of the g_leak share, in a fixed order
-    __shared__ double red[kAdjBlock];
-    red[threadIdx.x] = gl;
-    __syncthreads();
-    for (uint32_t o = blockDim.x / 2; o > 0; o >>= 1) {
-        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) gleak_acc[blockIdx.x] += red[0];
+    lv_io = lv;
+    ld_io = A.d_decay[side] * Ld;  // dL/dd_t
+    lr_io = A.r_decay[side] * Lr;
+    lge_out = lge;
+    lgi_out = lgi;
+    return gl;
 }
 
-// lambda_x[pre] = sum_post W[pre, post] lambda_g[post] for both sides (one warp per presynaptic
-// row: rows < E use W_E and lambda_ge, the others W_I and lambda_gi).  Rows are ld floats (ld a
-// multiple of 4, zero beyond N), read as float4; lambda_g is zero beyond N as well.
-__global__ void bsnn_adj_pullback(const float* __restrict__ WE, const float* __restrict__ WI, uint32_t E, uint32_t N,
-                                  uint32_t ld, const float* __restrict__ lam_ge, const float* __restrict__ lam_gi,
-                                  float* __restrict__ lam_x) {
-    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31u;
-    if (warp >= N) return;
-    const float4* row = reinterpret_cast<const float4*>(warp < E ? WE + static_cast<size_t>(warp) * ld
-                                                                  : WI + static_cast<size_t>(warp - E) * ld);
-    const float4* lam = reinterpret_cast<const float4*>(warp < E ? lam_ge : lam_gi);
-    const uint32_t n4 = ld >> 2;
+// ---- the backward pass of a segment as one persistent kernel ------------------------------------
+// The segment's steps walked backwards in one cooperative launch.  CTA b owns neurons [n0, n1) (an
+// even split of N): their adjoint state (lambda_v, the carried trace adjoints and lambda_x) stays in
+// shared memory for the launch, and the CTA computes both their neuron adjoints and their rows of
+// the pull-back.  Per step t:
+//   the own neurons' adjoints (adj_neuron_bwd_one): lambda_ge(t) into the segment's lambda_ge rows
+//   (kept for dL/dW_EE), lambda_gi(t) into one of two buffers by step parity;
+//   grid barrier (every CTA now needs every neuron's lambda_g);
+//   lambda_ge(t) and lambda_gi(t) into shared memory, then the own rows' pull-back: lambda_x(t) of
+//   the own neurons, which only this CTA's adjoints of step t - 1 read, so no second barrier is
+//   needed.  A lambda_gi buffer is written again two steps later, after every CTA has passed the
+//   barrier that follows its reads.
+// The pull-back splits each own row into kPbChunks pieces, one (row, piece) per warp at a time,
+// and adds a row's pieces in order.  The first `n_res` own rows of W are copied into shared memory
+// at launch start (W does not change during the pass); the others stream from L2, and their
+// pieces are taken first, so their loads are in flight while the resident rows are summed.
+// The g_leak shares are summed per thread over the segment, then over the CTA in a fixed order.
+// The barrier's wait is bounded (s_wait_limit_ns); a timeout sets the error word.
+struct AdjBwd {
+    const float *tv, *tu, *tge, *tgi;   // the segment's tape, [steps][N]
+    const uint8_t *ts, *tref;
+    float *lam_v, *lam_d, *lam_r, *lam_x;  // [N] carried between segments
+    const float *c_s, *c_v;              // [T] the loss sensitivities
+    float* lge_all;                      // [steps][ld] lambda_ge rows (zero beyond N)
+    float* lgi2;                         // [2][ld] lambda_gi by step parity (zero beyond N)
+    double* gl_acc;                      // [grid] g_leak shares, added to
+    unsigned long long* barrier;
+    int32_t* error;
+    unsigned long long wait_limit_ns;
+    uint32_t t0, steps, ld, max_own, n_res;
+    float beta;
+};
+constexpr uint32_t kAdjBwdThreads = 512;
+constexpr uint32_t kPbChunks = 4;
+
+// One warp: the piece [q0, q1) (in float4 units) of row `row` (ld floats) times lambda.
+template <bool SMEM>
+__device__ __forceinline__ float adj_pullback_piece(const float* row, const float* lam, uint32_t q0, uint32_t q1,
+                                                    uint32_t lane) {
+    const float4* r4 = reinterpret_cast<const float4*>(row);
+    const float4* l4 = reinterpret_cast<const float4*>(lam);
     float acc = 0.0f;
-#pragma unroll 4
-    for (uint32_t q = lane; q < n4; q += 32u) {
-        const float4 w = __ldg(row + q), l = __ldg(lam + q);
+#pragma unroll 8
+    for (uint32_t q = q0 + lane; q < q1; q += 32u) {
+        const float4 w = SMEM ? r4[q] : __ldg(r4 + q), l = l4[q];
         acc = fmaf(w.x, l.x, acc);
         acc = fmaf(w.y, l.y, acc);
         acc = fmaf(w.z, l.z, acc);
@@ -356,7 +373,114 @@ __global__ void bsnn_adj_pullback(const float* __restrict__ WE, const float* __r
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
-    if (lane == 0) lam_x[warp] = acc;
+    return acc;
+}
+
+__global__ void __launch_bounds__(kAdjBwdThreads, 1) bsnn_adj_backward_kernel(ADev A, AdjBwd B) {
+    // lambda_ge [ld], lambda_gi [ld], own state [4][max_own], pieces [max_own][kPbChunks], rows [n_res][ld]
+    extern __shared__ __align__(16) float adj_sm[];
+    __shared__ int s_ok;
+    __shared__ unsigned long long s_bar0;
+    __shared__ double s_red[kAdjBwdThreads / 32];
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u, nwarps = blockDim.x >> 5;
+    const uint32_t N = A.N, ld = B.ld;
+    const uint32_t n0 = static_cast<uint32_t>(static_cast<unsigned long long>(blockIdx.x) * N / gridDim.x);
+    const uint32_t n1 = static_cast<uint32_t>(static_cast<unsigned long long>(blockIdx.x + 1u) * N / gridDim.x);
+    const uint32_t own = n1 - n0;
+    float* s_lge = adj_sm;
+    float* s_lgi = adj_sm + ld;
+    float* s_lv = adj_sm + 2u * ld;
+    float* s_ld = s_lv + B.max_own;
+    float* s_lr = s_ld + B.max_own;
+    float* s_lx = s_lr + B.max_own;
+    float* s_part = s_lx + B.max_own;
+    float* s_w = adj_sm + 2u * ld + ((4u * B.max_own + kPbChunks * B.max_own + 3u) & ~3u);
+    const uint32_t n_res = own < B.n_res ? own : B.n_res;
+    for (uint32_t r = 0; r < n_res; ++r) {
+        const uint32_t pre = n0 + r;
+        const float4* src = reinterpret_cast<const float4*>(pre < A.E ? A.WE + static_cast<size_t>(pre) * ld
+                                                                        : A.WI + static_cast<size_t>(pre - A.E) * ld);
+        for (uint32_t q = tid; q < ld / 4u; q += blockDim.x)
+            reinterpret_cast<float4*>(s_w + static_cast<size_t>(r) * ld)[q] = __ldg(src + q);
+    }
+    if (tid == 0) {
+        s_wait_limit_ns = B.wait_limit_ns;
+        s_bar0 = ld_acquire_u64(B.barrier) / gridDim.x * gridDim.x;
+    }
+    for (uint32_t i = tid; i < own; i += blockDim.x) {
+        s_lv[i] = B.lam_v[n0 + i];
+        s_ld[i] = B.lam_d[n0 + i];
+        s_lr[i] = B.lam_r[n0 + i];
+        s_lx[i] = B.lam_x[n0 + i];
+    }
+    __syncthreads();
+    const unsigned long long bar0 = s_bar0;
+    double gl = 0.0;
+    for (uint32_t kk = 0; kk < B.steps; ++kk) {
+        const uint32_t k = B.steps - 1u - kk, t = B.t0 + k;
+        const size_t o = static_cast<size_t>(k) * N;
+        float* lge_row = B.lge_all + static_cast<size_t>(k) * ld;
+        float* lgi_buf = B.lgi2 + static_cast<size_t>(k & 1u) * ld;
+        const float c_s = B.c_s[t], c_v = B.c_v[t];
+        for (uint32_t i = tid; i < own; i += blockDim.x) {
+            const uint32_t n = n0 + i;
+            float lge, lgi;
+            gl += adj_neuron_bwd_one(A, n, B.tv[o + n], B.tu[o + n], B.tge[o + n], B.tgi[o + n], B.ts[o + n],
+                                     B.tref[o + n], s_lv[i], s_ld[i], s_lr[i], s_lx[i], c_s, c_v, B.beta, lge, lgi);
+            lge_row[n] = lge;
+            lgi_buf[n] = lgi;
+        }
+        if (!grid_barrier(B.barrier, B.error, bar0 + (kk + 1ull) * gridDim.x, &s_ok)) break;
+        // every neuron's lambda_g of step t (written by other CTAs: read from L2)
+        for (uint32_t q = tid; q < ld / 4u; q += blockDim.x) {
+            reinterpret_cast<float4*>(s_lge)[q] = __ldcg(reinterpret_cast<const float4*>(lge_row) + q);
+            reinterpret_cast<float4*>(s_lgi)[q] = __ldcg(reinterpret_cast<const float4*>(lgi_buf) + q);
+        }
+        __syncthreads();
+        {
+            const uint32_t n4 = ld / 4u, cq = (n4 + kPbChunks - 1u) / kPbChunks, n_str = own - n_res;
+            for (uint32_t p = warp; p < own * kPbChunks; p += nwarps) {
+                const uint32_t rr = p / kPbChunks, c = p % kPbChunks;
+                const uint32_t r = rr < n_str ? n_res + rr : rr - n_str;  // streamed rows first
+                const uint32_t pre = n0 + r;
+                const float* lam = pre < A.E ? s_lge : s_lgi;
+                const uint32_t q0 = c * cq < n4 ? c * cq : n4, q1 = q0 + cq < n4 ? q0 + cq : n4;
+                float acc;
+                if (r < n_res) {
+                    acc = adj_pullback_piece<true>(s_w + static_cast<size_t>(r) * ld, lam, q0, q1, lane);
+                } else {
+                    const float* row = pre < A.E ? A.WE + static_cast<size_t>(pre) * ld
+                                                 : A.WI + static_cast<size_t>(pre - A.E) * ld;
+                    acc = adj_pullback_piece<false>(row, lam, q0, q1, lane);
+                }
+                if (lane == 0) s_part[r * kPbChunks + c] = acc;
+            }
+        }
+        __syncthreads();
+        for (uint32_t i = tid; i < own; i += blockDim.x) {
+            float acc = 0.0f;
+#pragma unroll
+            for (uint32_t c = 0; c < kPbChunks; ++c) acc += s_part[i * kPbChunks + c];
+            s_lx[i] = acc;
+        }
+    }
+    // the CTA's g_leak share: warp sums, then the warps in order
+    double v = gl;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(kFull, v, off);
+    if (lane == 0) s_red[warp] = v;
+    __syncthreads();
+    if (tid == 0) {
+        double total = 0.0;
+        for (uint32_t w = 0; w < nwarps; ++w) total += s_red[w];
+        B.gl_acc[blockIdx.x] += total;
+    }
+    for (uint32_t i = tid; i < own; i += blockDim.x) {
+        B.lam_v[n0 + i] = s_lv[i];
+        B.lam_d[n0 + i] = s_ld[i];
+        B.lam_r[n0 + i] = s_lr[i];
+        B.lam_x[n0 + i] = s_lx[i];
+    }
 }
 
 // dW[pre, post] += sum_t X[t, pre] L[t, post] over one segment's steps (X: x_t of the E

@@ -281,8 +281,6 @@ struct SmemLayout {
     float* rowsum;      // [max_rows] running sum of each resident triplet row (see norm_rows)
     uint32_t* sbits;    // [spk_words] spike bitmask of the step whose plasticity is being applied
     uint32_t* gbits;    // [2][max_own/32 + 2] this CTA's spike bits, by step parity
-    uint32_t* gold;     // [max_own/32 + 2] the bits of this step's parity before the step (the
-                        // CTA's bits in the network bitmask the flush replaces)
     float* xown;        // [n_ts][max_own] x = d - r of the own neurons (this step)
     float2* rowfac;     // [2][n_plast][max_own] {rowA, rowB} of the own neurons, by step parity
     float* ns;          // [ns_fields][max_own] state of the own neurons (kNs* fields below)
@@ -298,8 +296,6 @@ struct SmemLayout {
     float* lzf;         // [max_rows] this step's GEMV weight of the row, x s qs
     float* lzw;         // [32] per-warp partial master sums of a spiking row (row-scaled forms)
     uint32_t* bits;     // [n_spike_monitors][max_own/32 + 2]
-    uint32_t* mold;     // the same shape: the CTA's bits in each monitor's ring slot of this step
-                        // before the step (read ahead in the grid-barrier window)
     unsigned char* desc;  // descriptor copies (DGroup, DTraceSet, DConn, DPlast, DMon, slot lists)
 };
 
@@ -345,7 +341,7 @@ __host__ __device__ __forceinline__ SmemSizes smem_sizes(uint32_t resident_float
     z.rowtgt = align16(sizeof(float) * max_rows);
     z.rowsum = align16(sizeof(float) * max_rows);
     z.sbits = align16(sizeof(uint32_t) * spk_words);
-    z.gbits = align16(sizeof(uint32_t) * 3 * (max_own / 32 + 2));
+    z.gbits = align16(sizeof(uint32_t) * 2 * (max_own / 32 + 2));
     z.xown = align16(sizeof(float) * n_ts * max_own);
     z.rowfac = align16(sizeof(float2) * 2 * n_plast * max_own);
     z.ns = align16(sizeof(float) * ns_fields * max_own);
@@ -355,7 +351,7 @@ __host__ __device__ __forceinline__ SmemSizes smem_sizes(uint32_t resident_float
                                align16(static_cast<size_t>(stage_warps) * (2u * sizeof(uint64_t) + sizeof(uint32_t)))
                          : 0;
     z.lz = align16(sizeof(float) * (5u * static_cast<size_t>(lazy_rows) + (lazy_rows ? 32u : 0u)));
-    z.bits = align16(sizeof(uint32_t) * 2 * n_spike_mons * (max_own / 32 + 2));
+    z.bits = align16(sizeof(uint32_t) * n_spike_mons * (max_own / 32 + 2));
     z.groups = align16(sizeof(DGroup) * n_groups);
     z.ts = align16(sizeof(DTraceSet) * n_ts);
     z.conns = align16(sizeof(DConn) * n_conns);
@@ -746,79 +742,49 @@ __device__ __forceinline__ void move_neuron_state(const DSim* S, const Desc& D, 
     }
 }
 
+// Writes this CTA's spike bits of each spike monitor into the ring slot of `clock`.  Each CTA
+// clears and sets only the bits of its own neurons, so the word updates of different CTAs commute.
+__device__ __forceinline__ void merge_bits(uint32_t* word, uint32_t mask, uint32_t bits) {
+    const uint32_t clear = mask & ~bits;
+    if (clear) atomicAnd(word, ~clear);
+    if (bits) atomicOr(word, bits);
+}
+
 __device__ __forceinline__ uint32_t range_mask(uint32_t w, uint32_t w0, uint32_t w1, uint32_t a, uint32_t b_end) {
     const uint32_t lo = w == w0 ? (a & 31u) : 0u;
     const uint32_t hi = w == w1 ? ((b_end - 1) & 31u) : 31u;
     return (hi == 31u ? 0xffffffffu : ((1u << (hi + 1u)) - 1u)) & ~((1u << lo) - 1u);
 }
 
-// The CTA's neurons in spike monitor m's group, as group-local indices [a, b_end); false if none.
-__device__ __forceinline__ bool monitor_range(const Desc& D, const DCta& cta, uint32_t m, uint32_t& a, uint32_t& b_end) {
-    const DMon& M = D.mons[m];
-    if (M.kind != kMonSpikes) return false;
-    const DGroup& G = D.groups[M.group];
-    a = cta.n0 > G.off ? cta.n0 - G.off : 0u;
-    b_end = cta.n1 - G.off < G.n ? cta.n1 - G.off : G.n;
-    return cta.n1 > G.off && a < b_end;
-}
-
-// Publishes the step's spike bits, on threads [0, nthreads) of the CTA: this CTA's bits in the
-// network-wide bitmask of the step's parity (read by every CTA's next weight pass) and in each
-// spike monitor's ring slot of `clock`.  The CTA knows the bits it replaces (gold: its bits of the
-// same parity two steps ago; mold: its bits in the ring slot, read ahead), so a word takes one
-// atomicXor of the changed bits, and a word whose bits did not change takes none.  Each CTA
-// changes only the bits of its own neurons, so the updates of different CTAs commute.
+// Runs on threads [0, nthreads) of the CTA.
 __device__ __forceinline__ void flush_spike_bits(const DSim* S, const Desc& D, const DCta& cta, uint32_t clock,
                                               uint32_t par, const SmemLayout& sm, uint32_t nthreads) {
+    // the network-wide spike bitmask of this step (read by every CTA's next weight pass)
     if (cta.n1 > cta.n0) {
         const uint32_t w0 = cta.n0 >> 5, w1 = (cta.n1 - 1) >> 5;
-        const uint32_t* now = sm.gbits + par * (D.max_own / 32u + 2u);
-        for (uint32_t w = w0 + threadIdx.x; w <= w1; w += nthreads) {
-            const uint32_t diff = (sm.gold[w - w0] ^ now[w - w0]) & range_mask(w, w0, w1, cta.n0, cta.n1);
-            if (diff) atomicXor(D.spk_bits[par] + w, diff);
-        }
+        for (uint32_t w = w0 + threadIdx.x; w <= w1; w += nthreads)
+            merge_bits(D.spk_bits[par] + w, range_mask(w, w0, w1, cta.n0, cta.n1),
+                       sm.gbits[par * (D.max_own / 32u + 2u) + w - w0]);
     }
     for (uint32_t m = 0; m < D.n_mons; ++m) {
-        uint32_t a, b_end;
-        if (!monitor_range(D, cta, m, a, b_end)) continue;
         const DMon& M = D.mons[m];
+        if (M.kind != kMonSpikes) continue;
+        const DGroup& G = D.groups[M.group];
+        const uint32_t a = cta.n0 > G.off ? cta.n0 - G.off : 0u;
+        const uint32_t b_end = cta.n1 - G.off < G.n ? cta.n1 - G.off : G.n;
+        if (cta.n1 <= G.off || a >= b_end) continue;
         const uint32_t w0 = a >> 5, w1 = (b_end - 1) >> 5;
         for (uint32_t w = w0 + threadIdx.x; w <= w1; w += nthreads) {
-            const uint32_t i = D.bitbase[m] + (w - w0);
-            const uint32_t diff = (sm.mold[i] ^ sm.bits[i]) & range_mask(w, w0, w1, a, b_end);
-            if (diff) atomicXor(M.bits + static_cast<size_t>(clock % M.interval) * M.words + w, diff);
+            const uint32_t lo = w == w0 ? (a & 31u) : 0u;
+            const uint32_t hi = w == w1 ? ((b_end - 1) & 31u) : 31u;
+            const uint32_t mask = (hi == 31u ? 0xffffffffu : ((1u << (hi + 1u)) - 1u)) & ~((1u << lo) - 1u);
+            const uint32_t bits = sm.bits[D.bitbase[m] + (w - w0)] & mask;
+            uint32_t* word = M.bits + static_cast<size_t>(clock % M.interval) * M.words + w;
+            const uint32_t clear = mask & ~bits;
+            if (clear) atomicAnd(word, ~clear);
+            if (bits) atomicOr(word, bits);
         }
     }
-}
-
-// The CTA's bits in each spike monitor's ring slot of `clock` (the bits that clock's flush
-// replaces) into sm.mold, on threads [first_thread, blockDim.x).
-__device__ __forceinline__ void read_ring_bits(const Desc& D, const DCta& cta, uint32_t clock, const SmemLayout& sm,
-                                               uint32_t first_thread) {
-    if (threadIdx.x < first_thread) return;
-    const uint32_t me = threadIdx.x - first_thread, nthreads = blockDim.x - first_thread;
-    for (uint32_t m = 0; m < D.n_mons; ++m) {
-        uint32_t a, b_end;
-        if (!monitor_range(D, cta, m, a, b_end)) continue;
-        const DMon& M = D.mons[m];
-        const uint32_t w0 = a >> 5, w1 = (b_end - 1) >> 5;
-        for (uint32_t w = w0 + me; w <= w1; w += nthreads)
-            sm.mold[D.bitbase[m] + (w - w0)] =
-                __ldcg(M.bits + static_cast<size_t>(clock % M.interval) * M.words + w) & range_mask(w, w0, w1, a, b_end);
-    }
-}
-
-// At launch start: the CTA's bits in the network bitmask of both parities (gbits, the bits the
-// flushes of the launch's first two steps replace) and in the monitors' ring slots of `clock0`.
-__device__ __forceinline__ void read_own_bits(const Desc& D, const DCta& cta, uint32_t clock0, const SmemLayout& sm) {
-    const uint32_t n_gbits = D.max_own / 32u + 2u;
-    if (cta.n1 > cta.n0) {
-        const uint32_t w0 = cta.n0 >> 5, w1 = (cta.n1 - 1) >> 5;
-        for (uint32_t p = 0; p < 2u; ++p)
-            for (uint32_t w = w0 + threadIdx.x; w <= w1; w += blockDim.x)
-                sm.gbits[p * n_gbits + w - w0] = __ldcg(D.spk_bits[p] + w) & range_mask(w, w0, w1, cta.n0, cta.n1);
-    }
-    read_ring_bits(D, cta, clock0, sm, 0u);
 }
 
 // Per-row data of the pending plasticity update for phase B and the normalisation pass: the row
@@ -1919,7 +1885,6 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : LAZY ? kMaxThreadsRows :
         sm.sbits = reinterpret_cast<uint32_t*>(p);
         p += z.sbits;
         sm.gbits = reinterpret_cast<uint32_t*>(p);
-        sm.gold = sm.gbits + 2u * (max_own / 32u + 2u);
         p += z.gbits;
         sm.xown = reinterpret_cast<float*>(p);
         p += z.xown;
@@ -1948,7 +1913,6 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : LAZY ? kMaxThreadsRows :
         sm.lzw = sm.lzf + max_rows;
         p += z.lz;
         sm.bits = reinterpret_cast<uint32_t*>(p);
-        sm.mold = sm.bits + n_spike_mons * (max_own / 32u + 2u);
         p += z.bits;
         sm.desc = p;
     }
@@ -2100,7 +2064,6 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : LAZY ? kMaxThreadsRows :
         }
     }
     draw_noise(D, cta, t0, sm, max_own, 0u);
-    read_own_bits(D, cta, clock0, sm);
     __syncthreads();
 #ifdef BSNN_PHASE_TIMING
     __shared__ unsigned long long s_tally_[kPhaseSlots];
@@ -2140,10 +2103,7 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : LAZY ? kMaxThreadsRows :
         }
         rows_pending(D, cta, pending, ppar, sm, max_own);
         for (uint32_t w = tid; w < n_bits_words; w += nthr) sm.bits[w] = 0u;
-        for (uint32_t w = tid; w < n_gbits; w += nthr) {
-            sm.gold[w] = sm.gbits[par * n_gbits + w];  // this CTA's bits of two steps ago
-            sm.gbits[par * n_gbits + w] = 0u;
-        }
+        for (uint32_t w = tid; w < n_gbits; w += nthr) sm.gbits[par * n_gbits + w] = 0u;
         __syncthreads();
         BSNN_TMARK(0);
         const bool norm_now = pending && s_has_norm;
@@ -2215,12 +2175,8 @@ __global__ void __launch_bounds__(CARRY ? kMaxThreads : LAZY ? kMaxThreadsRows :
         BSNN_TMARK(4);
         grid_arrive(D.barrier, t != D.skip_step || blockIdx.x != D.skip_cta);
         BSNN_TSTART(t_win_);
-        // the next step's Poisson counts and the monitors' ring bits it replaces, while the other
-        // CTAs finish (warp 0 waits)
-        if (k + 1u < n_steps) {
-            draw_noise(D, cta, t + 1ull, sm, max_own, nwarps > 1u ? 32u : 0u);
-            read_ring_bits(D, cta, clock + 1u, sm, nwarps > 1u ? 32u : 0u);
-        }
+        // the next step's Poisson counts while the other CTAs finish (warp 0 waits)
+        if (k + 1u < n_steps) draw_noise(D, cta, t + 1ull, sm, max_own, nwarps > 1u ? 32u : 0u);
         if (tid == 32u) BSNN_TSPAN(14, t_win_);
         if (!grid_wait(D.barrier, D.error, bar0 + (k + 1ull) * gridDim.x, &s_ok)) {
             ok = false;

@@ -207,9 +207,13 @@ def test_precision_forms_against_fp64():
 LARGE_FIXTURE = Path(__file__).resolve().parent / "golden" / "fp64_large_plastic_10125.npz"
 # Bounds per form: (voltage error after step 20 relative to the largest |v|, the larger relative
 # spike-count error of the two populations over the run, the larger plastic-weight drift
-# mean |w - w64| / mean |w64| over the sample): about twice the values measured on B200.
-LARGE_BOUNDS = {"f32": (1e-6, 0.5, 5e-2), "f32_rowscaled": (1e-6, 0.5, 5e-2), "bf16": (1e-2, 0.5, 0.1),
-                "fp8_e4m3": (5e-2, 0.5, 0.25)}
+# mean |w - w64| / mean |w64| over the sample): about twice the values measured on B200 over the
+# 5,001 steps (E 298 / I 125 spikes in the FP64 run), with a floor of 2 spikes (6.7e-3) on the
+# rate error.  Measured: f32 3.7e-7 / 0 / 4.8e-8; f32_rowscaled 3.7e-7 / 0 / 3.6e-8; bf16 3.7e-7 /
+# 6.7e-3 / 2.3e-4; fp8_e4m3 3.7e-7 / 3.0e-2 / 9.6e-4.  The voltage error after 1,000 steps (printed)
+# is 5e-6 in the FP32 forms and 5e-2 in BF16 / FP8, where single spikes have moved by then.
+LARGE_BOUNDS = {"f32": (8e-7, 6.7e-3, 1e-7), "f32_rowscaled": (8e-7, 6.7e-3, 1e-7), "bf16": (8e-7, 1.4e-2, 5e-4),
+                "fp8_e4m3": (8e-7, 6e-2, 2e-3)}
 
 
 def _large_form_run(spec, ref, form):
