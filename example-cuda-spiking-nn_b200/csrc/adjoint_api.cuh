@@ -323,6 +323,8 @@ BSNN_API bsnn_status bsnn_adjoint_create(const bsnn_adjoint_desc* desc, const bs
         cuda_check(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device), "smem attr");
         a->bwd_grid = std::max<uint32_t>(1u, std::min<uint32_t>(static_cast<uint32_t>(sms), (N + 7u) / 8u));
         a->bwd_max_own = (N + a->bwd_grid - 1) / a->bwd_grid;
+        require(a->bwd_max_own <= kAdjBwdThreads, BSNN_ERR_INVALID_ARGUMENT,
+                "network too large for the adjoint's backward kernel (one thread per neuron of a CTA)");
         // lambda_g vectors, own state and row pieces, then as many own rows of W as fit
         const size_t fixed = sizeof(float) * (2ull * ld + ((4ull * a->bwd_max_own + kPbChunks * a->bwd_max_own + 3u) & ~3ull));
         require(fixed + 2048 <= static_cast<size_t>(optin), BSNN_ERR_INVALID_ARGUMENT,

@@ -416,20 +416,42 @@ __global__ void __launch_bounds__(kAdjBwdThreads, 1) bsnn_adj_backward_kernel(AD
     __syncthreads();
     const unsigned long long bar0 = s_bar0;
     double gl = 0.0;
+    // Thread i steps own neuron i (own <= blockDim.x).  Its tape row and the loss sensitivities of
+    // the next step to walk are loaded before the grid barrier, so their latency hides behind it.
+    const bool mine = tid < own;
+    const uint32_t n = n0 + tid;
+    struct TapeRow {
+        float v, u, ge, gi, cs, cv;
+        uint8_t s, ref;
+    };
+    auto fetch = [&](uint32_t k) {
+        TapeRow r{};
+        const size_t o = static_cast<size_t>(k) * N + n;
+        r.cs = B.c_s[B.t0 + k];
+        r.cv = B.c_v[B.t0 + k];
+        if (mine) {
+            r.v = B.tv[o];
+            r.u = B.tu[o];
+            r.ge = B.tge[o];
+            r.gi = B.tgi[o];
+            r.s = B.ts[o];
+            r.ref = B.tref[o];
+        }
+        return r;
+    };
+    TapeRow cur = fetch(B.steps - 1u);
     for (uint32_t kk = 0; kk < B.steps; ++kk) {
-        const uint32_t k = B.steps - 1u - kk, t = B.t0 + k;
-        const size_t o = static_cast<size_t>(k) * N;
+        const uint32_t k = B.steps - 1u - kk;
         float* lge_row = B.lge_all + static_cast<size_t>(k) * ld;
         float* lgi_buf = B.lgi2 + static_cast<size_t>(k & 1u) * ld;
-        const float c_s = B.c_s[t], c_v = B.c_v[t];
-        for (uint32_t i = tid; i < own; i += blockDim.x) {
-            const uint32_t n = n0 + i;
+        if (mine) {
             float lge, lgi;
-            gl += adj_neuron_bwd_one(A, n, B.tv[o + n], B.tu[o + n], B.tge[o + n], B.tgi[o + n], B.ts[o + n],
-                                     B.tref[o + n], s_lv[i], s_ld[i], s_lr[i], s_lx[i], c_s, c_v, B.beta, lge, lgi);
+            gl += adj_neuron_bwd_one(A, n, cur.v, cur.u, cur.ge, cur.gi, cur.s, cur.ref, s_lv[tid], s_ld[tid], s_lr[tid],
+                                     s_lx[tid], cur.cs, cur.cv, B.beta, lge, lgi);
             lge_row[n] = lge;
             lgi_buf[n] = lgi;
         }
+        if (k > 0u) cur = fetch(k - 1u);
         if (!grid_barrier(B.barrier, B.error, bar0 + (kk + 1ull) * gridDim.x, &s_ok)) break;
         // every neuron's lambda_g of step t (written by other CTAs: read from L2)
         for (uint32_t q = tid; q < ld / 4u; q += blockDim.x) {
@@ -457,11 +479,11 @@ __global__ void __launch_bounds__(kAdjBwdThreads, 1) bsnn_adj_backward_kernel(AD
             }
         }
         __syncthreads();
-        for (uint32_t i = tid; i < own; i += blockDim.x) {
+        if (mine) {
             float acc = 0.0f;
 #pragma unroll
-            for (uint32_t c = 0; c < kPbChunks; ++c) acc += s_part[i * kPbChunks + c];
-            s_lx[i] = acc;
+            for (uint32_t c = 0; c < kPbChunks; ++c) acc += s_part[tid * kPbChunks + c];
+            s_lx[tid] = acc;
         }
     }
     // the CTA's g_leak share: warp sums, then the warps in order
