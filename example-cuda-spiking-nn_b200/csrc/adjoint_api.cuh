@@ -202,7 +202,7 @@ void adj_backward_segment(bsnn_adjoint* a, uint32_t c) {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     cuda_check(cudaLaunchKernelEx(&cfg, bsnn_adj_backward_kernel, a->h, B), "adjoint backward launch");
-    const dim3 og((E + 31) / 32, (E + 31) / 32);
+    const dim3 og((E + kOuterTile - 1) / kOuterTile, (E + kOuterTile - 1) / kOuterTile);
     bsnn_adj_outer<<<og, 256, 0, a->stream>>>(a->tx, N, a->lge_all, a->ld, steps, E, a->dW);
 }
 

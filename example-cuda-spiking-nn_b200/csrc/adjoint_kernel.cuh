@@ -507,33 +507,72 @@ __global__ void __launch_bounds__(kAdjBwdThreads, 1) bsnn_adj_backward_kernel(AD
 
 // dW[pre, post] += sum_t X[t, pre] L[t, post] over one segment's steps (X: x_t of the E
 // presynaptic neurons, rows of ldx floats; L: lambda_ge(t) of the E postsynaptic neurons, rows of
-// ldl floats).
-// 32 x 32 output tiles, the steps staged through shared memory 32 at a time.
-__global__ void bsnn_adj_outer(const float* __restrict__ X, uint32_t ldx, const float* __restrict__ L, uint32_t ldl,
-                               uint32_t steps, uint32_t E, float* __restrict__ dW) {
-    __shared__ float xs[32][33], ls[32][33];
-    const uint32_t pre0 = blockIdx.y * 32u, post0 = blockIdx.x * 32u;
-    const uint32_t tx = threadIdx.x & 31u, ty = threadIdx.x >> 5;  // 32 x 8 threads, 4 outputs each
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
-    for (uint32_t t0 = 0; t0 < steps; t0 += 32u) {
-        for (uint32_t k = ty; k < 32u; k += 8u) {
-            const uint32_t t = t0 + k;
-            xs[k][tx] = t < steps && pre0 + tx < E ? X[static_cast<size_t>(t) * ldx + pre0 + tx] : 0.0f;
-            ls[k][tx] = t < steps && post0 + tx < E ? L[static_cast<size_t>(t) * ldl + post0 + tx] : 0.0f;
-        }
-        __syncthreads();
-#pragma unroll 8
-        for (uint32_t k = 0; k < 32u; ++k) {
-            const float l = ls[k][tx];
+// ldl floats).  128 x 128 output tiles per block of 256 threads, 8 x 8 outputs per thread (pre =
+// ty + 16 i, post = tx + 16 j); the steps pass through shared memory 8 at a time, the next 8
+// loaded into registers while the current ones are used.  Each output adds its steps in order
+// with fmaf, then adds the sum to dW.
+constexpr uint32_t kOuterTile = 128, kOuterK = 8;
+__global__ void __launch_bounds__(256) bsnn_adj_outer(const float* __restrict__ X, uint32_t ldx,
+                                                      const float* __restrict__ L, uint32_t ldl, uint32_t steps,
+                                                      uint32_t E, float* __restrict__ dW) {
+    __shared__ float xs[2][kOuterK][kOuterTile], ls[2][kOuterK][kOuterTile];
+    const uint32_t pre0 = blockIdx.y * kOuterTile, post0 = blockIdx.x * kOuterTile;
+    const uint32_t tid = threadIdx.x, tx = tid & 15u, ty = tid >> 4;
+    // this thread's loads of a k-tile: step row lr, columns lc .. lc + 3 of both operands
+    const uint32_t lr = tid >> 5, lc = (tid & 31u) * 4u;
+    float ra[4], rb[4];
+    auto fetch = [&](uint32_t t0) {
+        const uint32_t t = t0 + lr;
 #pragma unroll
-            for (uint32_t q = 0; q < 4; ++q) acc[q] = fmaf(xs[k][ty + 8u * q], l, acc[q]);
+        for (uint32_t q = 0; q < 4; ++q) {
+            ra[q] = t < steps && pre0 + lc + q < E ? __ldg(X + static_cast<size_t>(t) * ldx + pre0 + lc + q) : 0.0f;
+            rb[q] = t < steps && post0 + lc + q < E ? __ldg(L + static_cast<size_t>(t) * ldl + post0 + lc + q) : 0.0f;
         }
+    };
+    auto stash = [&](uint32_t buf) {
+#pragma unroll
+        for (uint32_t q = 0; q < 4; ++q) {
+            xs[buf][lr][lc + q] = ra[q];
+            ls[buf][lr][lc + q] = rb[q];
+        }
+    };
+    float acc[8][8];
+#pragma unroll
+    for (uint32_t i = 0; i < 8; ++i)
+#pragma unroll
+        for (uint32_t j = 0; j < 8; ++j) acc[i][j] = 0.0f;
+    fetch(0);
+    stash(0);
+    __syncthreads();
+    uint32_t buf = 0;
+    for (uint32_t t0 = 0; t0 < steps; t0 += kOuterK) {
+        const bool more = t0 + kOuterK < steps;
+        if (more) fetch(t0 + kOuterK);
+#pragma unroll
+        for (uint32_t k = 0; k < kOuterK; ++k) {
+            float a[8], b[8];
+#pragma unroll
+            for (uint32_t i = 0; i < 8; ++i) a[i] = xs[buf][k][ty + 16u * i];
+#pragma unroll
+            for (uint32_t j = 0; j < 8; ++j) b[j] = ls[buf][k][tx + 16u * j];
+#pragma unroll
+            for (uint32_t i = 0; i < 8; ++i)
+#pragma unroll
+                for (uint32_t j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+        }
+        if (more) stash(buf ^ 1u);
         __syncthreads();
+        buf ^= 1u;
     }
 #pragma unroll
-    for (uint32_t q = 0; q < 4; ++q) {
-        const uint32_t pre = pre0 + ty + 8u * q, post = post0 + tx;
-        if (pre < E && post < E) dW[static_cast<size_t>(pre) * E + post] += acc[q];
+    for (uint32_t i = 0; i < 8; ++i) {
+        const uint32_t pre = pre0 + ty + 16u * i;
+        if (pre >= E) continue;
+#pragma unroll
+        for (uint32_t j = 0; j < 8; ++j) {
+            const uint32_t post = post0 + tx + 16u * j;
+            if (post < E) dW[static_cast<size_t>(pre) * E + post] += acc[i][j];
+        }
     }
 }
 
