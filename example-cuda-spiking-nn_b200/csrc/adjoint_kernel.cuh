@@ -83,8 +83,7 @@ __global__ void __launch_bounds__(kAdjBlock) bsnn_adj_neuron_fwd(ADev A, uint32_
         float id = flush_tiny(A.id[n] * G.bg_id_decay);
         uint32_t ne = 0, ni = 0;
         if (A.noise_on) {
-            if (G.has_bg_e) ne = poisson_knuth(G.exp_neg_mean_e, A.seed, n, t, 0u);
-            if (G.has_bg_i) ni = poisson_knuth(G.exp_neg_mean_i, A.seed, n, t, 1u);
+            poisson_knuth_pair(G.exp_neg_mean_e, G.has_bg_e, G.exp_neg_mean_i, G.has_bg_i, A.seed, n, t, ne, ni);
         }
         if (ne > 0u) {
             const float inc = static_cast<float>(ne);

@@ -419,8 +419,8 @@ __device__ __forceinline__ void noise_ahead(const BSim* S, const BInst* P, const
         const BInst& B = P[cur];
         const uint32_t j = n - B.nbase;
         const BGroupP& G = B.g[j < s_cls[B.cls].E ? 0 : 1];
-        const uint32_t ne = G.has_bg_e ? poisson_knuth(G.exp_neg_mean_e, B.seed, j, t, 0u) : 0u;
-        const uint32_t ni = G.has_bg_i ? poisson_knuth(G.exp_neg_mean_i, B.seed, j, t, 1u) : 0u;
+        uint32_t ne, ni;
+        poisson_knuth_pair(G.exp_neg_mean_e, G.has_bg_e, G.exp_neg_mean_i, G.has_bg_i, B.seed, j, t, ne, ni);
         nz[n - n0] = static_cast<uint16_t>(ne | (ni << 8));
     }
 }

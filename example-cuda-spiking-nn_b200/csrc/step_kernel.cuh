@@ -109,6 +109,68 @@ __device__ __forceinline__ uint32_t poisson_knuth(float exp_neg_mean, uint32_t s
     return k;
 }
 
+// Knuth's method continued from Philox block `block` with the running product p and count k (the
+// tail of poisson_knuth).
+__device__ __forceinline__ uint32_t poisson_knuth_from(float exp_neg_mean, uint32_t seed, uint32_t neuron,
+                                                       unsigned long long step, uint32_t channel, uint32_t block,
+                                                       float p, uint32_t k) {
+    for (; block < 64u; ++block) {
+        uint32_t c0 = neuron, c1 = static_cast<uint32_t>(step), c2 = static_cast<uint32_t>(step >> 32),
+                 c3 = (channel << 16) | block;
+        philox4x32_10(c0, c1, c2, c3, seed, 0u);
+        const uint32_t r[4] = {c0, c1, c2, c3};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float u = __fmul_rn(__uint2float_rn((r[i] >> 8) + 1u), 5.9604644775390625e-8f);
+            p = __fmul_rn(p, u);
+            if (p <= exp_neg_mean) return k;
+            if (++k >= 255u) return 255u;
+        }
+    }
+    return k;
+}
+
+// Both background channels of one neuron (channel 0: excitatory, channel 1: inhibitory; a channel
+// that is off counts 0): the same counts as two poisson_knuth calls.  The first Philox block of
+// the two channels is computed together, two independent chains the scheduler interleaves; the
+// rarer later blocks follow per channel.
+__device__ __forceinline__ void poisson_knuth_pair(float em0, bool on0, float em1, bool on1, uint32_t seed,
+                                                   uint32_t neuron, unsigned long long step, uint32_t& n0,
+                                                   uint32_t& n1) {
+    uint32_t a0 = neuron, a1 = static_cast<uint32_t>(step), a2 = static_cast<uint32_t>(step >> 32), a3 = 0u;
+    uint32_t b0 = neuron, b1 = a1, b2 = a2, b3 = 1u << 16;
+    philox4x32_10(a0, a1, a2, a3, seed, 0u);
+    philox4x32_10(b0, b1, b2, b3, seed, 0u);
+    const uint32_t ra[4] = {a0, a1, a2, a3}, rb[4] = {b0, b1, b2, b3};
+    // channel c from its first block: done (count) or the running product and count after 4 uniforms
+    auto first = [&](const uint32_t* r, float em, uint32_t& out) -> bool {
+        float p = 1.0f;
+        uint32_t k = 0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float u = __fmul_rn(__uint2float_rn((r[i] >> 8) + 1u), 5.9604644775390625e-8f);
+            p = __fmul_rn(p, u);
+            if (p <= em) {
+                out = k;
+                return true;
+            }
+            ++k;
+        }
+        out = __float_as_uint(p);  // the running product, continued below with k = 4
+        return false;
+    };
+    n0 = 0u;
+    n1 = 0u;
+    if (on0) {
+        uint32_t v;
+        n0 = first(ra, em0, v) ? v : poisson_knuth_from(em0, seed, neuron, step, 0u, 1u, __uint_as_float(v), 4u);
+    }
+    if (on1) {
+        uint32_t v;
+        n1 = first(rb, em1, v) ? v : poisson_knuth_from(em1, seed, neuron, step, 1u, 1u, __uint_as_float(v), 4u);
+    }
+}
+
 __device__ __forceinline__ float4 ld_col4(const float* p) { return __ldcg(reinterpret_cast<const float4*>(p)); }
 
 __device__ __forceinline__ float flush_tiny(float t) { return t < 1e-30f ? 0.0f : t; }
@@ -645,8 +707,7 @@ __device__ __forceinline__ void draw_noise(const Desc& D, const DCta& cta, unsig
         const DGroup& G = D.groups[g];
         uint32_t ne = 0, ni = 0;
         if (D.noise_mode == kNoisePhilox) {
-            if (G.has_bg_e) ne = poisson_knuth(G.exp_neg_mean_e, D.seed, j, t, 0u);
-            if (G.has_bg_i) ni = poisson_knuth(G.exp_neg_mean_i, D.seed, j, t, 1u);
+            poisson_knuth_pair(G.exp_neg_mean_e, G.has_bg_e, G.exp_neg_mean_i, G.has_bg_i, D.seed, j, t, ne, ni);
         } else if (D.noise_mode == kNoiseReplay && t < D.replay_steps) {
             const size_t base = (static_cast<size_t>(t) * D.N + j) * 2u;
             ne = D.replay[base];
