@@ -49,7 +49,9 @@ namespace bsnn {
 
 constexpr uint32_t kBatchMaxClasses = 8;
 constexpr uint32_t kBatchStages = 8;        // the largest shared-memory ring of operand stages
-constexpr uint32_t kBatchTmemCols = 256;    // accumulator columns (N <= 256)
+constexpr uint32_t kBatchTmemCols = 512;    // two accumulators of up to 256 columns (N <= 256)
+constexpr uint32_t kAccCols = 256;
+constexpr uint32_t kUnitRing = 4;           // units named ahead by the loader (phased form)
 constexpr uint32_t kBatchThreads = 512;
 constexpr uint32_t kATileBytes = 128u * 64u * 2u;  // one 128 x 64 BF16 A tile
 
@@ -424,22 +426,14 @@ __device__ __forceinline__ void noise_ahead(const BSim* S, const BInst* P, const
         nz[n - n0] = static_cast<uint16_t>(ne | (ni << 8));
     }
 }
-// The warps idle in phase B that draw the noise: (BSNN_BATCH_NOISE_WARPS = 1, the default) warps
-// 5-15 except those on the producer's scheduler (warp 4 runs on sub-partition 0, so warps 8 and 12
-// are left out: the single producer thread's issue latency gates the whole GEMM), or (0) all of
-// warps 5-15.
-#ifndef BSNN_BATCH_NOISE_WARPS
-#define BSNN_BATCH_NOISE_WARPS 1
-#endif
-__device__ __forceinline__ bool noise_warp(uint32_t warp) {
-    if (BSNN_BATCH_NOISE_WARPS == 1) return warp >= 5u && (warp & 3u) != 0u;
-    return warp >= 5u;
-}
+// The warps idle in phase B that draw the noise: warps 5-15 except those on sub-partition 0 (8 and
+// 12), where the loader thread (warp 4) and the MMA thread (warp 8) run: their single threads'
+// issue latency gates the GEMM.
+__device__ __forceinline__ bool noise_warp(uint32_t warp) { return warp >= 5u && (warp & 3u) != 0u; }
 __device__ __forceinline__ uint32_t noise_rank(uint32_t warp) {  // among the noise warps
-    if (BSNN_BATCH_NOISE_WARPS == 1) return (warp - 5u) - (warp >= 8u ? 1u : 0u) - (warp >= 12u ? 1u : 0u);
-    return warp - 5u;
+    return (warp - 5u) - (warp >= 8u ? 1u : 0u) - (warp >= 12u ? 1u : 0u);
 }
-constexpr uint32_t kNoiseWarps = BSNN_BATCH_NOISE_WARPS == 1 ? 9u : 11u;
+constexpr uint32_t kNoiseWarps = 9u;
 
 // The CTA's shared-memory state arrays (`per` neurons each, from `raw` on), from index `soff` on,
 // for neurons numbered from `base`.
@@ -507,6 +501,14 @@ struct BatchSmem {
     uint64_t ready[2];  // the producer has taken a unit (or found none left) and named it in unit[]
     uint32_t unit[2];
     uint64_t tfree;   // the 4 epilogue warps: the accumulator has been read
+    // the phased form's split producer: the loader names units in a ring (ufull: named; uempty:
+    // the MMA thread and the 4 epilogue warps are done with the slot), and the MMA thread fills
+    // two accumulators in turn (afull: committed; aempty: the 4 epilogue warps have read it)
+    uint64_t ufull[kUnitRing];
+    uint64_t uempty[kUnitRing];
+    uint32_t uid[kUnitRing];
+    uint64_t afull[2];
+    uint64_t aempty[2];
 };
 
 // The producer's ring and accumulator state (one thread).
@@ -640,7 +642,180 @@ __device__ __forceinline__ void batch_init_barriers(BatchSmem& bs, uint32_t n_st
     mbar_init(saddr(&bs.ready[0]), 1u);
     mbar_init(saddr(&bs.ready[1]), 1u);
     mbar_init(saddr(&bs.tfree), 4u);
+    for (uint32_t u = 0; u < kUnitRing; ++u) {
+        mbar_init(saddr(&bs.ufull[u]), 1u);
+        mbar_init(saddr(&bs.uempty[u]), 5u);
+    }
+    for (uint32_t b = 0; b < 2; ++b) {
+        mbar_init(saddr(&bs.afull[b]), 1u);
+        mbar_init(saddr(&bs.aempty[b]), 4u);
+    }
     fence_mbar_init();
+}
+
+// ---- phase B of the phased form: loader, MMA thread and epilogue as separate roles -------------
+// The loader (thread 128) takes units from the dispenser, names each in the unit ring and streams
+// its operand tiles into the stage ring.  The MMA thread (thread 256: warp 8, which draws no noise)
+// issues a unit's MMAs as its tiles land, into accumulator buffer (its count) mod 2.  The epilogue
+// warps 0-3 drain the buffers in the same order.  So the loader's copies, the MMA issue and the
+// drain of the previous unit overlap, instead of one thread doing the first two in turn.  Each
+// role keeps its own counters, carried across steps: the u-th fill of a ring slot or stage is
+// phase u of its barriers.
+struct SplitState {
+    uint32_t units = 0;  // units named (loader) or taken from the ring (MMA thread, epilogue)
+    uint32_t stage = 0;  // the next stage, and how many times it was used before
+    uint32_t use = 0;
+    uint32_t accs = 0;   // accumulators filled (MMA thread) or drained (epilogue)
+    uint32_t tiles = 0;  // k-tiles loaded (loader)
+};
+constexpr uint32_t kNoUnit = 0xFFFFFFFFu;
+
+// The loader for one step: every processed unit is followed by exactly one take (units grid,
+// grid + 1, ... after CTA b's first unit b), so a step makes n_units takes from t * n_units.
+__device__ __forceinline__ bool split_loader(const BSim* S, BatchSmem& bs, const BClass* s_cls, SplitState& L,
+                                             unsigned long long t, uint32_t smem_base, uint32_t stage_bytes,
+                                             uint32_t n_stages, uint64_t keep) {
+    const uint32_t n_units = S->n_units;
+    const unsigned long long take0 = t * n_units;
+    bool good = true;
+    uint32_t ui = blockIdx.x;
+    for (;;) {
+        const uint32_t slot = L.units % kUnitRing;
+        if (L.units >= kUnitRing && !mbar_wait(saddr(&bs.uempty[slot]), ((L.units / kUnitRing) - 1u) & 1u)) good = false;
+        const bool none = ui >= n_units || !good || bs.ok == 0u;
+        bs.uid[slot] = none ? kNoUnit : ui;
+        mbar_arrive(saddr(&bs.ufull[slot]));
+        ++L.units;
+        if (none) break;
+        const BUnit U = S->units[ui];
+        const BClass& C = s_cls[U.cls];
+        const uint32_t b_bytes = 2u * C.NP * 128u, nk = U.k1 - U.k0;
+        const unsigned char* a_src = reinterpret_cast<const unsigned char*>(C.A[U.side]) +
+                                     (static_cast<size_t>(U.mt) * C.KT[U.side] + U.k0) * kATileBytes;
+        const unsigned char* b_src =
+            reinterpret_cast<const unsigned char*>(C.X[U.side]) + static_cast<size_t>(U.k0) * b_bytes;
+        for (uint32_t i = 0; i < nk; ++i) {
+            // the stage's previous tiles have been read by their MMAs
+            if (L.use > 0u && !mbar_wait(saddr(&bs.empty[L.stage]), (L.use - 1u) & 1u)) {
+                good = false;
+                break;
+            }
+            const uint32_t bar = saddr(&bs.full[L.stage]), dst = smem_base + L.stage * stage_bytes;
+            mbar_expect_tx(bar, kATileBytes + b_bytes);
+            bulk_load_keep(dst, a_src + static_cast<size_t>(i) * kATileBytes, kATileBytes, bar, keep);
+            bulk_load(dst + kATileBytes, b_src + static_cast<size_t>(i) * b_bytes, b_bytes, bar);
+            ++L.tiles;
+            if (++L.stage == n_stages) {
+                L.stage = 0;
+                ++L.use;
+            }
+        }
+        ui = gridDim.x + static_cast<uint32_t>(atomicAdd(S->unit_ctr, 1ull) - take0);
+    }
+    return good;
+}
+
+// The MMA thread for one step.  Descriptors: the stage's A and B base descriptors plus the K
+// step's offset in the start-address field (shared-memory addresses stay below 256 KB).
+__device__ __forceinline__ bool split_mma(const BSim* S, BatchSmem& bs, const BClass* s_cls, SplitState& M,
+                                          uint32_t tmem, uint32_t smem_base, uint32_t stage_bytes, uint32_t n_stages) {
+    bool good = true;
+    for (;;) {
+        const uint32_t slot = M.units % kUnitRing;
+        if (!mbar_wait(saddr(&bs.ufull[slot]), (M.units / kUnitRing) & 1u)) return false;
+        const uint32_t ui = bs.uid[slot];
+        ++M.units;
+        if (ui == kNoUnit) {
+            mbar_arrive(saddr(&bs.uempty[slot]));
+            break;
+        }
+        const BUnit U = S->units[ui];
+        const BClass& C = s_cls[U.cls];
+        const uint32_t N = 2u * C.NP, nk = U.k1 - U.k0, idesc = idesc_bf16_m128(N);
+        const uint32_t buf = M.accs & 1u, fill = M.accs >> 1;
+        // the epilogue has read this buffer's previous unit
+        if (fill > 0u && !mbar_wait(saddr(&bs.aempty[buf]), (fill - 1u) & 1u)) good = false;
+        tc_fence_after();
+        const uint32_t d = tmem + buf * kAccCols;
+        const uint64_t a0 = smem_desc(smem_base, 2048u, 128u), b0 = smem_desc(smem_base + kATileBytes, N * 16u, 128u);
+        for (uint32_t i = 0; i < nk && good; ++i) {
+            if (!mbar_wait(saddr(&bs.full[M.stage]), M.use & 1u)) {
+                good = false;
+                break;
+            }
+            tc_fence_after();
+            const uint64_t so = (static_cast<uint64_t>(M.stage) * stage_bytes) >> 4;
+#pragma unroll
+            for (uint32_t ks = 0; ks < 4; ++ks)
+                tc_mma_bf16(d, a0 + so + ks * 256u, b0 + so + ks * (2u * N), idesc, (i | ks) != 0u);
+            tc_commit(saddr(&bs.empty[M.stage]));
+            if (++M.stage == n_stages) {
+                M.stage = 0;
+                ++M.use;
+            }
+        }
+        tc_commit(saddr(&bs.afull[buf]));  // also after a timeout, to release the epilogue
+        ++M.accs;
+        mbar_arrive(saddr(&bs.uempty[slot]));
+        if (!good) break;
+    }
+    return good;
+}
+
+// The epilogue warps 0-3 for one step (warp w drains accumulator lanes 32w .. 32w + 31).  Every
+// wait's outcome is made uniform over the warp before the warp-wide tensor-memory loads.
+__device__ __forceinline__ bool split_epilogue(const BSim* S, BatchSmem& bs, const BClass* s_cls, SplitState& E,
+                                               uint32_t tmem, uint32_t warp, uint32_t lane) {
+    const uint32_t row = 32u * warp + lane;
+    bool good = true;
+    for (;;) {
+        const uint32_t slot = E.units % kUnitRing;
+        if (!__all_sync(kFull, mbar_wait(saddr(&bs.ufull[slot]), (E.units / kUnitRing) & 1u))) return false;
+        const uint32_t ui = bs.uid[slot];
+        ++E.units;
+        if (ui == kNoUnit) {
+            if (lane == 0) mbar_arrive(saddr(&bs.uempty[slot]));
+            break;
+        }
+        const BUnit U = S->units[ui];
+        const BClass& C = s_cls[U.cls];
+        const uint32_t buf = E.accs & 1u, fill = E.accs >> 1;
+        if (!__all_sync(kFull, mbar_wait(saddr(&bs.afull[buf]), fill & 1u))) good = false;
+        ++E.accs;
+        tc_fence_after();
+        const uint32_t base = tmem + ((32u * warp) << 16) + buf * kAccCols;
+        float* part = S->partials + U.part;
+        for (uint32_t c0 = 0; c0 < C.NP; c0 += 16u) {
+            float hi[16], lo[16];
+            tmem_ld16(base + c0, hi);
+            tmem_ld16(base + C.NP + c0, lo);
+#pragma unroll
+            for (uint32_t q = 0; q < 16; ++q)
+                if (c0 + q < C.n_inst) part[static_cast<size_t>(c0 + q) * 128u + row] = hi[q] + lo[q];
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) {
+            mbar_arrive(saddr(&bs.aempty[buf]));
+            mbar_arrive(saddr(&bs.uempty[slot]));
+        }
+        if (!good) break;
+    }
+    return good;
+}
+
+// After a timeout: the loader waits (each wait bounded) for its last copies and the MMA thread for
+// its last MMAs, so that none is in flight when the CTA frees its tensor memory and exits.
+__device__ __forceinline__ void split_quiesce(BatchSmem& bs, const SplitState& L, const SplitState& M, bool loader,
+                                              uint32_t n_stages) {
+    if (loader) {
+        for (uint32_t j = 1; j <= n_stages && j <= L.tiles; ++j) {
+            const uint32_t q = L.tiles - j;
+            mbar_wait(saddr(&bs.full[q % n_stages]), (q / n_stages) & 1u);
+        }
+    } else if (M.accs > 0u) {
+        mbar_wait(saddr(&bs.afull[(M.accs - 1u) & 1u]), ((M.accs - 1u) >> 1) & 1u);
+    }
 }
 
 template <bool SMEM_STATE>
@@ -682,10 +857,8 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
     const uint32_t tmem = bs.tmem;
     const unsigned long long bar0 = s_bar0, t0 = s_t0;
     const uint32_t n_units = S->n_units;
-    ProducerState ps;              // the producer's ring state
-    uint32_t accum_ph = 0;         // the epilogue's accumulator phase
-    uint32_t ready_slot = 0, ready_ph = 0;  // the unit ring (producer and epilogue alike)
-    const bool producer = tid == 128u;  // warp 4: loads and MMAs; warps 0-3: the epilogue
+    // phase B roles: thread 128 the loader, thread 256 the MMA thread, warps 0-3 the epilogue
+    SplitState ls, ms, es;
     bool ok = true;
 #ifdef BSNN_PHASE_TIMING
     __shared__ unsigned long long s_tally_[8];
@@ -709,45 +882,21 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
             break;
         }
         BSNN_TMARK(1);
-        if (producer) {
+        if (tid == 128u) {
             fence_proxy_async_global();
-            const uint64_t keep = l2_evict_last_policy();
-            // Units are sorted longest first.  CTA b starts with unit b; after issuing a unit's MMAs
-            // it takes the next from a dispenser shared by all CTAs (units grid, grid + 1, ...), so
-            // the CTAs that finish early do the rest.  Every processed unit is followed by exactly
-            // one take, so a clock step makes n_units takes, numbered from t * n_units.
-            const unsigned long long take0 = t * n_units;
-            auto take = [&]() { return gridDim.x + static_cast<uint32_t>(atomicAdd(S->unit_ctr, 1ull) - take0); };
-            uint32_t ui = blockIdx.x;
-            for (;;) {
-                const bool none = ui >= n_units;
-                bs.unit[ready_slot] = none ? 0xFFFFFFFFu : ui;
-                mbar_arrive(saddr(&bs.ready[ready_slot]));
-                ready_slot ^= 1u;
-                if (none) break;
-                const BUnit U = S->units[ui];
-                if (bs.ok == 0u) {  // after a timeout: only release the epilogue
-                    tc_commit(saddr(&bs.accum));
-                } else if (!issue_unit(bs, ps, U, s_cls[U.cls], tmem, smem_base, stage_bytes, n_stages, keep)) {
-                    atomicExch(S->error, kErrStageTimeout);
-                    bs.ok = 0u;
-                }
-                ui = take();
+            if (!split_loader(S, bs, s_cls, ls, t, smem_base, stage_bytes, n_stages, l2_evict_last_policy())) {
+                atomicExch(S->error, kErrStageTimeout);
+                bs.ok = 0u;
+            }
+        } else if (tid == 256u) {
+            if (!split_mma(S, bs, s_cls, ms, tmem, smem_base, stage_bytes, n_stages)) {
+                atomicExch(S->error, kErrStageTimeout);
+                bs.ok = 0u;
             }
         } else if (warp < 4) {
-            for (;;) {
-                // the unit the producer took (or the end of the step's units)
-                if (!mbar_wait(saddr(&bs.ready[ready_slot]), (ready_ph >> ready_slot) & 1u)) {
-                    atomicExch(S->error, kErrStageTimeout);
-                    bs.ok = 0u;
-                    break;
-                }
-                ready_ph ^= 1u << ready_slot;
-                const uint32_t ui = bs.unit[ready_slot];
-                ready_slot ^= 1u;
-                if (ui == 0xFFFFFFFFu) break;
-                const BUnit U = S->units[ui];
-                drain_unit(S, bs, U, s_cls[U.cls], tmem, accum_ph, warp, lane);
+            if (!split_epilogue(S, bs, s_cls, es, tmem, warp, lane)) {
+                atomicExch(S->error, kErrStageTimeout);
+                bs.ok = 0u;
             }
         } else if (noise_warp(warp) && S->noise_on && k + 1u < n_steps) {
             noise_ahead(S, P, s_cls, s_nz, n0, n1, t + 1ull, 32u * noise_rank(warp) + lane, 32u * kNoiseWarps);
@@ -766,7 +915,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
     if (tid == 0)
         for (int i = 0; i < 8; ++i) S->phase_ns[blockIdx.x * 8u + i] += s_tally_[i];
 #endif
-    if (producer && bs.ok == 0u) producer_quiesce(bs, ps, n_stages);
+    if ((tid == 128u || tid == 256u) && bs.ok == 0u) split_quiesce(bs, ls, ms, tid == 128u, n_stages);
     tc_fence_before();
     __syncthreads();
     if constexpr (SMEM_STATE) state_copy(S, X, n0, n1, false);
@@ -947,7 +1096,9 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_flow_kernel(const
         // so it is bounded by twice the limit
         uint32_t accum_ph = 0, ready_slot = 0, ready_ph = 0;
         for (;;) {
-            if (!mbar_wait_for(saddr(&bs.ready[ready_slot]), (ready_ph >> ready_slot) & 1u, 2ull * s_wait_limit_ns)) {
+            // (made uniform over the warp before its warp-wide tensor-memory loads)
+            if (!__all_sync(kFull, mbar_wait_for(saddr(&bs.ready[ready_slot]), (ready_ph >> ready_slot) & 1u,
+                                                 2ull * s_wait_limit_ns))) {
                 atomicExch(S->error, kErrStageTimeout);
                 bs.ok = 0u;
                 break;
