@@ -206,13 +206,11 @@ __host__ __device__ __forceinline__ uint32_t core_offset(uint32_t rows, uint32_t
 __device__ __forceinline__ uint16_t bf16_bits_rn(float v) { return __bfloat16_as_ushort(__float2bfloat16_rn(v)); }
 
 // ---- phase A ------------------------------------------------------------------------------------
-// Each CTA takes a contiguous range of neurons, BSNN_BATCH_NEURONS_IN_FLIGHT per thread at a time:
-// all loads of those are issued before any is computed.  With the state in shared memory only
-// the partial sums come from L2, and one at a time measured fastest on B200 (38.5 us per clock
-// step for 192 networks, against 40.0 with two, 44.8 with four and 53.3 with eight in flight:
-// the extra registers cost more than the latency they hide).  An instance is
-// found by walking the instance table from the thread's previous neuron (neurons only move
-// forward).
+// Each CTA takes a contiguous range of neurons, one neuron per thread at a time, instance by
+// instance: a range covers a few instances, and each instance's lookups (groups, B-operand row,
+// partial-sum offsets, trace constants) are done once for its segment, not per neuron.  The
+// phase is bound by instruction issue at 16 warps per SM: two neurons in flight per thread, or
+// gathering the partial sums with many loads in flight first, measured slower or no faster.
 
 // The state a CTA steps: shared-memory arrays indexed by n - base (base = the CTA's first
 // neuron), or the global arrays (base = 0).  Spikes are bytes in shared memory, words in global.
@@ -222,13 +220,6 @@ struct BState {
     uint8_t* spike8;
     uint32_t* spike32;
     uint32_t base;
-};
-
-struct NeuronIn {
-    uint32_t n, inst;
-    bool valid;
-    float v, dge, dgi, istim, er, ed, ir, id, tr, td;
-    uint32_t refrac;
 };
 
 template <bool SMEM>
@@ -252,66 +243,85 @@ __device__ __forceinline__ uint32_t instance_of(const BInst* P, uint32_t n_inst,
     return lo;
 }
 
-// `cur`: the instance of this thread's previous neuron.
-template <bool SMEM>
-__device__ __forceinline__ void neuron_load(const BSim* S, const BInst* P, const BClass* s_cls, const BState& X,
-                                            uint32_t n, bool valid, unsigned long long t, uint32_t& cur, NeuronIn& a) {
-    a.n = n;
-    a.valid = valid;
-    if (!valid) return;
-    while (cur + 1u < S->n_inst && P[cur + 1u].nbase <= n) ++cur;
-    a.inst = cur;
-    const uint32_t i = n - X.base;
-    a.v = st_ld<SMEM>(X.v + i);
-    a.istim = st_ld<SMEM>(X.istim + i);
-    a.er = st_ld<SMEM>(X.er + i);
-    a.ed = st_ld<SMEM>(X.ed + i);
-    a.ir = st_ld<SMEM>(X.ir + i);
-    a.id = st_ld<SMEM>(X.id + i);
-    a.tr = st_ld<SMEM>(X.tr + i);
-    a.td = st_ld<SMEM>(X.td + i);
-    a.refrac = st_ld<SMEM>(X.refrac + i);
-    a.dge = 0.0f;
-    a.dgi = 0.0f;
-    if (t > 0) {  // the previous step's propagation, K chunks in order
-        const BInst& B = P[a.inst];
-        const BClass& C = s_cls[B.cls];
-        const uint32_t j = n - B.nbase, stride = C.NP * 128u;
-        const size_t tile = static_cast<size_t>(j >> 7), r = static_cast<size_t>(B.row) * 128u + (j & 127u);
-        const float* pe = S->partials + C.pbase[0] + tile * C.nkc[0] * stride + r;
-        const float* pi = S->partials + C.pbase[1] + tile * C.nkc[1] * stride + r;
-        for (uint32_t kc = 0; kc < C.nkc[0]; ++kc) a.dge += __ldcg(pe + kc * stride);
-        for (uint32_t kc = 0; kc < C.nkc[1]; ++kc) a.dgi += __ldcg(pi + kc * stride);
-    }
+// One instance's share of a CTA's neurons, with what every neuron of it needs, looked up once:
+// its groups, its row in the class's B operand, the offsets of its partial sums and the class's
+// connection traces.
+struct SegCtx {
+    const BGroupP* g;        // the instance's E and I groups (g[0], g[1])
+    uint32_t nbase, E, id, NP, row;
+    uint32_t pe, pi;         // float offsets of the partial sums of (side, post tile 0, chunk 0, row)
+    uint32_t te, ti;         // floats per post tile of each side (nkc * NP * 128)
+    uint32_t nkc0, nkc1, stride;
+    uint16_t *X0, *X1;
+    float r0, r1, d0, d1, m0, m1;  // connection trace decays and normalisation, by side
+};
+
+__device__ __forceinline__ SegCtx seg_ctx(const BInst& B, const BClass& C) {
+    SegCtx c;
+    c.g = B.g;
+    c.nbase = B.nbase;
+    c.E = C.E;
+    c.id = B.id;
+    c.NP = C.NP;
+    c.row = B.row;
+    c.stride = C.NP * 128u;
+    c.pe = static_cast<uint32_t>(C.pbase[0]) + B.row * 128u;
+    c.pi = static_cast<uint32_t>(C.pbase[1]) + B.row * 128u;
+    c.nkc0 = C.nkc[0];
+    c.nkc1 = C.nkc[1];
+    c.te = C.nkc[0] * c.stride;
+    c.ti = C.nkc[1] * c.stride;
+    c.X0 = C.X[0];
+    c.X1 = C.X[1];
+    c.r0 = C.r_decay[0];
+    c.r1 = C.r_decay[1];
+    c.d0 = C.d_decay[0];
+    c.d1 = C.d_decay[1];
+    c.m0 = C.norm[0];
+    c.m1 = C.norm[1];
+    return c;
 }
 
+// One neuron's step (n: its index, i = n - X.base its state index): g = the background of the
+// previous step (recomputed from its traces) + the previous step's propagation (K chunks in
+// order), background Poisson shot noise, the conductance-EIF Euler step, the step's stimulus
+// events, the connection traces, and x = d - r as BF16 hi / lo into the B operand.
 template <bool SMEM>
-__device__ __forceinline__ void neuron_step(const BSim* S, const BInst* P, const BClass* s_cls, const BState& X,
-                                            const uint16_t* nz, uint32_t n0, unsigned long long t, const NeuronIn& a) {
-    if (!a.valid) return;
-    const uint32_t n = a.n, i = n - X.base;
-    const BInst& B = P[a.inst];
-    const BClass& C = s_cls[B.cls];
-    const uint32_t j = n - B.nbase;  // index in the instance
-    const uint32_t side = j < C.E ? 0u : 1u;
-    const BGroupP& G = B.g[side];
-    const uint32_t loc = j - (side ? C.E : 0u);
+__device__ __forceinline__ void neuron_step(const BSim* S, const SegCtx& c, const BState& X, const uint16_t* nz,
+                                            uint32_t n0, uint32_t n, unsigned long long t) {
+    const uint32_t i = n - X.base;
+    const uint32_t j = n - c.nbase;  // index in the instance
+    const uint32_t side = j < c.E ? 0u : 1u;
+    const BGroupP& G = c.g[side];
+    const uint32_t loc = j - (side ? c.E : 0u);
+    float dge = 0.0f, dgi = 0.0f;
+    if (t > 0) {  // the previous step's propagation, K chunks in order
+        const float* pe = S->partials + c.pe + (j >> 7) * c.te + (j & 127u);
+        const float* pi = S->partials + c.pi + (j >> 7) * c.ti + (j & 127u);
+        for (uint32_t kc = 0; kc < c.nkc0; ++kc) dge += __ldcg(pe + kc * c.stride);
+        for (uint32_t kc = 0; kc < c.nkc1; ++kc) dgi += __ldcg(pi + kc * c.stride);
+    }
+    const float a_v = st_ld<SMEM>(X.v + i), a_istim = st_ld<SMEM>(X.istim + i);
+    const float a_er = st_ld<SMEM>(X.er + i), a_ed = st_ld<SMEM>(X.ed + i);
+    const float a_ir = st_ld<SMEM>(X.ir + i), a_id = st_ld<SMEM>(X.id + i);
+    const float a_tr = st_ld<SMEM>(X.tr + i), a_td = st_ld<SMEM>(X.td + i);
+    const uint32_t a_refrac = st_ld<SMEM>(X.refrac + i);
     // g = the background of the previous step (recomputed from its traces) + its propagation
-    float ge_used = (a.ed - a.er) * G.bg_scale_e, gi_used = (a.id - a.ir) * G.bg_scale_i;
+    float ge_used = (a_ed - a_er) * G.bg_scale_e, gi_used = (a_id - a_ir) * G.bg_scale_i;
     if (t > 0) {
-        ge_used = ge_used + a.dge;
-        gi_used = gi_used + a.dgi;
+        ge_used = ge_used + dge;
+        gi_used = gi_used + dgi;
     }
 
-    float er = flush_tiny(a.er * G.bg_er_decay);
-    float ir = flush_tiny(a.ir * G.bg_ir_decay);
-    float ed = flush_tiny(a.ed * G.bg_ed_decay);
-    float id = flush_tiny(a.id * G.bg_id_decay);
+    float er = flush_tiny(a_er * G.bg_er_decay);
+    float ir = flush_tiny(a_ir * G.bg_ir_decay);
+    float ed = flush_tiny(a_ed * G.bg_ed_decay);
+    float id = flush_tiny(a_id * G.bg_id_decay);
     uint32_t ne = 0, ni = 0;
     if (S->noise_on) {
-        const uint32_t c = nz[n - n0];
-        ne = c & 0xFFu;
-        ni = c >> 8;
+        const uint32_t cnt = nz[n - n0];
+        ne = cnt & 0xFFu;
+        ni = cnt >> 8;
     }
     if (ne > 0u) {
         const float inc = static_cast<float>(ne);
@@ -324,8 +334,8 @@ __device__ __forceinline__ void neuron_step(const BSim* S, const BInst* P, const
         id += inc;
     }
 
-    float v = a.v, istim = a.istim;
-    uint32_t refrac = a.refrac, spike = 0;
+    float v = a_v, istim = a_istim;
+    uint32_t refrac = a_refrac, spike = 0;
     if (refrac > 0) {
         --refrac;
         v = G.v_reset;
@@ -353,7 +363,7 @@ __device__ __forceinline__ void neuron_step(const BSim* S, const BInst* P, const
     X.refrac[i] = refrac;
     if constexpr (SMEM) X.spike8[i] = static_cast<uint8_t>(spike);
     else X.spike32[i] = spike;
-    if (spike) atomicAdd(S->spike_counts + 2u * B.id + side, 1ull);
+    if (spike) atomicAdd(S->spike_counts + 2u * c.id + side, 1ull);
 
     // stimulus events of this step act from the next step
     if (t < S->stim_len) {
@@ -373,41 +383,39 @@ __device__ __forceinline__ void neuron_step(const BSim* S, const BInst* P, const
     }
 
     // connection traces of the neuron's presynaptic side, and x as BF16 hi / lo in B
-    float d = flush_tiny(a.td * C.d_decay[side]);
-    float r = flush_tiny(a.tr * C.r_decay[side]);
+    float d = flush_tiny(a_td * (side ? c.d1 : c.d0));
+    float r = flush_tiny(a_tr * (side ? c.r1 : c.r0));
     if (spike == 1) {
-        r += C.norm[side];
-        d += C.norm[side];
+        const float m = side ? c.m1 : c.m0;
+        r += m;
+        d += m;
     }
     X.tr[i] = r;
     X.td[i] = d;
     const float x = d - r;
-    const uint16_t hi = bf16_bits_rn(x);
-    const float lo_f = x - __uint_as_float(static_cast<uint32_t>(hi) << 16);
-    const uint16_t lo = bf16_bits_rn(lo_f);
-    uint16_t* Xt = C.X[side] + static_cast<size_t>(loc >> 6) * (2u * C.NP * 64u);
-    Xt[core_offset(2u * C.NP, B.row, loc & 63u)] = hi;
-    Xt[core_offset(2u * C.NP, C.NP + B.row, loc & 63u)] = lo;
+    const uint16_t xhi = bf16_bits_rn(x);
+    const float lo_f = x - __uint_as_float(static_cast<uint32_t>(xhi) << 16);
+    const uint16_t xlo = bf16_bits_rn(lo_f);
+    uint16_t* Xt = (side ? c.X1 : c.X0) + static_cast<size_t>(loc >> 6) * (2u * c.NP * 64u);
+    Xt[core_offset(2u * c.NP, c.row, loc & 63u)] = xhi;
+    Xt[core_offset(2u * c.NP, c.NP + c.row, loc & 63u)] = xlo;
 }
 
-#ifndef BSNN_BATCH_NEURONS_IN_FLIGHT
-#define BSNN_BATCH_NEURONS_IN_FLIGHT 1
-#endif
-constexpr uint32_t kNeuronsInFlight = BSNN_BATCH_NEURONS_IN_FLIGHT;
-
-// Neurons [n0, n1), by `count` threads of the CTA, this one being number `me`.
+// Neurons [n0, n1), by `count` threads of the CTA, this one being number `me`: instance by
+// instance (a CTA's range covers a few), the instance's lookups done once per segment.
 template <bool SMEM>
 __device__ __forceinline__ void batch_neurons(const BSim* S, const BInst* P, const BClass* s_cls, const BState& X,
                                               const uint16_t* nz, uint32_t n0, uint32_t n1, unsigned long long t,
                                               uint32_t me, uint32_t count) {
-    uint32_t cur = instance_of(P, S->n_inst, n0 + me < n1 ? n0 + me : n0);
-    for (uint32_t n = n0 + me; n < n1; n += kNeuronsInFlight * count) {
-        NeuronIn a[kNeuronsInFlight];
-#pragma unroll
-        for (uint32_t q = 0; q < kNeuronsInFlight; ++q)
-            neuron_load<SMEM>(S, P, s_cls, X, n + q * count, n + q * count < n1, t, cur, a[q]);
-#pragma unroll
-        for (uint32_t q = 0; q < kNeuronsInFlight; ++q) neuron_step<SMEM>(S, P, s_cls, X, nz, n0, t, a[q]);
+    if (n0 >= n1) return;
+    uint32_t inst = instance_of(P, S->n_inst, n0);
+    for (uint32_t seg0 = n0; seg0 < n1; ++inst) {
+        const BInst& B = P[inst];
+        const BClass& C = s_cls[B.cls];
+        const uint32_t seg1 = min(n1, B.nbase + C.N);
+        const SegCtx c = seg_ctx(B, C);
+        for (uint32_t n = seg0 + me; n < seg1; n += count) neuron_step<SMEM>(S, c, X, nz, n0, n, t);
+        seg0 = seg1;
     }
 }
 
