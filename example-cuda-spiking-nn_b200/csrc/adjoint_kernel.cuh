@@ -452,11 +452,14 @@ __global__ void __launch_bounds__(kAdjBwdThreads, 1) bsnn_adj_backward_kernel(AD
         }
         if (k > 0u) cur = fetch(k - 1u);
         if (!grid_barrier(B.barrier, B.error, bar0 + (kk + 1ull) * gridDim.x, &s_ok)) break;
-        // every neuron's lambda_g of step t (written by other CTAs: read from L2)
-        for (uint32_t q = tid; q < ld / 4u; q += blockDim.x) {
-            reinterpret_cast<float4*>(s_lge)[q] = __ldcg(reinterpret_cast<const float4*>(lge_row) + q);
-            reinterpret_cast<float4*>(s_lgi)[q] = __ldcg(reinterpret_cast<const float4*>(lgi_buf) + q);
-        }
+        // every neuron's lambda_g of step t (written by other CTAs: read from L2); only the side the
+        // own rows pull back through (rows < E: lambda_ge, the others lambda_gi)
+        if (n0 < A.E)
+            for (uint32_t q = tid; q < ld / 4u; q += blockDim.x)
+                reinterpret_cast<float4*>(s_lge)[q] = __ldcg(reinterpret_cast<const float4*>(lge_row) + q);
+        if (n1 > A.E)
+            for (uint32_t q = tid; q < ld / 4u; q += blockDim.x)
+                reinterpret_cast<float4*>(s_lgi)[q] = __ldcg(reinterpret_cast<const float4*>(lgi_buf) + q);
         __syncthreads();
         {
             const uint32_t n4 = ld / 4u, cq = (n4 + kPbChunks - 1u) / kPbChunks, n_str = own - n_res;
