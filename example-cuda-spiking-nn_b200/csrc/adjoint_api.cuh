@@ -119,15 +119,33 @@ AdjGroupP adj_group(const bsnn_neuron_group_params& p) {
 
 // One forward step t: the neuron update (tape rows where the pointers are set; the step's E spike
 // count and voltage sums in the forward pass), then the propagation of x_{t+1}.
+// Both kernels are launched with programmatic dependent launch: each may launch while its
+// predecessor finishes, and waits for it (pdl_enter) before reading anything, which hides the
+// launch gap between the two kernels of a step and between steps.
 void adj_step(bsnn_adjoint* a, uint32_t t, size_t tape_row, bool tape, float* x_next, bool forward) {
     const uint32_t N = a->h.N;
     const dim3 pg((N + kAdjBlock - 1) / kAdjBlock, 2 * kAdjChunks);
-    bsnn_adj_neuron_fwd<<<a->nb, kAdjBlock, 0, a->stream>>>(
-        a->h, t, a->part, tape ? a->tv + tape_row : nullptr, tape ? a->tu + tape_row : nullptr,
-        tape ? a->tge + tape_row : nullptr, tape ? a->tgi + tape_row : nullptr, tape ? a->ts + tape_row : nullptr,
-        tape ? a->tref + tape_row : nullptr, x_next, forward ? a->counts + t : nullptr,
-        forward ? a->vsum + static_cast<size_t>(t) * a->nb : nullptr);
-    bsnn_adj_propagate<<<pg, kAdjBlock, 0, a->stream>>>(a->WE, a->WI, a->h.E, a->h.I, N, a->ld, x_next, a->part);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg{};
+    cfg.blockDim = dim3(kAdjBlock);
+    cfg.stream = a->stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cfg.gridDim = dim3(a->nb);
+    cuda_check(cudaLaunchKernelEx(&cfg, bsnn_adj_neuron_fwd, a->h, t, static_cast<const float*>(a->part),
+                                  tape ? a->tv + tape_row : nullptr, tape ? a->tu + tape_row : nullptr,
+                                  tape ? a->tge + tape_row : nullptr, tape ? a->tgi + tape_row : nullptr,
+                                  tape ? a->ts + tape_row : nullptr, tape ? a->tref + tape_row : nullptr, x_next,
+                                  forward ? a->counts + t : nullptr,
+                                  forward ? a->vsum + static_cast<size_t>(t) * a->nb : nullptr),
+               "adjoint neuron launch");
+    cfg.gridDim = pg;
+    cuda_check(cudaLaunchKernelEx(&cfg, bsnn_adj_propagate, static_cast<const float*>(a->WE),
+                                  static_cast<const float*>(a->WI), a->h.E, a->h.I, N, a->ld,
+                                  static_cast<const float*>(x_next), a->part),
+               "adjoint propagate launch");
 }
 
 // The last segment's steps from its restored checkpoint, keeping the tape (x_t in tape row k of

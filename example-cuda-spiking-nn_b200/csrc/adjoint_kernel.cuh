@@ -54,6 +54,14 @@ struct ADev {
 constexpr uint32_t kAdjChunks = 16;
 constexpr uint32_t kAdjBlock = 256;
 
+// Programmatic dependent launch (the forward pass's per-step kernels are launched with it): let the
+// next kernel in the stream launch now, then wait until the previous one has completed and its
+// writes are visible, before reading anything.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 __device__ __forceinline__ float adj_chunk_sum(const float* part, uint32_t side, uint32_t chunks, uint32_t N,
                                                uint32_t n) {
     float s = 0.0f;
@@ -70,6 +78,7 @@ __global__ void __launch_bounds__(kAdjBlock) bsnn_adj_neuron_fwd(ADev A, uint32_
                                                                  float* tape_gi, uint8_t* tape_s, uint8_t* tape_ref,
                                                                  float* x_next, uint32_t* e_spike_count,
                                                                  double* vsum_out) {
+    pdl_enter();
     const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
     double vpart = 0.0;
     if (n < A.N) {
@@ -176,6 +185,7 @@ __global__ void __launch_bounds__(kAdjBlock) bsnn_adj_propagate(const float* __r
                                                                 const float* __restrict__ WI, uint32_t E, uint32_t I,
                                                                 uint32_t N, uint32_t ld, const float* __restrict__ x,
                                                                 float* __restrict__ part) {
+    pdl_enter();
     __shared__ uint32_t srow[kAdjBlock];
     __shared__ float sx[kAdjBlock];
     __shared__ uint32_t wcount[kAdjBlock / 32];
