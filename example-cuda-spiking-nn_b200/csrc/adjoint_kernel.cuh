@@ -22,6 +22,7 @@
 // the segment's steps.  All arithmetic is FP32.
 #pragma once
 
+#include "batch_kernel.cuh"  // tensor-memory wrappers
 #include "step_kernel.cuh"
 
 namespace bsnn {
@@ -363,6 +364,13 @@ struct AdjBwd {
     float beta;
 };
 constexpr uint32_t kAdjBwdThreads = 512;
+constexpr uint32_t kAdjTmemCols = 256;  // tensor memory of the backward kernel: W rows shared memory cannot hold
+
+// One 32-bit column of this thread's tensor-memory lane.
+__device__ __forceinline__ void tmem_st1(uint32_t taddr, float v) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x1.b32 [%0], {%1};" ::"r"(taddr), "r"(__float_as_uint(v)) : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 constexpr uint32_t kPbChunks = 4;
 
 // One warp: the piece [q0, q1) (in float4 units) of row `row` (ld floats) times lambda.
@@ -391,6 +399,7 @@ __global__ void __launch_bounds__(kAdjBwdThreads, 1) bsnn_adj_backward_kernel(AD
     __shared__ int s_ok;
     __shared__ unsigned long long s_bar0;
     __shared__ double s_red[kAdjBwdThreads / 32];
+    __shared__ uint32_t s_tmem;
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u, nwarps = blockDim.x >> 5;
     const uint32_t N = A.N, ld = B.ld;
     const uint32_t n0 = static_cast<uint32_t>(static_cast<unsigned long long>(blockIdx.x) * N / gridDim.x);
@@ -412,6 +421,31 @@ __global__ void __launch_bounds__(kAdjBwdThreads, 1) bsnn_adj_backward_kernel(AD
         for (uint32_t q = tid; q < ld / 4u; q += blockDim.x)
             reinterpret_cast<float4*>(s_w + static_cast<size_t>(r) * ld)[q] = __ldg(src + q);
     }
+    // Own rows n_res .. n_res + n_tm - 1 in tensor memory: element e of streamed row sr at lane
+    // e mod 128, column sr * cpr + e / 128 (zero past ld).  Warp w reaches lanes 32 (w mod 4) ...
+    // (a row spans cpr <= 32 columns, read as two 16-column loads that stay inside the allocation)
+    const uint32_t cpr = (ld + 127u) / 128u, n_str = own - n_res;
+    const uint32_t tm_max = cpr <= 32u ? (kAdjTmemCols - 32u) / cpr + 1u : 0u;
+    const uint32_t n_tm = n_str < tm_max ? n_str : tm_max;
+    if (warp == 0) {
+        tmem_alloc(saddr(&s_tmem), kAdjTmemCols);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    if (warp < 4u) {
+        for (uint32_t sr = 0; sr < n_tm; ++sr) {
+            const uint32_t pre = n0 + n_res + sr;
+            const float* src = pre < A.E ? A.WE + static_cast<size_t>(pre) * ld : A.WI + static_cast<size_t>(pre - A.E) * ld;
+            for (uint32_t c = 0; c < cpr; ++c) {
+                const uint32_t e = c * 128u + 32u * warp + lane;
+                tmem_st1(tmem + ((32u * warp) << 16) + sr * cpr + c, e < ld ? __ldg(src + e) : 0.0f);
+            }
+        }
+        tmem_wait_st();
+    }
     if (tid == 0) {
         s_wait_limit_ns = B.wait_limit_ns;
         s_bar0 = ld_acquire_u64(B.barrier) / gridDim.x * gridDim.x;
@@ -422,7 +456,9 @@ __global__ void __launch_bounds__(kAdjBwdThreads, 1) bsnn_adj_backward_kernel(AD
         s_lr[i] = B.lam_r[n0 + i];
         s_lx[i] = B.lam_x[n0 + i];
     }
+    tc_fence_before();
     __syncthreads();
+    tc_fence_after();
     const unsigned long long bar0 = s_bar0;
     double gl = 0.0;
     // Thread i steps own neuron i (own <= blockDim.x).  Its tape row and the loss sensitivities of
@@ -472,10 +508,29 @@ __global__ void __launch_bounds__(kAdjBwdThreads, 1) bsnn_adj_backward_kernel(AD
                 reinterpret_cast<float4*>(s_lgi)[q] = __ldcg(reinterpret_cast<const float4*>(lgi_buf) + q);
         __syncthreads();
         {
-            const uint32_t n4 = ld / 4u, cq = (n4 + kPbChunks - 1u) / kPbChunks, n_str = own - n_res;
-            for (uint32_t p = warp; p < own * kPbChunks; p += nwarps) {
+            // the rows in tensor memory: the warps of lane quarter q = warp mod 4 take one row at a
+            // time, a quarter of its elements each; the 4 quarter sums go where a row's pieces go
+            const uint32_t q = warp & 3u;
+            for (uint32_t sr = warp >> 2; sr < n_tm; sr += nwarps >> 2) {
+                const float* lam = n0 + n_res + sr < A.E ? s_lge : s_lgi;
+                float v[32];
+                tmem_ld16(tmem + ((32u * q) << 16) + sr * cpr, v);
+                tmem_ld16(tmem + ((32u * q) << 16) + sr * cpr + 16u, v + 16);
+                float acc = 0.0f;
+#pragma unroll
+                for (uint32_t c = 0; c < 32u; ++c) {
+                    const uint32_t e = c * 128u + 32u * q + lane;
+                    if (c < cpr && e < ld) acc = fmaf(v[c], lam[e], acc);
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
+                if (lane == 0) s_part[(n_res + sr) * kPbChunks + q] = acc;
+            }
+            // the other rows in pieces: those streamed from L2 first, then those in shared memory
+            const uint32_t n4 = ld / 4u, cq = (n4 + kPbChunks - 1u) / kPbChunks, n_l2 = own - n_res - n_tm;
+            for (uint32_t p = warp; p < (n_res + n_l2) * kPbChunks; p += nwarps) {
                 const uint32_t rr = p / kPbChunks, c = p % kPbChunks;
-                const uint32_t r = rr < n_str ? n_res + rr : rr - n_str;  // streamed rows first
+                const uint32_t r = rr < n_l2 ? n_res + n_tm + rr : rr - n_l2;
                 const uint32_t pre = n0 + r;
                 const float* lam = pre < A.E ? s_lge : s_lgi;
                 const uint32_t q0 = c * cq < n4 ? c * cq : n4, q1 = q0 + cq < n4 ? q0 + cq : n4;
@@ -515,6 +570,9 @@ __global__ void __launch_bounds__(kAdjBwdThreads, 1) bsnn_adj_backward_kernel(AD
         B.lam_r[n0 + i] = s_lr[i];
         B.lam_x[n0 + i] = s_lx[i];
     }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, kAdjTmemCols);
 }
 
 // dW[pre, post] += sum_t X[t, pre] L[t, post] over one segment's steps (X: x_t of the E
