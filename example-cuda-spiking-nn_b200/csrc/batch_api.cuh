@@ -397,6 +397,17 @@ void batch_finalize(bsnn_batch* b) {
         break;
     }
     require(placed, BSNN_ERR_INVALID_ARGUMENT, "batch too large: the operand stages do not fit in shared memory");
+    // The phased form waits per size class instead of at grid barriers (BSNN_BATCH_CLASSWAIT=0: grid
+    // barriers); ctas_of[c] counts the CTAs whose neuron range holds neurons of class c.
+    const char* env_cw = std::getenv("BSNN_BATCH_CLASSWAIT");
+    h.classwait = !flow && !(env_cw && std::string(env_cw) == "0");
+    for (uint32_t c = 0; c < h.n_classes; ++c) {
+        h.ctas_of[c] = 0;
+        for (uint32_t cta = 0; cta < n_ctas; ++cta) {
+            const uint64_t a = static_cast<uint64_t>(cta) * h.per_cta, e = std::min<uint64_t>(a + h.per_cta, n_neurons);
+            if (a < e && a < cls_nbase[c] + cls_nlen[c] && cls_nbase[c] < e) ++h.ctas_of[c];
+        }
+    }
     cuda_check(cudaMemcpy(b->d_sim, &h, sizeof(BSim), cudaMemcpyHostToDevice), "H2D batch sim");
     if (flow)
         b->kernel = h.state_in_smem ? reinterpret_cast<const void*>(&bsnn_batch_flow_kernel<true>)

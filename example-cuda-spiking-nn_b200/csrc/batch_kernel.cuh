@@ -129,6 +129,11 @@ struct BSim {
     uint32_t units_of[kBatchMaxClasses];  // GEMM units per class
     unsigned long long* nready;           // [kBatchMaxClasses] CTA slices stepped (+1 per CTA per step)
     unsigned long long* udone;            // [kBatchMaxClasses] unit epilogue warps done (+4 per unit per step)
+    // the phased form's class waits instead of grid barriers (classwait): a unit waits until every
+    // CTA whose range holds neurons of its class has stepped them (nready[c] reaches
+    // (t + 1) * ctas_of[c]), a CTA's phase A until its classes' units of the previous step are done
+    uint32_t classwait;
+    uint32_t ctas_of[kBatchMaxClasses];
 };
 
 // ---- tcgen05 / tensor-memory wrappers ---------------------------------------------------------
@@ -661,6 +666,35 @@ __device__ __forceinline__ void batch_init_barriers(BatchSmem& bs, uint32_t n_st
     fence_mbar_init();
 }
 
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// One thread: bounded wait until the counter reaches `target`.  It polls with gpu-scope relaxed
+// loads and makes one acquire load once the target is reached: these waits run beside the other
+// roles' work, and an acquire load per poll would keep invalidating the SM's L1 under them.  Gives
+// up after s_wait_limit_ns, recording kErrBarrierTimeout, or when another CTA has given up.
+__device__ __forceinline__ bool count_wait(const unsigned long long* ctr, int32_t* error, unsigned long long target) {
+    unsigned long long t_start = 0;
+    uint32_t spins = 0;
+    while (static_cast<long long>(ld_relaxed_u64(ctr) - target) < 0) {
+        if ((++spins & 63u) == 0u) {
+            const unsigned long long now = globaltimer_ns();
+            if (t_start == 0) {
+                t_start = now;
+            } else if (now - t_start > s_wait_limit_ns) {
+                atomicExch(error, kErrBarrierTimeout);
+                return false;
+            }
+            if (ld_relaxed_s32(error) != kErrNone) return false;
+        }
+    }
+    ld_acquire_u64(ctr);  // orders this thread's later reads after the counted work
+    return true;
+}
+
 // ---- phase B of the phased form: loader, MMA thread and epilogue as separate roles -------------
 // The loader (thread 128) takes units from the dispenser, names each in the unit ring and streams
 // its operand tiles into the stage ring.  The MMA thread (thread 256: warp 8, which draws no noise)
@@ -670,6 +704,7 @@ __device__ __forceinline__ void batch_init_barriers(BatchSmem& bs, uint32_t n_st
 // role keeps its own counters, carried across steps: the u-th fill of a ring slot or stage is
 // phase u of its barriers.
 struct SplitState {
+    unsigned long long held = 0;  // class waits: the loader's ticket not yet processed
     uint32_t units = 0;  // units named (loader) or taken from the ring (MMA thread, epilogue)
     uint32_t stage = 0;  // the next stage, and how many times it was used before
     uint32_t use = 0;
@@ -685,12 +720,32 @@ __device__ __forceinline__ bool split_loader(const BSim* S, BatchSmem& bs, const
                                              uint32_t n_stages, uint64_t keep) {
     const uint32_t n_units = S->n_units;
     const unsigned long long take0 = t * n_units;
+    const bool classwait = S->classwait != 0u;
     bool good = true;
+    // Grid barriers: CTA b starts with unit b, then takes from the dispenser (numbered from
+    // t * n_units in the step).  Class waits: CTAs may be in different steps, so the dispenser is
+    // one ticket sequence over the launch (ticket q: unit q mod n_units of step q / n_units), and
+    // the loader holds its first ticket of a later step for that step's phase B.
     uint32_t ui = blockIdx.x;
+    if (classwait) {
+        const unsigned long long tq = L.held / n_units;
+        ui = tq == t ? static_cast<uint32_t>(L.held - tq * n_units) : n_units;
+    }
     for (;;) {
         const uint32_t slot = L.units % kUnitRing;
         if (L.units >= kUnitRing && !mbar_wait(saddr(&bs.uempty[slot]), ((L.units / kUnitRing) - 1u) & 1u)) good = false;
-        const bool none = ui >= n_units || !good || bs.ok == 0u;
+        bool none = ui >= n_units || !good || bs.ok == 0u;
+        if (!none && classwait) {
+            // every CTA holding neurons of the unit's class has stepped them (x tiles written by
+            // generic stores, read by the bulk copies below)
+            const uint32_t c = S->units[ui].cls;
+            if (count_wait(S->nready + c, S->error, (t + 1ull) * S->ctas_of[c])) {
+                fence_proxy_async_global();
+            } else {
+                good = false;
+                none = true;
+            }
+        }
         bs.uid[slot] = none ? kNoUnit : ui;
         mbar_arrive(saddr(&bs.ufull[slot]));
         ++L.units;
@@ -718,7 +773,13 @@ __device__ __forceinline__ bool split_loader(const BSim* S, BatchSmem& bs, const
                 ++L.use;
             }
         }
-        ui = gridDim.x + static_cast<uint32_t>(atomicAdd(S->unit_ctr, 1ull) - take0);
+        if (classwait) {
+            L.held = atomicAdd(S->unit_ctr, 1ull);
+            const unsigned long long tq = L.held / n_units;
+            ui = tq == t ? static_cast<uint32_t>(L.held - tq * n_units) : n_units;  // a later step's: held
+        } else {
+            ui = gridDim.x + static_cast<uint32_t>(atomicAdd(S->unit_ctr, 1ull) - take0);
+        }
     }
     return good;
 }
@@ -806,6 +867,7 @@ __device__ __forceinline__ bool split_epilogue(const BSim* S, BatchSmem& bs, con
         if (lane == 0) {
             mbar_arrive(saddr(&bs.aempty[buf]));
             mbar_arrive(saddr(&bs.uempty[slot]));
+            if (S->classwait) red_release_add_u64(S->udone + U.cls, 1ull);  // this warp's 32 posts are written
         }
         if (!good) break;
     }
@@ -879,13 +941,45 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
     if (S->noise_on) noise_ahead(S, P, s_cls, s_nz, n0, n1, t0, tid, blockDim.x);
     __syncthreads();
 
+    // the size classes this CTA's neurons belong to (bit c)
+    __shared__ uint32_t s_cmask;
+    if (tid == 0) {
+        uint32_t m = 0;
+        for (uint32_t c = 0; c < S->n_classes; ++c)
+            if (n0 < s_cls[c].nbase + s_cls[c].nlen && s_cls[c].nbase < n1) m |= 1u << c;
+        s_cmask = m;
+    }
+    __syncthreads();
+    const uint32_t cmask = s_cmask;
+    const bool classwait = S->classwait != 0u;
+    const unsigned long long ticket_end = (t0 + n_steps) * static_cast<unsigned long long>(S->n_units);
+    if (classwait && tid == 128u) ls.held = atomicAdd(S->unit_ctr, 1ull);  // this CTA's first ticket
     for (uint32_t k = 0; k < n_steps && ok; ++k) {
         const unsigned long long t = t0 + k;
+        if (classwait && t > 0) {
+            // the previous step's units of this CTA's classes are all done (4 counts per unit)
+            if (tid == 0) {
+                int good = 1;
+                for (uint32_t c = 0; c < S->n_classes && good; ++c)
+                    if ((cmask >> c) & 1u) good = count_wait(S->udone + c, S->error, 4ull * t * S->units_of[c]) ? 1 : 0;
+                s_ok = good;
+            }
+            __syncthreads();
+            if (!s_ok) {
+                ok = false;
+                break;
+            }
+        }
+        BSNN_TMARK(3);
         batch_neurons<SMEM_STATE>(S, P, s_cls, X, s_nz, n0, n1, t, tid, blockDim.x);
         fence_proxy_async_global();
         __syncthreads();
         BSNN_TMARK(0);
-        if (!grid_barrier(S->barrier, S->error, bar0 + (2ull * k + 1ull) * gridDim.x, &s_ok)) {
+        if (classwait) {
+            if (tid == 0)
+                for (uint32_t c = 0; c < S->n_classes; ++c)
+                    if ((cmask >> c) & 1u) red_release_add_u64(S->nready + c, 1ull);
+        } else if (!grid_barrier(S->barrier, S->error, bar0 + (2ull * k + 1ull) * gridDim.x, &s_ok)) {
             ok = false;
             break;
         }
@@ -913,17 +1007,19 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
         ok = bs.ok != 0u;  // the same for every thread of the CTA
         if (!ok) break;
         BSNN_TMARK(2);
-        if (!grid_barrier(S->barrier, S->error, bar0 + (2ull * k + 2ull) * gridDim.x, &s_ok)) {
+        if (!classwait && !grid_barrier(S->barrier, S->error, bar0 + (2ull * k + 2ull) * gridDim.x, &s_ok)) {
             ok = false;
             break;
         }
-        BSNN_TMARK(3);
     }
 #ifdef BSNN_PHASE_TIMING
     if (tid == 0)
         for (int i = 0; i < 8; ++i) S->phase_ns[blockIdx.x * 8u + i] += s_tally_[i];
 #endif
     if ((tid == 128u || tid == 256u) && bs.ok == 0u) split_quiesce(bs, ls, ms, tid == 128u, n_stages);
+    // class waits: the ticket past the launch's end is given back, so the next launch starts at
+    // (t0 + n_steps) * n_units
+    if (classwait && tid == 128u && ls.held >= ticket_end) atomicAdd(S->unit_ctr, ~0ull);
     tc_fence_before();
     __syncthreads();
     if constexpr (SMEM_STATE) state_copy(S, X, n0, n1, false);
@@ -962,35 +1058,6 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
 // producer's last take is past the end and is given back.
 constexpr uint32_t kFlowNeuronWarp0 = 5;
 constexpr uint32_t kFlowNeuronThreads = kBatchThreads - 32u * kFlowNeuronWarp0;
-
-__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
-    unsigned long long v;
-    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
-}
-
-// One thread: bounded wait until the counter reaches `target`.  It polls with gpu-scope relaxed
-// loads and makes one acquire load once the target is reached: these waits run beside the other
-// roles' work, and an acquire load per poll would keep invalidating the SM's L1 under them.  Gives
-// up after s_wait_limit_ns, recording kErrBarrierTimeout, or when another CTA has given up.
-__device__ __forceinline__ bool count_wait(const unsigned long long* ctr, int32_t* error, unsigned long long target) {
-    unsigned long long t_start = 0;
-    uint32_t spins = 0;
-    while (static_cast<long long>(ld_relaxed_u64(ctr) - target) < 0) {
-        if ((++spins & 63u) == 0u) {
-            const unsigned long long now = globaltimer_ns();
-            if (t_start == 0) {
-                t_start = now;
-            } else if (now - t_start > s_wait_limit_ns) {
-                atomicExch(error, kErrBarrierTimeout);
-                return false;
-            }
-            if (ld_relaxed_s32(error) != kErrNone) return false;
-        }
-    }
-    ld_acquire_u64(ctr);  // orders this thread's later reads after the counted work
-    return true;
-}
 
 // Bounded wait for an mbarrier phase with an explicit limit.
 __device__ __forceinline__ bool mbar_wait_for(uint32_t bar, uint32_t parity, unsigned long long limit_ns) {

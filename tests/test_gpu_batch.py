@@ -124,10 +124,11 @@ def test_batch_rates_against_fp64():
 
 @pytest.mark.parametrize("env", [{"BSNN_BATCH_STATE": "global"}, {"BSNN_BATCH_STAGES": "2"},
                                  {"BSNN_BATCH_STATE": "global", "BSNN_BATCH_STAGES": "4"},
-                                 {"BSNN_BATCH_STAGES": "8"}])
+                                 {"BSNN_BATCH_STAGES": "8"}, {"BSNN_BATCH_CLASSWAIT": "0"}])
 def test_batch_placements_are_bit_exact(env):
-    """Neuron state in shared memory (the default when it fits) or in global memory, and the
-    operand ring's depth, change where data lives, not the arithmetic: the states are identical."""
+    """Neuron state in shared memory (the default when it fits) or in global memory, the operand
+    ring's depth, and per-class waits (the default) or grid barriers between the phases change
+    where data lives and when work starts, not the arithmetic: the states are identical."""
     spec = bsnn.config4_batch(n_instances=6, steps=200, seed=9, sizes=(400, 900, 1600), stim_window=(10, 150))
     a = bsnn.BatchSimulation(spec)
     ia = a.info()
