@@ -926,7 +926,6 @@ __global__ void __launch_bounds__(kBatchThreads, 1) bsnn_batch_kernel(const BSim
     tc_fence_after();
     const uint32_t tmem = bs.tmem;
     const unsigned long long bar0 = s_bar0, t0 = s_t0;
-    const uint32_t n_units = S->n_units;
     // phase B roles: thread 128 the loader, thread 256 the MMA thread, warps 0-3 the epilogue
     SplitState ls, ms, es;
     bool ok = true;
