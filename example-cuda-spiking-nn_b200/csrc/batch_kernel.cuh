@@ -287,13 +287,35 @@ __device__ __forceinline__ SegCtx seg_ctx(const BInst& B, const BClass& C) {
     return c;
 }
 
+// What every neuron of a step reads from the launch descriptor, loaded once per step: the partial
+// sums, the spike counters, whether the background noise is on, and the step's stimulus events
+// [ev_lo, ev_hi) (sorted by neuron; empty on steps without events).
+struct StepCtx {
+    const float* partials;
+    unsigned long long* spike_counts;
+    uint32_t noise_on, ev_lo, ev_hi;
+};
+
+__device__ __forceinline__ StepCtx step_ctx(const BSim* S, unsigned long long t) {
+    StepCtx k;
+    k.partials = S->partials;
+    k.spike_counts = S->spike_counts;
+    k.noise_on = S->noise_on;
+    k.ev_lo = k.ev_hi = 0;
+    if (t < S->stim_len) {
+        k.ev_lo = __ldg(S->stim_off + t);
+        k.ev_hi = __ldg(S->stim_off + t + 1);
+    }
+    return k;
+}
+
 // One neuron's step (n: its index, i = n - X.base its state index): g = the background of the
 // previous step (recomputed from its traces) + the previous step's propagation (K chunks in
 // order), background Poisson shot noise, the conductance-EIF Euler step, the step's stimulus
 // events, the connection traces, and x = d - r as BF16 hi / lo into the B operand.
 template <bool SMEM>
-__device__ __forceinline__ void neuron_step(const BSim* S, const SegCtx& c, const BState& X, const uint16_t* nz,
-                                            uint32_t n0, uint32_t n, unsigned long long t) {
+__device__ __forceinline__ void neuron_step(const BSim* S, const StepCtx& sc, const SegCtx& c, const BState& X,
+                                            const uint16_t* nz, uint32_t n0, uint32_t n, unsigned long long t) {
     const uint32_t i = n - X.base;
     const uint32_t j = n - c.nbase;  // index in the instance
     const uint32_t side = j < c.E ? 0u : 1u;
@@ -301,10 +323,22 @@ __device__ __forceinline__ void neuron_step(const BSim* S, const SegCtx& c, cons
     const uint32_t loc = j - (side ? c.E : 0u);
     float dge = 0.0f, dgi = 0.0f;
     if (t > 0) {  // the previous step's propagation, K chunks in order
-        const float* pe = S->partials + c.pe + (j >> 7) * c.te + (j & 127u);
-        const float* pi = S->partials + c.pi + (j >> 7) * c.ti + (j & 127u);
-        for (uint32_t kc = 0; kc < c.nkc0; ++kc) dge += __ldcg(pe + kc * c.stride);
-        for (uint32_t kc = 0; kc < c.nkc1; ++kc) dgi += __ldcg(pi + kc * c.stride);
+        const float* pe = sc.partials + c.pe + (j >> 7) * c.te + (j & 127u);
+        const float* pi = sc.partials + c.pi + (j >> 7) * c.ti + (j & 127u);
+        if (c.nkc0 <= 2u && c.nkc1 <= 2u) {
+            // the usual case: every load issued before the first add (a loop over a count known
+            // only at run time would wait for each load before issuing the next)
+            const float e0 = __ldcg(pe), g0 = __ldcg(pi);
+            const float e1 = c.nkc0 > 1u ? __ldcg(pe + c.stride) : 0.0f;
+            const float g1 = c.nkc1 > 1u ? __ldcg(pi + c.stride) : 0.0f;
+            dge += e0;
+            if (c.nkc0 > 1u) dge += e1;
+            dgi += g0;
+            if (c.nkc1 > 1u) dgi += g1;
+        } else {
+            for (uint32_t kc = 0; kc < c.nkc0; ++kc) dge += __ldcg(pe + kc * c.stride);
+            for (uint32_t kc = 0; kc < c.nkc1; ++kc) dgi += __ldcg(pi + kc * c.stride);
+        }
     }
     const float a_v = st_ld<SMEM>(X.v + i), a_istim = st_ld<SMEM>(X.istim + i);
     const float a_er = st_ld<SMEM>(X.er + i), a_ed = st_ld<SMEM>(X.ed + i);
@@ -323,7 +357,7 @@ __device__ __forceinline__ void neuron_step(const BSim* S, const SegCtx& c, cons
     float ed = flush_tiny(a_ed * G.bg_ed_decay);
     float id = flush_tiny(a_id * G.bg_id_decay);
     uint32_t ne = 0, ni = 0;
-    if (S->noise_on) {
+    if (sc.noise_on) {
         const uint32_t cnt = nz[n - n0];
         ne = cnt & 0xFFu;
         ni = cnt >> 8;
@@ -368,11 +402,11 @@ __device__ __forceinline__ void neuron_step(const BSim* S, const SegCtx& c, cons
     X.refrac[i] = refrac;
     if constexpr (SMEM) X.spike8[i] = static_cast<uint8_t>(spike);
     else X.spike32[i] = spike;
-    if (spike) atomicAdd(S->spike_counts + 2u * c.id + side, 1ull);
+    if (spike) atomicAdd(sc.spike_counts + 2u * c.id + side, 1ull);
 
     // stimulus events of this step act from the next step
-    if (t < S->stim_len) {
-        uint32_t lo = __ldg(S->stim_off + t), hi = __ldg(S->stim_off + t + 1);
+    if (sc.ev_lo < sc.ev_hi) {
+        uint32_t lo = sc.ev_lo, hi = sc.ev_hi;
         const uint32_t end = hi;
         while (lo < hi) {
             const uint32_t mid = (lo + hi) >> 1;
@@ -413,13 +447,14 @@ __device__ __forceinline__ void batch_neurons(const BSim* S, const BInst* P, con
                                               const uint16_t* nz, uint32_t n0, uint32_t n1, unsigned long long t,
                                               uint32_t me, uint32_t count) {
     if (n0 >= n1) return;
+    const StepCtx sc = step_ctx(S, t);
     uint32_t inst = instance_of(P, S->n_inst, n0);
     for (uint32_t seg0 = n0; seg0 < n1; ++inst) {
         const BInst& B = P[inst];
         const BClass& C = s_cls[B.cls];
         const uint32_t seg1 = min(n1, B.nbase + C.N);
         const SegCtx c = seg_ctx(B, C);
-        for (uint32_t n = seg0 + me; n < seg1; n += count) neuron_step<SMEM>(S, c, X, nz, n0, n, t);
+        for (uint32_t n = seg0 + me; n < seg1; n += count) neuron_step<SMEM>(S, sc, c, X, nz, n0, n, t);
         seg0 = seg1;
     }
 }
