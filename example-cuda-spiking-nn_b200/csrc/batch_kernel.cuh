@@ -313,33 +313,53 @@ __device__ __forceinline__ StepCtx step_ctx(const BSim* S, unsigned long long t)
 // previous step (recomputed from its traces) + the previous step's propagation (K chunks in
 // order), background Poisson shot noise, the conductance-EIF Euler step, the step's stimulus
 // events, the connection traces, and x = d - r as BF16 hi / lo into the B operand.
+// The previous step's partial sums of neuron j of an instance whose sides have at most 2 K chunks
+// each, loaded but not yet added: the loads of the next neuron are issued before this one's
+// update (a loop over a count known only at run time would wait for each load before issuing
+// the next).
+struct PartRaw {
+    float e0, e1, g0, g1;
+};
+__device__ __forceinline__ PartRaw part_load(const StepCtx& sc, const SegCtx& c, uint32_t j) {
+    const float* pe = sc.partials + c.pe + (j >> 7) * c.te + (j & 127u);
+    const float* pi = sc.partials + c.pi + (j >> 7) * c.ti + (j & 127u);
+    PartRaw r;
+    r.e0 = __ldcg(pe);
+    r.g0 = __ldcg(pi);
+    r.e1 = c.nkc0 > 1u ? __ldcg(pe + c.stride) : 0.0f;
+    r.g1 = c.nkc1 > 1u ? __ldcg(pi + c.stride) : 0.0f;
+    return r;
+}
+// Their sums, K chunks in order from 0.
+__device__ __forceinline__ float2 part_sum(const PartRaw& r, const SegCtx& c) {
+    float dge = 0.0f, dgi = 0.0f;
+    dge += r.e0;
+    if (c.nkc0 > 1u) dge += r.e1;
+    dgi += r.g0;
+    if (c.nkc1 > 1u) dgi += r.g1;
+    return make_float2(dge, dgi);
+}
+// The same sums for any number of K chunks.
+__device__ __forceinline__ float2 part_sums_any(const StepCtx& sc, const SegCtx& c, uint32_t j) {
+    const float* pe = sc.partials + c.pe + (j >> 7) * c.te + (j & 127u);
+    const float* pi = sc.partials + c.pi + (j >> 7) * c.ti + (j & 127u);
+    float dge = 0.0f, dgi = 0.0f;
+    for (uint32_t kc = 0; kc < c.nkc0; ++kc) dge += __ldcg(pe + kc * c.stride);
+    for (uint32_t kc = 0; kc < c.nkc1; ++kc) dgi += __ldcg(pi + kc * c.stride);
+    return make_float2(dge, dgi);
+}
+
+// dg: the previous step's propagation onto the neuron (its partial sums; unused at t = 0).
 template <bool SMEM>
 __device__ __forceinline__ void neuron_step(const BSim* S, const StepCtx& sc, const SegCtx& c, const BState& X,
-                                            const uint16_t* nz, uint32_t n0, uint32_t n, unsigned long long t) {
+                                            const uint16_t* nz, uint32_t n0, uint32_t n, unsigned long long t,
+                                            float2 dg) {
     const uint32_t i = n - X.base;
     const uint32_t j = n - c.nbase;  // index in the instance
     const uint32_t side = j < c.E ? 0u : 1u;
     const BGroupP& G = c.g[side];
     const uint32_t loc = j - (side ? c.E : 0u);
-    float dge = 0.0f, dgi = 0.0f;
-    if (t > 0) {  // the previous step's propagation, K chunks in order
-        const float* pe = sc.partials + c.pe + (j >> 7) * c.te + (j & 127u);
-        const float* pi = sc.partials + c.pi + (j >> 7) * c.ti + (j & 127u);
-        if (c.nkc0 <= 2u && c.nkc1 <= 2u) {
-            // the usual case: every load issued before the first add (a loop over a count known
-            // only at run time would wait for each load before issuing the next)
-            const float e0 = __ldcg(pe), g0 = __ldcg(pi);
-            const float e1 = c.nkc0 > 1u ? __ldcg(pe + c.stride) : 0.0f;
-            const float g1 = c.nkc1 > 1u ? __ldcg(pi + c.stride) : 0.0f;
-            dge += e0;
-            if (c.nkc0 > 1u) dge += e1;
-            dgi += g0;
-            if (c.nkc1 > 1u) dgi += g1;
-        } else {
-            for (uint32_t kc = 0; kc < c.nkc0; ++kc) dge += __ldcg(pe + kc * c.stride);
-            for (uint32_t kc = 0; kc < c.nkc1; ++kc) dgi += __ldcg(pi + kc * c.stride);
-        }
-    }
+    const float dge = dg.x, dgi = dg.y;
     const float a_v = st_ld<SMEM>(X.v + i), a_istim = st_ld<SMEM>(X.istim + i);
     const float a_er = st_ld<SMEM>(X.er + i), a_ed = st_ld<SMEM>(X.ed + i);
     const float a_ir = st_ld<SMEM>(X.ir + i), a_id = st_ld<SMEM>(X.id + i);
@@ -454,7 +474,22 @@ __device__ __forceinline__ void batch_neurons(const BSim* S, const BInst* P, con
         const BClass& C = s_cls[B.cls];
         const uint32_t seg1 = min(n1, B.nbase + C.N);
         const SegCtx c = seg_ctx(B, C);
-        for (uint32_t n = seg0 + me; n < seg1; n += count) neuron_step<SMEM>(S, sc, c, X, nz, n0, n, t);
+        uint32_t n = seg0 + me;
+        if (t > 0 && c.nkc0 <= 2u && c.nkc1 <= 2u) {
+            PartRaw r{};
+            if (n < seg1) r = part_load(sc, c, n - c.nbase);
+            for (; n < seg1; n += count) {
+                const uint32_t nn = n + count;
+                PartRaw rn{};
+                if (nn < seg1) rn = part_load(sc, c, nn - c.nbase);  // in flight during this update
+                neuron_step<SMEM>(S, sc, c, X, nz, n0, n, t, part_sum(r, c));
+                r = rn;
+            }
+        } else {
+            for (; n < seg1; n += count)
+                neuron_step<SMEM>(S, sc, c, X, nz, n0, n, t,
+                                  t > 0 ? part_sums_any(sc, c, n - c.nbase) : make_float2(0.0f, 0.0f));
+        }
         seg0 = seg1;
     }
 }
