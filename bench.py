@@ -612,8 +612,8 @@ def run_batch(args, rank, world, K=None, W=None, seed=0):
                      "traffic": None, "peak_source": peak_kind, "flops_per_clock_step": flops_step,
                      "bf16_weight_bytes_per_clock_step": weight_bytes,
                      "weight_read_gbs": weight_bytes / step_s / 1e9,
-                     "note": "a GEMV-shaped GEMM (N = instances of a class x 2): bound by the weight stream "
-                             "from L2 and the step's two grid barriers, not by the tensor pipe"},
+                     "note": "a GEMV-shaped GEMM (N = instances of a class x 2): bound by the MMA thread's "
+                             "issue chain and the neuron phase between the GEMMs, not by the tensor pipe"},
         "clocks": clocks.summary(),
     }
     if world > 1:
