@@ -38,6 +38,7 @@ struct bsnn_adjoint {
     double* gl_acc = nullptr;     // [bwd_grid] per-CTA g_leak shares
     double* vsum = nullptr;       // [T][nb] per-block sums of the E voltages after each step
     uint32_t* counts = nullptr;   // [T] E spikes per step
+    std::vector<uint32_t> stim_off;  // [stimulus steps + 1] host copy of the stimulus offsets
     float* ckpt = nullptr;        // [n_ckpt][kAdjCkptArrays][N]
     uint32_t n_ckpt = 0, nb = 0;
     uint32_t ld = 0;              // row length of W_E, W_I and the lambda_g rows: N rounded up to 4
@@ -134,7 +135,9 @@ void adj_step(bsnn_adjoint* a, uint32_t t, size_t tape_row, bool tape, float* x_
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     cfg.gridDim = dim3(a->nb);
-    cuda_check(cudaLaunchKernelEx(&cfg, bsnn_adj_neuron_fwd, a->h, t, static_cast<const float*>(a->part),
+    const bool stim = t < a->stim_off.size() - 1;
+    const uint32_t ev_lo = stim ? a->stim_off[t] : 0u, ev_hi = stim ? a->stim_off[t + 1] : 0u;
+    cuda_check(cudaLaunchKernelEx(&cfg, bsnn_adj_neuron_fwd, a->h, t, ev_lo, ev_hi, static_cast<const float*>(a->part),
                                   tape ? a->tv + tape_row : nullptr, tape ? a->tu + tape_row : nullptr,
                                   tape ? a->tge + tape_row : nullptr, tape ? a->tgi + tape_row : nullptr,
                                   tape ? a->ts + tape_row : nullptr, tape ? a->tref + tape_row : nullptr, x_next,
@@ -405,6 +408,7 @@ BSNN_API bsnn_status bsnn_adjoint_create(const bsnn_adjoint_desc* desc, const bs
         h.ev_neuron = reinterpret_cast<const uint32_t*>(base + o_evn);
         h.ev_delta = F(o_evd);
         cuda_check(cudaMemcpy(base + o_soff, soff.data(), 4ull * soff.size(), cudaMemcpyHostToDevice), "H2D");
+        a->stim_off = soff;
         if (!evn.empty()) {
             cuda_check(cudaMemcpy(base + o_evn, evn.data(), 4ull * evn.size(), cudaMemcpyHostToDevice), "H2D");
             cuda_check(cudaMemcpy(base + o_evd, evd.data(), 4ull * evd.size(), cudaMemcpyHostToDevice), "H2D");

@@ -73,8 +73,10 @@ __device__ __forceinline__ float adj_chunk_sum(const float* part, uint32_t side,
 // One forward step t for every neuron: g_e / g_i of the step are the background of the previous
 // step plus the propagation partials; writes x_{t+1} (the trace value the next propagation uses)
 // and, when the tape pointers are set, the step's tape row.  Optional: the step's E spike count
-// and this block's sum of the E voltages after the step.
-__global__ void __launch_bounds__(kAdjBlock) bsnn_adj_neuron_fwd(ADev A, uint32_t t, const float* __restrict__ part,
+// and this block's sum of the E voltages after the step.  [ev_lo, ev_hi): the step's stimulus
+// events (from the host's copy of the stimulus offsets, so a step without events reads nothing).
+__global__ void __launch_bounds__(kAdjBlock) bsnn_adj_neuron_fwd(ADev A, uint32_t t, uint32_t ev_lo, uint32_t ev_hi,
+                                                                 const float* __restrict__ part,
                                                                  float* tape_v, float* tape_u, float* tape_ge,
                                                                  float* tape_gi, uint8_t* tape_s, uint8_t* tape_ref,
                                                                  float* x_next, uint32_t* e_spike_count,
@@ -148,8 +150,8 @@ __global__ void __launch_bounds__(kAdjBlock) bsnn_adj_neuron_fwd(ADev A, uint32_
         A.refrac[n] = refrac;
         A.ge[n] = bg_ge;  // the next step adds the propagation of x_{t+1}
         A.gi[n] = bg_gi;
-        if (t < A.stim_len) {
-            for (uint32_t k = A.stim_off[t]; k < A.stim_off[t + 1]; ++k)
+        if (ev_lo < ev_hi) {
+            for (uint32_t k = ev_lo; k < ev_hi; ++k)
                 if (A.ev_neuron[k] == n) istim = istim + A.ev_delta[k];
             A.istim[n] = istim;
         }
@@ -499,13 +501,30 @@ __global__ void __launch_bounds__(kAdjBwdThreads, 1) bsnn_adj_backward_kernel(AD
         if (k > 0u) cur = fetch(k - 1u);
         if (!grid_barrier(B.barrier, B.error, bar0 + (kk + 1ull) * gridDim.x, &s_ok)) break;
         // every neuron's lambda_g of step t (written by other CTAs: read from L2); only the side the
-        // own rows pull back through (rows < E: lambda_ge, the others lambda_gi)
-        if (n0 < A.E)
-            for (uint32_t q = tid; q < ld / 4u; q += blockDim.x)
-                reinterpret_cast<float4*>(s_lge)[q] = __ldcg(reinterpret_cast<const float4*>(lge_row) + q);
-        if (n1 > A.E)
-            for (uint32_t q = tid; q < ld / 4u; q += blockDim.x)
-                reinterpret_cast<float4*>(s_lgi)[q] = __ldcg(reinterpret_cast<const float4*>(lgi_buf) + q);
+        // own rows pull back through (rows < E: lambda_ge, the others lambda_gi).  A thread issues
+        // its loads of both sides, two float4 apart by blockDim each, before its first store, so
+        // they cost one L2 round trip (ld / 4 <= 2 * blockDim here) instead of one per load.
+        {
+            const uint32_t n4 = ld / 4u;
+            const bool use_e = n0 < A.E, use_i = n1 > A.E;
+            const float4* src_e = reinterpret_cast<const float4*>(lge_row);
+            const float4* src_i = reinterpret_cast<const float4*>(lgi_buf);
+            for (uint32_t q = tid; q < n4; q += 2u * blockDim.x) {
+                const uint32_t q2 = q + blockDim.x;
+                const bool two = q2 < n4;
+                const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                const float4 e0 = use_e ? __ldcg(src_e + q) : z, e1 = use_e && two ? __ldcg(src_e + q2) : z;
+                const float4 i0 = use_i ? __ldcg(src_i + q) : z, i1 = use_i && two ? __ldcg(src_i + q2) : z;
+                if (use_e) {
+                    reinterpret_cast<float4*>(s_lge)[q] = e0;
+                    if (two) reinterpret_cast<float4*>(s_lge)[q2] = e1;
+                }
+                if (use_i) {
+                    reinterpret_cast<float4*>(s_lgi)[q] = i0;
+                    if (two) reinterpret_cast<float4*>(s_lgi)[q2] = i1;
+                }
+            }
+        }
         __syncthreads();
         {
             // the rows in tensor memory: the warps of lane quarter q = warp mod 4 take one row at a
